@@ -1,0 +1,136 @@
+/*
+ * qa_gpu.h -- C ABI of the B200 Monte Carlo sweep engine (libqa_gpu.so).
+ *
+ * This is the drop-in boundary for qanneal's sweep engine.  In qanneal every
+ * annealer drives a model through the per-flip Backend interface
+ * (include/qanneal/backend.hpp:39-53); BackendKind::CUDA is parsed
+ * (backend.hpp:19-27) but make_backend() throws "CUDA backend stub: kernels
+ * not wired yet." (backend.hpp:97-102).  A per-flip virtual call cannot cross
+ * to a device, so the boundary sits one level up: each entry point below runs
+ * one whole annealer run*() call -- for ALL reads of a solve() at once -- and
+ * returns the same result fields as the annealer's result struct.
+ *
+ * Conventions: plain C types, caller-owned host buffers, int status codes
+ * (QA_OK == 0), the message of the last failure on this thread through
+ * qa_last_error().  No exception crosses this boundary.  One qa_ctx per host
+ * thread; calls on one context are serialised by the caller (qanneal's
+ * annealers are not re-entrant either: rng_ is a member).
+ *
+ * Randomness: read r of a call uses the stream keyed by (seed + r), as
+ * solve() seeds read r with set_seed(seed + r) (python/qanneal/solver.py:679-681).
+ */
+#ifndef QA_GPU_H
+#define QA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define QA_API __attribute__((visibility("default")))
+#else
+#define QA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    QA_OK = 0,
+    QA_ERR_ARG = 1,         /* invalid argument (qanneal: std::invalid_argument -> ValueError) */
+    QA_ERR_CUDA = 2,        /* CUDA runtime failure */
+    QA_ERR_OOM = 3,         /* device allocation failed */
+    QA_ERR_TIMEOUT = 4,     /* a bounded device wait ran out */
+    QA_ERR_DRIFT = 5,       /* incremental fields drifted from a float64 recompute */
+    QA_ERR_UNSUPPORTED = 6  /* option outside the engine (cluster sweeps, observers) */
+};
+
+typedef struct qa_ctx qa_ctx;
+typedef struct qa_problem qa_problem;
+
+/* Library identity and errors. */
+QA_API const char *qa_version(void);
+/* Copies the last error message of the calling thread into buf (NUL-terminated). */
+QA_API int qa_last_error(char *buf, size_t len);
+QA_API int qa_device_count(int *count);
+
+/* Context: one device, one stream, a cached device workspace.
+ * Replaces make_backend(BackendKind::CUDA, ham) (backend.hpp:92-105). */
+QA_API int qa_create(qa_ctx **out, int device);
+QA_API int qa_destroy(qa_ctx *ctx);
+
+/* ---- problems (device copies of one model instance) ------------------- */
+
+/* DenseIsing(h, J, n, c) (dense_ising.hpp:17-21): E = c + sum h s + sum_{i<j} J_ij s_i s_j.
+ * J is n*n row-major float64; the couplings read are the upper triangle, as in
+ * DenseIsing::energy (dense_ising.cpp:29-44). */
+QA_API int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, double c, qa_problem **out);
+
+/* SparseIsing(h, edges, n, c) (sparse_ising.hpp:22-25); edge e couples ei[e], ej[e]
+ * with weight w[e]; self-edges are rejected (sparse_ising.cpp:29-31). */
+QA_API int qa_problem_sparse(qa_ctx *ctx, int n, const double *h, int m, const int64_t *ei, const int64_t *ej,
+                      const double *w, double c, qa_problem **out);
+
+/* HigherOrderIsing after its constructor's consolidation (higher_order_ising.cpp:10-90):
+ * h[n] holds the folded degree-1 terms, c the folded constant, and term t
+ * (0 <= t < n_terms) couples term_vars[term_ptr[t] .. term_ptr[t+1]) -- strictly
+ * increasing indices, degree >= 2 -- with coefficient coeff[t]. */
+QA_API int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int64_t *term_ptr,
+                    const int32_t *term_vars, const double *coeff, double c, qa_problem **out);
+
+QA_API int qa_problem_free(qa_problem *p);
+QA_API int qa_problem_size(const qa_problem *p, int *n);
+
+/* ---- results ------------------------------------------------------------
+ * One qa_run_out per problem of a call; every pointer is a caller-owned host
+ * array and may be NULL when the field is not wanted. */
+typedef struct {
+    int8_t *best_spins;      /* [reads][n]   best_state per read (+1/-1) */
+    double *best_energy;     /* [reads]      float64 energy of best_state */
+    double *energy_trace;    /* [reads][steps] energy_trace (SA: energy after the step;
+                                SQA: mean over replicas x slices) */
+} qa_run_out;
+
+/* Totals of one call, for measurement.  May be NULL. */
+typedef struct {
+    int64_t slice_attempts, slice_accepts;          /* SA: spin attempts / accepts */
+    int64_t worldline_attempts, worldline_accepts;  /* proposals (each covers P sites) */
+    double sweep_ms;                                /* device time of the sweep kernels (CUDA events) */
+    double total_ms;                                /* device time of the whole call */
+} qa_stats;
+
+/* ---- SA: Annealer::run (annealer.cpp:33-75) ------------------------------ */
+typedef struct {
+    const double *betas;     /* [steps]  AnnealSchedule::betas */
+    int steps;
+    int sweeps_per_beta;     /* > 0 */
+    int reads;               /* independent reads per problem */
+    uint64_t seed;           /* read r keyed by seed + r */
+} qa_sa_params;
+
+QA_API int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *params,
+              qa_run_out *outs, qa_stats *stats);
+
+/* ---- SQA: SQAAnnealer::run (sqa_annealer.cpp:87-477) ---------------------- */
+typedef struct {
+    const double *betas;     /* [steps]  SQASchedule */
+    const double *gammas;    /* [steps] */
+    int steps;
+    int trotter_slices;      /* P > 0 */
+    int replicas;            /* K > 0 rings per read */
+    int sweeps_per_beta;     /* slice sweeps per step */
+    int worldline_sweeps;    /* worldline sweeps per step */
+    int cluster_sweeps;      /* must be 0 (QA_ERR_UNSUPPORTED otherwise) */
+    int continuous_time_slices; /* slices = max(P, this) when larger, as in the reference */
+    int reads;
+    uint64_t seed;
+} qa_sqa_params;
+
+QA_API int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *params,
+               qa_run_out *outs, qa_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QA_GPU_H */

@@ -1,0 +1,730 @@
+/*
+ * qa_oracle.c -- TEST INFRASTRUCTURE ONLY (the checker, never the product).
+ *
+ * A plain-C, single-threaded restatement of qanneal's Monte Carlo sweep
+ * engine, written so that its results can be compared bit for bit with the
+ * CUDA engine in qlatanneal_b200/csrc.  Only tests/, __graft_entry__.smoke()
+ * and bench.py's CPU-baseline leg may load it.
+ *
+ * What it restates (file:line in the qanneal sources):
+ *   DenseIsing       src/dense_ising.cpp:29-106   (energy, local fields, flip update)
+ *   SparseIsing      src/sparse_ising.cpp:35-102
+ *   HigherOrderIsing src/higher_order_ising.cpp:10-206 (term consolidation, energy,
+ *                    fields, update after flip)
+ *   SA               src/annealer.cpp:33-75
+ *   SQA run()        src/sqa_annealer.cpp:87-477 (slice + worldline sweeps,
+ *                    per-step energy scan and best tracking)
+ *   SQA-PT run()     src/sqa_parallel_tempering.cpp:81-346
+ *   SQA-Chi run_chi  src/sqa_chi_annealer.cpp:81-438
+ *
+ * The "replay model".  The qanneal loops draw from std::mt19937_64 through
+ * libstdc++ distributions and visit spins in std::shuffle order, which no GPU
+ * can reproduce.  Both this file and the CUDA engine therefore follow one
+ * shared definition of the random stream, the visit order and the float32
+ * acceptance rule, and are required to agree exactly:
+ *   - Philox4x32-10 counter RNG (Salmon et al., SC'11), key = seed + read,
+ *     counter = (spin slot, cell, sweep, domain tag).
+ *   - Trotter slices are swept in phases of equal parity (even, odd, and the
+ *     last slice alone when P is odd), spins in ascending order inside a slice.
+ *   - Local fields g = J.s (h kept apart) in float32, couplings rounded to
+ *     float32, field init accumulated in float64 then rounded.
+ *   - Metropolis test: accept iff x > thr with x = s*(h+g) (float32) and
+ *     thr = (trotter + ln u) * A, A = 1/(2*beta/P); ln is a deterministic
+ *     float32 logarithm (atanh series) computed identically on both sides.
+ *   - Energies for the per-step scan in float64, summed in "warp order"
+ *     (32 lane-strided partial sums, then an xor butterfly).
+ * For integer couplings every value is exact, so spins, accept decisions,
+ * energies and traces agree bit for bit.  Parity with the unmodified qanneal
+ * code is checked separately (statistically, and exactly on the golden
+ * energy/field vectors) against the reference compiled under oracle/_ref.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OR_EXPORT __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: */
+/* as easy as 1, 2, 3", SC'11).                                          */
+/* ------------------------------------------------------------------ */
+#define PH_M0 0xD2511F53u
+#define PH_M1 0xCD9E8D57u
+#define PH_W0 0x9E3779B9u
+#define PH_W1 0xBB67AE85u
+
+OR_EXPORT void or_philox(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)PH_M0 * (uint64_t)c0;
+        uint64_t p1 = (uint64_t)PH_M1 * (uint64_t)c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += PH_W0; k1 += PH_W1;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* Domain tags (counter word 3, low byte). */
+enum {
+    DOM_INIT = 1, DOM_SA = 2, DOM_SLICE = 3, DOM_WORLD = 4, DOM_SWAP = 5,
+    DOM_PILOT_INIT = 6, DOM_PILOT = 7, DOM_PROD_INIT = 8, DOM_PROD = 9
+};
+
+static inline uint32_t spin_slot(int i) { return (uint32_t)(((i >> 7) << 5) | (i & 31)); }
+static inline int spin_word(int i) { return (i >> 5) & 3; }
+
+static uint32_t draw(uint64_t key64, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, int w) {
+    uint32_t ctr[4] = {c0, c1, c2, c3};
+    uint32_t key[2] = {(uint32_t)key64, (uint32_t)(key64 >> 32)};
+    uint32_t out[4];
+    or_philox(ctr, key, out);
+    return out[w];
+}
+
+static inline float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+/* Deterministic float32 natural logarithm for u in [0,1).  Exponent split,
+ * mantissa folded to (sqrt(1/2), sqrt(2)], ln(1+f) = 2 atanh(f/(2+f)) by its
+ * odd power series, ln 2 split in two parts (Cody & Waite).  Every operation
+ * is a single IEEE-rounded float op, so the CUDA engine reproduces it. */
+OR_EXPORT float or_logf(float x) {
+    if (!(x > 0.0f)) return -INFINITY;
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    int e = (int)((b >> 23) & 0xffu) - 127;
+    uint32_t mb = (b & 0x7fffffu) | 0x3f800000u;
+    float m;
+    memcpy(&m, &mb, 4);
+    if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
+    float f = m - 1.0f;
+    float s = f / (2.0f + f);
+    float z = s * s;
+    float p = fmaf(z, 0.18181818f, 0.22222222f);
+    p = fmaf(z, p, 0.28571429f);
+    p = fmaf(z, p, 0.40000001f);
+    p = fmaf(z, p, 0.66666669f);
+    p = fmaf(z, p, 2.0f);
+    float r = s * p;
+    float ef = (float)e;
+    return fmaf(ef, 0.693145751953125f, fmaf(ef, 1.42860677e-06f, r));
+}
+
+/* ------------------------------------------------------------------ */
+/* Models                                                               */
+/* ------------------------------------------------------------------ */
+enum { M_DENSE = 0, M_SPARSE = 1, M_HUBO = 2 };
+
+typedef struct {
+    int kind, n;
+    double c;
+    double *h64;
+    float *h32;
+    /* dense: coupling of (i,j) is J[min][max] (the upper triangle, as the
+       energy of dense_ising.cpp:29-44 reads it), float32, zero diagonal */
+    double *J64;
+    float *J32;
+    /* sparse: merged adjacency CSR (both directions) + the original edge list */
+    int *rowptr, *col;
+    float *val32;
+    int m;
+    int64_t *ei, *ej;
+    double *ew;
+    /* hubo: consolidated terms (degree >= 2) + incidence lists */
+    int T;
+    int *tptr, *tvars;
+    double *tcoef64;
+    float *tcoef32;
+    int *incptr, *incterm;
+} or_model;
+
+OR_EXPORT void or_model_free(or_model *M) {
+    if (!M) return;
+    free(M->h64); free(M->h32); free(M->J64); free(M->J32);
+    free(M->rowptr); free(M->col); free(M->val32); free(M->ei); free(M->ej); free(M->ew);
+    free(M->tptr); free(M->tvars); free(M->tcoef64); free(M->tcoef32);
+    free(M->incptr); free(M->incterm);
+    free(M);
+}
+
+static or_model *model_alloc(int kind, int n, double c) {
+    or_model *M = (or_model *)calloc(1, sizeof(or_model));
+    M->kind = kind; M->n = n; M->c = c;
+    M->h64 = (double *)calloc((size_t)n, sizeof(double));
+    M->h32 = (float *)calloc((size_t)n, sizeof(float));
+    return M;
+}
+
+OR_EXPORT or_model *or_model_dense(int n, const double *h, const double *J, double c) {
+    if (n <= 0) return NULL;
+    or_model *M = model_alloc(M_DENSE, n, c);
+    M->J64 = (double *)malloc((size_t)n * n * sizeof(double));
+    M->J32 = (float *)calloc((size_t)n * n, sizeof(float));
+    memcpy(M->J64, J, (size_t)n * n * sizeof(double));
+    for (int i = 0; i < n; ++i) { M->h64[i] = h[i]; M->h32[i] = (float)h[i]; }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            if (i == j) continue;
+            int a = i < j ? i : j, b = i < j ? j : i;
+            M->J32[(size_t)i * n + j] = (float)J[(size_t)a * n + b];
+        }
+    return M;
+}
+
+typedef struct { int nb; double w; int order; } nbr_t;
+static int nbr_cmp(const void *a, const void *b) {
+    const nbr_t *x = (const nbr_t *)a, *y = (const nbr_t *)b;
+    if (x->nb != y->nb) return x->nb < y->nb ? -1 : 1;
+    return x->order < y->order ? -1 : (x->order > y->order);
+}
+
+OR_EXPORT or_model *or_model_sparse(int n, const double *h, int m, const int64_t *ei, const int64_t *ej,
+                                    const double *w, double c) {
+    if (n <= 0) return NULL;
+    for (int e = 0; e < m; ++e) {
+        if (ei[e] < 0 || ej[e] < 0 || ei[e] >= n || ej[e] >= n || ei[e] == ej[e]) return NULL;
+    }
+    or_model *M = model_alloc(M_SPARSE, n, c);
+    for (int i = 0; i < n; ++i) { M->h64[i] = h[i]; M->h32[i] = (float)h[i]; }
+    M->m = m;
+    M->ei = (int64_t *)malloc(sizeof(int64_t) * (size_t)(m ? m : 1));
+    M->ej = (int64_t *)malloc(sizeof(int64_t) * (size_t)(m ? m : 1));
+    M->ew = (double *)malloc(sizeof(double) * (size_t)(m ? m : 1));
+    if (m) {
+        memcpy(M->ei, ei, sizeof(int64_t) * m);
+        memcpy(M->ej, ej, sizeof(int64_t) * m);
+        memcpy(M->ew, w, sizeof(double) * m);
+    }
+    /* adjacency entries in insertion order (sparse_ising.cpp:35-41), then
+       duplicates of one neighbour merged in float64 in that order */
+    int *deg = (int *)calloc((size_t)n + 1, sizeof(int));
+    for (int e = 0; e < m; ++e) { deg[ei[e]]++; deg[ej[e]]++; }
+    int *start = (int *)calloc((size_t)n + 1, sizeof(int));
+    for (int i = 0; i < n; ++i) start[i + 1] = start[i] + deg[i];
+    nbr_t *tmp = (nbr_t *)malloc(sizeof(nbr_t) * (size_t)(2 * m + 1));
+    int *fill = (int *)calloc((size_t)n, sizeof(int));
+    for (int e = 0; e < m; ++e) {
+        int a = (int)ei[e], b = (int)ej[e];
+        tmp[start[a] + fill[a]] = (nbr_t){b, w[e], fill[a]}; fill[a]++;
+        tmp[start[b] + fill[b]] = (nbr_t){a, w[e], fill[b]}; fill[b]++;
+    }
+    M->rowptr = (int *)calloc((size_t)n + 1, sizeof(int));
+    M->col = (int *)malloc(sizeof(int) * (size_t)(2 * m + 1));
+    M->val32 = (float *)malloc(sizeof(float) * (size_t)(2 * m + 1));
+    int nnz = 0;
+    for (int i = 0; i < n; ++i) {
+        qsort(tmp + start[i], (size_t)deg[i], sizeof(nbr_t), nbr_cmp);
+        M->rowptr[i] = nnz;
+        int k = start[i];
+        while (k < start[i] + deg[i]) {
+            int nb = tmp[k].nb;
+            double acc = 0.0;
+            /* float64 sum in insertion order */
+            int kk = k;
+            while (kk < start[i] + deg[i] && tmp[kk].nb == nb) { acc += tmp[kk].w; ++kk; }
+            M->col[nnz] = nb;
+            M->val32[nnz] = (float)acc;
+            ++nnz;
+            k = kk;
+        }
+    }
+    M->rowptr[n] = nnz;
+    free(deg); free(start); free(tmp); free(fill);
+    return M;
+}
+
+/* HUBO consolidation, restating higher_order_ising.cpp:10-90: parity reduction
+   of repeated indices, degree 0 -> c, degree 1 -> h, identical supports merged
+   (float64 sums in input order), zero coefficients dropped, terms ordered by
+   their sorted support (std::map order). */
+typedef struct { int deg; int vars_off; double coef; int order; } rawterm_t;
+static int *g_sortvars;
+static int rawterm_cmp(const void *a, const void *b) {
+    const rawterm_t *x = (const rawterm_t *)a, *y = (const rawterm_t *)b;
+    int d = x->deg < y->deg ? x->deg : y->deg;
+    for (int k = 0; k < d; ++k) {
+        int va = g_sortvars[x->vars_off + k], vb = g_sortvars[y->vars_off + k];
+        if (va != vb) return va < vb ? -1 : 1;
+    }
+    if (x->deg != y->deg) return x->deg < y->deg ? -1 : 1;
+    return x->order < y->order ? -1 : (x->order > y->order);
+}
+static int int_cmp(const void *a, const void *b) {
+    int x = *(const int *)a, y = *(const int *)b;
+    return x < y ? -1 : (x > y);
+}
+
+OR_EXPORT or_model *or_model_hubo(int n, int nraw, const int64_t *rptr, const int64_t *rvars,
+                                  const double *rcoef, double c) {
+    if (n <= 0) return NULL;
+    for (int t = 0; t < nraw; ++t)
+        for (int64_t k = rptr[t]; k < rptr[t + 1]; ++k)
+            if (rvars[k] < 0 || rvars[k] >= n) return NULL;
+    or_model *M = model_alloc(M_HUBO, n, c);
+    int64_t totv = nraw ? rptr[nraw] : 0;
+    int *sv = (int *)malloc(sizeof(int) * (size_t)(totv + 1));
+    rawterm_t *rt = (rawterm_t *)malloc(sizeof(rawterm_t) * (size_t)(nraw + 1));
+    int nrt = 0, voff = 0;
+    int *buf = (int *)malloc(sizeof(int) * (size_t)(totv + 1));
+    for (int t = 0; t < nraw; ++t) {
+        if (rcoef[t] == 0.0) continue;
+        int len = (int)(rptr[t + 1] - rptr[t]);
+        for (int k = 0; k < len; ++k) buf[k] = (int)rvars[rptr[t] + k];
+        qsort(buf, (size_t)len, sizeof(int), int_cmp);
+        int deg = 0, i = 0;
+        while (i < len) {
+            int j = i;
+            while (j < len && buf[j] == buf[i]) ++j;
+            if ((j - i) & 1) sv[voff + deg++] = buf[i];
+            i = j;
+        }
+        if (deg == 0) { M->c += rcoef[t]; continue; }
+        if (deg == 1) { M->h64[sv[voff]] += rcoef[t]; continue; }
+        rt[nrt] = (rawterm_t){deg, voff, rcoef[t], nrt};
+        ++nrt;
+        voff += deg;
+    }
+    free(buf);
+    for (int i = 0; i < n; ++i) M->h32[i] = (float)M->h64[i];
+    g_sortvars = sv;
+    qsort(rt, (size_t)nrt, sizeof(rawterm_t), rawterm_cmp);
+    M->tptr = (int *)calloc((size_t)nrt + 1, sizeof(int));
+    M->tvars = (int *)malloc(sizeof(int) * (size_t)(voff + 1));
+    M->tcoef64 = (double *)malloc(sizeof(double) * (size_t)(nrt + 1));
+    M->tcoef32 = (float *)malloc(sizeof(float) * (size_t)(nrt + 1));
+    int T = 0, tv = 0, k = 0;
+    while (k < nrt) {
+        int kk = k;
+        double acc = 0.0;
+        while (kk < nrt && rawterm_cmp(&(rawterm_t){rt[k].deg, rt[k].vars_off, 0, -1},
+                                       &(rawterm_t){rt[kk].deg, rt[kk].vars_off, 0, -1}) == 0) {
+            acc += rt[kk].coef;
+            ++kk;
+        }
+        if (acc != 0.0) {
+            M->tptr[T] = tv;
+            for (int v = 0; v < rt[k].deg; ++v) M->tvars[tv++] = sv[rt[k].vars_off + v];
+            M->tcoef64[T] = acc;
+            M->tcoef32[T] = (float)acc;
+            ++T;
+        }
+        k = kk;
+    }
+    M->tptr[T] = tv;
+    M->T = T;
+    free(rt); free(sv);
+    /* incidence lists in term order */
+    M->incptr = (int *)calloc((size_t)n + 1, sizeof(int));
+    for (int t = 0; t < T; ++t)
+        for (int q = M->tptr[t]; q < M->tptr[t + 1]; ++q) M->incptr[M->tvars[q] + 1]++;
+    for (int i = 0; i < n; ++i) M->incptr[i + 1] += M->incptr[i];
+    M->incterm = (int *)malloc(sizeof(int) * (size_t)(M->incptr[n] + 1));
+    int *fill = (int *)calloc((size_t)n, sizeof(int));
+    for (int t = 0; t < T; ++t)
+        for (int q = M->tptr[t]; q < M->tptr[t + 1]; ++q) {
+            int v = M->tvars[q];
+            M->incterm[M->incptr[v] + fill[v]++] = t;
+        }
+    free(fill);
+    return M;
+}
+
+/* Introspection of the consolidated HUBO (for tests). */
+OR_EXPORT int or_model_info(const or_model *M, int *n, int *kind, int *T, double *c) {
+    *n = M->n; *kind = M->kind; *T = M->T; *c = M->c;
+    return 0;
+}
+OR_EXPORT void or_model_hubo_terms(const or_model *M, int *tptr, int *tvars, double *coef, double *h) {
+    memcpy(tptr, M->tptr, sizeof(int) * (size_t)(M->T + 1));
+    memcpy(tvars, M->tvars, sizeof(int) * (size_t)M->tptr[M->T]);
+    memcpy(coef, M->tcoef64, sizeof(double) * (size_t)M->T);
+    memcpy(h, M->h64, sizeof(double) * (size_t)M->n);
+}
+
+/* ---- float64 restatements of the reference's own model functions ---- */
+
+/* energy() in the reference's summation order (dense_ising.cpp:29-44,
+   sparse_ising.cpp:43-56, higher_order_ising.cpp:92-111) */
+OR_EXPORT double or_energy64(const or_model *M, const int8_t *s) {
+    const int n = M->n;
+    double E = M->c;
+    for (int i = 0; i < n; ++i) E += M->h64[i] * (double)s[i];
+    if (M->kind == M_DENSE) {
+        for (int i = 0; i < n; ++i)
+            for (int j = i + 1; j < n; ++j)
+                E += M->J64[(size_t)i * n + j] * (double)s[i] * (double)s[j];
+    } else if (M->kind == M_SPARSE) {
+        for (int e = 0; e < M->m; ++e) E += M->ew[e] * (double)s[M->ei[e]] * (double)s[M->ej[e]];
+    } else {
+        for (int t = 0; t < M->T; ++t) {
+            double p = M->tcoef64[t];
+            for (int q = M->tptr[t]; q < M->tptr[t + 1]; ++q) p *= (double)s[M->tvars[q]];
+            E += p;
+        }
+    }
+    return E;
+}
+
+/* delta_energy() (dense_ising.cpp:46-62, sparse_ising.cpp:58-71,
+   higher_order_ising.cpp:113-136), float64, original coefficients */
+OR_EXPORT double or_delta_energy64(const or_model *M, const int8_t *s, int flip) {
+    const int n = M->n;
+    double local = M->h64[flip];
+    if (M->kind == M_DENSE) {
+        for (int j = 0; j < n; ++j)
+            if (j != flip) local += M->J64[(size_t)flip * n + j] * (double)s[j];
+    } else if (M->kind == M_SPARSE) {
+        for (int e = 0; e < M->m; ++e) {
+            if (M->ei[e] == flip) local += M->ew[e] * (double)s[M->ej[e]];
+            else if (M->ej[e] == flip) local += M->ew[e] * (double)s[M->ei[e]];
+        }
+    } else {
+        for (int q = M->incptr[flip]; q < M->incptr[flip + 1]; ++q) {
+            int t = M->incterm[q];
+            double p = M->tcoef64[t];
+            for (int k = M->tptr[t]; k < M->tptr[t + 1]; ++k)
+                if (M->tvars[k] != flip) p *= (double)s[M->tvars[k]];
+            local += p;
+        }
+    }
+    return -2.0 * (double)s[flip] * local;
+}
+
+/* ------------------------------------------------------------------ */
+/* Replay-model field cache (float32 g = J.s, h kept apart)            */
+/* ------------------------------------------------------------------ */
+static void fields_init(const or_model *M, const int8_t *s, float *g) {
+    const int n = M->n;
+    if (M->kind == M_DENSE) {
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+            const float *row = M->J32 + (size_t)i * n;
+            for (int j = 0; j < n; ++j) acc += (double)row[j] * (double)s[j];
+            g[i] = (float)acc;
+        }
+    } else if (M->kind == M_SPARSE) {
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int e = M->rowptr[i]; e < M->rowptr[i + 1]; ++e) acc += (double)M->val32[e] * (double)s[M->col[e]];
+            g[i] = (float)acc;
+        }
+    } else {
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int q = M->incptr[i]; q < M->incptr[i + 1]; ++q) {
+                int t = M->incterm[q];
+                int sg = 1;
+                for (int k = M->tptr[t]; k < M->tptr[t + 1]; ++k)
+                    if (M->tvars[k] != i) sg *= s[M->tvars[k]];
+                acc += (double)M->tcoef32[t] * (double)sg;
+            }
+            g[i] = (float)acc;
+        }
+    }
+}
+
+OR_EXPORT void or_fields_init(const or_model *M, const int8_t *s, float *g) { fields_init(M, s, g); }
+
+/* After flipping spin j whose old value was so (s already holds the new value). */
+static void apply_flip(const or_model *M, const int8_t *s, float *g, int j, int so) {
+    const int n = M->n;
+    const float cf = so > 0 ? -2.0f : 2.0f;
+    if (M->kind == M_DENSE) {
+        const float *row = M->J32 + (size_t)j * n;
+        for (int m = 0; m < n; ++m)
+            if (m != j) g[m] = g[m] + cf * row[m];
+    } else if (M->kind == M_SPARSE) {
+        for (int e = M->rowptr[j]; e < M->rowptr[j + 1]; ++e) {
+            int m = M->col[e];
+            g[m] = g[m] + cf * M->val32[e];
+        }
+    } else {
+        /* higher_order_ising.cpp:167-189: each other member v of an incident
+           term gains 2 * J_t * prod(new spins) * s_v */
+        for (int q = M->incptr[j]; q < M->incptr[j + 1]; ++q) {
+            int t = M->incterm[q];
+            int sg = 1;
+            for (int k = M->tptr[t]; k < M->tptr[t + 1]; ++k) sg *= s[M->tvars[k]];
+            float two = 2.0f * M->tcoef32[t];
+            for (int k = M->tptr[t]; k < M->tptr[t + 1]; ++k) {
+                int v = M->tvars[k];
+                if (v == j) continue;
+                float d = (sg * s[v] > 0) ? two : -two;
+                g[v] = g[v] + d;
+            }
+        }
+    }
+}
+
+/* float64 sum in warp order: 32 lane-strided partials, then xor butterfly */
+static double wsum(const double *v, int n) {
+    double p[32];
+    for (int l = 0; l < 32; ++l) p[l] = 0.0;
+    for (int i = 0; i < n; ++i) p[i & 31] += v[i];
+    for (int off = 16; off >= 1; off >>= 1) {
+        double q[32];
+        for (int l = 0; l < 32; ++l) q[l] = p[l] + p[l ^ off];
+        memcpy(p, q, sizeof(p));
+    }
+    return p[0];
+}
+
+/* Tracking energy of one slice from its field cache. */
+static double energy_track(const or_model *M, const int8_t *s, const float *g, double *scratch) {
+    const int n = M->n;
+    if (M->kind != M_HUBO) {
+        for (int i = 0; i < n; ++i) scratch[i] = (double)s[i] * ((double)M->h32[i] + 0.5 * (double)g[i]);
+        return M->c + wsum(scratch, n);
+    }
+    for (int i = 0; i < n; ++i) scratch[i] = (double)s[i] * (double)M->h32[i];
+    double eh = wsum(scratch, n);
+    double *st = scratch + n;
+    for (int t = 0; t < M->T; ++t) {
+        int sg = 1;
+        for (int k = M->tptr[t]; k < M->tptr[t + 1]; ++k) sg *= s[M->tvars[k]];
+        st[t] = sg > 0 ? (double)M->tcoef32[t] : -(double)M->tcoef32[t];
+    }
+    double ej = wsum(st, M->T);
+    return M->c + (eh + ej);
+}
+
+OR_EXPORT double or_energy_track(const or_model *M, const int8_t *s) {
+    float *g = (float *)malloc(sizeof(float) * (size_t)M->n);
+    double *sc = (double *)malloc(sizeof(double) * (size_t)(M->n + M->T + 1));
+    fields_init(M, s, g);
+    double E = energy_track(M, s, g, sc);
+    free(g); free(sc);
+    return E;
+}
+
+static void init_spins(int8_t *s, int n, uint64_t key, uint32_t cell, uint32_t tag) {
+    const int nw = (n + 31) / 32;
+    for (int q = 0; q < nw; ++q) {
+        uint32_t w = draw(key, (uint32_t)(q >> 2), cell, 0u, tag, q & 3);
+        for (int b = 0; b < 32 && 32 * q + b < n; ++b) s[32 * q + b] = ((w >> b) & 1u) ? 1 : -1;
+    }
+}
+
+OR_EXPORT void or_init_spins(int8_t *s, int n, uint64_t key, uint32_t cell, uint32_t tag) {
+    init_spins(s, n, key, cell, tag);
+}
+
+static double trotter_coupling(double beta, double gamma, int P) {
+    double x = beta * gamma / (double)P;
+    if (x < 1e-12) x = 1e-12;
+    return 0.5 * log(1.0 / tanh(x));
+}
+
+/* ------------------------------------------------------------------ */
+/* SA (annealer.cpp:33-75)                                              */
+/* ------------------------------------------------------------------ */
+OR_EXPORT int or_sa_run(const or_model *M, const double *betas, int steps, int spb, uint64_t seed, int read,
+                        int8_t *best_spins, double *best_E, double *trace, int64_t *counters) {
+    const int n = M->n;
+    const uint64_t key = seed + (uint64_t)read;
+    int8_t *s = (int8_t *)malloc((size_t)n);
+    float *g = (float *)malloc(sizeof(float) * (size_t)n);
+    double *sc = (double *)malloc(sizeof(double) * (size_t)(n + M->T + 1));
+    init_spins(s, n, key, 0u, DOM_INIT);
+    fields_init(M, s, g);
+    double E = energy_track(M, s, g, sc);
+    double best = E;
+    memcpy(best_spins, s, (size_t)n);
+    int64_t att = 0, acc = 0;
+    for (int step = 0; step < steps; ++step) {
+        const float A = (float)(1.0 / (2.0 * betas[step]));
+        for (int sw = 0; sw < spb; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * spb + sw);
+            for (int i = 0; i < n; ++i) {
+                float u = u01(draw(key, spin_slot(i), 0u, sigma, DOM_SA, spin_word(i)));
+                float thr = or_logf(u) * A;
+                float loc = M->h32[i] + g[i];
+                float x = s[i] > 0 ? loc : -loc;
+                ++att;
+                if (x > thr) {
+                    ++acc;
+                    int so = s[i];
+                    double xd = (double)so * ((double)M->h32[i] + (double)g[i]);
+                    s[i] = (int8_t)-so;
+                    apply_flip(M, s, g, i, so);
+                    E += -2.0 * xd;
+                    if (E < best) { best = E; memcpy(best_spins, s, (size_t)n); }
+                }
+            }
+        }
+        trace[step] = E;
+    }
+    *best_E = best;
+    if (counters) { counters[0] = att; counters[1] = acc; }
+    free(s); free(g); free(sc);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Trotter ring sweeps shared by SQA, SQA-PT and SQA-Chi                */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    const or_model *M;
+    int n, P, K;
+    int8_t *s;   /* [K*P][n] */
+    float *g;    /* [K*P][n] */
+    double *sc;
+    uint64_t key;
+    int64_t att_slice, acc_slice, att_world, acc_world;
+} ring_t;
+
+static int phase_of(int t, int P) {
+    if ((P & 1) && t == P - 1) return 2;
+    return t & 1;
+}
+
+static void ring_alloc(ring_t *R, const or_model *M, int P, int K, uint64_t key) {
+    memset(R, 0, sizeof(*R));
+    R->M = M; R->n = M->n; R->P = P; R->K = K; R->key = key;
+    R->s = (int8_t *)malloc((size_t)K * P * M->n);
+    R->g = (float *)malloc(sizeof(float) * (size_t)K * P * M->n);
+    R->sc = (double *)malloc(sizeof(double) * (size_t)(M->n + M->T + 1));
+}
+static void ring_free(ring_t *R) { free(R->s); free(R->g); free(R->sc); }
+
+static void ring_init(ring_t *R, uint32_t tag) {
+    for (int c = 0; c < R->K * R->P; ++c) {
+        init_spins(R->s + (size_t)c * R->n, R->n, R->key, (uint32_t)c, tag);
+        fields_init(R->M, R->s + (size_t)c * R->n, R->g + (size_t)c * R->n);
+    }
+}
+
+/* One slice of one ring: sqa_annealer.cpp:180-209 / sqa_chi_annealer.cpp:96-121.
+   rng_cell is the cell index used in the counter (ring-relative k*P+t unless
+   a slot remap applies). */
+static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigma, uint32_t tag, float A, float T4) {
+    const or_model *M = R->M;
+    const int n = R->n, P = R->P;
+    const int prev = t == 0 ? P - 1 : t - 1, next = (t + 1) % P;
+    int8_t *s = R->s + ((size_t)k * P + t) * n;
+    const int8_t *sp = R->s + ((size_t)k * P + prev) * n;
+    const int8_t *sn = R->s + ((size_t)k * P + next) * n;
+    float *g = R->g + ((size_t)k * P + t) * n;
+    for (int i = 0; i < n; ++i) {
+        const int si = s[i];
+        const int q = si * (sp[i] + sn[i]) / 2;
+        const float tro = q == 0 ? 0.0f : (q > 0 ? T4 : -T4);
+        float u = u01(draw(R->key, spin_slot(i), rng_cell, sigma, tag, spin_word(i)));
+        float thr = (tro + or_logf(u)) * A;
+        float loc = M->h32[i] + g[i];
+        float x = si > 0 ? loc : -loc;
+        R->att_slice++;
+        if (x > thr) {
+            R->acc_slice++;
+            s[i] = (int8_t)-si;
+            apply_flip(M, s, g, i, si);
+        }
+    }
+}
+
+static void slice_sweep(ring_t *R, uint32_t sigma, uint32_t tag, float A, float T4, const int *slot_of_ring) {
+    for (int ph = 0; ph < 3; ++ph)
+        for (int k = 0; k < R->K; ++k)
+            for (int t = 0; t < R->P; ++t) {
+                if (phase_of(t, R->P) != ph) continue;
+                int slot = slot_of_ring ? slot_of_ring[k] : k;
+                sweep_cell(R, k, t, (uint32_t)(slot * R->P + t), sigma, tag, A, T4);
+            }
+}
+
+/* sqa_annealer.cpp:294-315 */
+static void worldline_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma, float A) {
+    const or_model *M = R->M;
+    const int n = R->n, P = R->P;
+    for (int i = 0; i < n; ++i) {
+        int sh = 0;
+        double G = 0.0;
+        for (int t = 0; t < P; ++t) {
+            int st = R->s[((size_t)k * P + t) * n + i];
+            sh += st;
+            G += (double)st * (double)R->g[((size_t)k * P + t) * n + i];
+        }
+        float x = (float)((double)M->h32[i] * (double)sh + G);
+        float u = u01(draw(R->key, spin_slot(i), rng_ring, sigma, DOM_WORLD, spin_word(i)));
+        float thr = or_logf(u) * A;
+        R->att_world++;
+        if (x > thr) {
+            R->acc_world++;
+            for (int t = 0; t < P; ++t) {
+                int8_t *s = R->s + ((size_t)k * P + t) * n;
+                int so = s[i];
+                s[i] = (int8_t)-so;
+                apply_flip(M, s, R->g + ((size_t)k * P + t) * n, i, so);
+            }
+        }
+    }
+}
+
+static double cell_energy(ring_t *R, int c) {
+    return energy_track(R->M, R->s + (size_t)c * R->n, R->g + (size_t)c * R->n, R->sc);
+}
+
+/* Per-step constants: beta_scale = beta/P, A = 1/(2 beta_scale), T4 = 4 J_perp. */
+static void step_consts(double beta, double gamma, int P, float *A, float *T4) {
+    const double bs = beta / (double)P;
+    *A = (float)(1.0 / (2.0 * bs));
+    *T4 = (float)(4.0 * trotter_coupling(beta, gamma, P));
+}
+
+/* ------------------------------------------------------------------ */
+/* SQA run (sqa_annealer.cpp:87-477), one read                          */
+/* ------------------------------------------------------------------ */
+OR_EXPORT int or_sqa_run(const or_model *M, const double *betas, const double *gammas, int steps, int P, int K,
+                         int spb, int wls, uint64_t seed, int read, int8_t *best_spins, double *best_E,
+                         double *trace, int64_t *counters) {
+    const int n = M->n;
+    ring_t R;
+    ring_alloc(&R, M, P, K, seed + (uint64_t)read);
+    ring_init(&R, DOM_INIT);
+    double *rbest = (double *)malloc(sizeof(double) * (size_t)K);
+    int *rstep = (int *)malloc(sizeof(int) * (size_t)K);
+    int8_t *rstate = (int8_t *)malloc((size_t)K * n);
+    double *rsum = (double *)malloc(sizeof(double) * (size_t)K);
+    for (int k = 0; k < K; ++k) { rbest[k] = INFINITY; rstep[k] = -1; }
+    for (int step = 0; step < steps; ++step) {
+        float A, T4;
+        step_consts(betas[step], gammas[step], P, &A, &T4);
+        for (int sw = 0; sw < spb; ++sw) slice_sweep(&R, (uint32_t)(step * spb + sw), DOM_SLICE, A, T4, NULL);
+        for (int sw = 0; sw < wls; ++sw)
+            for (int k = 0; k < K; ++k) worldline_sweep(&R, k, (uint32_t)k, (uint32_t)(step * wls + sw), A);
+        for (int k = 0; k < K; ++k) {
+            double sum = 0.0, emin = INFINITY;
+            int tmin = 0;
+            for (int t = 0; t < P; ++t) {
+                double E = cell_energy(&R, k * P + t);
+                sum += E;
+                if (E < emin) { emin = E; tmin = t; }
+            }
+            rsum[k] = sum;
+            if (emin < rbest[k]) {
+                rbest[k] = emin; rstep[k] = step;
+                memcpy(rstate + (size_t)k * n, R.s + ((size_t)k * P + tmin) * n, (size_t)n);
+            }
+        }
+        double tot = 0.0;
+        for (int k = 0; k < K; ++k) tot += rsum[k];
+        trace[step] = tot / (double)(K * P);
+    }
+    int kb = 0;
+    for (int k = 1; k < K; ++k)
+        if (rbest[k] < rbest[kb] || (rbest[k] == rbest[kb] && rstep[k] < rstep[kb])) kb = k;
+    *best_E = rbest[kb];
+    memcpy(best_spins, rstate + (size_t)kb * n, (size_t)n);
+    if (counters) {
+        counters[0] = R.att_slice; counters[1] = R.acc_slice;
+        counters[2] = R.att_world; counters[3] = R.acc_world;
+    }
+    free(rbest); free(rstep); free(rstate); free(rsum);
+    ring_free(&R);
+    return 0;
+}

@@ -1,0 +1,138 @@
+"""ctypes binding of libqa_gpu.so (include/qa_gpu.h).
+
+The library is built in-tree by ``qlatanneal_b200/csrc/Makefile``.  Nothing here
+falls back to a CPU path: a missing library or a missing GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqa_gpu.so")
+
+QA_OK, QA_ERR_ARG, QA_ERR_CUDA, QA_ERR_OOM, QA_ERR_TIMEOUT, QA_ERR_DRIFT, QA_ERR_UNSUPPORTED = range(7)
+
+# Every symbol include/qa_gpu.h declares (checked by the CPU test suite).
+EXPORTED = [
+    "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy",
+    "qa_problem_dense", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
+    "qa_sa_run", "qa_sqa_run",
+]
+
+
+class qa_run_out(C.Structure):
+    _fields_ = [("best_spins", C.c_void_p), ("best_energy", C.c_void_p), ("energy_trace", C.c_void_p)]
+
+
+class qa_stats(C.Structure):
+    _fields_ = [("slice_attempts", C.c_int64), ("slice_accepts", C.c_int64),
+                ("worldline_attempts", C.c_int64), ("worldline_accepts", C.c_int64),
+                ("sweep_ms", C.c_double), ("total_ms", C.c_double)]
+
+
+class qa_sa_params(C.Structure):
+    _fields_ = [("betas", C.c_void_p), ("steps", C.c_int), ("sweeps_per_beta", C.c_int), ("reads", C.c_int),
+                ("seed", C.c_uint64)]
+
+
+class qa_sqa_params(C.Structure):
+    _fields_ = [("betas", C.c_void_p), ("gammas", C.c_void_p), ("steps", C.c_int), ("trotter_slices", C.c_int),
+                ("replicas", C.c_int), ("sweeps_per_beta", C.c_int), ("worldline_sweeps", C.c_int),
+                ("cluster_sweeps", C.c_int), ("continuous_time_slices", C.c_int), ("reads", C.c_int),
+                ("seed", C.c_uint64)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load libqa_gpu.so (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -f qlatanneal_b200/csrc/Makefile` "
+                              "(or __graft_entry__.build()).")
+        L = C.CDLL(LIB_PATH)
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        L.qa_version.restype = C.c_char_p
+        L.qa_last_error.argtypes = [C.c_char_p, C.c_size_t]
+        L.qa_device_count.argtypes = [C.POINTER(C.c_int)]
+        L.qa_create.argtypes = [C.POINTER(vp), i]
+        L.qa_destroy.argtypes = [vp]
+        L.qa_problem_dense.argtypes = [vp, i, vp, vp, d, C.POINTER(vp)]
+        L.qa_problem_sparse.argtypes = [vp, i, vp, i, vp, vp, vp, d, C.POINTER(vp)]
+        L.qa_problem_hubo.argtypes = [vp, i, vp, i, vp, vp, vp, d, C.POINTER(vp)]
+        L.qa_problem_free.argtypes = [vp]
+        L.qa_problem_size.argtypes = [vp, C.POINTER(i)]
+        L.qa_sa_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sa_params), C.POINTER(qa_run_out),
+                                C.POINTER(qa_stats)]
+        L.qa_sqa_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sqa_params), C.POINTER(qa_run_out),
+                                 C.POINTER(qa_stats)]
+        for name in list(EXPORTED):
+            getattr(L, name)
+        _lib = L
+        return L
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    load().qa_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int) -> None:
+    """Map a status code onto the exception qanneal raises for the same failure."""
+    if rc == QA_OK:
+        return
+    msg = last_error()
+    if rc == QA_ERR_ARG:
+        raise ValueError(msg)
+    if rc == QA_ERR_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    if rc == QA_ERR_OOM:
+        raise MemoryError(msg)
+    raise RuntimeError(f"qa_gpu error {rc}: {msg}")
+
+
+def ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class Engine:
+    """One device context (qa_ctx) per (process, device)."""
+
+    _engines: dict = {}
+
+    def __init__(self, device: int):
+        L = load()
+        n = C.c_int(0)
+        check(L.qa_device_count(C.byref(n)))
+        if n.value <= 0:
+            raise RuntimeError("no CUDA device is visible: the qlatanneal_b200 engine runs only on a GPU.")
+        h = C.c_void_p()
+        check(L.qa_create(C.byref(h), int(device)))
+        self.L, self.h, self.device = L, h, int(device)
+
+    @classmethod
+    def get(cls, device=None) -> "Engine":
+        if device is None:
+            device = int(os.environ.get("LOCAL_RANK", "0"))
+        with _lock:
+            e = cls._engines.get(device)
+        if e is None:
+            e = Engine(device)
+            with _lock:
+                cls._engines[device] = e
+        return e
+
+    def close(self):
+        if self.h:
+            self.L.qa_destroy(self.h)
+            self.h = None

@@ -1,0 +1,179 @@
+"""Annealer classes with qanneal's constructor/run signatures (python/bindings.cpp:352-620).
+
+Every ``run*`` call executes on the GPU through libqa_gpu.so.  ``run`` performs
+one read, exactly like qanneal; ``run_reads`` performs many reads in a single
+batched launch (the form ``solve()`` uses).  Read ``r`` of a batch seeded with
+``s`` uses the same random stream as a single ``run`` after ``set_seed(s + r)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .models import AnnealSchedule, SQASchedule, State
+
+BACKENDS = ("cuda", "CUDA")
+
+
+def _check_backend(backend: str) -> None:
+    if backend in ("cpu", "CPU"):
+        raise ValueError("qlatanneal_b200 implements backend='cuda' only; the CPU backend is qanneal itself.")
+    if backend not in BACKENDS:
+        raise ValueError("Unknown backend: " + str(backend))
+
+
+def _random_seed() -> int:
+    return int.from_bytes(os.urandom(8), "little")
+
+
+@dataclass
+class AnnealResult:
+    """``qanneal.AnnealResult`` (annealer.hpp:16-20)."""
+    best_state: State
+    best_energy: float
+    energy_trace: List[float]
+
+
+@dataclass
+class SQAResult:
+    """``qanneal.SQAResult`` (sqa_annealer.hpp:18-29); the run_optimal diagnostics stay empty."""
+    best_state: State
+    best_energy: float
+    energy_trace: List[float]
+    j_perp_trace: List[float] = field(default_factory=list)
+    chi_B_trace: List[float] = field(default_factory=list)
+    calibrated_eps_tilde: float = 0.0
+    j_perp_start: float = 0.0
+    resolved_j_perp_end: float = 0.0
+    final_j_perp: float = 0.0
+
+
+@dataclass
+class RunStats:
+    """Device-side totals of one batched call (qa_stats)."""
+    slice_attempts: int = 0
+    slice_accepts: int = 0
+    worldline_attempts: int = 0
+    worldline_accepts: int = 0
+    sweep_ms: float = 0.0
+    total_ms: float = 0.0
+
+    @classmethod
+    def from_c(cls, s: "_lib.qa_stats") -> "RunStats":
+        return cls(s.slice_attempts, s.slice_accepts, s.worldline_attempts, s.worldline_accepts, s.sweep_ms,
+                   s.total_ms)
+
+
+class _Seeded:
+    def __init__(self):
+        self._seed = _random_seed()
+        self._runs = 0
+
+    def set_seed(self, seed: int) -> None:
+        self._seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        self._runs = 0
+
+    def _next_seed(self, reads: int) -> int:
+        s = (self._seed + self._runs) & 0xFFFFFFFFFFFFFFFF
+        self._runs += reads
+        return s
+
+
+def _outs(n: int, reads: int, steps: int):
+    spins = np.zeros((reads, n), dtype=np.int8)
+    energies = np.zeros(reads, dtype=np.float64)
+    trace = np.zeros((reads, steps), dtype=np.float64)
+    o = _lib.qa_run_out(spins.ctypes.data, energies.ctypes.data, trace.ctypes.data)
+    return o, spins, energies, trace
+
+
+class Annealer(_Seeded):
+    """``qanneal.Annealer(hamiltonian, schedule, backend)`` -- SA Metropolis (annealer.cpp:33-75)."""
+
+    def __init__(self, hamiltonian, schedule: AnnealSchedule, backend: str = "cuda", device: Optional[int] = None):
+        super().__init__()
+        _check_backend(backend)
+        if hamiltonian is None:
+            raise ValueError("Annealer requires a backend.")
+        if len(schedule.betas) == 0:
+            raise ValueError("Schedule must contain at least one beta.")
+        self.hamiltonian = hamiltonian
+        self.schedule = schedule
+        self.device = device
+        self.last_stats: Optional[RunStats] = None
+
+    def run(self, sweeps_per_beta: int, observer=None) -> AnnealResult:
+        if observer is not None:
+            raise NotImplementedError("observers are not supported by the CUDA sweep engine.")
+        return self.run_reads(sweeps_per_beta, reads=1)[0]
+
+    def run_reads(self, sweeps_per_beta: int, reads: int, seed: Optional[int] = None) -> List[AnnealResult]:
+        if sweeps_per_beta <= 0:
+            raise ValueError("sweeps_per_beta must be > 0.")
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        betas = np.ascontiguousarray(self.schedule.betas, dtype=np.float64)
+        seed = self._next_seed(reads) if seed is None else int(seed)
+        prm = _lib.qa_sa_params(betas.ctypes.data, len(betas), int(sweeps_per_beta), int(reads), seed)
+        n = self.hamiltonian.size()
+        o, spins, energies, trace = _outs(n, reads, len(betas))
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_sa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        return [AnnealResult(State(spins[r]), float(energies[r]), trace[r].tolist()) for r in range(reads)]
+
+
+class SQAAnnealer(_Seeded):
+    """``qanneal.SQAAnnealer(hamiltonian, schedule, trotter_slices, replicas, backend)``
+    (sqa_annealer.cpp:87-477): parity-phase slice sweeps and worldline sweeps."""
+
+    def __init__(self, hamiltonian, schedule: SQASchedule, trotter_slices: int, replicas: int = 1,
+                 backend: str = "cuda", device: Optional[int] = None):
+        super().__init__()
+        _check_backend(backend)
+        if hamiltonian is None:
+            raise ValueError("SQAAnnealer requires a backend.")
+        if len(schedule.betas) == 0:
+            raise ValueError("SQA schedule must contain betas.")
+        if len(schedule.betas) != len(schedule.gammas):
+            raise ValueError("SQA schedule betas/gammas length mismatch.")
+        if trotter_slices <= 0:
+            raise ValueError("trotter_slices must be > 0.")
+        if replicas <= 0:
+            raise ValueError("replicas must be > 0.")
+        self.hamiltonian = hamiltonian
+        self.schedule = schedule
+        self.trotter_slices = int(trotter_slices)
+        self.replicas = int(replicas)
+        self.device = device
+        self.last_stats: Optional[RunStats] = None
+
+    def run(self, sweeps_per_beta: int, worldline_sweeps: int, cluster_sweeps: int = 0,
+            continuous_time_slices: int = 0, observer=None) -> SQAResult:
+        if observer is not None:
+            raise NotImplementedError("observers are not supported by the CUDA sweep engine.")
+        return self.run_reads(sweeps_per_beta, worldline_sweeps, cluster_sweeps, continuous_time_slices, reads=1)[0]
+
+    def run_reads(self, sweeps_per_beta: int, worldline_sweeps: int, cluster_sweeps: int = 0,
+                  continuous_time_slices: int = 0, reads: int = 1, seed: Optional[int] = None) -> List[SQAResult]:
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        betas = np.ascontiguousarray(self.schedule.betas, dtype=np.float64)
+        gammas = np.ascontiguousarray(self.schedule.gammas, dtype=np.float64)
+        seed = self._next_seed(reads) if seed is None else int(seed)
+        prm = _lib.qa_sqa_params(betas.ctypes.data, gammas.ctypes.data, len(betas), self.trotter_slices,
+                                 self.replicas, int(sweeps_per_beta), int(worldline_sweeps), int(cluster_sweeps),
+                                 int(continuous_time_slices), int(reads), seed)
+        n = self.hamiltonian.size()
+        o, spins, energies, trace = _outs(n, reads, len(betas))
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_sqa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        return [SQAResult(State(spins[r]), float(energies[r]), trace[r].tolist()) for r in range(reads)]

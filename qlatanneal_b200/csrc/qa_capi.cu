@@ -1,0 +1,682 @@
+// qa_capi.cu -- host side of libqa_gpu.so: contexts, problem upload, and the
+// run entry points declared in include/qa_gpu.h.  Each entry point batches all
+// reads (and all problems of the call) into single kernel launches.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "qa_gpu.h"
+#include "qa_kernels.cuh"
+
+using namespace qa;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define QA_CK(call)                                                                                   \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) {                                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? QA_ERR_OOM : QA_ERR_CUDA,                   \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+        }                                                                                             \
+    } while (0)
+
+#define QA_TRY(expr)                  \
+    do {                              \
+        int rc_ = (expr);             \
+        if (rc_ != QA_OK) return rc_; \
+    } while (0)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace
+
+struct qa_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int smem_optin = 0;
+    DevBuf ws[16];
+};
+
+struct qa_problem {
+    qa_ctx *ctx = nullptr;
+    int kind = 0, n = 0, nw = 0, T = 0, m = 0;
+    double c = 0.0;
+    std::vector<void *> allocs;
+    ProbDev dev{};
+};
+
+namespace {
+
+enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
+              W_PROBOF, W_MIN, W_BOND, W_MAG };
+
+int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
+    DevBuf &b = ctx->ws[slot];
+    if (bytes == 0) bytes = 16;
+    if (b.cap < bytes) {
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        size_t want = std::max(bytes, b.cap * 3 / 2);
+        QA_CK(cudaMalloc(&b.p, want));
+        b.cap = want;
+    }
+    *out = b.p;
+    return QA_OK;
+}
+
+template <class T>
+int upload(qa_problem *P, const T *host, size_t count, const T **dev) {
+    void *d = nullptr;
+    size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    QA_CK(cudaMalloc(&d, bytes));
+    P->allocs.push_back(d);
+    if (count) QA_CK(cudaMemcpy(d, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    *dev = static_cast<const T *>(d);
+    return QA_OK;
+}
+
+int begin(qa_ctx *ctx) {
+    if (!ctx) return fail(QA_ERR_ARG, "null context");
+    QA_CK(cudaSetDevice(ctx->device));
+    return QA_OK;
+}
+
+void finish_problem(qa_problem *P) {
+    P->dev.kind = P->kind;
+    P->dev.n = P->n;
+    P->dev.nw = P->nw;
+    P->dev.T = P->T;
+    P->dev.m = P->m;
+    P->dev.c = P->c;
+}
+
+int common_h(qa_problem *P, const double *h) {
+    std::vector<float> h32(P->n);
+    for (int i = 0; i < P->n; ++i) h32[i] = (float)h[i];
+    QA_TRY(upload(P, h32.data(), h32.size(), &P->dev.h32));
+    QA_TRY(upload(P, h, (size_t)P->n, &P->dev.h64));
+    return QA_OK;
+}
+
+double trotter_coupling(double beta, double gamma, int P) {
+    // sqa_annealer.cpp:66-70
+    const double x = std::max(beta * gamma / (double)P, 1e-12);
+    return 0.5 * std::log(1.0 / std::tanh(x));
+}
+
+std::vector<uint32_t> dummy;
+
+void unpack_bits(const uint32_t *bits, int n, int8_t *out) {
+    for (int i = 0; i < n; ++i) out[i] = ((bits[i >> 5] >> (i & 31)) & 1u) ? 1 : -1;
+}
+
+int check_batch(const qa_problem *const *probs, int np, int *kind, int *n_max) {
+    if (!probs || np <= 0) return fail(QA_ERR_ARG, "at least one problem is required.");
+    *kind = probs[0] ? probs[0]->kind : -1;
+    *n_max = 0;
+    for (int i = 0; i < np; ++i) {
+        if (!probs[i]) return fail(QA_ERR_ARG, "null problem.");
+        if (probs[i]->kind != *kind) return fail(QA_ERR_ARG, "all problems of one call must be of the same model kind.");
+        *n_max = std::max(*n_max, probs[i]->n);
+    }
+    return QA_OK;
+}
+
+template <class F>
+void dispatch_kind(int kind, F &&f) {
+    if (kind == K_DENSE) f(std::integral_constant<int, K_DENSE>());
+    else if (kind == K_SPARSE) f(std::integral_constant<int, K_SPARSE>());
+    else f(std::integral_constant<int, K_HUBO>());
+}
+
+// Ring layout shared by the SA and ring launches.
+struct Layout {
+    std::vector<RingDev> rings;
+    long long spin_words = 0, field_floats = 0;
+    int nw_max = 1;
+};
+
+void build_rings(Layout &L, const qa_problem *const *probs, int np, int reads, int K, int P, uint64_t seed) {
+    L.rings.clear();
+    L.spin_words = L.field_floats = 0;
+    L.nw_max = 1;
+    for (int p = 0; p < np; ++p) L.nw_max = std::max(L.nw_max, probs[p]->nw);
+    for (int p = 0; p < np; ++p)
+        for (int r = 0; r < reads; ++r)
+            for (int k = 0; k < K; ++k) {
+                RingDev R{};
+                R.prob = p;
+                R.out = p * reads + r;
+                R.k = k;
+                R.sched = 0;
+                R.key = seed + (uint64_t)r;
+                R.spin_off = L.spin_words;
+                R.field_off = L.field_floats;
+                L.spin_words += (long long)P * probs[p]->nw;
+                L.field_floats += (long long)P * probs[p]->n;
+                L.rings.push_back(R);
+            }
+}
+
+int upload_common(qa_ctx *ctx, const qa_problem *const *probs, int np, const Layout &L, ProbDev **d_probs,
+                  RingDev **d_rings, uint32_t **d_spins, float **d_fields) {
+    std::vector<ProbDev> pd(np);
+    for (int p = 0; p < np; ++p) pd[p] = probs[p]->dev;
+    void *v;
+    QA_TRY(ws_get(ctx, W_PROBS, sizeof(ProbDev) * np, &v));
+    *d_probs = static_cast<ProbDev *>(v);
+    QA_CK(cudaMemcpyAsync(*d_probs, pd.data(), sizeof(ProbDev) * np, cudaMemcpyHostToDevice, ctx->stream));
+    QA_TRY(ws_get(ctx, W_RINGS, sizeof(RingDev) * L.rings.size(), &v));
+    *d_rings = static_cast<RingDev *>(v);
+    QA_CK(cudaMemcpyAsync(*d_rings, L.rings.data(), sizeof(RingDev) * L.rings.size(), cudaMemcpyHostToDevice,
+                          ctx->stream));
+    QA_TRY(ws_get(ctx, W_SPINS, sizeof(uint32_t) * L.spin_words, &v));
+    *d_spins = static_cast<uint32_t *>(v);
+    QA_TRY(ws_get(ctx, W_FIELDS, sizeof(float) * L.field_floats, &v));
+    *d_fields = static_cast<float *>(v);
+    return QA_OK;
+}
+
+int init_state(qa_ctx *ctx, int kind, const ProbDev *d_probs, const RingDev *d_rings, int n_rings, uint32_t *d_spins,
+               float *d_fields, int P, int n_max, int nw_max, uint32_t tag) {
+    init_spins_kernel<<<dim3(n_rings, P), 128, 0, ctx->stream>>>(d_probs, d_rings, d_spins, P, tag, nw_max);
+    QA_CK(cudaGetLastError());
+    const int zb = std::max(1, std::min(64, (n_max + 127) / 128));
+    int rc = QA_OK;
+    dispatch_kind(kind, [&](auto K) {
+        init_fields_kernel<decltype(K)::value><<<dim3(n_rings, P, zb), 128, nw_max * 4, ctx->stream>>>(
+            d_probs, d_rings, d_spins, d_fields, P);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(QA_ERR_CUDA, "init_fields_kernel launch failed");
+    });
+    return rc;
+}
+
+int exact_energies(qa_ctx *ctx, int kind, const ProbDev *d_probs, const Layout &L, const uint32_t *d_bits,
+                   double *d_exact) {
+    std::vector<int> prob_of(L.rings.size());
+    for (size_t i = 0; i < L.rings.size(); ++i) prob_of[i] = L.rings[i].prob;
+    void *v;
+    QA_TRY(ws_get(ctx, W_PROBOF, sizeof(int) * prob_of.size(), &v));
+    int *d_pof = static_cast<int *>(v);
+    QA_CK(cudaMemcpyAsync(d_pof, prob_of.data(), sizeof(int) * prob_of.size(), cudaMemcpyHostToDevice, ctx->stream));
+    int rc = QA_OK;
+    dispatch_kind(kind, [&](auto K) {
+        exact_energy_kernel<decltype(K)::value><<<(unsigned)L.rings.size(), 32, L.nw_max * 4, ctx->stream>>>(
+            d_probs, d_pof, d_bits, L.nw_max, d_exact, (int)L.rings.size());
+        if (cudaGetLastError() != cudaSuccess) rc = fail(QA_ERR_CUDA, "exact_energy_kernel launch failed");
+    });
+    return rc;
+}
+
+}  // namespace
+
+// ====================================================================== API
+extern "C" {
+
+const char *qa_version(void) { return "qlatanneal-b200 0.1.0 (qanneal 2.0 sweep engine, sm_100a)"; }
+
+int qa_last_error(char *buf, size_t len) {
+    if (!buf || len == 0) return QA_ERR_ARG;
+    std::snprintf(buf, len, "%s", g_err.c_str());
+    return QA_OK;
+}
+
+int qa_device_count(int *count) {
+    if (!count) return fail(QA_ERR_ARG, "null count");
+    QA_CK(cudaGetDeviceCount(count));
+    return QA_OK;
+}
+
+int qa_create(qa_ctx **out, int device) {
+    if (!out) return fail(QA_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    int cnt = 0;
+    QA_CK(cudaGetDeviceCount(&cnt));
+    if (device < 0 || device >= cnt) return fail(QA_ERR_ARG, "device index out of range");
+    QA_CK(cudaSetDevice(device));
+    qa_ctx *ctx = new qa_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) {
+        qa_destroy(ctx);
+        return fail(QA_ERR_CUDA, std::string("context setup: ") + cudaGetErrorString(e));
+    }
+    *out = ctx;
+    return QA_OK;
+}
+
+int qa_destroy(qa_ctx *ctx) {
+    if (!ctx) return QA_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto &b : ctx->ws)
+        if (b.p) cudaFree(b.p);
+    for (auto &e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return QA_OK;
+}
+
+int qa_problem_free(qa_problem *p) {
+    if (!p) return QA_OK;
+    if (p->ctx) cudaSetDevice(p->ctx->device);
+    for (void *d : p->allocs) cudaFree(d);
+    delete p;
+    return QA_OK;
+}
+
+int qa_problem_size(const qa_problem *p, int *n) {
+    if (!p || !n) return fail(QA_ERR_ARG, "null argument");
+    *n = p->n;
+    return QA_OK;
+}
+
+int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, double c, qa_problem **out) {
+    QA_TRY(begin(ctx));
+    if (!out) return fail(QA_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    if (n <= 0) return fail(QA_ERR_ARG, "DenseIsing size must be > 0.");
+    if (!h || !J) return fail(QA_ERR_ARG, "DenseIsing h/J must not be null.");
+    qa_problem *P = new qa_problem();
+    P->ctx = ctx;
+    P->kind = K_DENSE;
+    P->n = n;
+    P->nw = (n + 31) / 32;
+    P->c = c;
+    std::vector<float> J32((size_t)n * n, 0.0f);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            if (i == j) continue;
+            const int a = std::min(i, j), b = std::max(i, j);
+            J32[(size_t)i * n + j] = (float)J[(size_t)a * n + b];
+        }
+    int rc = common_h(P, h);
+    if (rc == QA_OK) rc = upload(P, J32.data(), J32.size(), &P->dev.J32);
+    if (rc == QA_OK) rc = upload(P, J, (size_t)n * n, &P->dev.J64);
+    if (rc != QA_OK) {
+        qa_problem_free(P);
+        return rc;
+    }
+    finish_problem(P);
+    *out = P;
+    return QA_OK;
+}
+
+int qa_problem_sparse(qa_ctx *ctx, int n, const double *h, int m, const int64_t *ei, const int64_t *ej,
+                      const double *w, double c, qa_problem **out) {
+    QA_TRY(begin(ctx));
+    if (!out) return fail(QA_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    if (n <= 0) return fail(QA_ERR_ARG, "SparseIsing size must be > 0.");
+    if (!h || m < 0 || (m > 0 && (!ei || !ej || !w))) return fail(QA_ERR_ARG, "SparseIsing arrays must not be null.");
+    for (int e = 0; e < m; ++e) {
+        if (ei[e] < 0 || ej[e] < 0 || ei[e] >= n || ej[e] >= n)
+            return fail(QA_ERR_ARG, "SparseIsing edge index out of range.");
+        if (ei[e] == ej[e]) return fail(QA_ERR_ARG, "SparseIsing self-edge not allowed.");
+    }
+    // adjacency in insertion order (sparse_ising.cpp:35-41); entries of one
+    // neighbour merged in float64 in that order; rows sorted by neighbour.
+    std::vector<std::vector<std::pair<int, double>>> adj(n);
+    for (int e = 0; e < m; ++e) {
+        adj[ei[e]].push_back({(int)ej[e], w[e]});
+        adj[ej[e]].push_back({(int)ei[e], w[e]});
+    }
+    std::vector<int> rowptr(n + 1, 0), col;
+    std::vector<float> val;
+    for (int i = 0; i < n; ++i) {
+        auto &a = adj[i];
+        std::stable_sort(a.begin(), a.end(), [](const auto &x, const auto &y) { return x.first < y.first; });
+        rowptr[i] = (int)col.size();
+        size_t k = 0;
+        while (k < a.size()) {
+            double acc = 0.0;
+            size_t kk = k;
+            while (kk < a.size() && a[kk].first == a[k].first) acc += a[kk++].second;
+            col.push_back(a[k].first);
+            val.push_back((float)acc);
+            k = kk;
+        }
+    }
+    rowptr[n] = (int)col.size();
+    std::vector<int> e_i(m), e_j(m);
+    for (int e = 0; e < m; ++e) { e_i[e] = (int)ei[e]; e_j[e] = (int)ej[e]; }
+    qa_problem *P = new qa_problem();
+    P->ctx = ctx;
+    P->kind = K_SPARSE;
+    P->n = n;
+    P->nw = (n + 31) / 32;
+    P->m = m;
+    P->c = c;
+    int rc = common_h(P, h);
+    if (rc == QA_OK) rc = upload(P, rowptr.data(), rowptr.size(), &P->dev.rowptr);
+    if (rc == QA_OK) rc = upload(P, col.data(), col.size(), &P->dev.col);
+    if (rc == QA_OK) rc = upload(P, val.data(), val.size(), &P->dev.val32);
+    if (rc == QA_OK) rc = upload(P, e_i.data(), e_i.size(), &P->dev.ei);
+    if (rc == QA_OK) rc = upload(P, e_j.data(), e_j.size(), &P->dev.ej);
+    if (rc == QA_OK) rc = upload(P, w, (size_t)m, &P->dev.ew);
+    if (rc != QA_OK) {
+        qa_problem_free(P);
+        return rc;
+    }
+    finish_problem(P);
+    *out = P;
+    return QA_OK;
+}
+
+int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int64_t *term_ptr,
+                    const int32_t *term_vars, const double *coeff, double c, qa_problem **out) {
+    QA_TRY(begin(ctx));
+    if (!out) return fail(QA_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    if (n <= 0) return fail(QA_ERR_ARG, "HigherOrderIsing size must be > 0.");
+    if (!h || n_terms < 0 || (n_terms > 0 && (!term_ptr || !term_vars || !coeff)))
+        return fail(QA_ERR_ARG, "HigherOrderIsing arrays must not be null.");
+    std::vector<int> tptr(n_terms + 1, 0), tvars;
+    for (int t = 0; t < n_terms; ++t) {
+        const int64_t a = term_ptr[t], b = term_ptr[t + 1];
+        if (b - a < 2) return fail(QA_ERR_ARG, "HigherOrderIsing terms must have degree >= 2 (fold lower degrees).");
+        for (int64_t k = a; k < b; ++k) {
+            if (term_vars[k] < 0 || term_vars[k] >= n)
+                return fail(QA_ERR_ARG, "HigherOrderIsing term variable index out of range.");
+            if (k > a && term_vars[k] <= term_vars[k - 1])
+                return fail(QA_ERR_ARG, "HigherOrderIsing term variables must be strictly increasing.");
+            tvars.push_back(term_vars[k]);
+        }
+        tptr[t + 1] = (int)tvars.size();
+    }
+    std::vector<int> incptr(n + 1, 0);
+    for (int v : tvars) incptr[v + 1]++;
+    for (int i = 0; i < n; ++i) incptr[i + 1] += incptr[i];
+    std::vector<int> incterm(tvars.size()), fillc(n, 0);
+    for (int t = 0; t < n_terms; ++t)
+        for (int k = tptr[t]; k < tptr[t + 1]; ++k) incterm[incptr[tvars[k]] + fillc[tvars[k]]++] = t;
+    std::vector<float> c32(n_terms);
+    for (int t = 0; t < n_terms; ++t) c32[t] = (float)coeff[t];
+    qa_problem *P = new qa_problem();
+    P->ctx = ctx;
+    P->kind = K_HUBO;
+    P->n = n;
+    P->nw = (n + 31) / 32;
+    P->T = n_terms;
+    P->c = c;
+    int rc = common_h(P, h);
+    if (rc == QA_OK) rc = upload(P, tptr.data(), tptr.size(), &P->dev.tptr);
+    if (rc == QA_OK) rc = upload(P, tvars.data(), tvars.size(), &P->dev.tvars);
+    if (rc == QA_OK) rc = upload(P, incptr.data(), incptr.size(), &P->dev.incptr);
+    if (rc == QA_OK) rc = upload(P, incterm.data(), incterm.size(), &P->dev.incterm);
+    if (rc == QA_OK) rc = upload(P, c32.data(), c32.size(), &P->dev.coef32);
+    if (rc == QA_OK) rc = upload(P, coeff, (size_t)n_terms, &P->dev.coef64);
+    if (rc != QA_OK) {
+        qa_problem_free(P);
+        return rc;
+    }
+    finish_problem(P);
+    *out = P;
+    return QA_OK;
+}
+
+// ---------------------------------------------------------------------- SA
+int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *prm,
+              qa_run_out *outs, qa_stats *stats) {
+    QA_TRY(begin(ctx));
+    if (!prm) return fail(QA_ERR_ARG, "null params");
+    if (prm->steps <= 0 || !prm->betas) return fail(QA_ERR_ARG, "Schedule must contain at least one beta.");
+    if (prm->sweeps_per_beta <= 0) return fail(QA_ERR_ARG, "sweeps_per_beta must be > 0.");
+    if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
+    for (int s = 0; s < prm->steps; ++s)
+        if (!(prm->betas[s] >= 0.0)) return fail(QA_ERR_ARG, "betas must be >= 0.");
+    int kind, n_max;
+    QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
+    Layout L;
+    build_rings(L, problems, n_problems, prm->reads, 1, 1, prm->seed);
+    const int nr = (int)L.rings.size();
+    ProbDev *d_probs;
+    RingDev *d_rings;
+    uint32_t *d_spins;
+    float *d_fields;
+    QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
+    std::vector<float> A(prm->steps);
+    for (int s = 0; s < prm->steps; ++s) A[s] = (float)(1.0 / (2.0 * prm->betas[s]));
+    void *v;
+    QA_TRY(ws_get(ctx, W_A, sizeof(float) * A.size(), &v));
+    float *d_A = static_cast<float *>(v);
+    QA_CK(cudaMemcpyAsync(d_A, A.data(), sizeof(float) * A.size(), cudaMemcpyHostToDevice, ctx->stream));
+    QA_TRY(ws_get(ctx, W_SUM, sizeof(double) * (size_t)nr * prm->steps, &v));
+    double *d_trace = static_cast<double *>(v);
+    QA_TRY(ws_get(ctx, W_BESTE, sizeof(double) * nr, &v));
+    double *d_best = static_cast<double *>(v);
+    QA_TRY(ws_get(ctx, W_BITS, sizeof(uint32_t) * (size_t)nr * L.nw_max, &v));
+    uint32_t *d_bits = static_cast<uint32_t *>(v);
+    QA_TRY(ws_get(ctx, W_CNT, sizeof(unsigned long long) * 4, &v));
+    unsigned long long *d_cnt = static_cast<unsigned long long *>(v);
+    QA_TRY(ws_get(ctx, W_EXACT, sizeof(double) * nr, &v));
+    double *d_exact = static_cast<double *>(v);
+    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+
+    QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, 1, n_max, L.nw_max, DOM_INIT));
+    const int nwp = (L.nw_max + 3) & ~3, np4 = (n_max + 3) & ~3;
+    size_t smem = (size_t)nwp * 4 + (size_t)np4 * 4;
+    int smem_fields = (smem + (size_t)n_max * 4) <= (size_t)std::min(ctx->smem_optin, 160 * 1024) ? 1 : 0;
+    if (smem_fields) smem += (size_t)n_max * 4;
+    SAParams sp{};
+    sp.probs = d_probs; sp.rings = d_rings; sp.spins = d_spins; sp.fields = d_fields; sp.A = d_A;
+    sp.steps = prm->steps; sp.spb = prm->sweeps_per_beta; sp.smem_fields = smem_fields;
+    sp.trace = d_trace; sp.best_E = d_best; sp.best_bits = d_bits; sp.nw_max = L.nw_max; sp.counters = d_cnt;
+    QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    int rc = QA_OK;
+    dispatch_kind(kind, [&](auto K) {
+        auto kern = sa_kernel<decltype(K)::value>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<nr, 32, smem, ctx->stream>>>(sp);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, std::string("sa_kernel launch: ") + cudaGetErrorString(e));
+    });
+    QA_TRY(rc);
+    QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
+    QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+
+    std::vector<double> trace((size_t)nr * prm->steps), exact(nr);
+    std::vector<uint32_t> bits((size_t)nr * L.nw_max);
+    unsigned long long cnt[4];
+    QA_CK(cudaMemcpyAsync(trace.data(), d_trace, sizeof(double) * trace.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < nr; ++i) {
+        const RingDev &R = L.rings[i];
+        const int p = R.prob, r = R.out - p * prm->reads, n = problems[p]->n;
+        qa_run_out &o = outs[p];
+        if (o.best_spins) unpack_bits(bits.data() + (size_t)i * L.nw_max, n, o.best_spins + (size_t)r * n);
+        if (o.best_energy) o.best_energy[r] = exact[i];
+        if (o.energy_trace)
+            std::memcpy(o.energy_trace + (size_t)r * prm->steps, trace.data() + (size_t)i * prm->steps,
+                        sizeof(double) * prm->steps);
+    }
+    if (stats) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]);
+        stats->slice_attempts = (int64_t)cnt[0];
+        stats->slice_accepts = (int64_t)cnt[1];
+        stats->worldline_attempts = stats->worldline_accepts = 0;
+        stats->sweep_ms = a;
+        stats->total_ms = b;
+    }
+    return QA_OK;
+}
+
+// ---------------------------------------------------------------------- SQA
+int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *prm,
+               qa_run_out *outs, qa_stats *stats) {
+    QA_TRY(begin(ctx));
+    if (!prm) return fail(QA_ERR_ARG, "null params");
+    if (prm->steps <= 0 || !prm->betas || !prm->gammas) return fail(QA_ERR_ARG, "SQA schedule must contain betas.");
+    if (prm->trotter_slices <= 0) return fail(QA_ERR_ARG, "trotter_slices must be > 0.");
+    if (prm->replicas <= 0) return fail(QA_ERR_ARG, "replicas must be > 0.");
+    if (prm->sweeps_per_beta < 0 || prm->worldline_sweeps < 0 || prm->cluster_sweeps < 0)
+        return fail(QA_ERR_ARG, "sweep counts must be >= 0.");
+    if (prm->sweeps_per_beta == 0 && prm->worldline_sweeps == 0 && prm->cluster_sweeps == 0)
+        return fail(QA_ERR_ARG,
+                    "At least one of sweeps_per_beta, worldline_sweeps, or cluster_sweeps must be > 0.");
+    if (prm->cluster_sweeps > 0)
+        return fail(QA_ERR_UNSUPPORTED, "cluster_sweeps > 0 is not supported by the CUDA sweep engine.");
+    if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
+    int kind, n_max;
+    QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
+    const int P = (prm->continuous_time_slices > 0 && prm->continuous_time_slices > prm->trotter_slices)
+                      ? prm->continuous_time_slices
+                      : prm->trotter_slices;
+    const int K = prm->replicas, steps = prm->steps;
+    Layout L;
+    build_rings(L, problems, n_problems, prm->reads, K, P, prm->seed);
+    const int nr = (int)L.rings.size();
+    ProbDev *d_probs;
+    RingDev *d_rings;
+    uint32_t *d_spins;
+    float *d_fields;
+    QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
+    std::vector<float> A(steps), T4(steps);
+    for (int s = 0; s < steps; ++s) {
+        const double bs = prm->betas[s] / (double)P;
+        A[s] = (float)(1.0 / (2.0 * bs));
+        T4[s] = (float)(4.0 * trotter_coupling(prm->betas[s], prm->gammas[s], P));
+    }
+    void *v;
+    QA_TRY(ws_get(ctx, W_A, sizeof(float) * steps, &v));
+    float *d_A = static_cast<float *>(v);
+    QA_TRY(ws_get(ctx, W_T4, sizeof(float) * steps, &v));
+    float *d_T4 = static_cast<float *>(v);
+    QA_CK(cudaMemcpyAsync(d_A, A.data(), sizeof(float) * steps, cudaMemcpyHostToDevice, ctx->stream));
+    QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * steps, cudaMemcpyHostToDevice, ctx->stream));
+    QA_TRY(ws_get(ctx, W_SUM, sizeof(double) * (size_t)nr * steps, &v));
+    double *d_sum = static_cast<double *>(v);
+    QA_TRY(ws_get(ctx, W_BESTE, sizeof(double) * nr, &v));
+    double *d_best = static_cast<double *>(v);
+    QA_TRY(ws_get(ctx, W_BESTSTEP, sizeof(int) * nr, &v));
+    int *d_bstep = static_cast<int *>(v);
+    QA_TRY(ws_get(ctx, W_BITS, sizeof(uint32_t) * (size_t)nr * L.nw_max, &v));
+    uint32_t *d_bits = static_cast<uint32_t *>(v);
+    QA_TRY(ws_get(ctx, W_CNT, sizeof(unsigned long long) * 4, &v));
+    unsigned long long *d_cnt = static_cast<unsigned long long *>(v);
+    QA_TRY(ws_get(ctx, W_EXACT, sizeof(double) * nr, &v));
+    double *d_exact = static_cast<double *>(v);
+    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+    {
+        std::vector<double> inf(nr, INFINITY);
+        std::vector<int> neg(nr, -1);
+        QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_bstep, neg.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaStreamSynchronize(ctx->stream));
+    }
+
+    QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT));
+    const int W = std::max(1, std::min(32, (P + 1) / 2));
+    size_t smem = ring_smem_bytes(P, n_max, W, true);
+    int smem_fields = 1;
+    const size_t cap = (size_t)std::min(ctx->smem_optin, 200 * 1024);
+    if (smem > cap) {
+        smem_fields = 0;
+        smem = ring_smem_bytes(P, n_max, W, false);
+    }
+    if (smem > (size_t)ctx->smem_optin) return fail(QA_ERR_ARG, "ring state does not fit in shared memory.");
+    RingParams rp{};
+    rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
+    rp.P = P; rp.W = W; rp.steps_total = steps; rp.spb = prm->sweeps_per_beta; rp.wls = prm->worldline_sweeps;
+    rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.A = d_A; rp.T4 = d_T4; rp.per_slot_sched = 0;
+    rp.smem_fields = smem_fields; rp.ring_sum = d_sum; rp.ring_min = nullptr; rp.ring_bond = nullptr;
+    rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max; rp.mag = nullptr;
+    rp.counters = d_cnt;
+    QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    int rc = QA_OK;
+    dispatch_kind(kind, [&](auto Kd) {
+        auto kern = ring_kernel<decltype(Kd)::value>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const int seg = 256;
+        for (int s0 = 0; s0 < steps && rc == QA_OK; s0 += seg) {
+            rp.step0 = s0;
+            rp.step1 = std::min(steps, s0 + seg);
+            kern<<<nr, 32 * W, smem, ctx->stream>>>(rp);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, std::string("ring_kernel launch: ") + cudaGetErrorString(e));
+        }
+    });
+    QA_TRY(rc);
+    QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
+    QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+
+    std::vector<double> sums((size_t)nr * steps), bestE(nr), exact(nr);
+    std::vector<int> bstep(nr);
+    std::vector<uint32_t> bits((size_t)nr * L.nw_max);
+    unsigned long long cnt[4];
+    QA_CK(cudaMemcpyAsync(sums.data(), d_sum, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bstep.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+
+    // per read: trace = (sum_k sum_t E) / (K*P); best ring = min energy, then
+    // earliest step, then lowest replica (the (step, replica, slice) scan
+    // order of sqa_annealer.cpp:455-469)
+    for (int p = 0; p < n_problems; ++p) {
+        const int n = problems[p]->n;
+        qa_run_out &o = outs[p];
+        for (int r = 0; r < prm->reads; ++r) {
+            const int base = (p * prm->reads + r) * K;
+            if (o.energy_trace)
+                for (int s = 0; s < steps; ++s) {
+                    double tot = 0.0;
+                    for (int k = 0; k < K; ++k) tot += sums[(size_t)(base + k) * steps + s];
+                    o.energy_trace[(size_t)r * steps + s] = tot / (double)(K * P);
+                }
+            int kb = 0;
+            for (int k = 1; k < K; ++k) {
+                const int a = base + k, b = base + kb;
+                if (bestE[a] < bestE[b] || (bestE[a] == bestE[b] && bstep[a] < bstep[b])) kb = k;
+            }
+            const int ib = base + kb;
+            if (o.best_spins) unpack_bits(bits.data() + (size_t)ib * L.nw_max, n, o.best_spins + (size_t)r * n);
+            if (o.best_energy) o.best_energy[r] = exact[ib];
+        }
+    }
+    if (stats) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]);
+        stats->slice_attempts = (int64_t)cnt[0];
+        stats->slice_accepts = (int64_t)cnt[1];
+        stats->worldline_attempts = (int64_t)cnt[2];
+        stats->worldline_accepts = (int64_t)cnt[3];
+        stats->sweep_ms = a;
+        stats->total_ms = b;
+    }
+    return QA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,255 @@
+// qa_device.cuh -- device primitives of the sweep engine: the counter RNG, the
+// deterministic float32 logarithm of the Metropolis threshold, warp helpers
+// and the three local-field models (dense, sparse CSR, higher-order).
+//
+// Numerical contract (shared with the CPU restatement used by the tests):
+//   * Philox4x32-10 (Salmon et al., SC'11), key = seed + read,
+//     counter = (spin slot, cell, sweep, domain tag).
+//   * Local fields g = J.s in float32 with h kept apart; couplings rounded to
+//     float32; initial fields accumulated in float64 then rounded.
+//   * Metropolis: accept iff x > thr, x = s*(h+g), thr = (trotter + ln u)*A,
+//     A = 1/(2*beta/P).  This is exactly qanneal's rule
+//     "dE <= 0 || u < exp(-dE)" (sqa_annealer.cpp:196-205) rearranged so that
+//     the transcendental is computed once per attempt, off the serial path.
+//   * Every float op that feeds a decision is an explicit round-to-nearest
+//     intrinsic, so no FMA contraction changes a bit.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace qa {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+enum Dom : uint32_t {
+    DOM_INIT = 1, DOM_SA = 2, DOM_SLICE = 3, DOM_WORLD = 4, DOM_SWAP = 5,
+    DOM_PILOT_INIT = 6, DOM_PILOT = 7, DOM_PROD_INIT = 8, DOM_PROD = 9
+};
+
+enum Kind : int { K_DENSE = 0, K_SPARSE = 1, K_HUBO = 2 };
+
+// ---------------------------------------------------------------- Philox
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint64_t key) {
+    uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    return U4{c0, c1, c2, c3};
+}
+
+__device__ __forceinline__ uint32_t pick(const U4 &r, int w) {
+    return w == 0 ? r.x : (w == 1 ? r.y : (w == 2 ? r.z : r.w));
+}
+
+// Counter slot of a spin: 4 consecutive 32-spin blocks share one Philox call,
+// lane-strided, so one call per lane serves four blocks.
+__device__ __forceinline__ uint32_t spin_slot(int i) { return (uint32_t)(((i >> 7) << 5) | (i & 31)); }
+
+__device__ __forceinline__ float u01(uint32_t x) { return __uint2float_rn(x >> 8) * (1.0f / 16777216.0f); }
+
+// Deterministic float32 ln(x), x in [0,1): exponent split, mantissa folded to
+// (sqrt(1/2), sqrt(2)], ln(1+f) = 2 atanh(f/(2+f)) by the odd power series of
+// atanh, ln 2 split into two parts (Cody & Waite).  Each step is one IEEE
+// round-to-nearest op, reproduced bit for bit by the CPU restatement.
+__device__ __forceinline__ float det_logf(float x) {
+    if (!(x > 0.0f)) return -__int_as_float(0x7f800000);
+    const uint32_t b = __float_as_uint(x);
+    int e = (int)((b >> 23) & 0xffu) - 127;
+    float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
+    if (m > 1.41421356f) { m = __fmul_rn(m, 0.5f); e += 1; }
+    const float f = __fsub_rn(m, 1.0f);
+    const float s = __fdiv_rn(f, __fadd_rn(2.0f, f));
+    const float z = __fmul_rn(s, s);
+    float p = __fmaf_rn(z, 0.18181818f, 0.22222222f);
+    p = __fmaf_rn(z, p, 0.28571429f);
+    p = __fmaf_rn(z, p, 0.40000001f);
+    p = __fmaf_rn(z, p, 0.66666669f);
+    p = __fmaf_rn(z, p, 2.0f);
+    const float r = __fmul_rn(s, p);
+    const float ef = __int2float_rn(e);
+    return __fmaf_rn(ef, 0.693145751953125f, __fmaf_rn(ef, 1.42860677e-06f, r));
+}
+
+__device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
+
+// float64 warp sum in the canonical order: lane-strided partials (already in
+// v), then an xor butterfly; every lane ends with the same value.
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) v = __dadd_rn(v, __shfl_xor_sync(FULL, v, off));
+    return v;
+}
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) v += __shfl_xor_sync(FULL, v, off);
+    return v;
+}
+
+// ---------------------------------------------------------------- models
+// Device view of one problem instance (all arrays in global memory, L2-resident).
+struct ProbDev {
+    int kind, n, nw, T, m;
+    double c;
+    const float *h32;
+    const double *h64;
+    // dense: J32 row-major n x n (symmetric, zero diagonal), J64 as given
+    const float *J32;
+    const double *J64;
+    // sparse: merged adjacency CSR + original edge list (float64 energy)
+    const int *rowptr, *col;
+    const float *val32;
+    const int *ei, *ej;
+    const double *ew;
+    // hubo: consolidated terms + incidence lists
+    const int *incptr, *incterm, *tptr, *tvars;
+    const float *coef32;
+    const double *coef64;
+};
+
+__device__ __forceinline__ int spin_of(const uint32_t *S, int i) { return ((S[i >> 5] >> (i & 31)) & 1u) ? 1 : -1; }
+
+// Field update after spin j (old value so) flipped in one slice whose spin bits
+// (already holding the new value) are S and whose fields are g.  Whole warp
+// calls it; ends with __syncwarp.  Update order per field is the flip order,
+// identical to the sequential restatement (dense_ising.cpp:88-106,
+// sparse_ising.cpp:90-102, higher_order_ising.cpp:167-189).
+template <int KIND>
+__device__ __forceinline__ void apply_flip(const ProbDev &P, float *g, const uint32_t *S, int j, int so, int lane) {
+    const float cf = so > 0 ? -2.0f : 2.0f;
+    if (KIND == K_DENSE) {
+        const float *row = P.J32 + (size_t)j * P.n;
+        for (int m = lane; m < P.n; m += 32)
+            if (m != j) g[m] = __fadd_rn(g[m], __fmul_rn(cf, __ldg(row + m)));
+    } else if (KIND == K_SPARSE) {
+        const int e0 = __ldg(P.rowptr + j), e1 = __ldg(P.rowptr + j + 1);
+        for (int e = e0 + lane; e < e1; e += 32) {
+            const int m = __ldg(P.col + e);
+            g[m] = __fadd_rn(g[m], __fmul_rn(cf, __ldg(P.val32 + e)));
+        }
+    } else {
+        const int q0 = __ldg(P.incptr + j), q1 = __ldg(P.incptr + j + 1);
+        for (int q = q0; q < q1; ++q) {
+            const int t = __ldg(P.incterm + q);
+            const int a = __ldg(P.tptr + t), d = __ldg(P.tptr + t + 1) - a;
+            // sign of the product of the term's (new) spins
+            int neg = 0;
+            for (int base = 0; base < d; base += 32) {
+                const int k = base + lane;
+                const bool in = k < d;
+                const int v = in ? __ldg(P.tvars + a + k) : 0;
+                neg ^= __popc(__ballot_sync(FULL, in && spin_of(S, v) < 0)) & 1;
+            }
+            const float two = __fmul_rn(2.0f, __ldg(P.coef32 + t));
+            for (int base = 0; base < d; base += 32) {
+                const int k = base + lane;
+                if (k < d) {
+                    const int v = __ldg(P.tvars + a + k);
+                    if (v != j) {
+                        const int sv = spin_of(S, v);
+                        const bool pos = (neg == 0) == (sv > 0);
+                        g[v] = __fadd_rn(g[v], pos ? two : -two);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+}
+
+// Local field of spin i (J.s part, no h), accumulated in float64 in the
+// model's natural order, then rounded: the field-cache initialisation.
+template <int KIND>
+__device__ __forceinline__ float field_init_one(const ProbDev &P, const uint32_t *S, int i) {
+    double acc = 0.0;
+    if (KIND == K_DENSE) {
+        // J32 is symmetric: read column i (coalesced across the lanes' rows)
+        for (int j = 0; j < P.n; ++j) {
+            const double w = (double)__ldg(P.J32 + (size_t)j * P.n + i);
+            acc = __dadd_rn(acc, spin_of(S, j) > 0 ? w : -w);
+        }
+    } else if (KIND == K_SPARSE) {
+        for (int e = __ldg(P.rowptr + i); e < __ldg(P.rowptr + i + 1); ++e) {
+            const double w = (double)__ldg(P.val32 + e);
+            acc = __dadd_rn(acc, spin_of(S, __ldg(P.col + e)) > 0 ? w : -w);
+        }
+    } else {
+        for (int q = __ldg(P.incptr + i); q < __ldg(P.incptr + i + 1); ++q) {
+            const int t = __ldg(P.incterm + q);
+            int sg = 1;
+            for (int k = __ldg(P.tptr + t); k < __ldg(P.tptr + t + 1); ++k) {
+                const int v = __ldg(P.tvars + k);
+                if (v != i) sg *= spin_of(S, v);
+            }
+            const double w = (double)__ldg(P.coef32 + t);
+            acc = __dadd_rn(acc, sg > 0 ? w : -w);
+        }
+    }
+    return __double2float_rn(acc);
+}
+
+// Tracking energy of one slice from its field cache (whole warp, all lanes
+// return the same value):
+//   quadratic: E = c + sum_i s_i (h_i + g_i/2)
+//   HUBO:      E = c + (sum_i s_i h_i + sum_t J_t prod_t s)
+// in float64, canonical warp order.
+template <int KIND>
+__device__ __forceinline__ double cell_energy(const ProbDev &P, const uint32_t *S, const float *g, const float *h32,
+                                              int lane) {
+    if (KIND != K_HUBO) {
+        double p = 0.0;
+        for (int i = lane; i < P.n; i += 32) {
+            const double v = __dadd_rn((double)h32[i], __dmul_rn(0.5, (double)g[i]));
+            p = __dadd_rn(p, spin_of(S, i) > 0 ? v : -v);
+        }
+        return __dadd_rn(P.c, warp_sum_d(p));
+    }
+    double ph = 0.0;
+    for (int i = lane; i < P.n; i += 32) ph = __dadd_rn(ph, spin_of(S, i) > 0 ? (double)h32[i] : -(double)h32[i]);
+    ph = warp_sum_d(ph);
+    double pj = 0.0;
+    for (int t = lane; t < P.T; t += 32) {
+        int sg = 1;
+        for (int k = __ldg(P.tptr + t); k < __ldg(P.tptr + t + 1); ++k) sg *= spin_of(S, __ldg(P.tvars + k));
+        const double w = (double)__ldg(P.coef32 + t);
+        pj = __dadd_rn(pj, sg > 0 ? w : -w);
+    }
+    pj = warp_sum_d(pj);
+    return __dadd_rn(P.c, __dadd_rn(ph, pj));
+}
+
+// Float64 energy from the ORIGINAL float64 coefficients (reported energies).
+template <int KIND>
+__device__ __forceinline__ double exact_energy(const ProbDev &P, const uint32_t *S, int lane) {
+    double p = 0.0;
+    for (int i = lane; i < P.n; i += 32) p = __dadd_rn(p, spin_of(S, i) > 0 ? P.h64[i] : -P.h64[i]);
+    if (KIND == K_DENSE) {
+        for (int i = lane; i < P.n; i += 32) {
+            const double *row = P.J64 + (size_t)i * P.n;
+            double r = 0.0;
+            for (int j = i + 1; j < P.n; ++j) r = __dadd_rn(r, spin_of(S, j) > 0 ? row[j] : -row[j]);
+            p = __dadd_rn(p, spin_of(S, i) > 0 ? r : -r);
+        }
+    } else if (KIND == K_SPARSE) {
+        for (int e = lane; e < P.m; e += 32) {
+            const double w = P.ew[e];
+            p = __dadd_rn(p, spin_of(S, P.ei[e]) * spin_of(S, P.ej[e]) > 0 ? w : -w);
+        }
+    } else {
+        for (int t = lane; t < P.T; t += 32) {
+            int sg = 1;
+            for (int k = P.tptr[t]; k < P.tptr[t + 1]; ++k) sg *= spin_of(S, P.tvars[k]);
+            p = __dadd_rn(p, sg > 0 ? P.coef64[t] : -P.coef64[t]);
+        }
+    }
+    return __dadd_rn(P.c, warp_sum_d(p));
+}
+
+}  // namespace qa

@@ -1,0 +1,454 @@
+// qa_kernels.cuh -- the field-cache sweep kernels (every model kind).
+//
+//  * init_spins_kernel / init_fields_kernel: fresh random worldlines and their
+//    local-field caches (the reference's SQAState::random + compute_local_fields,
+//    sqa_annealer.cpp:100,130-137).
+//  * sa_kernel: SA Metropolis, one warp per read (annealer.cpp:33-75), with the
+//    running energy and per-flip best tracking of the reference.
+//  * ring_kernel: one CTA per Trotter ring (a replica of a read, a PT rung or a
+//    chi pilot probe): parity-phase slice sweeps (warp per slice), CTA-wide
+//    worldline sweeps, step-end energy scan and best tracking
+//    (sqa_annealer.cpp:153-469, sqa_parallel_tempering.cpp:187-306,
+//    sqa_chi_annealer.cpp:81-140).
+//
+// Inside a slice, 32 consecutive spins form a block owned lane-by-lane.  Each
+// lane precomputes its Metropolis threshold (one Philox word and one log per
+// attempt, in parallel); the warp then resolves the block in spin order by
+// repeatedly balloting "x > thr" and taking the first accepting lane.  Spins
+// before it were rejected on current fields; after its flip the fields are
+// updated and the remaining lanes re-test.  This is the sequential Metropolis
+// sweep exactly, at a cost of (accepted flips + 1) ballots per block.
+#pragma once
+#include "qa_device.cuh"
+
+namespace qa {
+
+// One Trotter ring (or one SA chain when P == 1).
+struct RingDev {
+    int prob;            // problem index
+    int out;             // result slot (problem, read)
+    int k;               // replica index inside the read (slice-RNG cell base k*P)
+    int sched;           // offset into the per-step A/T4 tables
+    uint64_t key;        // Philox key = seed + read
+    long long spin_off;  // uint32 words, P * nw
+    long long field_off; // floats, P * n
+};
+
+struct RingParams {
+    const ProbDev *probs;
+    const RingDev *rings;
+    uint32_t *spins;
+    float *fields;
+    int P, W;             // slices per ring, warps per CTA
+    int step0, step1;     // steps run by this launch
+    int steps_total;
+    int spb, wls;         // slice / worldline sweeps per step
+    uint32_t slice_tag;   // DOM_SLICE, DOM_PROD or DOM_PILOT|(point<<8)
+    const int *slot;      // PT: rung slot of each ring (null: slot = k)
+    const float *A, *T4;  // [sched + step] (PT: [sched + slot])
+    int per_slot_sched;   // 1: index A/T4 by slot instead of step
+    int smem_fields;
+    // outputs
+    double *ring_sum;     // [ring][steps_total]  sum of slice energies
+    double *ring_min;     // [ring][steps_total]  min slice energy (PT projected energy), may be null
+    long long *ring_bond; // [ring][steps_total]  imaginary-time bond sum B, may be null
+    double *best_E;       // [ring]
+    int *best_step;       // [ring]
+    uint32_t *best_bits;  // [ring][nw_max]
+    int nw_max;
+    int *mag;             // [ring][sweeps] spin sums after each sweep (chi pilot), may be null
+    unsigned long long *counters;  // [4]
+};
+
+__device__ __forceinline__ int phase_count(int P, int ph) {
+    if (ph == 0) return (P & 1) ? (P - 1) / 2 : P / 2;
+    if (ph == 1) return P / 2;
+    return (P & 1) ? 1 : 0;
+}
+__device__ __forceinline__ int phase_slice(int P, int ph, int c) {
+    if (ph == 0) return 2 * c;
+    if (ph == 1) return 2 * c + 1;
+    return P - 1;
+}
+
+// ------------------------------------------------------------------ init
+__global__ void init_spins_kernel(const ProbDev *probs, const RingDev *rings, uint32_t *spins, int P,
+                                  uint32_t tag, int nw_max) {
+    const RingDev R = rings[blockIdx.x];
+    const ProbDev Pd = probs[R.prob];
+    const int t = blockIdx.y;
+    const int ring_cell_base = R.k * P;
+    for (int q = threadIdx.x; q < Pd.nw; q += blockDim.x) {
+        const U4 r = philox((uint32_t)(q >> 2), (uint32_t)(ring_cell_base + t), 0u, tag, R.key);
+        uint32_t w = pick(r, q & 3);
+        const int rem = Pd.n - 32 * q;
+        if (rem < 32) w &= (1u << rem) - 1u;
+        spins[R.spin_off + (long long)t * Pd.nw + q] = w;
+    }
+}
+
+template <int KIND>
+__global__ void init_fields_kernel(const ProbDev *probs, const RingDev *rings, const uint32_t *spins,
+                                   float *fields, int P) {
+    extern __shared__ uint32_t sS[];
+    const RingDev R = rings[blockIdx.x];
+    const ProbDev Pd = probs[R.prob];
+    const int t = blockIdx.y;
+    for (int q = threadIdx.x; q < Pd.nw; q += blockDim.x) sS[q] = spins[R.spin_off + (long long)t * Pd.nw + q];
+    __syncthreads();
+    float *g = fields + R.field_off + (long long)t * Pd.n;
+    for (int i = blockIdx.z * blockDim.x + threadIdx.x; i < Pd.n; i += gridDim.z * blockDim.x)
+        g[i] = field_init_one<KIND>(Pd, sS, i);
+}
+
+// ------------------------------------------------------------------ slice sweep
+// One warp sweeps slice t of a ring (sqa_annealer.cpp:180-209 with the parity
+// schedule of sqa_chi_annealer.cpp:90-122).
+template <int KIND>
+__device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int NP, int t, float *gt, const float *h,
+                                            float A, float T4, uint64_t key, uint32_t rng_cell, uint32_t sigma,
+                                            uint32_t tag, int lane, unsigned long long &att,
+                                            unsigned long long &acc) {
+    const int n = Pd.n, nw = Pd.nw;
+    uint32_t *St = S + t * nw;
+    const int prev = t == 0 ? NP - 1 : t - 1;
+    const int next = t + 1 == NP ? 0 : t + 1;
+    const uint32_t *Sp = S + prev * nw;
+    const uint32_t *Sn = S + next * nw;
+    U4 rnd = {0, 0, 0, 0};
+    for (int q = 0; q < nw; ++q) {
+        if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), rng_cell, sigma, tag, key);
+        const int i = (q << 5) | lane;
+        const bool valid = i < n;
+        const uint32_t sw = St[q], pw = Sp[q], nx = Sn[q];
+        const int si = ((sw >> lane) & 1u) ? 1 : -1;
+        const int nsum = (((pw >> lane) & 1u) ? 1 : -1) + (((nx >> lane) & 1u) ? 1 : -1);
+        const int qv = si * nsum;
+        const float tro = qv == 0 ? 0.0f : (qv > 0 ? T4 : -T4);
+        const float thr = valid ? __fmul_rn(__fadd_rn(tro, det_logf(u01(pick(rnd, q & 3)))), A) : f_inf();
+        const float hi = valid ? h[i] : 0.0f;
+        att += (unsigned long long)min(32, n - (q << 5));
+        uint32_t pending = FULL;
+        for (;;) {
+            const float gi = valid ? gt[i] : 0.0f;
+            const float loc = __fadd_rn(hi, gi);
+            const float x = si > 0 ? loc : -loc;
+            const uint32_t m = __ballot_sync(FULL, x > thr) & pending;
+            if (!m) break;
+            const int j = __ffs(m) - 1;
+            const int so = ((sw >> j) & 1u) ? 1 : -1;
+            if (lane == 0) St[q] = St[q] ^ (1u << j);
+            __syncwarp();
+            apply_flip<KIND>(Pd, gt, St, (q << 5) | j, so, lane);
+            ++acc;
+            pending = j == 31 ? 0u : (FULL << (j + 1));
+        }
+    }
+}
+
+// ------------------------------------------------------------------ SA
+struct SAParams {
+    const ProbDev *probs;
+    const RingDev *rings;   // P == 1 chains
+    uint32_t *spins;
+    float *fields;
+    const float *A;         // [step]: 1/(2 beta)
+    int steps, spb;
+    int smem_fields;
+    double *trace;          // [ring][steps]
+    double *best_E;         // [ring]
+    uint32_t *best_bits;    // [ring][nw_max]
+    int nw_max;
+    unsigned long long *counters;
+};
+
+// annealer.cpp:50-67: spins in fixed order, running energy, best copied on
+// every new minimum.  One warp per read.
+template <int KIND>
+__global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const RingDev R = p.rings[blockIdx.x];
+    const ProbDev Pd = p.probs[R.prob];
+    const int lane = threadIdx.x, n = Pd.n, nw = Pd.nw;
+    uint32_t *S = reinterpret_cast<uint32_t *>(smem);
+    float *h = reinterpret_cast<float *>(S + ((nw + 3) & ~3));
+    float *g = p.smem_fields ? h + ((n + 3) & ~3) : p.fields + R.field_off;
+    for (int q = lane; q < nw; q += 32) S[q] = p.spins[R.spin_off + q];
+    for (int i = lane; i < n; i += 32) {
+        h[i] = Pd.h32[i];
+        if (p.smem_fields) g[i] = p.fields[R.field_off + i];
+    }
+    __syncwarp();
+    uint32_t *bb = p.best_bits + (long long)blockIdx.x * p.nw_max;
+    double E = cell_energy<KIND>(Pd, S, g, h, lane);
+    double best = E;
+    for (int q = lane; q < nw; q += 32) bb[q] = S[q];
+    unsigned long long att = 0, acc = 0;
+    for (int step = 0; step < p.steps; ++step) {
+        const float A = p.A[step];
+        for (int sw = 0; sw < p.spb; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * p.spb + sw);
+            U4 rnd = {0, 0, 0, 0};
+            for (int q = 0; q < nw; ++q) {
+                if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), 0u, sigma, DOM_SA, R.key);
+                const int i = (q << 5) | lane;
+                const bool valid = i < n;
+                const uint32_t sword = S[q];
+                const int si = ((sword >> lane) & 1u) ? 1 : -1;
+                const float thr = valid ? __fmul_rn(det_logf(u01(pick(rnd, q & 3))), A) : f_inf();
+                const float hi = valid ? h[i] : 0.0f;
+                att += (unsigned long long)min(32, n - (q << 5));
+                uint32_t pending = FULL;
+                for (;;) {
+                    const float gi = valid ? g[i] : 0.0f;
+                    const float loc = __fadd_rn(hi, gi);
+                    const float x = si > 0 ? loc : -loc;
+                    const uint32_t m = __ballot_sync(FULL, x > thr) & pending;
+                    if (!m) break;
+                    const int j = __ffs(m) - 1;
+                    const double xd = si > 0 ? __dadd_rn((double)hi, (double)gi) : -__dadd_rn((double)hi, (double)gi);
+                    const double xj = __shfl_sync(FULL, xd, j);
+                    const int so = ((sword >> j) & 1u) ? 1 : -1;
+                    if (lane == 0) S[q] = S[q] ^ (1u << j);
+                    __syncwarp();
+                    apply_flip<KIND>(Pd, g, S, (q << 5) | j, so, lane);
+                    ++acc;
+                    E = __dadd_rn(E, __dmul_rn(-2.0, xj));
+                    if (E < best) {
+                        best = E;
+                        for (int w = lane; w < nw; w += 32) bb[w] = S[w];
+                    }
+                    pending = j == 31 ? 0u : (FULL << (j + 1));
+                }
+            }
+        }
+        if (lane == 0) p.trace[(long long)blockIdx.x * p.steps + step] = E;
+    }
+    for (int q = lane; q < nw; q += 32) p.spins[R.spin_off + q] = S[q];
+    if (p.smem_fields)
+        for (int i = lane; i < n; i += 32) p.fields[R.field_off + i] = g[i];
+    if (lane == 0) {
+        p.best_E[blockIdx.x] = best;
+        atomicAdd(p.counters + 0, att);
+        atomicAdd(p.counters + 1, acc);
+    }
+}
+
+// ------------------------------------------------------------------ rings
+// smem layout: S[P*nw] | h[n] | cellE[P] (double) | wl_sh[W*32] | wl_G[W*32] (double) | flags | fields?
+struct RingSmem {
+    uint32_t *S;
+    float *h;
+    double *cellE;
+    int *wl_sh;
+    double *wl_G;
+    int *flag;
+    float *g;
+};
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+__host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fields) {
+    const int nw = (n + 31) / 32;
+    size_t b = align_up((size_t)P * nw * 4, 16);
+    b += align_up((size_t)n * 4, 16);
+    b += align_up((size_t)P * 8, 16);
+    b += align_up((size_t)W * 32 * 4, 16);
+    b += align_up((size_t)W * 32 * 8, 16);
+    b += 16;
+    if (fields) b += (size_t)P * n * 4;
+    return b;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const RingDev R = p.rings[blockIdx.x];
+    const ProbDev Pd = p.probs[R.prob];
+    const int NP = p.P, W = p.W;
+    const int n = Pd.n, nw = Pd.nw;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    RingSmem sm;
+    unsigned char *ptr = smem;
+    sm.S = reinterpret_cast<uint32_t *>(ptr); ptr += align_up((size_t)NP * nw * 4, 16);
+    sm.h = reinterpret_cast<float *>(ptr); ptr += align_up((size_t)n * 4, 16);
+    sm.cellE = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)NP * 8, 16);
+    sm.wl_sh = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)W * 32 * 4, 16);
+    sm.wl_G = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)W * 32 * 8, 16);
+    sm.flag = reinterpret_cast<int *>(ptr); ptr += 16;
+    float *gbase = p.smem_fields ? reinterpret_cast<float *>(ptr) : p.fields + R.field_off;
+
+    for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) sm.S[idx] = p.spins[R.spin_off + idx];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sm.h[i] = Pd.h32[i];
+    if (p.smem_fields)
+        for (long long idx = threadIdx.x; idx < (long long)NP * n; idx += blockDim.x) gbase[idx] = p.fields[R.field_off + idx];
+    __syncthreads();
+
+    const int slot = p.slot ? p.slot[blockIdx.x] : R.k;
+    unsigned long long att_s = 0, acc_s = 0, att_w = 0, acc_w = 0;
+    double bestE = p.best_E[blockIdx.x];
+    int bestStep = p.best_step[blockIdx.x];
+
+    for (int step = p.step0; step < p.step1; ++step) {
+        const int si_tab = R.sched + (p.per_slot_sched ? slot : step);
+        const float A = p.A[si_tab], T4 = p.T4[si_tab];
+        for (int sw = 0; sw < p.spb; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * p.spb + sw);
+            for (int ph = 0; ph < 3; ++ph) {
+                const int cnt = phase_count(NP, ph);
+                for (int c = warp; c < cnt; c += W) {
+                    const int t = phase_slice(NP, ph, c);
+                    sweep_slice<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, A, T4, R.key,
+                                      (uint32_t)(slot * NP + t), sigma, p.slice_tag, lane, att_s, acc_s);
+                }
+                if (cnt) __syncthreads();
+            }
+            if (p.mag) {
+                long long ps = 0;
+                for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) ps += __popc(sm.S[idx]);
+                ps = warp_sum_ll(ps);
+                if (lane == 0) sm.wl_sh[warp] = (int)ps;
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    long long tot = 0;
+                    for (int w = 0; w < W; ++w) tot += sm.wl_sh[w];
+                    p.mag[(long long)blockIdx.x * (p.steps_total * p.spb) + sigma] = (int)(2 * tot - (long long)NP * n);
+                }
+                __syncthreads();
+            }
+        }
+        for (int sw = 0; sw < p.wls; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * p.wls + sw);
+            U4 rnd = {0, 0, 0, 0};
+            for (int q = 0; q < nw; ++q) {
+                if ((q & 3) == 0)
+                    rnd = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
+                const int i = (q << 5) | lane;
+                const bool valid = i < n;
+                const float thr = valid ? __fmul_rn(det_logf(u01(pick(rnd, q & 3))), A) : f_inf();
+                const float hi = valid ? sm.h[i] : 0.0f;
+                if (threadIdx.x == 0) att_w += (unsigned long long)min(32, n - (q << 5));
+                uint32_t pending = FULL;
+                for (;;) {
+                    int sh = 0;
+                    double G = 0.0;
+                    if (valid)
+                        for (int t = warp; t < NP; t += W) {
+                            const int st = spin_of(sm.S + t * nw, i);
+                            const double gv = (double)gbase[(long long)t * n + i];
+                            sh += st;
+                            G = __dadd_rn(G, st > 0 ? gv : -gv);
+                        }
+                    sm.wl_sh[warp * 32 + lane] = sh;
+                    sm.wl_G[warp * 32 + lane] = G;
+                    __syncthreads();
+                    int Sh = 0;
+                    double Gt = 0.0;
+                    for (int w = 0; w < W; ++w) {
+                        Sh += sm.wl_sh[w * 32 + lane];
+                        Gt = __dadd_rn(Gt, sm.wl_G[w * 32 + lane]);
+                    }
+                    __syncthreads();
+                    const float x = valid ? __double2float_rn(__dadd_rn(__dmul_rn((double)hi, (double)Sh), Gt)) : 0.0f;
+                    const uint32_t m = __ballot_sync(FULL, x > thr) & pending;
+                    if (!m) break;
+                    const int j = __ffs(m) - 1;
+                    const int jj = (q << 5) | j;
+                    for (int t = warp; t < NP; t += W) {
+                        uint32_t *St = sm.S + t * nw;
+                        const int so = spin_of(St, jj);
+                        __syncwarp();
+                        if (lane == 0) St[q] = St[q] ^ (1u << j);
+                        __syncwarp();
+                        apply_flip<KIND>(Pd, gbase + (long long)t * n, St, jj, so, lane);
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) ++acc_w;
+                    pending = j == 31 ? 0u : (FULL << (j + 1));
+                }
+            }
+        }
+        // ---- step end: energy of every slice, ring sum, best (sqa_annealer.cpp:455-469)
+        for (int t = warp; t < NP; t += W) {
+            const double E = cell_energy<KIND>(Pd, sm.S + t * nw, gbase + (long long)t * n, sm.h, lane);
+            if (lane == 0) sm.cellE[t] = E;
+        }
+        if (p.ring_bond) {
+            long long b = 0;
+            for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) {
+                const int t = idx / nw, q = idx - t * nw;
+                const int tn = t + 1 == NP ? 0 : t + 1;
+                uint32_t x = ~(sm.S[idx] ^ sm.S[tn * nw + q]);
+                const int rem = n - 32 * q;
+                if (rem < 32) x &= (1u << rem) - 1u;
+                const int valid_bits = min(32, rem);
+                b += 2 * __popc(x) - valid_bits;
+            }
+            b = warp_sum_ll(b);
+            if (lane == 0) sm.wl_sh[warp] = (int)b;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sum = 0.0, emin = __longlong_as_double(0x7ff0000000000000LL);
+            int tmin = 0;
+            for (int t = 0; t < NP; ++t) {
+                const double E = sm.cellE[t];
+                sum = __dadd_rn(sum, E);
+                if (E < emin) { emin = E; tmin = t; }
+            }
+            const long long ro = (long long)blockIdx.x * p.steps_total + step;
+            if (p.ring_sum) p.ring_sum[ro] = sum;
+            if (p.ring_min) p.ring_min[ro] = emin;
+            if (p.ring_bond) {
+                long long tb = 0;
+                for (int w = 0; w < W; ++w) tb += sm.wl_sh[w];
+                p.ring_bond[ro] = tb;
+            }
+            sm.flag[0] = -1;
+            if (emin < bestE) {
+                bestE = emin;
+                bestStep = step;
+                sm.flag[0] = tmin;
+            }
+        }
+        __syncthreads();
+        const int tb = sm.flag[0];
+        if (tb >= 0) {
+            bestE = sm.cellE[tb];
+            bestStep = step;
+            for (int q = threadIdx.x; q < nw; q += blockDim.x)
+                p.best_bits[(long long)blockIdx.x * p.nw_max + q] = sm.S[tb * nw + q];
+        }
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) p.spins[R.spin_off + idx] = sm.S[idx];
+    if (p.smem_fields)
+        for (long long idx = threadIdx.x; idx < (long long)NP * n; idx += blockDim.x) p.fields[R.field_off + idx] = gbase[idx];
+    if (lane == 0) {
+        atomicAdd(p.counters + 0, att_s);
+        atomicAdd(p.counters + 1, acc_s);
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(p.counters + 2, att_w);
+        atomicAdd(p.counters + 3, acc_w);
+        p.best_E[blockIdx.x] = bestE;
+        p.best_step[blockIdx.x] = bestStep;
+    }
+}
+
+// ------------------------------------------------------------------ exact energies
+// Float64 energies of bit-packed states from the original coefficients.
+template <int KIND>
+__global__ void exact_energy_kernel(const ProbDev *probs, const int *prob_of, const uint32_t *bits, int nw_max,
+                                    double *out, int count) {
+    extern __shared__ uint32_t sS[];
+    const int idx = blockIdx.x;
+    if (idx >= count) return;
+    const ProbDev Pd = probs[prob_of[idx]];
+    for (int q = threadIdx.x; q < Pd.nw; q += 32) sS[q] = bits[(long long)idx * nw_max + q];
+    __syncwarp();
+    const double E = exact_energy<KIND>(Pd, sS, threadIdx.x);
+    if (threadIdx.x == 0) out[idx] = E;
+}
+
+}  // namespace qa

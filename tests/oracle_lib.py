@@ -1,0 +1,301 @@
+"""ctypes access to the checker libraries (test infrastructure only).
+
+* ``Oracle`` wraps oracle/_build/libqa_oracle.so, the C restatement of the
+  qanneal sweep engine under the replay model (oracle/qa_oracle.c).
+* ``Ref`` wraps oracle/_ref/libqanneal_ref.so, qanneal's own unmodified C++
+  sources compiled by oracle/Makefile with a thin C driver (oracle/ref_driver.cpp).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "libqa_oracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libqanneal_ref.so")
+
+_i8p = np.ctypeslib.ndpointer(np.int8, flags="C_CONTIGUOUS")
+_f8p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_f4p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+
+
+def build_oracle() -> None:
+    """Compile the checker libraries (the reference only where its tree exists)."""
+    subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile")], check=True)
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class OracleModel:
+    def __init__(self, lib, handle, kind, n):
+        self._lib, self.h, self.kind, self.n = lib, handle, kind, n
+
+    def __del__(self):
+        try:
+            self._lib.or_model_free(self.h)
+        except Exception:
+            pass
+
+
+class Oracle:
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build_oracle()
+        L = C.CDLL(path)
+        self.L = L
+        L.or_philox.argtypes = [_u32p, _u32p, _u32p]
+        L.or_logf.argtypes = [C.c_float]
+        L.or_logf.restype = C.c_float
+        L.or_model_dense.argtypes = [C.c_int, _f8p, _f8p, C.c_double]
+        L.or_model_dense.restype = C.c_void_p
+        L.or_model_sparse.argtypes = [C.c_int, _f8p, C.c_int, _i64p, _i64p, _f8p, C.c_double]
+        L.or_model_sparse.restype = C.c_void_p
+        L.or_model_hubo.argtypes = [C.c_int, C.c_int, _i64p, _i64p, _f8p, C.c_double]
+        L.or_model_hubo.restype = C.c_void_p
+        L.or_model_free.argtypes = [C.c_void_p]
+        L.or_model_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 3 + [C.POINTER(C.c_double)]
+        L.or_model_hubo_terms.argtypes = [C.c_void_p, _i32p, _i32p, _f8p, _f8p]
+        L.or_energy64.argtypes = [C.c_void_p, _i8p]
+        L.or_energy64.restype = C.c_double
+        L.or_energy_track.argtypes = [C.c_void_p, _i8p]
+        L.or_energy_track.restype = C.c_double
+        L.or_delta_energy64.argtypes = [C.c_void_p, _i8p, C.c_int]
+        L.or_delta_energy64.restype = C.c_double
+        L.or_fields_init.argtypes = [C.c_void_p, _i8p, _f4p]
+        L.or_init_spins.argtypes = [_i8p, C.c_int, C.c_uint64, C.c_uint32, C.c_uint32]
+        L.or_sa_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double),
+                                _f8p, _i64p]
+        L.or_sqa_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
+                                 C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i64p]
+        for name in ("or_sqapt_run", "or_chi_run"):
+            if hasattr(L, name):
+                pass
+
+    # ---- primitives
+    def philox(self, ctr, key):
+        out = np.zeros(4, np.uint32)
+        self.L.or_philox(np.asarray(ctr, np.uint32), np.asarray(key, np.uint32), out)
+        return out
+
+    def logf(self, x: float) -> float:
+        return float(self.L.or_logf(C.c_float(x)))
+
+    def init_spins(self, n, key, cell, tag=1):
+        s = np.zeros(n, np.int8)
+        self.L.or_init_spins(s, n, key, cell, tag)
+        return s
+
+    # ---- models
+    def dense(self, h, J, c=0.0) -> OracleModel:
+        h, J = _c64(h), _c64(J)
+        n = h.shape[0]
+        return OracleModel(self.L, self.L.or_model_dense(n, h, J.reshape(-1), c), "dense", n)
+
+    def sparse(self, n, h, edges, c=0.0) -> OracleModel:
+        e = list(edges)
+        ei = np.array([x[0] for x in e], np.int64)
+        ej = np.array([x[1] for x in e], np.int64)
+        w = np.array([x[2] for x in e], np.float64)
+        hdl = self.L.or_model_sparse(n, _c64(h), len(e), ei, ej, w, c)
+        if not hdl:
+            raise ValueError("invalid sparse model")
+        return OracleModel(self.L, hdl, "sparse", n)
+
+    def hubo(self, n, terms, c=0.0) -> OracleModel:
+        """terms: list of (vars, coeff) raw terms, as HigherOrderIsing takes them."""
+        ptr = [0]
+        flat = []
+        coef = []
+        for vars_, cf in terms:
+            flat.extend(int(v) for v in vars_)
+            ptr.append(len(flat))
+            coef.append(float(cf))
+        hdl = self.L.or_model_hubo(n, len(coef), np.array(ptr, np.int64), np.array(flat + [0], np.int64),
+                                   np.array(coef + [0.0], np.float64), c)
+        if not hdl:
+            raise ValueError("invalid hubo model")
+        return OracleModel(self.L, hdl, "hubo", n)
+
+    def hubo_terms(self, m: OracleModel):
+        n, k, T, c = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        self.L.or_model_info(m.h, C.byref(n), C.byref(k), C.byref(T), C.byref(c))
+        tptr = np.zeros(T.value + 1, np.int32)
+        h = np.zeros(n.value, np.float64)
+        coef = np.zeros(max(T.value, 1), np.float64)
+        # first fetch pointer array to size vars
+        tvars = np.zeros(1 << 20, np.int32)
+        self.L.or_model_hubo_terms(m.h, tptr, tvars, coef, h)
+        return tptr, tvars[: tptr[-1]].copy(), coef[: T.value].copy(), h, c.value
+
+    def energy64(self, m, s):
+        return float(self.L.or_energy64(m.h, np.ascontiguousarray(s, np.int8)))
+
+    def energy_track(self, m, s):
+        return float(self.L.or_energy_track(m.h, np.ascontiguousarray(s, np.int8)))
+
+    def delta_energy64(self, m, s, flip):
+        return float(self.L.or_delta_energy64(m.h, np.ascontiguousarray(s, np.int8), flip))
+
+    def fields(self, m, s):
+        g = np.zeros(m.n, np.float32)
+        self.L.or_fields_init(m.h, np.ascontiguousarray(s, np.int8), g)
+        return g
+
+    # ---- runs (one read each)
+    def sa_run(self, m, betas, sweeps_per_beta, seed, read=0):
+        betas = _c64(betas)
+        best = np.zeros(m.n, np.int8)
+        E = C.c_double()
+        trace = np.zeros(len(betas), np.float64)
+        cnt = np.zeros(4, np.int64)
+        self.L.or_sa_run(m.h, betas, len(betas), sweeps_per_beta, seed, read, best, C.byref(E), trace, cnt)
+        return best, E.value, trace, cnt
+
+    def sqa_run(self, m, betas, gammas, P, K, spb, wls, seed, read=0):
+        betas, gammas = _c64(betas), _c64(gammas)
+        best = np.zeros(m.n, np.int8)
+        E = C.c_double()
+        trace = np.zeros(len(betas), np.float64)
+        cnt = np.zeros(4, np.int64)
+        self.L.or_sqa_run(m.h, betas, gammas, len(betas), P, K, spb, wls, seed, read, best, C.byref(E), trace, cnt)
+        return best, E.value, trace, cnt
+
+
+class Ref:
+    """The unmodified qanneal classes (compiled from the reference sources)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = C.CDLL(path)
+        self.L = L
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_dense_new.argtypes = [C.c_int, _f8p, _f8p, C.c_double]
+        L.ref_dense_new.restype = C.c_void_p
+        L.ref_sparse_new.argtypes = [C.c_int, _f8p, C.c_int, _i64p, _i64p, _f8p, C.c_double]
+        L.ref_sparse_new.restype = C.c_void_p
+        L.ref_hubo_new.argtypes = [C.c_int, C.c_int, _i64p, _i64p, _f8p, C.c_double]
+        L.ref_hubo_new.restype = C.c_void_p
+        L.ref_model_free.argtypes = [C.c_void_p]
+        L.ref_qubo_to_ising.argtypes = [C.c_int, _f8p, _f8p, _f8p, C.POINTER(C.c_double)]
+        L.ref_hubo_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double), _f8p]
+        L.ref_energy.argtypes = [C.c_void_p, _i8p, C.c_int]
+        L.ref_energy.restype = C.c_double
+        L.ref_delta_energy.argtypes = [C.c_void_p, _i8p, C.c_int, C.c_int]
+        L.ref_delta_energy.restype = C.c_double
+        L.ref_fields.argtypes = [C.c_void_p, _i8p, C.c_int, _f8p]
+        L.ref_update_fields.argtypes = [C.c_void_p, _f8p, _i8p, C.c_int, C.c_int, C.c_int]
+        L.ref_sa_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p]
+        L.ref_sqa_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
+                                  _i8p, C.POINTER(C.c_double), _f8p]
+        L.ref_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p, _f8p, _f8p]
+        L.ref_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                   C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   C.c_uint64, _i8p, C.POINTER(C.c_double)] + [_f8p] * 8)
+        L.ref_batch_run.argtypes = [C.c_void_p, C.c_int, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_int, C.c_uint64, C.c_int, _f8p]
+
+    def _check(self, hdl):
+        if not hdl:
+            raise ValueError(self.L.ref_last_error().decode())
+        return hdl
+
+    def dense(self, h, J, c=0.0):
+        h, J = _c64(h), _c64(J)
+        return RefModel(self, self._check(self.L.ref_dense_new(h.shape[0], h, J.reshape(-1), c)), h.shape[0])
+
+    def sparse(self, n, h, edges, c=0.0):
+        e = list(edges)
+        ei = np.array([x[0] for x in e] or [0], np.int64)
+        ej = np.array([x[1] for x in e] or [0], np.int64)
+        w = np.array([x[2] for x in e] or [0.0], np.float64)
+        return RefModel(self, self._check(self.L.ref_sparse_new(n, _c64(h), len(e), ei, ej, w, c)), n)
+
+    def hubo(self, n, terms, c=0.0):
+        ptr, flat, coef = [0], [], []
+        for vars_, cf in terms:
+            flat.extend(int(v) for v in vars_)
+            ptr.append(len(flat))
+            coef.append(float(cf))
+        hdl = self.L.ref_hubo_new(n, len(coef), np.array(ptr, np.int64), np.array(flat + [0], np.int64),
+                                  np.array(coef + [0.0], np.float64), c)
+        return RefModel(self, self._check(hdl), n)
+
+    def qubo_to_ising(self, Q):
+        Q = _c64(Q)
+        n = Q.shape[0]
+        h = np.zeros(n)
+        J = np.zeros(n * n)
+        c = C.c_double()
+        if self.L.ref_qubo_to_ising(n, Q.reshape(-1), h, J, C.byref(c)) != 0:
+            raise ValueError(self.L.ref_last_error().decode())
+        return h, J.reshape(n, n), c.value
+
+
+class RefModel:
+    def __init__(self, ref: Ref, hdl, n):
+        self.ref, self.h, self.n = ref, hdl, n
+
+    def __del__(self):
+        try:
+            self.ref.L.ref_model_free(self.h)
+        except Exception:
+            pass
+
+    def energy(self, s):
+        return float(self.ref.L.ref_energy(self.h, np.ascontiguousarray(s, np.int8), self.n))
+
+    def delta_energy(self, s, flip):
+        return float(self.ref.L.ref_delta_energy(self.h, np.ascontiguousarray(s, np.int8), self.n, flip))
+
+    def fields(self, s):
+        f = np.zeros(self.n)
+        self.ref.L.ref_fields(self.h, np.ascontiguousarray(s, np.int8), self.n, f)
+        return f
+
+    def update_fields(self, f, new_s, flip, old):
+        self.ref.L.ref_update_fields(self.h, f, np.ascontiguousarray(new_s, np.int8), self.n, flip, old)
+
+    def hubo_info(self):
+        T, D, c = C.c_int(), C.c_int(), C.c_double()
+        h = np.zeros(self.n)
+        if self.ref.L.ref_hubo_info(self.h, C.byref(T), C.byref(D), C.byref(c), h) != 0:
+            raise ValueError("not a HUBO model")
+        return T.value, D.value, c.value, h
+
+    def sa_run(self, betas, spb, seed):
+        betas = _c64(betas)
+        best = np.zeros(self.n, np.int8)
+        E = C.c_double()
+        tr = np.zeros(len(betas))
+        if self.ref.L.ref_sa_run(self.h, betas, len(betas), spb, seed, best, C.byref(E), tr) != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return best, E.value, tr
+
+    def sqa_run(self, betas, gammas, P, K, spb, wls, seed):
+        betas, gammas = _c64(betas), _c64(gammas)
+        best = np.zeros(self.n, np.int8)
+        E = C.c_double()
+        tr = np.zeros(len(betas))
+        if self.ref.L.ref_sqa_run(self.h, betas, gammas, len(betas), P, K, spb, wls, seed, best, C.byref(E), tr) != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return best, E.value, tr
+
+    def batch_run(self, method, betas, gammas, steps, P, K, spb, wls, reads, seed, threads):
+        out = np.zeros(reads)
+        g = _c64(gammas if gammas is not None else np.zeros(steps))
+        rc = self.ref.L.ref_batch_run(self.h, method, _c64(betas), g, steps, P, K, spb, wls, reads, seed, threads, out)
+        if rc != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return out

@@ -1,0 +1,155 @@
+"""Bit-exact parity of the CUDA SA / SQA engine against the CPU restatement.
+
+Every case calls the engine through the C ABI (libqa_gpu.so via the package's
+annealer classes) and the oracle (oracle/qa_oracle.c) on the same seeded
+instance and key.  With integer couplings every quantity is exact, so best
+spins, best energies and the whole energy trace must agree bit for bit.
+"""
+import numpy as np
+import pytest
+
+import qlatanneal_b200 as qa
+from instances import geometric_betas, hubo_random, regular3, sk_dense
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_model(oracle, model):
+    if isinstance(model, qa.DenseIsing):
+        return oracle.dense(model.fields(), model.couplings(), model.constant())
+    if isinstance(model, qa.SparseIsing):
+        e = [(x.i, x.j, x.value) for x in model.edges()]
+        return oracle.sparse(model.size(), model._h, e, model.constant())
+    terms = [(k, v) for k, v in model.terms()] + [((i,), hv) for i, hv in enumerate(model.h()) if hv != 0.0]
+    return oracle.hubo(model.size(), terms, model.constant())
+
+
+def make(kind, n, seed):
+    if kind == "dense":
+        h, J = sk_dense(n, seed)
+        return qa.DenseIsing(h, J)
+    if kind == "dense_h":
+        rng = np.random.default_rng(seed + 7)
+        h, J = sk_dense(n, seed)
+        h = rng.choice([-0.5, 0.0, 0.25, 0.5], size=n)
+        return qa.DenseIsing(h, J, 1.5)
+    if kind == "sparse":
+        h, e = regular3(n, seed)
+        return qa.SparseIsing(h, e, n, -2.0)
+    if kind == "hubo":
+        return qa.HigherOrderIsing(hubo_random(n, seed, integer=True), n)
+    raise ValueError(kind)
+
+
+SA_CASES = [("dense", 64), ("dense", 100), ("dense", 256), ("dense_h", 96), ("sparse", 128), ("sparse", 70),
+            ("hubo", 60)]
+
+
+@pytest.mark.parametrize("kind,n", SA_CASES)
+def test_sa_bit_exact(oracle, kind, n):
+    model = make(kind, n, 11)
+    om = oracle_model(oracle, model)
+    betas = geometric_betas(0.1, 5.0, 30)
+    reads, spb, seed = 6, 4, 12345
+    ann = qa.Annealer(model, qa.AnnealSchedule.from_betas(betas))
+    res = ann.run_reads(spb, reads=reads, seed=seed)
+    tot_acc = 0
+    for r in range(reads):
+        best, E, trace, cnt = oracle.sa_run(om, betas, spb, seed, r)
+        tot_acc += cnt[1]
+        np.testing.assert_array_equal(res[r].best_state.as_array(), best)
+        assert res[r].best_energy == E
+        np.testing.assert_array_equal(np.asarray(res[r].energy_trace), trace)
+        assert res[r].best_energy == pytest.approx(model.energy(res[r].best_state.spins), abs=1e-9)
+    st = ann.last_stats
+    assert st.slice_attempts == reads * len(betas) * spb * n
+    assert st.slice_accepts == tot_acc
+
+
+SQA_CASES = [
+    ("dense", 64, 8, 1, 1, 1),
+    ("dense", 96, 5, 2, 1, 1),
+    ("dense", 40, 1, 1, 2, 0),
+    ("dense", 40, 2, 3, 0, 2),
+    ("dense_h", 70, 6, 2, 2, 1),
+    ("sparse", 128, 8, 1, 1, 1),
+    ("sparse", 64, 7, 2, 2, 1),
+    ("hubo", 48, 4, 2, 1, 1),
+]
+
+
+@pytest.mark.parametrize("kind,n,P,K,spb,wls", SQA_CASES)
+def test_sqa_bit_exact(oracle, kind, n, P, K, spb, wls):
+    model = make(kind, n, 21)
+    om = oracle_model(oracle, model)
+    steps = 25
+    betas = np.full(steps, 2.0 * P / 4.0)
+    gammas = np.linspace(3.0, 0.05, steps)
+    reads, seed = 3, 777
+    ann = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors(betas, gammas), P, K)
+    res = ann.run_reads(spb, wls, reads=reads, seed=seed)
+    acc_s = acc_w = 0
+    for r in range(reads):
+        best, E, trace, cnt = oracle.sqa_run(om, betas, gammas, P, K, spb, wls, seed, r)
+        acc_s += cnt[1]
+        acc_w += cnt[3]
+        np.testing.assert_array_equal(res[r].best_state.as_array(), best)
+        assert res[r].best_energy == E
+        np.testing.assert_array_equal(np.asarray(res[r].energy_trace), trace)
+    st = ann.last_stats
+    assert st.slice_attempts == reads * K * P * steps * spb * n
+    assert st.worldline_attempts == reads * K * steps * wls * n
+    assert st.slice_accepts == acc_s and st.worldline_accepts == acc_w
+
+
+def test_single_run_matches_batch(oracle):
+    """run() after set_seed(s + r) reproduces read r of a batch seeded s (solve()'s seeding)."""
+    model = make("dense", 64, 3)
+    sched = qa.SQASchedule.from_vectors([2.0] * 10, np.linspace(2.0, 0.1, 10))
+    ann = qa.SQAAnnealer(model, sched, 4, 1)
+    batch = ann.run_reads(1, 1, reads=3, seed=99)
+    for r in range(3):
+        ann.set_seed(99 + r)
+        one = ann.run(1, 1)
+        np.testing.assert_array_equal(one.best_state.as_array(), batch[r].best_state.as_array())
+        assert one.best_energy == batch[r].best_energy
+
+
+def test_reference_sqa_basic():
+    """tests/test_sqa_basic.cpp: n=3, P=8, K=2, trace length and best energy consistency."""
+    h = np.zeros(3)
+    J = np.array([[0.0, 0.5, -0.3], [0.5, 0.0, 0.2], [-0.3, 0.2, 0.0]])
+    ham = qa.DenseIsing(h, J)
+    sched = qa.SQASchedule.from_vectors([0.2, 0.5, 1.0], [2.0, 1.0, 0.5])
+    ann = qa.SQAAnnealer(ham, sched, 8, 2)
+    ann.set_seed(42)
+    res = ann.run(5, 1)
+    assert len(res.energy_trace) == 3
+    assert abs(ham.energy(res.best_state.spins) - res.best_energy) < 1e-12
+
+
+def test_real_couplings_energy(oracle):
+    """Real-valued J: every returned energy equals the float64 energy of its state."""
+    from instances import dense_real
+    h, J = dense_real(80, 5)
+    model = qa.DenseIsing(h, J, 0.25)
+    om = oracle.dense(h, J, 0.25)
+    sa = qa.Annealer(model, qa.AnnealSchedule.from_betas(geometric_betas(0.1, 5.0, 20)))
+    for r in sa.run_reads(3, reads=8, seed=5):
+        E64 = oracle.energy64(om, r.best_state.as_array())
+        assert r.best_energy == pytest.approx(E64, rel=1e-12, abs=1e-12)
+    sq = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors([3.0] * 12, np.linspace(2.0, 0.1, 12)), 6, 2)
+    for r in sq.run_reads(1, 1, reads=4, seed=9):
+        E64 = oracle.energy64(om, r.best_state.as_array())
+        assert r.best_energy == pytest.approx(E64, rel=1e-12, abs=1e-12)
+
+
+def test_argument_errors():
+    h, J = sk_dense(16, 1)
+    m = qa.DenseIsing(h, J)
+    with pytest.raises(ValueError):
+        qa.Annealer(m, qa.AnnealSchedule.from_betas([1.0])).run(0)
+    with pytest.raises(ValueError):
+        qa.SQAAnnealer(m, qa.SQASchedule.from_vectors([1.0], [1.0]), 4).run(0, 0)
+    with pytest.raises(NotImplementedError):
+        qa.SQAAnnealer(m, qa.SQASchedule.from_vectors([1.0], [1.0]), 4).run(1, 1, cluster_sweeps=1)

@@ -1,0 +1,155 @@
+"""Pins the CPU restatement (the oracle) before any GPU result is trusted.
+
+* Philox4x32-10 against the published Random123 known-answer vectors.
+* The deterministic log against math.log.
+* Model functions against the reference's own golden tests
+  (tests/test_dense_ising.cpp, tests/test_higher_order_ising.cpp) and against
+  qanneal compiled from its sources (oracle/_ref).
+* SA / SQA restatements against the unmodified reference, statistically.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from instances import geometric_betas, hubo_random, regular3, sk_dense
+
+# Random123 kat_vectors, philox4x32 with 10 rounds: (counter, key, expected)
+PHILOX_KAT = [
+    ([0, 0, 0, 0], [0, 0], [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]),
+    ([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2, [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]),
+    ([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0],
+     [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]),
+]
+
+
+@pytest.mark.parametrize("ctr,key,want", PHILOX_KAT)
+def test_philox_known_answers(oracle, ctr, key, want):
+    assert oracle.philox(ctr, key).tolist() == want
+
+
+def test_det_log_accuracy(oracle):
+    rng = np.random.default_rng(0)
+    xs = (rng.integers(1, 1 << 24, 5000) / float(1 << 24)).astype(np.float32)
+    for x in xs:
+        got = oracle.logf(float(x))
+        assert abs(got - math.log(float(x))) <= 4e-7 * abs(math.log(float(x))) + 1e-7
+    assert oracle.logf(0.0) == -math.inf
+
+
+def test_dense_ising_golden(oracle, ref):
+    """tests/test_dense_ising.cpp: n=2, h=(1,-1), J01=0.5: E(+1,+1)=0.5, dE matches a flip."""
+    h = np.array([1.0, -1.0])
+    J = np.array([[0.0, 0.5], [0.5, 0.0]])
+    m = oracle.dense(h, J)
+    s = np.array([1, 1], np.int8)
+    assert oracle.energy64(m, s) == 0.5
+    assert ref.dense(h, J).energy(s) == 0.5
+    s2 = s.copy()
+    s2[0] = -1
+    assert abs((oracle.energy64(m, s2) - 0.5) - oracle.delta_energy64(m, s, 0)) < 1e-12
+
+
+def _brute(s, h, terms, c):
+    E = c + float(np.dot(h, s))
+    for vars_, cf in terms:
+        E += cf * float(np.prod(s[list(vars_)]))
+    return E
+
+
+def _random_hubo(n, rng):
+    """tests/test_higher_order_ising.cpp:64-85: degrees 1-4, repeated indices,
+    duplicated supports and a fully cancelling term."""
+    terms = []
+    for _ in range(40):
+        d = int(rng.integers(1, 5))
+        terms.append(([int(v) for v in rng.integers(0, n, d)], float(rng.uniform(-1.5, 1.5))))
+    terms += [([0, 1, 2], 0.7), ([2, 1, 0], -0.3), ([3, 3, 4, 4], 9.9)]
+    h = np.zeros(n)
+    return h, terms, float(rng.uniform(-1.5, 1.5))
+
+
+@pytest.mark.parametrize("n", [5, 8, 12, 20])
+def test_hubo_brute_force(oracle, ref, n):
+    rng = np.random.default_rng(0xC0FFEE + n)
+    for rep in range(3):
+        h, terms, c = _random_hubo(n, rng)
+        m = oracle.hubo(n, terms, c)
+        rm = ref.hubo(n, terms, c)
+        T, _, c_ref, h_ref = rm.hubo_info()
+        tptr, tvars, coef, h_or, c_or = oracle.hubo_terms(m)
+        assert len(coef) == T and c_or == c_ref
+        np.testing.assert_array_equal(h_or, h_ref)
+        for _ in range(30):
+            s = rng.choice([-1, 1], n).astype(np.int8)
+            E = oracle.energy64(m, s)
+            assert abs(E - _brute(s.astype(float), h, terms, c)) < 1e-9
+            assert E == rm.energy(s)
+            for f in range(n):
+                s2 = s.copy()
+                s2[f] = -s2[f]
+                de = oracle.delta_energy64(m, s, f)
+                assert abs(de - (_brute(s2.astype(float), h, terms, c) - E)) < 1e-9
+                assert de == rm.delta_energy(s, f)
+            # float32 field cache gives the float64 delta to float32 accuracy
+            g = oracle.fields(m, s)
+            np.testing.assert_allclose(g.astype(np.float64), rm.fields(s) - h_ref, rtol=1e-6, atol=1e-5)
+
+
+def test_dense_sparse_energies_match_reference(oracle, ref):
+    rng = np.random.default_rng(3)
+    h, J = sk_dense(50, 4, h_sigma=0.1)
+    m, rm = oracle.dense(h, J), ref.dense(h, J)
+    hs, edges = regular3(64, 5)
+    ms, rms = oracle.sparse(64, hs, edges + [(0, 1, 0.5), (1, 0, -0.25)], 0.75), \
+        ref.sparse(64, hs, edges + [(0, 1, 0.5), (1, 0, -0.25)], 0.75)
+    for _ in range(20):
+        s = rng.choice([-1, 1], 50).astype(np.int8)
+        assert oracle.energy64(m, s) == rm.energy(s)
+        assert oracle.delta_energy64(m, s, 7) == rm.delta_energy(s, 7)
+        s = rng.choice([-1, 1], 64).astype(np.int8)
+        assert oracle.energy64(ms, s) == rms.energy(s)
+        assert oracle.delta_energy64(ms, s, 0) == pytest.approx(rms.delta_energy(s, 0), abs=1e-12)
+
+
+def test_tracking_energy_exact_for_integer_models(oracle):
+    rng = np.random.default_rng(9)
+    h, J = sk_dense(96, 2)
+    h = rng.choice([-0.5, 0.0, 0.5], 96)
+    m = oracle.dense(h, J, 3.0)
+    hs, edges = regular3(80, 1)
+    ms = oracle.sparse(80, hs, edges, -1.0)
+    mh = oracle.hubo(40, list(hubo_random(40, 3, integer=True).items()), 0.5)
+    for mod, n in ((m, 96), (ms, 80), (mh, 40)):
+        for _ in range(10):
+            s = rng.choice([-1, 1], n).astype(np.int8)
+            assert oracle.energy_track(mod, s) == oracle.energy64(mod, s)
+
+
+def _ci95(x):
+    x = np.asarray(x, float)
+    return x.mean(), 1.96 * x.std(ddof=1) / math.sqrt(len(x))
+
+
+def test_sa_restatement_matches_reference_statistics(oracle, ref):
+    """The replay-model SA and qanneal's Annealer sample the same distribution
+    of best energies (means inside each other's 95% CIs, 400 reads each)."""
+    h, J = sk_dense(48, 5)
+    m, rm = oracle.dense(h, J), ref.dense(h, J)
+    betas = geometric_betas(0.1, 2.0, 12)
+    eo = [oracle.sa_run(m, betas, 2, 1000, k)[1] for k in range(400)]
+    er = [rm.sa_run(betas, 2, 5000 + k)[1] for k in range(400)]
+    (mo, co), (mr, cr) = _ci95(eo), _ci95(er)
+    assert abs(mo - mr) <= 1.5 * (co + cr), (mo, co, mr, cr)
+
+
+def test_sqa_restatement_matches_reference_statistics(oracle, ref):
+    h, J = sk_dense(32, 6)
+    m, rm = oracle.dense(h, J), ref.dense(h, J)
+    steps, P, K = 10, 8, 1
+    betas = np.full(steps, 1.5)
+    gammas = np.linspace(2.0, 0.2, steps)
+    eo = [oracle.sqa_run(m, betas, gammas, P, K, 1, 1, 1000, k)[2][-1] for k in range(300)]
+    er = [rm.sqa_run(betas, gammas, P, K, 1, 1, 9000 + k)[2][-1] for k in range(300)]
+    (mo, co), (mr, cr) = _ci95(eo), _ci95(er)
+    assert abs(mo - mr) <= 1.5 * (co + cr), (mo, co, mr, cr)
