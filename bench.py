@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 sweep engine on the dense SQA workload.
+
+Workload (one bench step = one full anneal, all reads in one batched call):
+  dense Sherrington-Kirkpatrick Ising, n=512, J_ij in {-1,+1} (seeded), h_i ~ N(0, 0.1^2)
+  stored float32; Trotterized SQA with P=32 slices, beta = 0.5*P, Gamma linear
+  3.0 -> 0.01 over 1000 steps, 1 slice sweep + 1 worldline sweep per step,
+  256 reads (1 replica each).  Synthetic, seeded data.
+
+Metric: site-attempts/s (a slice proposal counts 1 site, a worldline proposal P).
+  value : device time of the engine's own kernels (CUDA events on the launching
+          stream), problem already resident in HBM, L2 flushed between steps.
+  e2e   : the same metric through the public API from host arrays: problem
+          upload (H2D), the run, and the results back on the host (D2H), wall time.
+  roofline : the sweep kernel's algorithmic bytes (per-attempt field/spin reads
+          plus one coupling row per accepted flip, 1 byte per +/-1 coupling)
+          over its event-timed duration, against the measured HBM copy bandwidth.
+  cpu_baseline : qanneal's own SQAAnnealer (compiled from its sources under
+          oracle/_ref) on a bounded sample of the same workload, all host threads.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 launch one process per GPU with torch.distributed.run; every rank runs
+the full workload on its GPU (independent reads: weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WL = dict(n=512, P=32, reads=256, steps=1000, spb=1, wls=1, beta_over_P=0.5, gamma0=3.0, gamma1=0.01,
+          h_sigma=0.1, instance_seed=2026, run_seed=1)
+WORKLOAD_NAME = ("dense SQA, SK n=512 J=+-1, h~N(0,0.1^2) fp32, P=32, beta=0.5P, Gamma 3.0->0.01 linear over "
+                 "1000 steps, 1 slice + 1 worldline sweep per step, 256 reads")
+
+
+def schedule(steps=None):
+    steps = WL["steps"] if steps is None else steps
+    P = WL["P"]
+    betas = np.full(WL["steps"], WL["beta_over_P"] * P)[:steps]
+    gammas = np.linspace(WL["gamma0"], WL["gamma1"], WL["steps"])[:steps]
+    return betas, gammas
+
+
+def instance():
+    from qlatanneal_b200.instances import sk_dense
+    return sk_dense(WL["n"], WL["instance_seed"], h_sigma=WL["h_sigma"])
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """dram bytes per sweep-kernel launch from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "ring_kernel_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    vals = {}
+    for line in open(p):
+        if ":" in line and not line.startswith("#"):
+            k, v = line.split(":", 1)
+            vals[k.strip()] = v.strip()
+    try:
+        return float(vals["dram_bytes_per_launch"])
+    except (KeyError, ValueError):
+        return None
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.device), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        try:
+            for line in open(self.f.name):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def site_attempts(st, P):
+    return st.slice_attempts + st.worldline_attempts * P
+
+
+def algorithmic_bytes(st, n, P, b_J=1.0):
+    """Dense-model sweep traffic: every site attempt reads its 4-byte field and
+    3 spin bits; every accepted site reads one coupling row of n entries."""
+    n_att = st.slice_attempts + st.worldline_attempts * P
+    n_acc = st.slice_accepts + st.worldline_accepts * P
+    return n_acc * n * b_J + n_att * (4.0 + 3.0 / 8.0)
+
+
+def cpu_reference_sample(target_s=12.0, threads=None):
+    """qanneal's SQAAnnealer on a bounded sample of the workload, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import REF_SO, Ref
+    if not os.path.exists(REF_SO):
+        return None
+    threads = threads or os.cpu_count() or 1
+    h, J = instance()
+    rm = Ref().dense(h, J)
+    P = WL["P"]
+    # calibrate with one read of 20 steps
+    b, g = schedule(20)
+    t0 = time.perf_counter()
+    rm.batch_run(1, b, g, 20, P, 1, WL["spb"], WL["wls"], 1, 7, 1)
+    per_read_step = (time.perf_counter() - t0) / 20.0
+    reads = threads
+    steps = int(max(10, min(WL["steps"], target_s / max(per_read_step, 1e-6))))
+    b, g = schedule(steps)
+    t0 = time.perf_counter()
+    rm.batch_run(1, b, g, steps, P, 1, WL["spb"], WL["wls"], reads, 11, threads)
+    dt = time.perf_counter() - t0
+    sites = reads * steps * (WL["spb"] + WL["wls"]) * P * WL["n"]
+    return {"value": sites / dt, "unit": "site-attempts/s", "cores": threads, "kind": "reference",
+            "sample": f"{reads} reads x first {steps} of {WL['steps']} schedule steps "
+                      f"({sites:.3e} site-attempts, {dt:.1f} s, one SQAAnnealer per thread)"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import REF_SO
+    if not os.path.exists(REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libqanneal_ref.so was not built"}))
+        return 0
+    vals = []
+    per_step_target = 8.0
+    for it in range(args.warmup + args.steps):
+        r = cpu_reference_sample(per_step_target)
+        if it >= args.warmup:
+            vals.append(r)
+    v = float(np.mean([r["value"] for r in vals]))
+    base = vals[-1]
+    line = {
+        "impl": "reference", "metric": "spin-flip attempts/s (site-attempts)", "value": v, "unit": "site-attempts/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "sample": base["sample"]},
+        "cpu_baseline": {"value": v, "unit": "site-attempts/s", "cores": base["cores"], "kind": "reference",
+                         "sample": base["sample"]},
+        "e2e": {"value": v, "unit": "site-attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def flush_l2(torch, dev):
+    buf = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    buf.fill_(1)
+    del buf
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    import qlatanneal_b200 as qa
+    from qlatanneal_b200 import _lib
+    _lib.Engine.get(local)
+
+    n, P, reads = WL["n"], WL["P"], WL["reads"]
+    h, J = instance()
+    betas, gammas = schedule()
+    sched = qa.SQASchedule.from_vectors(betas, gammas)
+    model = qa.DenseIsing(h, J)
+    ann = qa.SQAAnnealer(model, sched, P, 1, device=local)
+    seed = WL["run_seed"] + 1000003 * rank
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ann.run_reads(WL["spb"], WL["wls"], reads=reads, seed=seed)
+
+    # ---- device-timed region (problem resident in HBM)
+    stats = []
+    with Clocks(local) as clk:
+        barrier()
+        for _ in range(args.steps):
+            flush_l2(torch, dev)
+            torch.cuda.synchronize()
+            res = ann.run_reads(WL["spb"], WL["wls"], reads=reads, seed=seed)
+            stats.append(ann.last_stats)
+        barrier()
+    clocks = clk.summary()
+    dev_ms = sum(s.total_ms for s in stats)
+    sweep_ms = sum(s.sweep_ms for s in stats)
+    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms_max = float(t.item())
+    sites_step = site_attempts(stats[0], P)
+    value = world * sites_step * args.steps / (dev_ms_max / 1e3)
+
+    # ---- end-to-end through the public API from host arrays
+    e2e_times, h2d, d2h = [], 0, 0
+    barrier()
+    for _ in range(args.steps):
+        flush_l2(torch, dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m2 = qa.DenseIsing(h, J)
+        a2 = qa.SQAAnnealer(m2, sched, P, 1, device=local)
+        out = a2.run_reads(WL["spb"], WL["wls"], reads=reads, seed=seed)
+        best = min(r.best_energy for r in out)
+        m2.release()
+        e2e_times.append(time.perf_counter() - t0)
+        st = a2.last_stats
+        h2d = n * 12 + n * n * 12 + st.h2d_bytes
+        d2h = st.d2h_bytes
+    barrier()
+    t = torch.tensor([sum(e2e_times)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * sites_step * args.steps / float(t.item())
+
+    # ---- roofline of the sweep kernel
+    peak, peak_kind = load_peaks()
+    bytes_step = algorithmic_bytes(stats[0], n, P)
+    launches = stats[0].sweep_launches
+    avg_launch_ms = sweep_ms / (args.steps * launches)
+    achieved = (bytes_step / launches) / (avg_launch_ms / 1e3) / 1e9
+    traffic = load_traffic()
+
+    # best energy over all ranks (the MINLOC of qanneal's MPI reads helper)
+    be = torch.tensor([min(r.best_energy for r in res)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(be, op=dist.ReduceOp.MIN)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_sample()
+
+    if rank == 0:
+        st = stats[0]
+        line = {
+            "metric": "spin-flip attempts/s (site-attempts)",
+            "value": value,
+            "unit": "site-attempts/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": dev_ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "n": n, "trotter_slices": P, "reads_per_gpu": reads,
+                       "steps": WL["steps"], "sweeps_per_step": [WL["spb"], WL["wls"]],
+                       "site_attempts_per_step": sites_step, "l2": "flushed (256 MiB write) between steps",
+                       "parallelism": f"replicas x{world}", "best_energy": float(be.item()),
+                       "slice_accept_rate": st.slice_accepts / max(1, st.slice_attempts),
+                       "worldline_accept_rate": st.worldline_accepts / max(1, st.worldline_attempts)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "ring_kernel (slice + worldline sweeps)",
+                         "avg_launch_ms": avg_launch_ms, "launches_per_step": launches,
+                         "algorithmic_bytes_per_launch": bytes_step / launches},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "site-attempts/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * float(np.mean(e2e_times))},
+            "gpu_launches": int(sum(s.launches for s in stats)),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

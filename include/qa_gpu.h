@@ -97,6 +97,9 @@ typedef struct {
     int64_t worldline_attempts, worldline_accepts;  /* proposals (each covers P sites) */
     double sweep_ms;                                /* device time of the sweep kernels (CUDA events) */
     double total_ms;                                /* device time of the whole call */
+    int64_t launches;                               /* kernels launched by the call */
+    int64_t sweep_launches;                         /* of which sweep-kernel launches */
+    int64_t h2d_bytes, d2h_bytes;                   /* host<->device bytes moved by the call */
 } qa_stats;
 
 /* ---- SA: Annealer::run (annealer.cpp:33-75) ------------------------------ */

@@ -28,11 +28,14 @@
  *     last slice alone when P is odd), spins in ascending order inside a slice.
  *   - Local fields g = J.s (h kept apart) in float32, couplings rounded to
  *     float32, field init accumulated in float64 then rounded.
- *   - Metropolis test: accept iff x > thr with x = s*(h+g) (float32) and
- *     thr = (trotter + ln u) * A, A = 1/(2*beta/P); ln is a deterministic
- *     float32 logarithm (atanh series) computed identically on both sides.
+ *   - Metropolis test on y = -dE in float32: y = x*B - trotter with
+ *     x = s*(h+g), B = 2*beta/P (2*beta for SA), trotter = 2 J_perp s (s_prev +
+ *     s_next); accept iff y >= 0 or (y > -17 and u < e^y), with a
+ *     deterministic float32 e^y (Taylor series of 2^f) computed identically
+ *     on both sides.
  *   - Energies for the per-step scan in float64, summed in "warp order"
- *     (32 lane-strided partial sums, then an xor butterfly).
+ *     (32 lane-strided partial sums, then an xor butterfly):
+ *     E = c + (sum s h + sum s g / 2) for quadratic models.
  * For integer couplings every value is exact, so spins, accept decisions,
  * energies and traces agree bit for bit.  Parity with the unmodified qanneal
  * code is checked separately (statistically, and exactly on the golden
@@ -89,31 +92,33 @@ static uint32_t draw(uint64_t key64, uint32_t c0, uint32_t c1, uint32_t c2, uint
 
 static inline float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
 
-/* Deterministic float32 natural logarithm for u in [0,1).  Exponent split,
- * mantissa folded to (sqrt(1/2), sqrt(2)], ln(1+f) = 2 atanh(f/(2+f)) by its
- * odd power series, ln 2 split in two parts (Cody & Waite).  Every operation
- * is a single IEEE-rounded float op, so the CUDA engine reproduces it. */
-OR_EXPORT float or_logf(float x) {
-    if (!(x > 0.0f)) return -INFINITY;
+/* Deterministic float32 e^y for y in (-17, 0]: y*log2(e) split into a nearest
+ * integer k and a remainder f in [-1/2, 1/2], 2^f by its Taylor series
+ * (coefficients ln2^n/n!, n <= 6, Horner with fmaf), 2^k applied to the
+ * exponent field.  Single IEEE-rounded operations throughout. */
+OR_EXPORT float or_expf(float y) {
+    float t = y * 1.44269504f;
+    float kf = rintf(t);
+    int k = (int)kf;
+    float f = t - kf;
+    float p = fmaf(1.5403530e-4f, f, 1.3333558e-3f);
+    p = fmaf(p, f, 9.6181291e-3f);
+    p = fmaf(p, f, 5.5504109e-2f);
+    p = fmaf(p, f, 2.4022651e-1f);
+    p = fmaf(p, f, 6.9314718e-1f);
+    p = fmaf(p, f, 1.0f);
     uint32_t b;
-    memcpy(&b, &x, 4);
-    int e = (int)((b >> 23) & 0xffu) - 127;
-    uint32_t mb = (b & 0x7fffffu) | 0x3f800000u;
-    float m;
-    memcpy(&m, &mb, 4);
-    if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
-    float f = m - 1.0f;
-    float s = f / (2.0f + f);
-    float z = s * s;
-    float p = fmaf(z, 0.18181818f, 0.22222222f);
-    p = fmaf(z, p, 0.28571429f);
-    p = fmaf(z, p, 0.40000001f);
-    p = fmaf(z, p, 0.66666669f);
-    p = fmaf(z, p, 2.0f);
-    float r = s * p;
-    float ef = (float)e;
-    return fmaf(ef, 0.693145751953125f, fmaf(ef, 1.42860677e-06f, r));
+    memcpy(&b, &p, 4);
+    b += (uint32_t)k << 23;
+    memcpy(&p, &b, 4);
+    return p;
 }
+
+/* The Metropolis decision of the replay model.  y = -dE (float32), u uniform:
+ * qanneal accepts iff dE <= 0 || u < exp(-dE) (annealer.cpp:55,
+ * sqa_annealer.cpp:198).  Moves with y <= -17 are rejected outright:
+ * exp(-17) = 4.1e-8 is already below the finest step of u (2^-24 = 6.0e-8). */
+static inline int metropolis(float y, float u) { return y >= 0.0f || (y > -17.0f && u < or_expf(y)); }
 
 /* ------------------------------------------------------------------ */
 /* Models                                                               */
@@ -477,12 +482,12 @@ static double wsum(const double *v, int n) {
 /* Tracking energy of one slice from its field cache. */
 static double energy_track(const or_model *M, const int8_t *s, const float *g, double *scratch) {
     const int n = M->n;
-    if (M->kind != M_HUBO) {
-        for (int i = 0; i < n; ++i) scratch[i] = (double)s[i] * ((double)M->h32[i] + 0.5 * (double)g[i]);
-        return M->c + wsum(scratch, n);
-    }
     for (int i = 0; i < n; ++i) scratch[i] = (double)s[i] * (double)M->h32[i];
     double eh = wsum(scratch, n);
+    if (M->kind != M_HUBO) {
+        for (int i = 0; i < n; ++i) scratch[i] = (double)s[i] * (double)g[i];
+        return M->c + (eh + 0.5 * wsum(scratch, n));
+    }
     double *st = scratch + n;
     for (int t = 0; t < M->T; ++t) {
         int sg = 1;
@@ -537,16 +542,15 @@ OR_EXPORT int or_sa_run(const or_model *M, const double *betas, int steps, int s
     memcpy(best_spins, s, (size_t)n);
     int64_t att = 0, acc = 0;
     for (int step = 0; step < steps; ++step) {
-        const float A = (float)(1.0 / (2.0 * betas[step]));
+        const float B = (float)(2.0 * betas[step]);
         for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * spb + sw);
             for (int i = 0; i < n; ++i) {
                 float u = u01(draw(key, spin_slot(i), 0u, sigma, DOM_SA, spin_word(i)));
-                float thr = or_logf(u) * A;
                 float loc = M->h32[i] + g[i];
                 float x = s[i] > 0 ? loc : -loc;
                 ++att;
-                if (x > thr) {
+                if (metropolis(x * B, u)) {
                     ++acc;
                     int so = s[i];
                     double xd = (double)so * ((double)M->h32[i] + (double)g[i]);
@@ -602,7 +606,7 @@ static void ring_init(ring_t *R, uint32_t tag) {
 /* One slice of one ring: sqa_annealer.cpp:180-209 / sqa_chi_annealer.cpp:96-121.
    rng_cell is the cell index used in the counter (ring-relative k*P+t unless
    a slot remap applies). */
-static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigma, uint32_t tag, float A, float T4) {
+static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigma, uint32_t tag, float B, float T4) {
     const or_model *M = R->M;
     const int n = R->n, P = R->P;
     const int prev = t == 0 ? P - 1 : t - 1, next = (t + 1) % P;
@@ -615,11 +619,10 @@ static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigm
         const int q = si * (sp[i] + sn[i]) / 2;
         const float tro = q == 0 ? 0.0f : (q > 0 ? T4 : -T4);
         float u = u01(draw(R->key, spin_slot(i), rng_cell, sigma, tag, spin_word(i)));
-        float thr = (tro + or_logf(u)) * A;
         float loc = M->h32[i] + g[i];
         float x = si > 0 ? loc : -loc;
         R->att_slice++;
-        if (x > thr) {
+        if (metropolis(x * B - tro, u)) {
             R->acc_slice++;
             s[i] = (int8_t)-si;
             apply_flip(M, s, g, i, si);
@@ -627,18 +630,18 @@ static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigm
     }
 }
 
-static void slice_sweep(ring_t *R, uint32_t sigma, uint32_t tag, float A, float T4, const int *slot_of_ring) {
+static void slice_sweep(ring_t *R, uint32_t sigma, uint32_t tag, float B, float T4, const int *slot_of_ring) {
     for (int ph = 0; ph < 3; ++ph)
         for (int k = 0; k < R->K; ++k)
             for (int t = 0; t < R->P; ++t) {
                 if (phase_of(t, R->P) != ph) continue;
                 int slot = slot_of_ring ? slot_of_ring[k] : k;
-                sweep_cell(R, k, t, (uint32_t)(slot * R->P + t), sigma, tag, A, T4);
+                sweep_cell(R, k, t, (uint32_t)(slot * R->P + t), sigma, tag, B, T4);
             }
 }
 
 /* sqa_annealer.cpp:294-315 */
-static void worldline_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma, float A) {
+static void worldline_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma, float B) {
     const or_model *M = R->M;
     const int n = R->n, P = R->P;
     for (int i = 0; i < n; ++i) {
@@ -651,9 +654,8 @@ static void worldline_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma,
         }
         float x = (float)((double)M->h32[i] * (double)sh + G);
         float u = u01(draw(R->key, spin_slot(i), rng_ring, sigma, DOM_WORLD, spin_word(i)));
-        float thr = or_logf(u) * A;
         R->att_world++;
-        if (x > thr) {
+        if (metropolis(x * B, u)) {
             R->acc_world++;
             for (int t = 0; t < P; ++t) {
                 int8_t *s = R->s + ((size_t)k * P + t) * n;
@@ -669,10 +671,10 @@ static double cell_energy(ring_t *R, int c) {
     return energy_track(R->M, R->s + (size_t)c * R->n, R->g + (size_t)c * R->n, R->sc);
 }
 
-/* Per-step constants: beta_scale = beta/P, A = 1/(2 beta_scale), T4 = 4 J_perp. */
-static void step_consts(double beta, double gamma, int P, float *A, float *T4) {
+/* Per-step constants: beta_scale = beta/P, B = 2 beta_scale, T4 = 4 J_perp. */
+static void step_consts(double beta, double gamma, int P, float *B, float *T4) {
     const double bs = beta / (double)P;
-    *A = (float)(1.0 / (2.0 * bs));
+    *B = (float)(2.0 * bs);
     *T4 = (float)(4.0 * trotter_coupling(beta, gamma, P));
 }
 
@@ -692,11 +694,11 @@ OR_EXPORT int or_sqa_run(const or_model *M, const double *betas, const double *g
     double *rsum = (double *)malloc(sizeof(double) * (size_t)K);
     for (int k = 0; k < K; ++k) { rbest[k] = INFINITY; rstep[k] = -1; }
     for (int step = 0; step < steps; ++step) {
-        float A, T4;
-        step_consts(betas[step], gammas[step], P, &A, &T4);
-        for (int sw = 0; sw < spb; ++sw) slice_sweep(&R, (uint32_t)(step * spb + sw), DOM_SLICE, A, T4, NULL);
+        float B, T4;
+        step_consts(betas[step], gammas[step], P, &B, &T4);
+        for (int sw = 0; sw < spb; ++sw) slice_sweep(&R, (uint32_t)(step * spb + sw), DOM_SLICE, B, T4, NULL);
         for (int sw = 0; sw < wls; ++sw)
-            for (int k = 0; k < K; ++k) worldline_sweep(&R, k, (uint32_t)k, (uint32_t)(step * wls + sw), A);
+            for (int k = 0; k < K; ++k) worldline_sweep(&R, k, (uint32_t)k, (uint32_t)(step * wls + sw), B);
         for (int k = 0; k < K; ++k) {
             double sum = 0.0, emin = INFINITY;
             int tmin = 0;

@@ -31,7 +31,8 @@ class qa_run_out(C.Structure):
 class qa_stats(C.Structure):
     _fields_ = [("slice_attempts", C.c_int64), ("slice_accepts", C.c_int64),
                 ("worldline_attempts", C.c_int64), ("worldline_accepts", C.c_int64),
-                ("sweep_ms", C.c_double), ("total_ms", C.c_double)]
+                ("sweep_ms", C.c_double), ("total_ms", C.c_double), ("launches", C.c_int64),
+                ("sweep_launches", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
 
 
 class qa_sa_params(C.Structure):

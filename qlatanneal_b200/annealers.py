@@ -62,11 +62,15 @@ class RunStats:
     worldline_accepts: int = 0
     sweep_ms: float = 0.0
     total_ms: float = 0.0
+    launches: int = 0
+    sweep_launches: int = 0
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
 
     @classmethod
     def from_c(cls, s: "_lib.qa_stats") -> "RunStats":
         return cls(s.slice_attempts, s.slice_accepts, s.worldline_attempts, s.worldline_accepts, s.sweep_ms,
-                   s.total_ms)
+                   s.total_ms, s.launches, s.sweep_launches, s.h2d_bytes, s.d2h_bytes)
 
 
 class _Seeded:

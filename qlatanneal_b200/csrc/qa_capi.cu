@@ -11,6 +11,7 @@
 
 #include "qa_gpu.h"
 #include "qa_kernels.cuh"
+#include "qa_pm1.cuh"
 
 using namespace qa;
 
@@ -195,9 +196,10 @@ int upload_common(qa_ctx *ctx, const qa_problem *const *probs, int np, const Lay
 }
 
 int init_state(qa_ctx *ctx, int kind, const ProbDev *d_probs, const RingDev *d_rings, int n_rings, uint32_t *d_spins,
-               float *d_fields, int P, int n_max, int nw_max, uint32_t tag) {
+               float *d_fields, int P, int n_max, int nw_max, uint32_t tag, bool with_fields = true) {
     init_spins_kernel<<<dim3(n_rings, P), 128, 0, ctx->stream>>>(d_probs, d_rings, d_spins, P, tag, nw_max);
     QA_CK(cudaGetLastError());
+    if (!with_fields) return QA_OK;
     const int zb = std::max(1, std::min(64, (n_max + 127) / 128));
     int rc = QA_OK;
     dispatch_kind(kind, [&](auto K) {
@@ -310,9 +312,25 @@ int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, doubl
             const int a = std::min(i, j), b = std::max(i, j);
             J32[(size_t)i * n + j] = (float)J[(size_t)a * n + b];
         }
+    // couplings all in {-1,+1}: bit-packed rows for ring_pm1_kernel
+    bool pm1 = true;
+    for (int i = 0; i < n && pm1; ++i)
+        for (int j = i + 1; j < n; ++j) {
+            const double v = J[(size_t)i * n + j];
+            if (v != 1.0 && v != -1.0) { pm1 = false; break; }
+        }
+    std::vector<uint32_t> Jw;
+    if (pm1) {
+        const int nw = (n + 31) / 32;
+        Jw.assign((size_t)nw * n, 0u);
+        for (int m = 0; m < n; ++m)
+            for (int j = 0; j < n; ++j)
+                if (j != m && J32[(size_t)m * n + j] > 0.0f) Jw[(size_t)(j >> 5) * n + m] |= 1u << (j & 31);
+    }
     int rc = common_h(P, h);
     if (rc == QA_OK) rc = upload(P, J32.data(), J32.size(), &P->dev.J32);
     if (rc == QA_OK) rc = upload(P, J, (size_t)n * n, &P->dev.J64);
+    if (rc == QA_OK && pm1) rc = upload(P, Jw.data(), Jw.size(), &P->dev.Jw);
     if (rc != QA_OK) {
         qa_problem_free(P);
         return rc;
@@ -456,7 +474,7 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
     float *d_fields;
     QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
     std::vector<float> A(prm->steps);
-    for (int s = 0; s < prm->steps; ++s) A[s] = (float)(1.0 / (2.0 * prm->betas[s]));
+    for (int s = 0; s < prm->steps; ++s) A[s] = (float)(2.0 * prm->betas[s]);  // B = 2 beta
     void *v;
     QA_TRY(ws_get(ctx, W_A, sizeof(float) * A.size(), &v));
     float *d_A = static_cast<float *>(v);
@@ -480,7 +498,7 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
     int smem_fields = (smem + (size_t)n_max * 4) <= (size_t)std::min(ctx->smem_optin, 160 * 1024) ? 1 : 0;
     if (smem_fields) smem += (size_t)n_max * 4;
     SAParams sp{};
-    sp.probs = d_probs; sp.rings = d_rings; sp.spins = d_spins; sp.fields = d_fields; sp.A = d_A;
+    sp.probs = d_probs; sp.rings = d_rings; sp.spins = d_spins; sp.fields = d_fields; sp.B = d_A;
     sp.steps = prm->steps; sp.spb = prm->sweeps_per_beta; sp.smem_fields = smem_fields;
     sp.trace = d_trace; sp.best_E = d_best; sp.best_bits = d_bits; sp.nw_max = L.nw_max; sp.counters = d_cnt;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
@@ -524,6 +542,12 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
         stats->worldline_attempts = stats->worldline_accepts = 0;
         stats->sweep_ms = a;
         stats->total_ms = b;
+        stats->launches = 4;
+        stats->sweep_launches = 1;
+        stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + sizeof(float) * A.size() +
+                                     sizeof(int) * nr);
+        stats->d2h_bytes = (int64_t)(sizeof(double) * trace.size() + sizeof(double) * nr +
+                                     sizeof(uint32_t) * bits.size() + sizeof(cnt));
     }
     return QA_OK;
 }
@@ -561,7 +585,7 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     std::vector<float> A(steps), T4(steps);
     for (int s = 0; s < steps; ++s) {
         const double bs = prm->betas[s] / (double)P;
-        A[s] = (float)(1.0 / (2.0 * bs));
+        A[s] = (float)(2.0 * bs);  // B = 2 beta / P
         T4[s] = (float)(4.0 * trotter_coupling(prm->betas[s], prm->gammas[s], P));
     }
     void *v;
@@ -593,8 +617,12 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     }
 
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT));
     const int W = std::max(1, std::min(32, (P + 1) / 2));
+    // dense +-1 couplings: the bit-packed kernel (fields built in-kernel)
+    bool use_pm1 = kind == K_DENSE && P <= 64 && n_max <= 1024 &&
+                   pm1_smem_bytes(P, n_max) <= (size_t)ctx->smem_optin && !std::getenv("QA_DISABLE_PM1");
+    for (int p = 0; p < n_problems && use_pm1; ++p) use_pm1 = problems[p]->dev.Jw != nullptr;
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !use_pm1));
     size_t smem = ring_smem_bytes(P, n_max, W, true);
     int smem_fields = 1;
     const size_t cap = (size_t)std::min(ctx->smem_optin, 200 * 1024);
@@ -606,24 +634,39 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.W = W; rp.steps_total = steps; rp.spb = prm->sweeps_per_beta; rp.wls = prm->worldline_sweeps;
-    rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.A = d_A; rp.T4 = d_T4; rp.per_slot_sched = 0;
+    rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.B = d_A; rp.T4 = d_T4; rp.per_slot_sched = 0;
     rp.smem_fields = smem_fields; rp.ring_sum = d_sum; rp.ring_min = nullptr; rp.ring_bond = nullptr;
     rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max; rp.mag = nullptr;
     rp.counters = d_cnt;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     int rc = QA_OK;
-    dispatch_kind(kind, [&](auto Kd) {
-        auto kern = ring_kernel<decltype(Kd)::value>;
-        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        const int seg = 256;
-        for (int s0 = 0; s0 < steps && rc == QA_OK; s0 += seg) {
+    const int seg = 256;
+    const int n_seg = (steps + seg - 1) / seg;
+    if (use_pm1) {
+        const size_t sm1 = pm1_smem_bytes(P, n_max);
+        if (sm1 > 48 * 1024)
+            QA_CK(cudaFuncSetAttribute(ring_pm1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+        for (int s0 = 0; s0 < steps; s0 += seg) {
             rp.step0 = s0;
             rp.step1 = std::min(steps, s0 + seg);
-            kern<<<nr, 32 * W, smem, ctx->stream>>>(rp);
-            cudaError_t e = cudaGetLastError();
-            if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, std::string("ring_kernel launch: ") + cudaGetErrorString(e));
+            rp.init_fields = s0 == 0;
+            ring_pm1_kernel<<<nr, 32 * W, sm1, ctx->stream>>>(rp);
+            QA_CK(cudaGetLastError());
         }
-    });
+    } else {
+        dispatch_kind(kind, [&](auto Kd) {
+            auto kern = ring_kernel<decltype(Kd)::value>;
+            if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            for (int s0 = 0; s0 < steps && rc == QA_OK; s0 += seg) {
+                rp.step0 = s0;
+                rp.step1 = std::min(steps, s0 + seg);
+                kern<<<nr, 32 * W, smem, ctx->stream>>>(rp);
+                cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess)
+                    rc = fail(QA_ERR_CUDA, std::string("ring_kernel launch: ") + cudaGetErrorString(e));
+            }
+        });
+    }
     QA_TRY(rc);
     QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
@@ -675,6 +718,12 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
         stats->worldline_accepts = (int64_t)cnt[3];
         stats->sweep_ms = a;
         stats->total_ms = b;
+        stats->sweep_launches = n_seg;
+        stats->launches = (use_pm1 ? 2 : 3) + n_seg;
+        stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * steps +
+                                     (sizeof(double) + sizeof(int)) * nr + sizeof(int) * nr);
+        stats->d2h_bytes = (int64_t)(sizeof(double) * sums.size() + (2 * sizeof(double) + sizeof(int)) * nr +
+                                     sizeof(uint32_t) * bits.size() + sizeof(cnt));
     }
     return QA_OK;
 }

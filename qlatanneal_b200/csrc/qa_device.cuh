@@ -7,10 +7,10 @@
 //     counter = (spin slot, cell, sweep, domain tag).
 //   * Local fields g = J.s in float32 with h kept apart; couplings rounded to
 //     float32; initial fields accumulated in float64 then rounded.
-//   * Metropolis: accept iff x > thr, x = s*(h+g), thr = (trotter + ln u)*A,
-//     A = 1/(2*beta/P).  This is exactly qanneal's rule
-//     "dE <= 0 || u < exp(-dE)" (sqa_annealer.cpp:196-205) rearranged so that
-//     the transcendental is computed once per attempt, off the serial path.
+//   * Metropolis on y = -dE = x*B - trotter, x = s*(h+g), B = 2*beta/P
+//     (2*beta for SA): accept iff y >= 0 or (y > -17 and u < e^y), the rule
+//     "dE <= 0 || u < exp(-dE)" of sqa_annealer.cpp:196-205 with a
+//     deterministic float32 e^y.
 //   * Every float op that feeds a decision is an explicit round-to-nearest
 //     intrinsic, so no FMA contraction changes a bit.
 #pragma once
@@ -54,27 +54,29 @@ __device__ __forceinline__ uint32_t spin_slot(int i) { return (uint32_t)(((i >> 
 
 __device__ __forceinline__ float u01(uint32_t x) { return __uint2float_rn(x >> 8) * (1.0f / 16777216.0f); }
 
-// Deterministic float32 ln(x), x in [0,1): exponent split, mantissa folded to
-// (sqrt(1/2), sqrt(2)], ln(1+f) = 2 atanh(f/(2+f)) by the odd power series of
-// atanh, ln 2 split into two parts (Cody & Waite).  Each step is one IEEE
-// round-to-nearest op, reproduced bit for bit by the CPU restatement.
-__device__ __forceinline__ float det_logf(float x) {
-    if (!(x > 0.0f)) return -__int_as_float(0x7f800000);
-    const uint32_t b = __float_as_uint(x);
-    int e = (int)((b >> 23) & 0xffu) - 127;
-    float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
-    if (m > 1.41421356f) { m = __fmul_rn(m, 0.5f); e += 1; }
-    const float f = __fsub_rn(m, 1.0f);
-    const float s = __fdiv_rn(f, __fadd_rn(2.0f, f));
-    const float z = __fmul_rn(s, s);
-    float p = __fmaf_rn(z, 0.18181818f, 0.22222222f);
-    p = __fmaf_rn(z, p, 0.28571429f);
-    p = __fmaf_rn(z, p, 0.40000001f);
-    p = __fmaf_rn(z, p, 0.66666669f);
-    p = __fmaf_rn(z, p, 2.0f);
-    const float r = __fmul_rn(s, p);
-    const float ef = __int2float_rn(e);
-    return __fmaf_rn(ef, 0.693145751953125f, __fmaf_rn(ef, 1.42860677e-06f, r));
+// Deterministic float32 e^y for y in (-17, 0]: y*log2(e) split into its
+// nearest integer k and a remainder f in [-1/2, 1/2]; 2^f by its Taylor series
+// (coefficients ln2^n/n!, n <= 6, Horner); 2^k added to the exponent field.
+// Each step is one IEEE round-to-nearest op, reproduced bit for bit by the
+// CPU restatement.
+__device__ __forceinline__ float det_expf(float y) {
+    const float t = __fmul_rn(y, 1.44269504f);
+    const int k = __float2int_rn(t);
+    const float f = __fsub_rn(t, __int2float_rn(k));
+    float p = __fmaf_rn(1.5403530e-4f, f, 1.3333558e-3f);
+    p = __fmaf_rn(p, f, 9.6181291e-3f);
+    p = __fmaf_rn(p, f, 5.5504109e-2f);
+    p = __fmaf_rn(p, f, 2.4022651e-1f);
+    p = __fmaf_rn(p, f, 6.9314718e-1f);
+    p = __fmaf_rn(p, f, 1.0f);
+    return __int_as_float(__float_as_int(p) + (k << 23));
+}
+
+// Metropolis decision on y = -dE: qanneal accepts iff dE <= 0 || u < exp(-dE)
+// (annealer.cpp:55, sqa_annealer.cpp:198).  Moves with y <= -17 are rejected
+// outright: e^-17 = 4.1e-8 is below the finest step of u (2^-24).
+__device__ __forceinline__ bool metropolis(float y, float u) {
+    return y >= 0.0f || (y > -17.0f && u < det_expf(y));
 }
 
 __device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
@@ -111,6 +113,9 @@ struct ProbDev {
     const int *incptr, *incterm, *tptr, *tvars;
     const float *coef32;
     const double *coef64;
+    // dense with every coupling in {-1,+1}: bit-packed rows, Jw[q*n + m] =
+    // bits J[m][32q .. 32q+31] (1 = +1; diagonal and padding bits 0); else null
+    const uint32_t *Jw;
 };
 
 __device__ __forceinline__ int spin_of(const uint32_t *S, int i) { return ((S[i >> 5] >> (i & 31)) & 1u) ? 1 : -1; }
@@ -197,23 +202,20 @@ __device__ __forceinline__ float field_init_one(const ProbDev &P, const uint32_t
 
 // Tracking energy of one slice from its field cache (whole warp, all lanes
 // return the same value):
-//   quadratic: E = c + sum_i s_i (h_i + g_i/2)
+//   quadratic: E = c + (sum_i s_i h_i + (sum_i s_i g_i) / 2)
 //   HUBO:      E = c + (sum_i s_i h_i + sum_t J_t prod_t s)
-// in float64, canonical warp order.
+// in float64, each sum in canonical warp order.
 template <int KIND>
 __device__ __forceinline__ double cell_energy(const ProbDev &P, const uint32_t *S, const float *g, const float *h32,
                                               int lane) {
-    if (KIND != K_HUBO) {
-        double p = 0.0;
-        for (int i = lane; i < P.n; i += 32) {
-            const double v = __dadd_rn((double)h32[i], __dmul_rn(0.5, (double)g[i]));
-            p = __dadd_rn(p, spin_of(S, i) > 0 ? v : -v);
-        }
-        return __dadd_rn(P.c, warp_sum_d(p));
-    }
     double ph = 0.0;
     for (int i = lane; i < P.n; i += 32) ph = __dadd_rn(ph, spin_of(S, i) > 0 ? (double)h32[i] : -(double)h32[i]);
     ph = warp_sum_d(ph);
+    if (KIND != K_HUBO) {
+        double pg = 0.0;
+        for (int i = lane; i < P.n; i += 32) pg = __dadd_rn(pg, spin_of(S, i) > 0 ? (double)g[i] : -(double)g[i]);
+        return __dadd_rn(P.c, __dadd_rn(ph, __dmul_rn(0.5, warp_sum_d(pg))));
+    }
     double pj = 0.0;
     for (int t = lane; t < P.T; t += 32) {
         int sg = 1;

@@ -12,12 +12,12 @@
 //    sqa_chi_annealer.cpp:81-140).
 //
 // Inside a slice, 32 consecutive spins form a block owned lane-by-lane.  Each
-// lane precomputes its Metropolis threshold (one Philox word and one log per
-// attempt, in parallel); the warp then resolves the block in spin order by
-// repeatedly balloting "x > thr" and taking the first accepting lane.  Spins
-// before it were rejected on current fields; after its flip the fields are
-// updated and the remaining lanes re-test.  This is the sequential Metropolis
-// sweep exactly, at a cost of (accepted flips + 1) ballots per block.
+// lane draws its uniform (one Philox call serves four blocks) and tests its own
+// spin; the warp then resolves the block in spin order by balloting the
+// decisions and taking the first accepting lane.  Spins before it were
+// rejected on current fields; after its flip the fields are updated and the
+// remaining lanes re-test.  This is the sequential Metropolis sweep exactly,
+// at a cost of (accepted flips + 1) ballots per block.
 #pragma once
 #include "qa_device.cuh"
 
@@ -45,9 +45,10 @@ struct RingParams {
     int spb, wls;         // slice / worldline sweeps per step
     uint32_t slice_tag;   // DOM_SLICE, DOM_PROD or DOM_PILOT|(point<<8)
     const int *slot;      // PT: rung slot of each ring (null: slot = k)
-    const float *A, *T4;  // [sched + step] (PT: [sched + slot])
+    const float *B, *T4;  // [sched + step] (PT: [sched + slot]): B = 2 beta/P, T4 = 4 J_perp
     int per_slot_sched;   // 1: index A/T4 by slot instead of step
     int smem_fields;
+    int init_fields;      // ring_pm1_kernel: build the int32 fields from the spins first
     // outputs
     double *ring_sum;     // [ring][steps_total]  sum of slice energies
     double *ring_min;     // [ring][steps_total]  min slice energy (PT projected energy), may be null
@@ -106,7 +107,7 @@ __global__ void init_fields_kernel(const ProbDev *probs, const RingDev *rings, c
 // schedule of sqa_chi_annealer.cpp:90-122).
 template <int KIND>
 __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int NP, int t, float *gt, const float *h,
-                                            float A, float T4, uint64_t key, uint32_t rng_cell, uint32_t sigma,
+                                            float B, float T4, uint64_t key, uint32_t rng_cell, uint32_t sigma,
                                             uint32_t tag, int lane, unsigned long long &att,
                                             unsigned long long &acc) {
     const int n = Pd.n, nw = Pd.nw;
@@ -125,7 +126,7 @@ __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int 
         const int nsum = (((pw >> lane) & 1u) ? 1 : -1) + (((nx >> lane) & 1u) ? 1 : -1);
         const int qv = si * nsum;
         const float tro = qv == 0 ? 0.0f : (qv > 0 ? T4 : -T4);
-        const float thr = valid ? __fmul_rn(__fadd_rn(tro, det_logf(u01(pick(rnd, q & 3)))), A) : f_inf();
+        const float u = u01(pick(rnd, q & 3));
         const float hi = valid ? h[i] : 0.0f;
         att += (unsigned long long)min(32, n - (q << 5));
         uint32_t pending = FULL;
@@ -133,7 +134,8 @@ __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int 
             const float gi = valid ? gt[i] : 0.0f;
             const float loc = __fadd_rn(hi, gi);
             const float x = si > 0 ? loc : -loc;
-            const uint32_t m = __ballot_sync(FULL, x > thr) & pending;
+            const bool ok = valid && metropolis(__fsub_rn(__fmul_rn(x, B), tro), u);
+            const uint32_t m = __ballot_sync(FULL, ok) & pending;
             if (!m) break;
             const int j = __ffs(m) - 1;
             const int so = ((sw >> j) & 1u) ? 1 : -1;
@@ -152,7 +154,7 @@ struct SAParams {
     const RingDev *rings;   // P == 1 chains
     uint32_t *spins;
     float *fields;
-    const float *A;         // [step]: 1/(2 beta)
+    const float *B;         // [step]: 2 beta
     int steps, spb;
     int smem_fields;
     double *trace;          // [ring][steps]
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
     for (int q = lane; q < nw; q += 32) bb[q] = S[q];
     unsigned long long att = 0, acc = 0;
     for (int step = 0; step < p.steps; ++step) {
-        const float A = p.A[step];
+        const float B = p.B[step];
         for (int sw = 0; sw < p.spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
             U4 rnd = {0, 0, 0, 0};
@@ -195,7 +197,7 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
                 const bool valid = i < n;
                 const uint32_t sword = S[q];
                 const int si = ((sword >> lane) & 1u) ? 1 : -1;
-                const float thr = valid ? __fmul_rn(det_logf(u01(pick(rnd, q & 3))), A) : f_inf();
+                const float u = u01(pick(rnd, q & 3));
                 const float hi = valid ? h[i] : 0.0f;
                 att += (unsigned long long)min(32, n - (q << 5));
                 uint32_t pending = FULL;
@@ -203,7 +205,8 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
                     const float gi = valid ? g[i] : 0.0f;
                     const float loc = __fadd_rn(hi, gi);
                     const float x = si > 0 ? loc : -loc;
-                    const uint32_t m = __ballot_sync(FULL, x > thr) & pending;
+                    const bool ok = valid && metropolis(__fmul_rn(x, B), u);
+                    const uint32_t m = __ballot_sync(FULL, ok) & pending;
                     if (!m) break;
                     const int j = __ffs(m) - 1;
                     const double xd = si > 0 ? __dadd_rn((double)hi, (double)gi) : -__dadd_rn((double)hi, (double)gi);
@@ -291,14 +294,14 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
 
     for (int step = p.step0; step < p.step1; ++step) {
         const int si_tab = R.sched + (p.per_slot_sched ? slot : step);
-        const float A = p.A[si_tab], T4 = p.T4[si_tab];
+        const float B = p.B[si_tab], T4 = p.T4[si_tab];
         for (int sw = 0; sw < p.spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
             for (int ph = 0; ph < 3; ++ph) {
                 const int cnt = phase_count(NP, ph);
                 for (int c = warp; c < cnt; c += W) {
                     const int t = phase_slice(NP, ph, c);
-                    sweep_slice<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, A, T4, R.key,
+                    sweep_slice<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, B, T4, R.key,
                                       (uint32_t)(slot * NP + t), sigma, p.slice_tag, lane, att_s, acc_s);
                 }
                 if (cnt) __syncthreads();
@@ -325,7 +328,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                     rnd = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
                 const int i = (q << 5) | lane;
                 const bool valid = i < n;
-                const float thr = valid ? __fmul_rn(det_logf(u01(pick(rnd, q & 3))), A) : f_inf();
+                const float u = u01(pick(rnd, q & 3));
                 const float hi = valid ? sm.h[i] : 0.0f;
                 if (threadIdx.x == 0) att_w += (unsigned long long)min(32, n - (q << 5));
                 uint32_t pending = FULL;
@@ -350,7 +353,8 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                     }
                     __syncthreads();
                     const float x = valid ? __double2float_rn(__dadd_rn(__dmul_rn((double)hi, (double)Sh), Gt)) : 0.0f;
-                    const uint32_t m = __ballot_sync(FULL, x > thr) & pending;
+                    const bool ok = valid && metropolis(__fmul_rn(x, B), u);
+                    const uint32_t m = __ballot_sync(FULL, ok) & pending;
                     if (!m) break;
                     const int j = __ffs(m) - 1;
                     const int jj = (q << 5) | j;

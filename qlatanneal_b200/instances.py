@@ -1,4 +1,4 @@
-"""Seeded synthetic instances shared by the tests and bench.py.
+"""Seeded synthetic problem instances (benchmark and test workloads).
 
 The shapes and value distributions follow the benchmark configurations of the
 sweep engine: dense Sherrington-Kirkpatrick (J in {-1,+1}), random 3-regular

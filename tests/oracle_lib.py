@@ -54,8 +54,8 @@ class Oracle:
         L = C.CDLL(path)
         self.L = L
         L.or_philox.argtypes = [_u32p, _u32p, _u32p]
-        L.or_logf.argtypes = [C.c_float]
-        L.or_logf.restype = C.c_float
+        L.or_expf.argtypes = [C.c_float]
+        L.or_expf.restype = C.c_float
         L.or_model_dense.argtypes = [C.c_int, _f8p, _f8p, C.c_double]
         L.or_model_dense.restype = C.c_void_p
         L.or_model_sparse.argtypes = [C.c_int, _f8p, C.c_int, _i64p, _i64p, _f8p, C.c_double]
@@ -87,8 +87,8 @@ class Oracle:
         self.L.or_philox(np.asarray(ctr, np.uint32), np.asarray(key, np.uint32), out)
         return out
 
-    def logf(self, x: float) -> float:
-        return float(self.L.or_logf(C.c_float(x)))
+    def expf(self, y: float) -> float:
+        return float(self.L.or_expf(C.c_float(y)))
 
     def init_spins(self, n, key, cell, tag=1):
         s = np.zeros(n, np.int8)

@@ -8,7 +8,7 @@ import pytest
 
 import qlatanneal_b200 as qa
 from qlatanneal_b200 import _lib
-from instances import hubo_random, regular3, sk_dense
+from qlatanneal_b200.instances import hubo_random, regular3, sk_dense
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import qlatanneal_b200 as qa
-from instances import geometric_betas, hubo_random, regular3, sk_dense
+from qlatanneal_b200.instances import geometric_betas, hubo_random, regular3, sk_dense
 
 pytestmark = pytest.mark.gpu
 
@@ -33,6 +33,10 @@ def make(kind, n, seed):
         h, J = sk_dense(n, seed)
         h = rng.choice([-0.5, 0.0, 0.25, 0.5], size=n)
         return qa.DenseIsing(h, J, 1.5)
+    if kind == "dense_int":
+        rng = np.random.default_rng(seed)
+        J = np.triu(rng.choice([-2.0, -1.0, 1.0, 2.0], size=(n, n)), 1)
+        return qa.DenseIsing(rng.choice([-1.0, 0.0, 1.0], size=n), J + J.T)
     if kind == "sparse":
         h, e = regular3(n, seed)
         return qa.SparseIsing(h, e, n, -2.0)
@@ -67,23 +71,40 @@ def test_sa_bit_exact(oracle, kind, n):
 
 
 SQA_CASES = [
-    ("dense", 64, 8, 1, 1, 1),
-    ("dense", 96, 5, 2, 1, 1),
-    ("dense", 40, 1, 1, 2, 0),
-    ("dense", 40, 2, 3, 0, 2),
-    ("dense_h", 70, 6, 2, 2, 1),
-    ("sparse", 128, 8, 1, 1, 1),
-    ("sparse", 64, 7, 2, 2, 1),
-    ("hubo", 48, 4, 2, 1, 1),
+    # +-1 dense couplings run on the bit-packed kernel (ring_pm1_kernel)
+    ("dense", 64, 8, 1, 1, 1, 1.0),
+    ("dense", 96, 5, 2, 1, 1, 1.0),
+    ("dense", 40, 1, 1, 2, 0, 1.0),
+    ("dense", 40, 2, 3, 0, 2, 1.0),
+    ("dense", 512, 32, 1, 1, 1, 2.0),
+    ("dense", 100, 64, 1, 1, 2, 0.25),
+    ("dense", 33, 3, 1, 2, 3, 0.1),
+    ("dense_h", 70, 6, 2, 2, 1, 0.5),
+    # the generic field-cache kernel
+    ("dense_int", 80, 8, 2, 1, 1, 0.5),
+    ("sparse", 128, 8, 1, 1, 1, 1.0),
+    ("sparse", 64, 7, 2, 2, 1, 1.0),
+    ("hubo", 48, 4, 2, 1, 1, 1.0),
 ]
 
 
-@pytest.mark.parametrize("kind,n,P,K,spb,wls", SQA_CASES)
-def test_sqa_bit_exact(oracle, kind, n, P, K, spb, wls):
+@pytest.mark.parametrize("kind,n,P,K,spb,wls,bscale", SQA_CASES)
+def test_sqa_bit_exact(oracle, kind, n, P, K, spb, wls, bscale):
+    _sqa_case(oracle, kind, n, P, K, spb, wls, bscale)
+
+
+@pytest.mark.parametrize("kind,n,P,K,spb,wls,bscale", [("dense", 64, 8, 2, 1, 1, 1.0), ("dense", 200, 16, 1, 1, 1, 0.3)])
+def test_sqa_generic_kernel_on_pm1_models(oracle, monkeypatch, kind, n, P, K, spb, wls, bscale):
+    """The generic field-cache kernel gives the same bits as the +-1 kernel."""
+    monkeypatch.setenv("QA_DISABLE_PM1", "1")
+    _sqa_case(oracle, kind, n, P, K, spb, wls, bscale)
+
+
+def _sqa_case(oracle, kind, n, P, K, spb, wls, bscale):
     model = make(kind, n, 21)
     om = oracle_model(oracle, model)
     steps = 25
-    betas = np.full(steps, 2.0 * P / 4.0)
+    betas = np.full(steps, bscale * 2.0 * P / 4.0)
     gammas = np.linspace(3.0, 0.05, steps)
     reads, seed = 3, 777
     ann = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors(betas, gammas), P, K)
@@ -130,7 +151,7 @@ def test_reference_sqa_basic():
 
 def test_real_couplings_energy(oracle):
     """Real-valued J: every returned energy equals the float64 energy of its state."""
-    from instances import dense_real
+    from qlatanneal_b200.instances import dense_real
     h, J = dense_real(80, 5)
     model = qa.DenseIsing(h, J, 0.25)
     om = oracle.dense(h, J, 0.25)

@@ -1,7 +1,7 @@
 """Pins the CPU restatement (the oracle) before any GPU result is trusted.
 
 * Philox4x32-10 against the published Random123 known-answer vectors.
-* The deterministic log against math.log.
+* The deterministic exp of the Metropolis test against math.exp.
 * Model functions against the reference's own golden tests
   (tests/test_dense_ising.cpp, tests/test_higher_order_ising.cpp) and against
   qanneal compiled from its sources (oracle/_ref).
@@ -12,7 +12,7 @@ import math
 import numpy as np
 import pytest
 
-from instances import geometric_betas, hubo_random, regular3, sk_dense
+from qlatanneal_b200.instances import geometric_betas, hubo_random, regular3, sk_dense
 
 # Random123 kat_vectors, philox4x32 with 10 rounds: (counter, key, expected)
 PHILOX_KAT = [
@@ -28,13 +28,12 @@ def test_philox_known_answers(oracle, ctr, key, want):
     assert oracle.philox(ctr, key).tolist() == want
 
 
-def test_det_log_accuracy(oracle):
-    rng = np.random.default_rng(0)
-    xs = (rng.integers(1, 1 << 24, 5000) / float(1 << 24)).astype(np.float32)
-    for x in xs:
-        got = oracle.logf(float(x))
-        assert abs(got - math.log(float(x))) <= 4e-7 * abs(math.log(float(x))) + 1e-7
-    assert oracle.logf(0.0) == -math.inf
+def test_det_exp_accuracy(oracle):
+    ys = np.linspace(-16.999, 0.0, 20001).astype(np.float32)
+    for y in ys[::7]:
+        got = oracle.expf(float(y))
+        assert abs(got - math.exp(float(y))) <= 1.5e-6 * math.exp(float(y))
+    assert oracle.expf(0.0) == 1.0
 
 
 def test_dense_ising_golden(oracle, ref):
