@@ -171,7 +171,7 @@ void build_rings(Layout &L, const qa_problem *const *probs, int np, int reads, i
                 R.spin_off = L.spin_words;
                 R.field_off = L.field_floats;
                 L.spin_words += (long long)P * probs[p]->nw;
-                L.field_floats += (long long)P * probs[p]->n;
+                L.field_floats += (long long)P * pm1_npad(probs[p]->n);  // rows padded for ring_pm1_kernel
                 L.rings.push_back(R);
             }
 }
@@ -321,11 +321,11 @@ int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, doubl
         }
     std::vector<uint32_t> Jw;
     if (pm1) {
-        const int nw = (n + 31) / 32;
-        Jw.assign((size_t)nw * n, 0u);
+        const int nw = (n + 31) / 32, np = pm1_npad(n);
+        Jw.assign((size_t)nw * np, 0u);
         for (int m = 0; m < n; ++m)
             for (int j = 0; j < n; ++j)
-                if (j != m && J32[(size_t)m * n + j] > 0.0f) Jw[(size_t)(j >> 5) * n + m] |= 1u << (j & 31);
+                if (j != m && J32[(size_t)m * n + j] > 0.0f) Jw[(size_t)(j >> 5) * np + m] |= 1u << (j & 31);
     }
     int rc = common_h(P, h);
     if (rc == QA_OK) rc = upload(P, J32.data(), J32.size(), &P->dev.J32);

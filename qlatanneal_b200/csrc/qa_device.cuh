@@ -79,6 +79,14 @@ __device__ __forceinline__ bool metropolis(float y, float u) {
     return y >= 0.0f || (y > -17.0f && u < det_expf(y));
 }
 
+// The same decision without divergent branches: e^y is evaluated on y
+// clamped to [-17, 0] and only used where -17 < y < 0, so the result is
+// identical to metropolis().
+__device__ __forceinline__ bool metropolis_nb(float y, float u) {
+    const float p = det_expf(fminf(fmaxf(y, -17.0f), 0.0f));
+    return (y >= 0.0f) | ((y > -17.0f) & (u < p));
+}
+
 __device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
 
 // float64 warp sum in the canonical order: lane-strided partials (already in

@@ -134,7 +134,7 @@ __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int 
             const float gi = valid ? gt[i] : 0.0f;
             const float loc = __fadd_rn(hi, gi);
             const float x = si > 0 ? loc : -loc;
-            const bool ok = valid && metropolis(__fsub_rn(__fmul_rn(x, B), tro), u);
+            const bool ok = valid & metropolis_nb(__fsub_rn(__fmul_rn(x, B), tro), u);
             const uint32_t m = __ballot_sync(FULL, ok) & pending;
             if (!m) break;
             const int j = __ffs(m) - 1;
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
                     const float gi = valid ? g[i] : 0.0f;
                     const float loc = __fadd_rn(hi, gi);
                     const float x = si > 0 ? loc : -loc;
-                    const bool ok = valid && metropolis(__fmul_rn(x, B), u);
+                    const bool ok = valid & metropolis_nb(__fmul_rn(x, B), u);
                     const uint32_t m = __ballot_sync(FULL, ok) & pending;
                     if (!m) break;
                     const int j = __ffs(m) - 1;
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                     }
                     __syncthreads();
                     const float x = valid ? __double2float_rn(__dadd_rn(__dmul_rn((double)hi, (double)Sh), Gt)) : 0.0f;
-                    const bool ok = valid && metropolis(__fmul_rn(x, B), u);
+                    const bool ok = valid & metropolis_nb(__fmul_rn(x, B), u);
                     const uint32_t m = __ballot_sync(FULL, ok) & pending;
                     if (!m) break;
                     const int j = __ffs(m) - 1;

@@ -3,33 +3,40 @@
 //
 // Same replay semantics as ring_kernel (qa_kernels.cuh), different data path:
 //  * J is bit-packed (1 bit per coupling) and staged once per CTA in shared
-//    memory: Jw[q*n + m] holds bits J[m][32q .. 32q+31] (J is symmetric, so it
-//    is also column m).  n = 512 takes 32 KB.
+//    memory: Jw[q*npad + m] holds bits J[m][32q .. 32q+31] (J is symmetric, so
+//    it is also column m); rows are padded to npad, a multiple of 128.
 //  * Local fields are exact int32 (g = J.s is an integer) in shared memory.
-//  * A block of 32 spins is resolved as in ring_kernel, but the fields of the
-//    whole slice are updated once per block, for all flips F of the block
-//    together: g[m] += 2|F| - 4 popc(~(Jw[q*n+m] ^ s_old) & F), i.e. a few
-//    integer ops per field instead of one update per flip.
-//  * Worldline moves (sqa_annealer.cpp:294-315) are evaluated speculatively for
-//    all remaining spins at once (thread per spin, sum over the P slices),
-//    then the first accepted spin in sweep order is applied and the pass
-//    repeats from the next spin: the sequential sweep, with one CTA barrier
-//    pair per accepted move instead of per spin.
+//  * A block of 32 spins is resolved in spin order by ballots; the fields of
+//    the whole slice are then updated once for all flips F of the block:
+//        g[m] += 2|F| - 4 popc(~(Jw[q*npad+m] ^ s_old) & F)
+//    four fields per lane per 128-bit shared-memory access.
+//  * Worldline moves (sqa_annealer.cpp:294-315): the slice sums
+//    G_i = sum_t s_t,i g_t,i are built once per sweep; decisions for all
+//    remaining spins are taken in parallel; the first block holding an
+//    accepted move is resolved in spin order by one warp, its flips applied to
+//    every slice by the block update above, and the sums of later spins
+//    corrected exactly by  dG_i = -2 J_ij (P - 2 popc(W_i ^ W_j))  where W_i
+//    is spin i's worldline (its bits over the P slices).  The result is the
+//    sequential sweep; the cost is one parallel pass per block with moves.
 #pragma once
 #include "qa_kernels.cuh"
 
 namespace qa {
 
+__host__ __device__ inline int pm1_npad(int n) { return (n + 127) / 128 * 128; }
+
 __host__ __device__ inline size_t pm1_smem_bytes(int P, int n) {
-    const int nw = (n + 31) / 32;
-    size_t b = align_up((size_t)nw * n * 4, 16);  // Jw
+    const int nw = (n + 31) / 32, np = pm1_npad(n);
+    size_t b = (size_t)nw * np * 4;                // Jw
     b += align_up((size_t)P * nw * 4, 16);         // S
-    b += align_up((size_t)n * 4, 16);              // h
-    b += align_up((size_t)P * n * 4, 16);          // G
+    b += (size_t)np * 4;                           // h
+    b += (size_t)P * np * 4;                       // G
+    b += (size_t)np * 8;                           // W (worldline bits)
+    b += (size_t)np * 4;                           // Gsum (worldline slice sums)
+    b += (size_t)np * 4;                           // uw (worldline uniforms)
     b += align_up((size_t)P * 8, 16);              // cellE
-    b += align_up((size_t)32 * 4, 16);             // per-block accept masks (nw <= 32)
-    b += 32;                                       // flags + per-warp partials
-    return b + 128;
+    b += 32 * 4 + 32 * 8 + 32 * 4 + 64;            // masks, old worldlines, partials, flags
+    return b + 64;
 }
 
 __device__ __forceinline__ int warp_sum_i(int v) {
@@ -38,99 +45,149 @@ __device__ __forceinline__ int warp_sum_i(int v) {
     return v;
 }
 
-// One warp sweeps slice t.
-__device__ __forceinline__ void pm1_sweep_slice(const uint32_t *Jw, uint32_t *S, int *G, const float *h, int n, int nw,
-                                                int NP, int t, float B, float T4, uint64_t key, uint32_t rng_cell,
-                                                uint32_t sigma, uint32_t tag, int lane, unsigned long long &att,
+// x = s*(h+g) with the sign taken from the spin bit (bit 1 = +1).
+__device__ __forceinline__ float signed_by_bit(float v, uint32_t bit) {
+    return __int_as_float(__float_as_int(v) ^ (int)((bit ^ 1u) << 31));
+}
+
+__device__ __forceinline__ int flip_delta(uint32_t jw, uint32_t sold, uint32_t Fm) {
+    return 2 * __popc(Fm) - 4 * __popc(~(jw ^ sold) & Fm);
+}
+
+// Fields of one slice after the spins F of block q (old word sold) flipped.
+// Whole warp; the field of a flipped spin excludes its own (zero) diagonal.
+__device__ __forceinline__ void pm1_block_update(int *Gt, const uint32_t *Jw, int npad, int n, int q, uint32_t F,
+                                                 uint32_t sold, int lane) {
+    const uint32_t *Jq = Jw + q * npad;
+    for (int base = lane * 4; base < n; base += 128) {
+        const uint4 jw = *reinterpret_cast<const uint4 *>(Jq + base);
+        int4 g = *reinterpret_cast<int4 *>(Gt + base);
+        const uint32_t d = (base >> 5) == q ? (1u << (base & 31)) : 0u;
+        g.x += flip_delta(jw.x, sold, F & ~d);
+        g.y += flip_delta(jw.y, sold, F & ~(d << 1));
+        g.z += flip_delta(jw.z, sold, F & ~(d << 2));
+        g.w += flip_delta(jw.w, sold, F & ~(d << 3));
+        *reinterpret_cast<int4 *>(Gt + base) = g;
+    }
+}
+
+// One block of 32 spins (lane = spin) of slice t; rw is this lane's Philox word.
+__device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, const uint32_t *Sp, const uint32_t *Sn,
+                                          int *Gt, unsigned long long *Wc, const float *h, int n, int npad, int q,
+                                          int t, uint32_t rw, float B, float T4, int lane, unsigned long long &acc) {
+    const int i = (q << 5) | lane;
+    const bool valid = i < n;
+    const uint32_t sw = St[q];
+    const uint32_t sbit = (sw >> lane) & 1u;
+    // s*(s_prev + s_next)/2 = 1 - (number of Trotter neighbours that differ)
+    const int d = (int)(((sw ^ Sp[q]) >> lane) & 1u) + (int)(((sw ^ Sn[q]) >> lane) & 1u);
+    const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
+    const float u = u01(rw);
+    const float hi = h[i];
+    const int gi = Gt[i];
+    bool ok = valid & metropolis_nb(
+        __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gi)), sbit), B), tro), u);
+    uint32_t m = __ballot_sync(FULL, ok);
+    if (m == 0) return;
+    // resolve the block in spin order; gk is this lane's field with the
+    // block's earlier flips applied
+    const uint32_t jd = Jw[q * npad + i];
+    uint32_t F = 0;
+    int gk = gi;
+    do {
+        const int j = __ffs(m) - 1;
+        F |= 1u << j;
+        if (lane != j) gk += (((sw ^ jd) >> j) & 1u) ? 2 : -2;
+        const uint32_t pending = j == 31 ? 0u : (FULL << (j + 1));
+        ok = valid & metropolis_nb(
+            __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gk)), sbit), B), tro), u);
+        m = __ballot_sync(FULL, ok) & pending;
+        ++acc;
+    } while (m);
+    if (lane == 0) St[q] = sw ^ F;
+    if ((F >> lane) & 1u) atomicXor(Wc + i, 1ull << t);
+    pm1_block_update(Gt, Jw, npad, n, q, F, sw, lane);
+    __syncwarp();
+}
+
+// One warp sweeps slice t; one Philox call per lane serves four blocks.
+__device__ __forceinline__ void pm1_sweep_slice(const uint32_t *Jw, uint32_t *S, int *G, unsigned long long *Wc,
+                                                const float *h, int n, int nw, int npad, int NP, int t, float B,
+                                                float T4, uint64_t key, uint32_t rng_cell, uint32_t sigma,
+                                                uint32_t tag, int lane, unsigned long long &att,
                                                 unsigned long long &acc) {
     uint32_t *St = S + t * nw;
     const uint32_t *Sp = S + (t == 0 ? NP - 1 : t - 1) * nw;
     const uint32_t *Sn = S + (t + 1 == NP ? 0 : t + 1) * nw;
-    int *Gt = G + t * n;
-    U4 rnd = {0, 0, 0, 0};
-    for (int q = 0; q < nw; ++q) {
-        if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), rng_cell, sigma, tag, key);
-        const int i = (q << 5) | lane;
-        const bool valid = i < n;
-        const uint32_t sw = St[q], pw = Sp[q], nx = Sn[q];
-        const int si = ((sw >> lane) & 1u) ? 1 : -1;
-        const int qv = si * ((((pw >> lane) & 1u) ? 1 : -1) + (((nx >> lane) & 1u) ? 1 : -1));
-        const float tro = qv == 0 ? 0.0f : (qv > 0 ? T4 : -T4);
-        const float u = u01(pick(rnd, q & 3));
-        const float hi = valid ? h[i] : 0.0f;
-        const int gi = valid ? Gt[i] : 0;
-        att += (unsigned long long)min(32, n - (q << 5));
-        float loc = __fadd_rn(hi, __int2float_rn(gi));
-        bool ok = valid && metropolis(__fsub_rn(__fmul_rn(si > 0 ? loc : -loc, B), tro), u);
-        uint32_t m = __ballot_sync(FULL, ok);
-        if (m == 0) continue;
-        // resolve the block in spin order; gk is this lane's field with the
-        // block's earlier flips applied
-        const uint32_t jd = valid ? Jw[q * n + i] : 0u;
-        uint32_t F = 0;
-        int gk = gi;
-        do {
-            const int j = __ffs(m) - 1;
-            F |= 1u << j;
-            if (lane != j) gk += (((sw ^ jd) >> j) & 1u) ? 2 : -2;
-            const uint32_t pending = j == 31 ? 0u : (FULL << (j + 1));
-            loc = __fadd_rn(hi, __int2float_rn(gk));
-            ok = valid && metropolis(__fsub_rn(__fmul_rn(si > 0 ? loc : -loc, B), tro), u);
-            m = __ballot_sync(FULL, ok) & pending;
-            ++acc;
-        } while (m);
-        if (lane == 0) St[q] = sw ^ F;
-        for (int qq = 0; qq < nw; ++qq) {
-            const int mm = (qq << 5) | lane;
-            if (mm < n) {
-                const uint32_t Fm = qq == q ? (F & ~(1u << lane)) : F;
-                const int agree = __popc(~(Jw[q * n + mm] ^ sw) & Fm);
-                Gt[mm] += 2 * __popc(Fm) - 4 * agree;
-            }
-        }
-        __syncwarp();
+    int *Gt = G + t * npad;
+    att += (unsigned long long)n;
+    for (int q4 = 0; q4 < nw; q4 += 4) {
+        const U4 r = philox((uint32_t)(((q4 >> 2) << 5) | lane), rng_cell, sigma, tag, key);
+        pm1_block(Jw, St, Sp, Sn, Gt, Wc, h, n, npad, q4, t, r.x, B, T4, lane, acc);
+        if (q4 + 1 < nw) pm1_block(Jw, St, Sp, Sn, Gt, Wc, h, n, npad, q4 + 1, t, r.y, B, T4, lane, acc);
+        if (q4 + 2 < nw) pm1_block(Jw, St, Sp, Sn, Gt, Wc, h, n, npad, q4 + 2, t, r.z, B, T4, lane, acc);
+        if (q4 + 3 < nw) pm1_block(Jw, St, Sp, Sn, Gt, Wc, h, n, npad, q4 + 3, t, r.w, B, T4, lane, acc);
     }
+}
+
+__device__ __forceinline__ bool pm1_world_ok(const float *h, const int *Gs, const unsigned long long *Wc,
+                                             const float *uw, int i, int n, int NP, float B) {
+    const int sh = 2 * __popcll(Wc[i]) - NP;
+    const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)h[i], (double)sh), (double)Gs[i]));
+    return (i < n) & metropolis_nb(__fmul_rn(x, B), uw[i]);
 }
 
 __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const RingDev R = p.rings[blockIdx.x];
     const ProbDev Pd = p.probs[R.prob];
-    const int NP = p.P, W = p.W, n = Pd.n, nw = Pd.nw;
+    const int NP = p.P, W = p.W, n = Pd.n, nw = Pd.nw, npad = pm1_npad(n);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char *ptr = smem;
-    uint32_t *Jw = reinterpret_cast<uint32_t *>(ptr); ptr += align_up((size_t)nw * n * 4, 16);
+    uint32_t *Jw = reinterpret_cast<uint32_t *>(ptr); ptr += (size_t)nw * npad * 4;
     uint32_t *S = reinterpret_cast<uint32_t *>(ptr); ptr += align_up((size_t)NP * nw * 4, 16);
-    float *h = reinterpret_cast<float *>(ptr); ptr += align_up((size_t)n * 4, 16);
-    int *G = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)NP * n * 4, 16);
+    float *h = reinterpret_cast<float *>(ptr); ptr += (size_t)npad * 4;
+    int *G = reinterpret_cast<int *>(ptr); ptr += (size_t)NP * npad * 4;
+    unsigned long long *Wc = reinterpret_cast<unsigned long long *>(ptr); ptr += (size_t)npad * 8;
+    int *Gs = reinterpret_cast<int *>(ptr); ptr += (size_t)npad * 4;
+    float *uw = reinterpret_cast<float *>(ptr); ptr += (size_t)npad * 4;
     double *cellE = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)NP * 8, 16);
-    uint32_t *mask = reinterpret_cast<uint32_t *>(ptr); ptr += align_up((size_t)32 * 4, 16);
-    int *flag = reinterpret_cast<int *>(ptr); ptr += 32;
-    int *wpart = reinterpret_cast<int *>(ptr);  // [32]
+    uint32_t *mask = reinterpret_cast<uint32_t *>(ptr); ptr += 32 * 4;
+    unsigned long long *Wold = reinterpret_cast<unsigned long long *>(ptr); ptr += 32 * 8;
+    int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
+    int *flag = reinterpret_cast<int *>(ptr);  // [0]: best slice, [1]: block flips F, [2]: block index
 
-    for (int idx = threadIdx.x; idx < nw * n; idx += blockDim.x) Jw[idx] = Pd.Jw[idx];
+    for (int idx = threadIdx.x; idx < nw * npad; idx += blockDim.x) Jw[idx] = Pd.Jw[idx];
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) S[idx] = p.spins[R.spin_off + idx];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) h[i] = Pd.h32[i];
+    for (int i = threadIdx.x; i < npad; i += blockDim.x) h[i] = i < n ? Pd.h32[i] : 0.0f;
     int *Gg = reinterpret_cast<int *>(p.fields) + R.field_off;
     __syncthreads();
     if (p.init_fields) {
         // g_m = sum_{j != m} J_mj s_j by popcount over the packed rows
-        for (int idx = threadIdx.x; idx < NP * n; idx += blockDim.x) {
-            const int t = idx / n, mm = idx - t * n;
+        for (int idx = threadIdx.x; idx < NP * npad; idx += blockDim.x) {
+            const int t = idx / npad, mm = idx - t * npad;
             int g = 0;
-            for (int q = 0; q < nw; ++q) {
-                const int rem = n - 32 * q;
-                uint32_t vm = rem >= 32 ? FULL : ((1u << rem) - 1u);
-                if (q == (mm >> 5)) vm &= ~(1u << (mm & 31));
-                g += 2 * __popc(~(Jw[q * n + mm] ^ S[t * nw + q]) & vm) - __popc(vm);
-            }
+            if (mm < n)
+                for (int q = 0; q < nw; ++q) {
+                    const int rem = n - 32 * q;
+                    uint32_t vm = rem >= 32 ? FULL : ((1u << rem) - 1u);
+                    if (q == (mm >> 5)) vm &= ~(1u << (mm & 31));
+                    g += 2 * __popc(~(Jw[q * npad + mm] ^ S[t * nw + q]) & vm) - __popc(vm);
+                }
             G[idx] = g;
         }
     } else {
-        for (int idx = threadIdx.x; idx < NP * n; idx += blockDim.x) G[idx] = Gg[idx];
+        for (int idx = threadIdx.x; idx < NP * npad; idx += blockDim.x) G[idx] = Gg[idx];
+    }
+    for (int i = threadIdx.x; i < npad; i += blockDim.x) {
+        unsigned long long wc = 0;
+        if (i < n)
+            for (int t = 0; t < NP; ++t) wc |= (unsigned long long)((S[t * nw + (i >> 5)] >> (i & 31)) & 1u) << t;
+        Wc[i] = wc;
     }
     __syncthreads();
 
+    const unsigned long long pmask = NP == 64 ? ~0ull : ((1ull << NP) - 1ull);
     const int slot = p.slot ? p.slot[blockIdx.x] : R.k;
     unsigned long long att_s = 0, acc_s = 0, att_w = 0, acc_w = 0;
     double bestE = p.best_E[blockIdx.x];
@@ -145,8 +202,8 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 const int cnt = phase_count(NP, ph);
                 for (int c = warp; c < cnt; c += W) {
                     const int t = phase_slice(NP, ph, c);
-                    pm1_sweep_slice(Jw, S, G, h, n, nw, NP, t, B, T4, R.key, (uint32_t)(slot * NP + t), sigma,
-                                    p.slice_tag, lane, att_s, acc_s);
+                    pm1_sweep_slice(Jw, S, G, Wc, h, n, nw, npad, NP, t, B, T4, R.key, (uint32_t)(slot * NP + t),
+                                    sigma, p.slice_tag, lane, att_s, acc_s);
                 }
                 if (cnt) __syncthreads();
             }
@@ -166,51 +223,84 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
         }
         for (int sw = 0; sw < p.wls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
-            int start = 0;
-            for (;;) {
-                const int q0 = start >> 5;
-                for (int q = q0 + warp; q < nw; q += W) {
-                    const int i = (q << 5) | lane;
-                    int sh = 0, gs = 0;
-                    if (i < n)
-                        for (int t = 0; t < NP; ++t) {
-                            const int st = ((S[t * nw + q] >> lane) & 1u) ? 1 : -1;
-                            sh += st;
-                            gs += st * G[t * n + i];
-                        }
-                    const float hi = i < n ? h[i] : 0.0f;
-                    const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)hi, (double)sh), (double)gs));
-                    const U4 r = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
-                    const bool ok = i < n && i >= start && metropolis(__fmul_rn(x, B), u01(pick(r, q & 3)));
-                    const uint32_t m = __ballot_sync(FULL, ok);
-                    if (lane == 0) mask[q] = m;
-                }
-                __syncthreads();
-                int first = -1;
-                for (int q = q0; q < nw; ++q) {
-                    const uint32_t m = mask[q];
-                    if (m) {
-                        first = (q << 5) | (__ffs(m) - 1);
-                        break;
+            // slice sums and uniforms of every spin (thread per spin; a warp
+            // holds one 32-spin block, so lane == spin & 31)
+            for (int i = threadIdx.x; i < npad; i += blockDim.x) {
+                const int q = i >> 5;
+                int gs = 0;
+                if (i < n)
+                    for (int t = 0; t < NP; ++t) {
+                        const int g = G[t * npad + i];
+                        gs += ((S[t * nw + q] >> lane) & 1u) ? g : -g;
                     }
+                Gs[i] = gs;
+                const U4 r = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
+                uw[i] = u01(pick(r, q & 3));
+            }
+            if (threadIdx.x == 0) att_w += (unsigned long long)n;
+            __syncthreads();
+            int q0 = 0;
+            for (;;) {
+                for (int i = threadIdx.x + q0 * 32; i < npad; i += blockDim.x) {
+                    const uint32_t m = __ballot_sync(FULL, pm1_world_ok(h, Gs, Wc, uw, i, n, NP, B));
+                    if (lane == 0) mask[i >> 5] = m;
                 }
-                if (threadIdx.x == 0) att_w += (unsigned long long)((first < 0 ? n : first + 1) - start);
-                __syncthreads();  // every thread has read mask[] before the next pass rewrites it
-                if (first < 0) break;
-                const int fq = first >> 5, fj = first & 31;
-                for (int t = warp; t < NP; t += W) {
-                    const uint32_t sw0 = S[t * nw + fq];
-                    __syncwarp();
-                    if (lane == 0) S[t * nw + fq] = sw0 ^ (1u << fj);
-                    const uint32_t sj = (sw0 >> fj) & 1u;
-                    int *Gt = G + t * n;
-                    for (int mm = lane; mm < n; mm += 32)
-                        if (mm != first) Gt[mm] += (((Jw[fq * n + mm] >> fj) & 1u) == sj) ? -2 : 2;
-                }
-                if (threadIdx.x == 0) ++acc_w;
                 __syncthreads();
-                start = first + 1;
-                if (start >= n) break;
+                int qs = -1;
+                for (int q = q0; q < nw; ++q)
+                    if (mask[q]) { qs = q; break; }
+                if (qs < 0) {
+                    __syncthreads();  // every thread has read mask[] before it is rewritten
+                    break;
+                }
+                if (warp == 0) {
+                    // resolve block qs in spin order
+                    const int i = (qs << 5) | lane;
+                    const unsigned long long wi = Wc[i];
+                    const uint32_t jd = Jw[qs * npad + i];
+                    int gk = Gs[i];
+                    uint32_t m = mask[qs], F = 0;
+                    do {
+                        const int j = __ffs(m) - 1;
+                        F |= 1u << j;
+                        const unsigned long long wj = __shfl_sync(FULL, wi, j);
+                        const int overlap = NP - 2 * __popcll(wi ^ wj);  // sum_t s_t,i s_t,j
+                        if (lane != j) gk += ((jd >> j) & 1u) ? -2 * overlap : 2 * overlap;
+                        const uint32_t pending = j == 31 ? 0u : (FULL << (j + 1));
+                        Gs[i] = gk;
+                        __syncwarp();
+                        m = __ballot_sync(FULL, pm1_world_ok(h, Gs, Wc, uw, i, n, NP, B)) & pending;
+                        __syncwarp();
+                    } while (m);
+                    Wold[lane] = wi;
+                    if (lane == 0) { flag[1] = (int)F; flag[2] = qs; }
+                }
+                __syncthreads();
+                const uint32_t F = (uint32_t)flag[1];
+                // later spins: exact correction of their slice sums
+                for (int i = threadIdx.x + (qs + 1) * 32; i < n; i += blockDim.x) {
+                    const unsigned long long wi = Wc[i];
+                    const uint32_t jd = Jw[qs * npad + i];
+                    int dg = 0;
+                    for (uint32_t f = F; f; f &= f - 1) {
+                        const int j = __ffs(f) - 1;
+                        const int overlap = NP - 2 * __popcll(wi ^ Wold[j]);
+                        dg += ((jd >> j) & 1u) ? -2 * overlap : 2 * overlap;
+                    }
+                    Gs[i] += dg;
+                }
+                // every slice: flip the spins F of block qs and update its fields
+                for (int t = warp; t < NP; t += W) {
+                    const uint32_t sold = S[t * nw + qs];
+                    __syncwarp();
+                    if (lane == 0) S[t * nw + qs] = sold ^ F;
+                    pm1_block_update(G + t * npad, Jw, npad, n, qs, F, sold, lane);
+                }
+                if (warp == 0 && ((F >> lane) & 1u)) Wc[(qs << 5) | lane] = Wold[lane] ^ pmask;
+                if (threadIdx.x == 0) acc_w += (unsigned long long)__popc(F);
+                __syncthreads();
+                q0 = qs + 1;
+                if (q0 >= nw) break;
             }
         }
         // ---- step end: slice energies E = c + (sum s h + (sum s g)/2), ring sum, best
@@ -220,7 +310,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
             for (int i = lane; i < n; i += 32) {
                 const bool up = (S[t * nw + (i >> 5)] >> (i & 31)) & 1u;
                 ph = __dadd_rn(ph, up ? (double)h[i] : -(double)h[i]);
-                pg += up ? G[t * n + i] : -G[t * n + i];
+                pg += up ? G[t * npad + i] : -G[t * npad + i];
             }
             ph = warp_sum_d(ph);
             pg = warp_sum_i(pg);
@@ -268,7 +358,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
         __syncthreads();
     }
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) p.spins[R.spin_off + idx] = S[idx];
-    for (int idx = threadIdx.x; idx < NP * n; idx += blockDim.x) Gg[idx] = G[idx];
+    for (int idx = threadIdx.x; idx < NP * npad; idx += blockDim.x) Gg[idx] = G[idx];
     if (lane == 0) {
         atomicAdd(p.counters + 0, att_s);
         atomicAdd(p.counters + 1, acc_s);

@@ -79,6 +79,7 @@ SQA_CASES = [
     ("dense", 512, 32, 1, 1, 1, 2.0),
     ("dense", 100, 64, 1, 1, 2, 0.25),
     ("dense", 33, 3, 1, 2, 3, 0.1),
+    ("dense", 256, 16, 1, 0, 3, 0.05),  # many accepted worldline moves
     ("dense_h", 70, 6, 2, 2, 1, 0.5),
     # the generic field-cache kernel
     ("dense_int", 80, 8, 2, 1, 1, 0.5),
