@@ -132,6 +132,26 @@ typedef struct {
 QA_API int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *params,
                qa_run_out *outs, qa_stats *stats);
 
+/* ---- SA on a dense model without any allocation by this library --------
+ * No counterpart in the reference.  For callers that cannot let a library
+ * call cudaMalloc/cudaFree: their device memory belongs to a framework
+ * allocator (PyTorch's caching allocator, JAX/XLA reserving most of HBM) or
+ * to a fixed serving budget, so an allocation inside the call could fail or
+ * stall them.  The caller passes device pointers: d_h[n], d_J[n*n] (float64,
+ * as for qa_problem_dense) and the outputs d_best_spins[reads*n] (int8),
+ * d_best_energy[reads], d_energy_trace[reads*steps]; params->betas stays a
+ * host array.  The run is the same as qa_sa_run's (bit for bit) and uses a
+ * 16 MiB static device array as scratch (held by every GPU that loads the
+ * library until exit); runs needing more (about 4 n^2 + 8 reads n +
+ * 4 steps bytes) are rejected with QA_ERR_ARG.  The first call on a device
+ * looks up that array's device address: make it before any stream capture.
+ * Calls share the array, so calls that overlap on the GPU race; serialise
+ * them.  stream may be NULL (the legacy default stream); the call returns
+ * after the run has finished on it.  stats may be NULL (counters only). */
+QA_API int qa_sa_dense_run_noalloc(int device, void *stream, int n, const double *d_h, const double *d_J, double c,
+                                   const qa_sa_params *params, int8_t *d_best_spins, double *d_best_energy,
+                                   double *d_energy_trace, qa_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

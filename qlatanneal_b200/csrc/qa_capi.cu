@@ -46,6 +46,14 @@ struct DevBuf {
 
 }  // namespace
 
+namespace qa {
+// Lets the other translation units of the library report through qa_last_error().
+int set_last_error(int code, const char *msg) {
+    g_err = msg;
+    return code;
+}
+}  // namespace qa
+
 struct qa_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;

@@ -73,7 +73,7 @@ __device__ __forceinline__ int phase_slice(int P, int ph, int c) {
 }
 
 // ------------------------------------------------------------------ init
-__global__ void init_spins_kernel(const ProbDev *probs, const RingDev *rings, uint32_t *spins, int P,
+static __global__ void init_spins_kernel(const ProbDev *probs, const RingDev *rings, uint32_t *spins, int P,
                                   uint32_t tag, int nw_max) {
     const RingDev R = rings[blockIdx.x];
     const ProbDev Pd = probs[R.prob];
