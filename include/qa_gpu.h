@@ -132,6 +132,37 @@ typedef struct {
 QA_API int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *params,
                qa_run_out *outs, qa_stats *stats);
 
+/* ---- SQA parallel tempering: SQAParallelTemperingAnnealer::run
+ *      (sqa_parallel_tempering.cpp:81-346) ----------------------------------
+ * rungs (beta_r, Gamma_r) pairs, one Trotter ring per rung, swaps of
+ * neighbouring rungs every swap_interval steps. */
+typedef struct {
+    const double *betas;     /* [rungs] */
+    const double *gammas;    /* [rungs] */
+    int rungs;               /* >= 2 */
+    int trotter_slices;
+    int sweeps_per_step;     /* slice sweeps per step */
+    int worldline_sweeps;
+    int steps;               /* pt_steps */
+    int swap_interval;       /* > 0 */
+    int cluster_sweeps;      /* must be 0 */
+    int continuous_time_slices;
+    int reads;
+    uint64_t seed;
+} qa_sqapt_params;
+
+typedef struct {
+    int8_t *best_spins;              /* [reads][n] */
+    double *best_energy;             /* [reads] */
+    int8_t *final_spins;             /* [reads][rungs][n]  final_states */
+    double *final_energies;          /* [reads][rungs]     projected energies (min over slices) */
+    double *average_energy_trace;    /* [reads][steps] */
+    double *swap_acceptance_trace;   /* [reads][steps] */
+} qa_sqapt_out;
+
+QA_API int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
+                        const qa_sqapt_params *params, qa_sqapt_out *outs, qa_stats *stats);
+
 /* ---- SA on a dense model without any allocation by this library --------
  * No counterpart in the reference.  For callers that cannot let a library
  * call cudaMalloc/cudaFree: their device memory belongs to a framework

@@ -730,3 +730,122 @@ OR_EXPORT int or_sqa_run(const or_model *M, const double *betas, const double *g
     ring_free(&R);
     return 0;
 }
+
+/* Step-end scan of one ring: sum and minimum of the slice energies, the
+   slice of the minimum, and the imaginary-time bond sum
+   B = sum_t sum_i s_t,i s_t+1,i (sqa_parallel_tempering.cpp:128-170). */
+static void ring_scan(ring_t *R, int k, double *sum, double *emin, int *tmin, long long *bond) {
+    const int n = R->n, P = R->P;
+    double s = 0.0, em = INFINITY;
+    int tm = 0;
+    for (int t = 0; t < P; ++t) {
+        double E = cell_energy(R, k * P + t);
+        s += E;
+        if (E < em) { em = E; tm = t; }
+    }
+    long long b = 0;
+    for (int t = 0; t < P; ++t) {
+        const int8_t *a = R->s + ((size_t)k * P + t) * n;
+        const int8_t *c = R->s + ((size_t)k * P + (t + 1) % P) * n;
+        for (int i = 0; i < n; ++i) b += a[i] * c[i];
+    }
+    *sum = s; *emin = em; *tmin = tm; *bond = b;
+}
+
+/* ------------------------------------------------------------------ */
+/* SQA parallel tempering (sqa_parallel_tempering.cpp:81-346), one read  */
+/* Rung r ("slot") keeps its (beta_r, Gamma_r) and its random streams;   */
+/* swaps exchange which ring sits in which slot, pairs r = 0..R-2 in     */
+/* order (cascading), every swap_interval steps.                         */
+/* ------------------------------------------------------------------ */
+OR_EXPORT int or_sqapt_run(const or_model *M, const double *betas, const double *gammas, int Rn, int P, int spb,
+                           int wls, int steps, int swap_interval, uint64_t seed, int read, int8_t *best_spins,
+                           double *best_E, double *final_E, int8_t *final_spins, double *avg_trace,
+                           double *swap_trace, int64_t *counters) {
+    const int n = M->n;
+    ring_t R;
+    ring_alloc(&R, M, P, Rn, seed + (uint64_t)read);
+    ring_init(&R, DOM_INIT);
+    int *slot_of = (int *)malloc(sizeof(int) * (size_t)Rn), *ring_in = (int *)malloc(sizeof(int) * (size_t)Rn);
+    float *B = (float *)malloc(sizeof(float) * (size_t)Rn), *T4 = (float *)malloc(sizeof(float) * (size_t)Rn);
+    double *bp = (double *)malloc(sizeof(double) * (size_t)Rn), *jp = (double *)malloc(sizeof(double) * (size_t)Rn);
+    double *Esum = (double *)malloc(sizeof(double) * (size_t)Rn), *Emin = (double *)malloc(sizeof(double) * (size_t)Rn);
+    int *tmin = (int *)malloc(sizeof(int) * (size_t)Rn);
+    long long *bond = (long long *)malloc(sizeof(long long) * (size_t)Rn);
+    for (int k = 0; k < Rn; ++k) {
+        slot_of[k] = ring_in[k] = k;
+        step_consts(betas[k], gammas[k], P, &B[k], &T4[k]);
+        bp[k] = betas[k] / (double)P;
+        jp[k] = trotter_coupling(betas[k], gammas[k], P);
+    }
+    double best = INFINITY;
+    for (int k = 0; k < Rn; ++k) ring_scan(&R, k, &Esum[k], &Emin[k], &tmin[k], &bond[k]);
+    for (int r = 0; r < Rn; ++r) {
+        const int k = ring_in[r];
+        if (Emin[k] < best) {
+            best = Emin[k];
+            memcpy(best_spins, R.s + ((size_t)k * P + tmin[k]) * n, (size_t)n);
+        }
+    }
+    for (int step = 0; step < steps; ++step) {
+        for (int sw = 0; sw < spb; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * spb + sw);
+            for (int ph = 0; ph < 3; ++ph)
+                for (int k = 0; k < Rn; ++k)
+                    for (int t = 0; t < P; ++t) {
+                        if (phase_of(t, P) != ph) continue;
+                        const int sl = slot_of[k];
+                        sweep_cell(&R, k, t, (uint32_t)(sl * P + t), sigma, DOM_SLICE, B[sl], T4[sl]);
+                    }
+        }
+        for (int sw = 0; sw < wls; ++sw)
+            for (int k = 0; k < Rn; ++k)
+                worldline_sweep(&R, k, (uint32_t)slot_of[k], (uint32_t)(step * wls + sw), B[slot_of[k]]);
+        for (int k = 0; k < Rn; ++k) ring_scan(&R, k, &Esum[k], &Emin[k], &tmin[k], &bond[k]);
+        for (int r = 0; r < Rn; ++r) {
+            const int k = ring_in[r];
+            if (Emin[k] < best) {
+                best = Emin[k];
+                memcpy(best_spins, R.s + ((size_t)k * P + tmin[k]) * n, (size_t)n);
+            }
+        }
+        double acc = 0.0, att = 0.0;
+        if ((step + 1) % swap_interval == 0) {
+            const uint32_t w = (uint32_t)((step + 1) / swap_interval - 1);
+            for (int r = 0; r + 1 < Rn; ++r) {
+                const int a = ring_in[r], b = ring_in[r + 1];
+                const double e_aa = bp[r] * Esum[a] - jp[r] * (double)bond[a];
+                const double e_bb = bp[r + 1] * Esum[b] - jp[r + 1] * (double)bond[b];
+                const double e_ab = bp[r] * Esum[b] - jp[r] * (double)bond[b];
+                const double e_ba = bp[r + 1] * Esum[a] - jp[r + 1] * (double)bond[a];
+                const double delta = (e_ab + e_ba) - (e_aa + e_bb);
+                att += 1.0;
+                const float u = u01(draw(R.key, (uint32_t)r, 0u, w, DOM_SWAP, 0));
+                if (metropolis((float)(-delta), u)) {
+                    ring_in[r] = b;
+                    ring_in[r + 1] = a;
+                    slot_of[b] = r;
+                    slot_of[a] = r + 1;
+                    acc += 1.0;
+                }
+            }
+        }
+        double avg = 0.0;
+        for (int r = 0; r < Rn; ++r) avg += Emin[ring_in[r]];
+        avg_trace[step] = avg / (double)Rn;
+        swap_trace[step] = att > 0.0 ? acc / att : 0.0;
+    }
+    for (int r = 0; r < Rn; ++r) {
+        const int k = ring_in[r];
+        final_E[r] = Emin[k];
+        memcpy(final_spins + (size_t)r * n, R.s + ((size_t)k * P + tmin[k]) * n, (size_t)n);
+    }
+    *best_E = best;
+    if (counters) {
+        counters[0] = R.att_slice; counters[1] = R.acc_slice;
+        counters[2] = R.att_world; counters[3] = R.acc_world;
+    }
+    free(slot_of); free(ring_in); free(B); free(T4); free(bp); free(jp); free(Esum); free(Emin); free(tmin); free(bond);
+    ring_free(&R);
+    return 0;
+}

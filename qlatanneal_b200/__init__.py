@@ -19,9 +19,11 @@ from .models import (  # noqa: F401
 from .annealers import (  # noqa: F401
     AnnealResult,
     SQAResult,
+    SQAParallelTemperingResult,
     RunStats,
     Annealer,
     SQAAnnealer,
+    SQAParallelTemperingAnnealer,
 )
 
 version_major, version_minor, version_patch = 2, 0, 0

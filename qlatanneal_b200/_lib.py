@@ -20,7 +20,7 @@ QA_OK, QA_ERR_ARG, QA_ERR_CUDA, QA_ERR_OOM, QA_ERR_TIMEOUT, QA_ERR_DRIFT, QA_ERR
 EXPORTED = [
     "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy",
     "qa_problem_dense", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
-    "qa_sa_run", "qa_sqa_run",
+    "qa_sa_run", "qa_sqa_run", "qa_sqapt_run",
 ]
 
 
@@ -45,6 +45,19 @@ class qa_sqa_params(C.Structure):
                 ("replicas", C.c_int), ("sweeps_per_beta", C.c_int), ("worldline_sweeps", C.c_int),
                 ("cluster_sweeps", C.c_int), ("continuous_time_slices", C.c_int), ("reads", C.c_int),
                 ("seed", C.c_uint64)]
+
+
+class qa_sqapt_params(C.Structure):
+    _fields_ = [("betas", C.c_void_p), ("gammas", C.c_void_p), ("rungs", C.c_int), ("trotter_slices", C.c_int),
+                ("sweeps_per_step", C.c_int), ("worldline_sweeps", C.c_int), ("steps", C.c_int),
+                ("swap_interval", C.c_int), ("cluster_sweeps", C.c_int), ("continuous_time_slices", C.c_int),
+                ("reads", C.c_int), ("seed", C.c_uint64)]
+
+
+class qa_sqapt_out(C.Structure):
+    _fields_ = [("best_spins", C.c_void_p), ("best_energy", C.c_void_p), ("final_spins", C.c_void_p),
+                ("final_energies", C.c_void_p), ("average_energy_trace", C.c_void_p),
+                ("swap_acceptance_trace", C.c_void_p)]
 
 
 _lib = None
@@ -76,6 +89,8 @@ def load():
                                 C.POINTER(qa_stats)]
         L.qa_sqa_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sqa_params), C.POINTER(qa_run_out),
                                  C.POINTER(qa_stats)]
+        L.qa_sqapt_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sqapt_params), C.POINTER(qa_sqapt_out),
+                                   C.POINTER(qa_stats)]
         for name in list(EXPORTED):
             getattr(L, name)
         _lib = L

@@ -54,6 +54,24 @@ class SQAResult:
 
 
 @dataclass
+class SQAParallelTemperingResult:
+    """``qanneal.SQAParallelTemperingResult`` (sqa_parallel_tempering.hpp:15-29);
+    the run_optimal diagnostics stay empty."""
+    final_states: List[State]
+    final_energies: List[float]
+    best_state: State
+    best_energy: float
+    average_energy_trace: List[float]
+    swap_acceptance_trace: List[float]
+    j_perp_trace: List[float] = field(default_factory=list)
+    chi_B_trace: List[float] = field(default_factory=list)
+    calibrated_eps_tilde: float = 0.0
+    j_perp_start: float = 0.0
+    resolved_j_perp_end: float = 0.0
+    final_j_perp: float = 0.0
+
+
+@dataclass
 class RunStats:
     """Device-side totals of one batched call (qa_stats)."""
     slice_attempts: int = 0
@@ -181,3 +199,61 @@ class SQAAnnealer(_Seeded):
         _lib.check(eng.L.qa_sqa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         return [SQAResult(State(spins[r]), float(energies[r]), trace[r].tolist()) for r in range(reads)]
+
+
+class SQAParallelTemperingAnnealer(_Seeded):
+    """``qanneal.SQAParallelTemperingAnnealer(hamiltonian, betas, gammas, trotter_slices, backend)``
+    (sqa_parallel_tempering.cpp:81-346): one Trotter ring per (beta, Gamma) rung,
+    swaps of neighbouring rungs every ``swap_interval`` steps."""
+
+    def __init__(self, hamiltonian, betas: Sequence[float], gammas: Sequence[float], trotter_slices: int,
+                 backend: str = "cuda", device: Optional[int] = None):
+        super().__init__()
+        _check_backend(backend)
+        if hamiltonian is None:
+            raise ValueError("SQAParallelTemperingAnnealer requires a backend.")
+        if len(betas) < 2 or len(betas) != len(gammas):
+            raise ValueError("SQA parallel tempering requires >=2 beta/gamma pairs.")
+        if trotter_slices <= 0:
+            raise ValueError("trotter_slices must be > 0.")
+        self.hamiltonian = hamiltonian
+        self.betas = [float(b) for b in betas]
+        self.gammas = [float(g) for g in gammas]
+        self.trotter_slices = int(trotter_slices)
+        self.device = device
+        self.last_stats: Optional[RunStats] = None
+
+    def run(self, sweeps_per_step: int, worldline_sweeps: int, steps: int, swap_interval: int = 1,
+            cluster_sweeps: int = 0, continuous_time_slices: int = 0) -> SQAParallelTemperingResult:
+        return self.run_reads(sweeps_per_step, worldline_sweeps, steps, swap_interval, cluster_sweeps,
+                              continuous_time_slices, reads=1)[0]
+
+    def run_reads(self, sweeps_per_step: int, worldline_sweeps: int, steps: int, swap_interval: int = 1,
+                  cluster_sweeps: int = 0, continuous_time_slices: int = 0, reads: int = 1,
+                  seed: Optional[int] = None) -> List[SQAParallelTemperingResult]:
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        betas = np.ascontiguousarray(self.betas, dtype=np.float64)
+        gammas = np.ascontiguousarray(self.gammas, dtype=np.float64)
+        R = len(betas)
+        seed = self._next_seed(reads) if seed is None else int(seed)
+        prm = _lib.qa_sqapt_params(betas.ctypes.data, gammas.ctypes.data, R, self.trotter_slices,
+                                   int(sweeps_per_step), int(worldline_sweeps), int(steps), int(swap_interval),
+                                   int(cluster_sweeps), int(continuous_time_slices), int(reads), seed)
+        n = self.hamiltonian.size()
+        steps_ = max(int(steps), 1)
+        best = np.zeros((reads, n), np.int8)
+        bestE = np.zeros(reads)
+        fin = np.zeros((reads, R, n), np.int8)
+        finE = np.zeros((reads, R))
+        avg = np.zeros((reads, steps_))
+        swp = np.zeros((reads, steps_))
+        o = _lib.qa_sqapt_out(best.ctypes.data, bestE.ctypes.data, fin.ctypes.data, finE.ctypes.data,
+                              avg.ctypes.data, swp.ctypes.data)
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_sqapt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        return [SQAParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
+                                           float(bestE[r]), avg[r].tolist(), swp[r].tolist())
+                for r in range(reads)]

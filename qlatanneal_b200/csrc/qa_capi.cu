@@ -12,6 +12,7 @@
 #include "qa_gpu.h"
 #include "qa_kernels.cuh"
 #include "qa_pm1.cuh"
+#include "qa_pt.cuh"
 
 using namespace qa;
 
@@ -59,7 +60,7 @@ struct qa_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int smem_optin = 0;
-    DevBuf ws[16];
+    DevBuf ws[32];
 };
 
 struct qa_problem {
@@ -73,7 +74,7 @@ struct qa_problem {
 namespace {
 
 enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
-              W_PROBOF, W_MIN, W_BOND, W_MAG };
+              W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP };
 
 int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
     DevBuf &b = ctx->ws[slot];
@@ -233,6 +234,64 @@ int exact_energies(qa_ctx *ctx, int kind, const ProbDev *d_probs, const Layout &
         if (cudaGetLastError() != cudaSuccess) rc = fail(QA_ERR_CUDA, "exact_energy_kernel launch failed");
     });
     return rc;
+}
+
+// Which ring kernel a batch runs on, and with what launch shape.
+struct RingPlan {
+    bool pm1 = false;
+    int W = 1;
+    size_t smem = 0;
+    int smem_fields = 1;
+};
+
+int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, int P, int n_max, RingPlan *pl) {
+    pl->W = std::max(1, std::min(32, (P + 1) / 2));
+    pl->pm1 = kind == K_DENSE && P <= 64 && n_max <= 1024 &&
+              pm1_smem_bytes(P, n_max) <= (size_t)ctx->smem_optin && !std::getenv("QA_DISABLE_PM1");
+    for (int p = 0; p < np && pl->pm1; ++p) pl->pm1 = probs[p]->dev.Jw != nullptr;
+    if (pl->pm1) {
+        pl->smem = pm1_smem_bytes(P, n_max);
+        pl->smem_fields = 0;
+        return QA_OK;
+    }
+    pl->smem = ring_smem_bytes(P, n_max, pl->W, true);
+    pl->smem_fields = 1;
+    if (pl->smem > (size_t)std::min(ctx->smem_optin, 200 * 1024)) {
+        pl->smem_fields = 0;
+        pl->smem = ring_smem_bytes(P, n_max, pl->W, false);
+    }
+    if (pl->smem > (size_t)ctx->smem_optin) return fail(QA_ERR_ARG, "ring state does not fit in shared memory.");
+    return QA_OK;
+}
+
+// One launch of the planned ring kernel over steps [rp.step0, rp.step1).
+int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n_rings) {
+    rp.W = pl.W;
+    rp.smem_fields = pl.smem_fields;
+    if (pl.pm1) {
+        if (pl.smem > 48 * 1024)
+            QA_CK(cudaFuncSetAttribute(ring_pm1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        ring_pm1_kernel<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
+        QA_CK(cudaGetLastError());
+        return QA_OK;
+    }
+    int rc = QA_OK;
+    dispatch_kind(kind, [&](auto Kd) {
+        auto kern = ring_kernel<decltype(Kd)::value>;
+        if (pl.smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+        kern<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, std::string("ring_kernel launch: ") + cudaGetErrorString(e));
+    });
+    return rc;
+}
+
+template <class T>
+int ws_array(qa_ctx *ctx, int slot, size_t count, T **out) {
+    void *v;
+    QA_TRY(ws_get(ctx, slot, sizeof(T) * count, &v));
+    *out = static_cast<T *>(v);
+    return QA_OK;
 }
 
 }  // namespace
@@ -646,6 +705,8 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     rp.smem_fields = smem_fields; rp.ring_sum = d_sum; rp.ring_min = nullptr; rp.ring_bond = nullptr;
     rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max; rp.mag = nullptr;
     rp.counters = d_cnt;
+    rp.rec_base = 0;
+    rp.rec_stride = steps;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     int rc = QA_OK;
     const int seg = 256;
@@ -732,6 +793,196 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
                                      (sizeof(double) + sizeof(int)) * nr + sizeof(int) * nr);
         stats->d2h_bytes = (int64_t)(sizeof(double) * sums.size() + (2 * sizeof(double) + sizeof(int)) * nr +
                                      sizeof(uint32_t) * bits.size() + sizeof(cnt));
+    }
+    return QA_OK;
+}
+
+// ---------------------------------------------------------------------- SQA-PT
+int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqapt_params *prm,
+                 qa_sqapt_out *outs, qa_stats *stats) {
+    QA_TRY(begin(ctx));
+    if (!prm) return fail(QA_ERR_ARG, "null params");
+    if (prm->rungs < 2 || !prm->betas || !prm->gammas)
+        return fail(QA_ERR_ARG, "SQA parallel tempering requires >=2 beta/gamma pairs.");
+    if (prm->trotter_slices <= 0) return fail(QA_ERR_ARG, "trotter_slices must be > 0.");
+    if (prm->steps <= 0) return fail(QA_ERR_ARG, "steps must be > 0.");
+    if (prm->swap_interval <= 0) return fail(QA_ERR_ARG, "swap_interval must be > 0.");
+    if (prm->sweeps_per_step < 0 || prm->worldline_sweeps < 0 || prm->cluster_sweeps < 0)
+        return fail(QA_ERR_ARG, "sweep counts must be >= 0.");
+    if (prm->sweeps_per_step == 0 && prm->worldline_sweeps == 0 && prm->cluster_sweeps == 0)
+        return fail(QA_ERR_ARG, "At least one of sweeps_per_step/worldline_sweeps/cluster_sweeps must be > 0.");
+    if (prm->cluster_sweeps > 0)
+        return fail(QA_ERR_UNSUPPORTED, "cluster_sweeps > 0 is not supported by the CUDA sweep engine.");
+    if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
+    int kind, n_max;
+    QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
+    const int P = (prm->continuous_time_slices > 0 && prm->continuous_time_slices > prm->trotter_slices)
+                      ? prm->continuous_time_slices
+                      : prm->trotter_slices;
+    const int Rn = prm->rungs, steps = prm->steps, reads_total = n_problems * prm->reads;
+    Layout L;
+    build_rings(L, problems, n_problems, prm->reads, Rn, P, prm->seed);
+    const int nr = (int)L.rings.size();
+    ProbDev *d_probs;
+    RingDev *d_rings;
+    uint32_t *d_spins;
+    float *d_fields;
+    QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
+    std::vector<float> B(Rn), T4(Rn);
+    std::vector<double> bpjp(2 * Rn);
+    for (int r = 0; r < Rn; ++r) {
+        B[r] = (float)(2.0 * (prm->betas[r] / (double)P));
+        T4[r] = (float)(4.0 * trotter_coupling(prm->betas[r], prm->gammas[r], P));
+        bpjp[r] = prm->betas[r] / (double)P;
+        bpjp[Rn + r] = trotter_coupling(prm->betas[r], prm->gammas[r], P);
+    }
+    float *d_B, *d_T4;
+    double *d_bpjp, *d_sum, *d_min, *d_best, *d_exact, *d_avg, *d_swp;
+    long long *d_bond;
+    int *d_bstep, *d_bslot, *d_slot, *d_rin;
+    uint32_t *d_bits, *d_fbits;
+    unsigned long long *d_cnt;
+    const size_t rec = (size_t)nr * (steps + 1);
+    QA_TRY(ws_array(ctx, W_A, Rn, &d_B));
+    QA_TRY(ws_array(ctx, W_T4, Rn, &d_T4));
+    QA_TRY(ws_array(ctx, W_BPJP, 2 * Rn, &d_bpjp));
+    QA_TRY(ws_array(ctx, W_SUM, rec, &d_sum));
+    QA_TRY(ws_array(ctx, W_MIN, rec, &d_min));
+    QA_TRY(ws_array(ctx, W_BOND, rec, &d_bond));
+    QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
+    QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
+    QA_TRY(ws_array(ctx, W_BSLOT, nr, &d_bslot));
+    QA_TRY(ws_array(ctx, W_SLOT, nr, &d_slot));
+    QA_TRY(ws_array(ctx, W_RIN, (size_t)reads_total * Rn, &d_rin));
+    QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
+    QA_TRY(ws_array(ctx, W_FBITS, (size_t)nr * L.nw_max, &d_fbits));
+    QA_TRY(ws_array(ctx, W_EXACT, nr, &d_exact));
+    QA_TRY(ws_array(ctx, W_AVG, (size_t)reads_total * steps, &d_avg));
+    QA_TRY(ws_array(ctx, W_SWP, (size_t)reads_total * steps, &d_swp));
+    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    {
+        std::vector<double> inf(nr, INFINITY);
+        std::vector<int> neg(nr, -2), slot(nr), rin((size_t)reads_total * Rn);
+        for (int i = 0; i < nr; ++i) slot[i] = L.rings[i].k;
+        for (size_t i = 0; i < rin.size(); ++i) rin[i] = (int)(i % Rn);
+        QA_CK(cudaMemcpyAsync(d_B, B.data(), sizeof(float) * Rn, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * Rn, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_bpjp, bpjp.data(), sizeof(double) * 2 * Rn, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_bstep, neg.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_bslot, slot.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_slot, slot.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_rin, rin.data(), sizeof(int) * rin.size(), cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+        QA_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    RingPlan pl;
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
+    QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.pm1));
+    RingParams rp{};
+    rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
+    rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_step; rp.wls = prm->worldline_sweeps;
+    rp.slice_tag = DOM_SLICE; rp.slot = d_slot; rp.B = d_B; rp.T4 = d_T4; rp.per_slot_sched = 1;
+    rp.ring_sum = d_sum; rp.ring_min = d_min; rp.ring_bond = d_bond; rp.rec_base = 1; rp.rec_stride = steps + 1;
+    rp.best_E = d_best; rp.best_step = d_bstep; rp.best_slot = d_bslot; rp.best_bits = d_bits;
+    rp.final_bits = d_fbits; rp.nw_max = L.nw_max; rp.counters = d_cnt;
+    PTSegParams sp{};
+    sp.rings = d_rings; sp.reads = reads_total; sp.R = Rn; sp.bp = d_bpjp; sp.jp = d_bpjp + Rn;
+    sp.ring_sum = d_sum; sp.ring_min = d_min; sp.ring_bond = d_bond; sp.rec_base = 1; sp.rec_stride = steps + 1;
+    sp.ring_in = d_rin; sp.slot_of = d_slot; sp.avg_trace = d_avg; sp.swap_trace = d_swp; sp.steps_total = steps;
+    QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    int n_seg = 0;
+    float ring_ms = 0.0f;
+    for (int s0 = 0; s0 < steps;) {
+        const int s1 = std::min({steps, (s0 / prm->swap_interval + 1) * prm->swap_interval, s0 + 256});
+        rp.step0 = s0;
+        rp.step1 = s1;
+        rp.init_scan = s0 == 0;
+        rp.init_fields = s0 == 0;
+        QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+        sp.s0 = s0;
+        sp.s1 = s1;
+        sp.swap = s1 % prm->swap_interval == 0;
+        sp.round = (uint32_t)(s1 / prm->swap_interval - 1);
+        pt_segment_kernel<<<(reads_total + 127) / 128, 128, 0, ctx->stream>>>(sp);
+        QA_CK(cudaGetLastError());
+        ++n_seg;
+        s0 = s1;
+    }
+    QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
+    QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    (void)ring_ms;
+
+    std::vector<double> bestE(nr), exact(nr), lastmin(nr), avg((size_t)reads_total * steps),
+        swp((size_t)reads_total * steps);
+    std::vector<int> bstep(nr), bslot(nr), rin((size_t)reads_total * Rn);
+    std::vector<uint32_t> bits((size_t)nr * L.nw_max), fbits((size_t)nr * L.nw_max);
+    unsigned long long cnt[4];
+    QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpy2DAsync(lastmin.data(), sizeof(double), d_min + steps, sizeof(double) * (steps + 1),
+                            sizeof(double), nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(avg.data(), d_avg, sizeof(double) * avg.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(swp.data(), d_swp, sizeof(double) * swp.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bstep.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bslot.data(), d_bslot, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(rin.data(), d_rin, sizeof(int) * rin.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(fbits.data(), d_fbits, sizeof(uint32_t) * fbits.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+
+    // best of a read: lowest energy, then earliest step (the starting state is
+    // step -1), then lowest slot -- the (step, slot) scan order of
+    // sqa_parallel_tempering.cpp:177-185, 299-306
+    for (int p = 0; p < n_problems; ++p) {
+        const int n = problems[p]->n;
+        qa_sqapt_out &o = outs[p];
+        for (int r = 0; r < prm->reads; ++r) {
+            const int q = p * prm->reads + r, base = q * Rn;
+            int kb = 0;
+            for (int k = 1; k < Rn; ++k) {
+                const int a = base + k, b = base + kb;
+                if (bestE[a] < bestE[b] || (bestE[a] == bestE[b] && (bstep[a] < bstep[b] ||
+                                                                     (bstep[a] == bstep[b] && bslot[a] < bslot[b]))))
+                    kb = k;
+            }
+            if (o.best_spins) unpack_bits(bits.data() + (size_t)(base + kb) * L.nw_max, n, o.best_spins + (size_t)r * n);
+            if (o.best_energy) o.best_energy[r] = exact[base + kb];
+            for (int s = 0; s < Rn; ++s) {
+                const int k = rin[(size_t)q * Rn + s];
+                if (o.final_energies) o.final_energies[(size_t)r * Rn + s] = lastmin[base + k];
+                if (o.final_spins)
+                    unpack_bits(fbits.data() + (size_t)(base + k) * L.nw_max, n,
+                                o.final_spins + ((size_t)r * Rn + s) * n);
+            }
+            if (o.average_energy_trace)
+                std::memcpy(o.average_energy_trace + (size_t)r * steps, avg.data() + (size_t)q * steps,
+                            sizeof(double) * steps);
+            if (o.swap_acceptance_trace)
+                std::memcpy(o.swap_acceptance_trace + (size_t)r * steps, swp.data() + (size_t)q * steps,
+                            sizeof(double) * steps);
+        }
+    }
+    if (stats) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]);
+        stats->slice_attempts = (int64_t)cnt[0];
+        stats->slice_accepts = (int64_t)cnt[1];
+        stats->worldline_attempts = (int64_t)cnt[2];
+        stats->worldline_accepts = (int64_t)cnt[3];
+        stats->sweep_ms = a;
+        stats->total_ms = b;
+        stats->sweep_launches = n_seg;
+        stats->launches = (pl.pm1 ? 2 : 3) + 2 * n_seg;
+        stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * Rn +
+                                     2 * sizeof(double) * Rn + (sizeof(double) + 3 * sizeof(int)) * nr +
+                                     sizeof(int) * rin.size());
+        stats->d2h_bytes = (int64_t)(sizeof(double) * (3 * nr + avg.size() + swp.size()) + 3 * sizeof(int) * nr +
+                                     sizeof(int) * rin.size() + sizeof(uint32_t) * 2 * bits.size() + sizeof(cnt));
     }
     return QA_OK;
 }

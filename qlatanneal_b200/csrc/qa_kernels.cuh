@@ -49,13 +49,18 @@ struct RingParams {
     int per_slot_sched;   // 1: index A/T4 by slot instead of step
     int smem_fields;
     int init_fields;      // ring_pm1_kernel: build the int32 fields from the spins first
+    int init_scan;        // score the starting state as "step -1" before step0 (PT)
+    int rec_base;         // per-step records live at [ring][rec_base + step]
+    int rec_stride;       //   with this row stride
     // outputs
-    double *ring_sum;     // [ring][steps_total]  sum of slice energies
-    double *ring_min;     // [ring][steps_total]  min slice energy (PT projected energy), may be null
-    long long *ring_bond; // [ring][steps_total]  imaginary-time bond sum B, may be null
+    double *ring_sum;     // sum of slice energies per (ring, step)
+    double *ring_min;     // min slice energy (PT projected energy) per (ring, step), may be null
+    long long *ring_bond; // imaginary-time bond sum B per (ring, step), may be null
     double *best_E;       // [ring]
     int *best_step;       // [ring]
+    int *best_slot;       // [ring] slot the ring held at its best step, may be null
     uint32_t *best_bits;  // [ring][nw_max]
+    uint32_t *final_bits; // [ring][nw_max] min-energy slice after the last step, may be null
     int nw_max;
     int *mag;             // [ring][sweeps] spin sums after each sweep (chi pilot), may be null
     unsigned long long *counters;  // [4]
@@ -292,10 +297,12 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     double bestE = p.best_E[blockIdx.x];
     int bestStep = p.best_step[blockIdx.x];
 
-    for (int step = p.step0; step < p.step1; ++step) {
-        const int si_tab = R.sched + (p.per_slot_sched ? slot : step);
+    for (int step = p.step0 - (p.init_scan ? 1 : 0); step < p.step1; ++step) {
+        // step -1 (init_scan) only scores the starting state
+        const int spb = step >= 0 ? p.spb : 0, wls = step >= 0 ? p.wls : 0;
+        const int si_tab = R.sched + (p.per_slot_sched ? slot : max(step, 0));
         const float B = p.B[si_tab], T4 = p.T4[si_tab];
-        for (int sw = 0; sw < p.spb; ++sw) {
+        for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
             for (int ph = 0; ph < 3; ++ph) {
                 const int cnt = phase_count(NP, ph);
@@ -320,7 +327,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                 __syncthreads();
             }
         }
-        for (int sw = 0; sw < p.wls; ++sw) {
+        for (int sw = 0; sw < wls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
             U4 rnd = {0, 0, 0, 0};
             for (int q = 0; q < nw; ++q) {
@@ -400,7 +407,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                 sum = __dadd_rn(sum, E);
                 if (E < emin) { emin = E; tmin = t; }
             }
-            const long long ro = (long long)blockIdx.x * p.steps_total + step;
+            const long long ro = (long long)blockIdx.x * p.rec_stride + p.rec_base + step;
             if (p.ring_sum) p.ring_sum[ro] = sum;
             if (p.ring_min) p.ring_min[ro] = emin;
             if (p.ring_bond) {
@@ -409,6 +416,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                 p.ring_bond[ro] = tb;
             }
             sm.flag[0] = -1;
+            sm.flag[1] = tmin;
             if (emin < bestE) {
                 bestE = emin;
                 bestStep = step;
@@ -420,9 +428,13 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
         if (tb >= 0) {
             bestE = sm.cellE[tb];
             bestStep = step;
+            if (threadIdx.x == 0 && p.best_slot) p.best_slot[blockIdx.x] = slot;
             for (int q = threadIdx.x; q < nw; q += blockDim.x)
                 p.best_bits[(long long)blockIdx.x * p.nw_max + q] = sm.S[tb * nw + q];
         }
+        if (p.final_bits && step == p.steps_total - 1)
+            for (int q = threadIdx.x; q < nw; q += blockDim.x)
+                p.final_bits[(long long)blockIdx.x * p.nw_max + q] = sm.S[sm.flag[1] * nw + q];
         __syncthreads();
     }
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) p.spins[R.spin_off + idx] = sm.S[idx];

@@ -193,10 +193,12 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     double bestE = p.best_E[blockIdx.x];
     int bestStep = p.best_step[blockIdx.x];
 
-    for (int step = p.step0; step < p.step1; ++step) {
-        const int si_tab = R.sched + (p.per_slot_sched ? slot : step);
+    for (int step = p.step0 - (p.init_scan ? 1 : 0); step < p.step1; ++step) {
+        // step -1 (init_scan) only scores the starting state
+        const int spb = step >= 0 ? p.spb : 0, wls = step >= 0 ? p.wls : 0;
+        const int si_tab = R.sched + (p.per_slot_sched ? slot : max(step, 0));
         const float B = p.B[si_tab], T4 = p.T4[si_tab];
-        for (int sw = 0; sw < p.spb; ++sw) {
+        for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
             for (int ph = 0; ph < 3; ++ph) {
                 const int cnt = phase_count(NP, ph);
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 __syncthreads();
             }
         }
-        for (int sw = 0; sw < p.wls; ++sw) {
+        for (int sw = 0; sw < wls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
             // slice sums and uniforms of every spin (thread per spin; a warp
             // holds one 32-spin block, so lane == spin & 31)
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 sum = __dadd_rn(sum, E);
                 if (E < emin) { emin = E; tmin = t; }
             }
-            const long long ro = (long long)blockIdx.x * p.steps_total + step;
+            const long long ro = (long long)blockIdx.x * p.rec_stride + p.rec_base + step;
             if (p.ring_sum) p.ring_sum[ro] = sum;
             if (p.ring_min) p.ring_min[ro] = emin;
             if (p.ring_bond) {
@@ -346,15 +348,20 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 p.ring_bond[ro] = tb;
             }
             flag[0] = emin < bestE ? tmin : -1;
+            flag[3] = tmin;
         }
         __syncthreads();
         const int tb = flag[0];
         if (tb >= 0) {
             bestE = cellE[tb];
             bestStep = step;
+            if (threadIdx.x == 0 && p.best_slot) p.best_slot[blockIdx.x] = slot;
             for (int q = threadIdx.x; q < nw; q += blockDim.x)
                 p.best_bits[(long long)blockIdx.x * p.nw_max + q] = S[tb * nw + q];
         }
+        if (p.final_bits && step == p.steps_total - 1)
+            for (int q = threadIdx.x; q < nw; q += blockDim.x)
+                p.final_bits[(long long)blockIdx.x * p.nw_max + q] = S[flag[3] * nw + q];
         __syncthreads();
     }
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) p.spins[R.spin_off + idx] = S[idx];

@@ -77,9 +77,8 @@ class Oracle:
                                 _f8p, _i64p]
         L.or_sqa_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
                                  C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i64p]
-        for name in ("or_sqapt_run", "or_chi_run"):
-            if hasattr(L, name):
-                pass
+        L.or_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i8p, _f8p, _f8p, _i64p]
 
     # ---- primitives
     def philox(self, ctr, key):
@@ -169,6 +168,21 @@ class Oracle:
         cnt = np.zeros(4, np.int64)
         self.L.or_sqa_run(m.h, betas, gammas, len(betas), P, K, spb, wls, seed, read, best, C.byref(E), trace, cnt)
         return best, E.value, trace, cnt
+
+    def sqapt_run(self, m, betas, gammas, P, spb, wls, steps, swap_interval, seed, read=0):
+        """Returns (best, best_E, final_E[R], final_spins[R][n], avg_trace, swap_trace, counters)."""
+        betas, gammas = _c64(betas), _c64(gammas)
+        R = len(betas)
+        best = np.zeros(m.n, np.int8)
+        E = C.c_double()
+        fE = np.zeros(R)
+        fs = np.zeros(R * m.n, np.int8)
+        avg = np.zeros(steps)
+        swp = np.zeros(steps)
+        cnt = np.zeros(4, np.int64)
+        self.L.or_sqapt_run(m.h, betas, gammas, R, P, spb, wls, steps, swap_interval, seed, read, best, C.byref(E),
+                            fE, fs, avg, swp, cnt)
+        return best, E.value, fE, fs.reshape(R, m.n), avg, swp, cnt
 
 
 class Ref:
@@ -291,6 +305,18 @@ class RefModel:
         if self.ref.L.ref_sqa_run(self.h, betas, gammas, len(betas), P, K, spb, wls, seed, best, C.byref(E), tr) != 0:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return best, E.value, tr
+
+    def sqapt_run(self, betas, gammas, P, spb, wls, steps, swap_interval, seed):
+        betas, gammas = _c64(betas), _c64(gammas)
+        R = len(betas)
+        best = np.zeros(self.n, np.int8)
+        E = C.c_double()
+        fE, avg, swp = np.zeros(R), np.zeros(steps), np.zeros(steps)
+        rc = self.ref.L.ref_sqapt_run(self.h, betas, gammas, R, P, spb, wls, steps, swap_interval, seed, best,
+                                      C.byref(E), fE, avg, swp)
+        if rc != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return best, E.value, fE, avg, swp
 
     def batch_run(self, method, betas, gammas, steps, P, K, spb, wls, reads, seed, threads):
         out = np.zeros(reads)

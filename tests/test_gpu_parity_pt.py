@@ -1,0 +1,73 @@
+"""SQA parallel tempering on the GPU against the CPU restatement, bit for bit.
+
+Covers the ladder sweeps (per-rung beta/Gamma and random streams), the
+cascading replica swaps with the path-integral action, the starting-state
+scoring, the average-energy and swap-acceptance traces and the final states.
+"""
+import numpy as np
+import pytest
+
+import qlatanneal_b200 as qa
+from qlatanneal_b200.instances import hubo_random, regular3, sk_dense
+from test_gpu_parity_sa_sqa import make, oracle_model
+
+pytestmark = pytest.mark.gpu
+
+PT_CASES = [
+    # kind, n, P, rungs, spb, wls, steps, swap_interval
+    ("dense", 64, 8, 4, 1, 1, 12, 1),
+    ("dense", 96, 5, 3, 2, 1, 10, 3),
+    ("dense_int", 48, 6, 5, 1, 1, 9, 2),
+    ("sparse", 100, 4, 6, 2, 1, 8, 2),
+    ("hubo", 40, 4, 3, 1, 1, 7, 1),
+]
+
+
+@pytest.mark.parametrize("kind,n,P,R,spb,wls,steps,swap", PT_CASES)
+def test_sqapt_bit_exact(oracle, kind, n, P, R, spb, wls, steps, swap):
+    model = make(kind, n, 31)
+    om = oracle_model(oracle, model)
+    betas = np.geomspace(0.3, 3.0, R) * P / 8.0
+    gammas = np.linspace(2.5, 0.05, R)
+    reads, seed = 3, 2468
+    ann = qa.SQAParallelTemperingAnnealer(model, betas, gammas, P)
+    res = ann.run_reads(spb, wls, steps, swap, reads=reads, seed=seed)
+    swaps_seen = 0.0
+    for r in range(reads):
+        best, E, fE, fs, avg, swp, cnt = oracle.sqapt_run(om, betas, gammas, P, spb, wls, steps, swap, seed, r)
+        np.testing.assert_array_equal(res[r].best_state.as_array(), best)
+        assert res[r].best_energy == E
+        np.testing.assert_array_equal(np.asarray(res[r].final_energies), fE)
+        for k in range(R):
+            np.testing.assert_array_equal(res[r].final_states[k].as_array(), fs[k])
+        np.testing.assert_array_equal(np.asarray(res[r].average_energy_trace), avg)
+        np.testing.assert_array_equal(np.asarray(res[r].swap_acceptance_trace), swp)
+        swaps_seen += float(np.sum(swp))
+    assert swaps_seen > 0.0  # the ladder actually exchanged states
+
+
+def test_reference_sqapt_shapes():
+    """tests/test_sqa_parallel_tempering.cpp: n=3, 3 rungs, P=8, 5 steps."""
+    h = np.zeros(3)
+    J = np.array([[0.0, 0.5, -0.2], [0.5, 0.0, 0.3], [-0.2, 0.3, 0.0]])
+    ham = qa.DenseIsing(h, J)
+    ann = qa.SQAParallelTemperingAnnealer(ham, [0.2, 0.5, 1.0], [2.0, 1.0, 0.5], 8)
+    ann.set_seed(123)
+    res = ann.run(4, 1, 5, 1)
+    assert len(res.final_states) == 3 and len(res.final_energies) == 3
+    assert len(res.average_energy_trace) == 5 and len(res.swap_acceptance_trace) == 5
+    assert abs(ham.energy(res.best_state.spins) - res.best_energy) < 1e-12
+
+
+def test_sqapt_argument_errors():
+    h, J = sk_dense(8, 1)
+    m = qa.DenseIsing(h, J)
+    with pytest.raises(ValueError):
+        qa.SQAParallelTemperingAnnealer(m, [1.0], [1.0], 4)
+    ann = qa.SQAParallelTemperingAnnealer(m, [1.0, 2.0], [1.0, 0.5], 4)
+    with pytest.raises(ValueError):
+        ann.run(1, 1, 0)
+    with pytest.raises(ValueError):
+        ann.run(1, 1, 5, 0)
+    with pytest.raises(NotImplementedError):
+        ann.run(1, 1, 5, 1, cluster_sweeps=1)

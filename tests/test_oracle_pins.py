@@ -142,6 +142,24 @@ def test_sa_restatement_matches_reference_statistics(oracle, ref):
     assert abs(mo - mr) <= 1.5 * (co + cr), (mo, co, mr, cr)
 
 
+def test_sqapt_restatement_matches_reference_statistics(oracle, ref):
+    """Replay-model SQA-PT vs qanneal's SQAParallelTemperingAnnealer: final
+    average projected energy and mean swap acceptance inside 95% CIs."""
+    h, J = sk_dense(24, 7)
+    m, rm = oracle.dense(h, J), ref.dense(h, J)
+    betas = np.geomspace(0.3, 3.0, 4)
+    gammas = np.linspace(2.0, 0.1, 4)
+    P, steps = 6, 8
+    eo, er, so, sr = [], [], [], []
+    for k in range(250):
+        o = oracle.sqapt_run(m, betas, gammas, P, 1, 1, steps, 2, 100, k)
+        r = rm.sqapt_run(betas, gammas, P, 1, 1, steps, 2, 7000 + k)
+        eo.append(o[4][-1]); er.append(r[3][-1]); so.append(o[5].sum()); sr.append(r[4].sum())
+    for a, b in ((eo, er), (so, sr)):
+        (ma, ca), (mb, cb) = _ci95(a), _ci95(b)
+        assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
+
+
 def test_sqa_restatement_matches_reference_statistics(oracle, ref):
     h, J = sk_dense(32, 6)
     m, rm = oracle.dense(h, J), ref.dense(h, J)
