@@ -163,6 +163,47 @@ typedef struct {
 QA_API int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
                         const qa_sqapt_params *params, qa_sqapt_out *outs, qa_stats *stats);
 
+/* ---- SQA-Chi: SQAChiAnnealer::run_chi (sqa_chi_annealer.cpp:146-438) -----
+ * Stage 1, the pilot chi_B scan (scan_points fresh worldlines per read, all
+ * reads and points in one launch); Stage 2, the schedule built from the curve
+ * (host, float64, as the reference does); Stage 3, the production anneal.
+ * With scan_chi_in != NULL, Stage 1 is skipped and scan_chi_in
+ * [reads][scan_points] is used as the chi_B curve of each read (a predicted
+ * curve; the learned-schedule path). */
+typedef struct {
+    int trotter_slices;
+    int replicas;
+    double beta, gamma_start, gamma_end;
+    int num_steps;            /* >= 2 */
+    int sweeps_per_step;      /* > 0 */
+    int scan_points;          /* >= 4 */
+    int scan_sweeps;          /* > 0 */
+    int scan_burn;
+    double chi_floor_fraction;
+    double driver_A0;         /* <= 0: gamma_start */
+    double beta_ramp_fraction;
+    double beta_ramp_start;
+    int reads;
+    uint64_t seed;
+    const double *scan_chi_in;
+} qa_chi_params;
+
+typedef struct {
+    int8_t *best_spins;       /* [reads][n] */
+    double *best_energy;      /* [reads] */
+    double *energy_trace;     /* [reads][num_steps] mean slice energy per step */
+    double *beta_schedule;    /* [reads][num_steps] */
+    double *gamma_schedule;   /* [reads][num_steps] */
+    double *s_schedule;       /* [reads][num_steps] */
+    double *scan_s;           /* [reads][scan_points] */
+    double *scan_gamma;       /* [reads][scan_points] */
+    double *scan_chi_B;       /* [reads][scan_points] */
+    double *scalars;          /* [reads][5]: s_star, gamma_star, j_perp_star, chi_floor, driver_A0 */
+} qa_chi_out;
+
+QA_API int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_chi_params *params,
+                      qa_chi_out *outs, qa_stats *stats);
+
 /* ---- SA on a dense model without any allocation by this library --------
  * No counterpart in the reference.  For callers that cannot let a library
  * call cudaMalloc/cudaFree: their device memory belongs to a framework

@@ -849,3 +849,191 @@ OR_EXPORT int or_sqapt_run(const or_model *M, const double *betas, const double 
     ring_free(&R);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* SQA-Chi (sqa_chi_annealer.cpp:146-438), one read                     */
+/* ------------------------------------------------------------------ */
+static double chi_s_to_gamma(double A0, double s) {
+    s = s < 1e-10 ? 1e-10 : s;
+    s = s > 1.0 - 1e-10 ? 1.0 - 1e-10 : s;
+    return A0 * (1.0 - s) / s;
+}
+
+/* Stage 2 (sqa_chi_annealer.cpp:283-387): the chi_B peak, the floor, the
+   4096-point trapezoid CDF of w(s) = max(chi_B(s), floor) and its inverse at
+   uniform targets, and the phase-1 beta ramp.  scalars = {s*, Gamma*, J_perp*,
+   floor}. */
+OR_EXPORT void or_chi_schedule(int Pts, const double *scan_s, const double *scan_gamma, const double *chi,
+                               double beta, double gamma_start, double gamma_end, double A0, int slices,
+                               int num_steps, double chi_floor_fraction, double beta_ramp_fraction,
+                               double beta_ramp_start, double *betas, double *gammas, double *s_sched,
+                               double *scalars) {
+    int peak = 0;
+    for (int m = 1; m < Pts; ++m)
+        if (chi[m] > chi[peak]) peak = m;
+    scalars[0] = scan_s[peak];
+    scalars[1] = scan_gamma[peak];
+    scalars[2] = trotter_coupling(beta, scan_gamma[peak], slices);
+    const double max_chi = chi[peak];
+    const int degenerate = !(max_chi > 0.0) || !isfinite(max_chi);
+    double floor_ = 1.0;
+    if (!degenerate) {
+        floor_ = chi_floor_fraction * max_chi;
+        if (floor_ < 1e-12) floor_ = 1e-12;
+    }
+    scalars[3] = floor_;
+    const double s_lo = A0 / (A0 + gamma_start), s_hi = A0 / (A0 + gamma_end);
+    int n1 = 0;
+    if (beta_ramp_fraction > 0.0) {
+        n1 = (int)(size_t)(beta_ramp_fraction * (double)num_steps);
+        if (n1 > num_steps - 2) n1 = num_steps - 2;
+    }
+    const int n2 = num_steps - n1;
+    enum { GRID = 4096 };
+    const double hs = (s_hi - s_lo) / (double)GRID;
+    double *Wcum = (double *)calloc(GRID + 2, sizeof(double));
+#define WEIGHT_AT(S, OUT)                                                   \
+    do {                                                                    \
+        const double s_ = (S);                                              \
+        double c_;                                                          \
+        if (s_ <= scan_s[0]) c_ = chi[0];                                   \
+        else if (s_ >= scan_s[Pts - 1]) c_ = chi[Pts - 1];                  \
+        else {                                                              \
+            int hi_ = 1;                                                    \
+            while (hi_ < Pts && scan_s[hi_] < s_) ++hi_;                    \
+            const int lo_ = hi_ - 1;                                        \
+            const double t_ = (s_ - scan_s[lo_]) / (scan_s[hi_] - scan_s[lo_]); \
+            c_ = chi[lo_] + t_ * (chi[hi_] - chi[lo_]);                     \
+        }                                                                   \
+        (OUT) = c_ > floor_ ? c_ : floor_;                                  \
+    } while (0)
+    double prev_w;
+    WEIGHT_AT(s_lo, prev_w);
+    for (int k = 1; k <= GRID; ++k) {
+        const double sk = s_lo + (double)k * hs;
+        double cur_w;
+        WEIGHT_AT(sk, cur_w);
+        Wcum[k] = Wcum[k - 1] + 0.5 * (prev_w + cur_w) * hs;
+        prev_w = cur_w;
+    }
+#undef WEIGHT_AT
+    const double W_total = Wcum[GRID];
+    for (int s = 0; s < num_steps; ++s) { betas[s] = beta; gammas[s] = gamma_start; s_sched[s] = s_lo; }
+    for (int step = 0; step < n1; ++step) {
+        const double frac = n1 > 1 ? (double)step / (double)(n1 - 1) : 1.0;
+        betas[step] = beta_ramp_start + (beta - beta_ramp_start) * frac;
+    }
+    int k_idx = 0;
+    for (int t = 0; t < n2; ++t) {
+        const double target = W_total > 0.0 ? ((double)t / (double)(n2 - 1)) * W_total : 0.0;
+        while (k_idx < GRID && Wcum[k_idx + 1] < target) ++k_idx;
+        const double w0 = Wcum[k_idx], w1 = Wcum[k_idx + 1];
+        const double frac = w1 > w0 ? (target - w0) / (w1 - w0) : 0.0;
+        const double s_t = s_lo + ((double)k_idx + frac) * hs;
+        double g_t = chi_s_to_gamma(A0, s_t);
+        if (g_t < gamma_end) g_t = gamma_end;
+        if (g_t > gamma_start) g_t = gamma_start;
+        s_sched[n1 + t] = s_t;
+        gammas[n1 + t] = g_t;
+    }
+    free(Wcum);
+}
+
+/* The pilot probe of one s point (sqa_chi_annealer.cpp:232-266): a fresh
+   worldline, burn + measure parity-phase sweeps, chi_B from the pooled
+   per-replica magnetisations. */
+static double chi_pilot_point(const or_model *M, int P, int K, uint64_t key, int m, float B, float T4, int sweeps,
+                              int burn) {
+    const int n = M->n;
+    ring_t R;
+    ring_alloc(&R, M, P, K, key);
+    ring_init(&R, DOM_PILOT_INIT | ((uint32_t)m << 8));
+    const double inv_nM = 1.0 / (double)(n * P);
+    double m2_sum = 0.0, mabs_sum = 0.0;
+    long long count = 0;
+    for (int sw = 0; sw < burn + sweeps; ++sw) {
+        slice_sweep(&R, (uint32_t)sw, DOM_PILOT | ((uint32_t)m << 8), B, T4, NULL);
+        if (sw >= burn)
+            for (int k = 0; k < K; ++k) {
+                long long sum = 0;
+                for (size_t i = 0; i < (size_t)P * n; ++i) sum += R.s[(size_t)k * P * n + i];
+                const double mm = (double)sum * inv_nM;
+                m2_sum += mm * mm;
+                mabs_sum += fabs(mm);
+                ++count;
+            }
+    }
+    ring_free(&R);
+    if (count < 2) return 0.0;
+    const double m2_mean = m2_sum / (double)count, mabs_mean = mabs_sum / (double)count;
+    const double chi = (double)(n * P) * (m2_mean - mabs_mean * mabs_mean);
+    return chi > 0.0 ? chi : 0.0;
+}
+
+/* scan_chi_in != NULL replaces Stage 1 (the learned-schedule path). */
+OR_EXPORT int or_chi_run(const or_model *M, int P, int K, double beta, double gamma_start, double gamma_end,
+                         int num_steps, int spb, int scan_points, int scan_sweeps, int scan_burn,
+                         double chi_floor_fraction, double driver_A0, double beta_ramp_fraction,
+                         double beta_ramp_start, uint64_t seed, int read, const double *scan_chi_in,
+                         int8_t *best_spins, double *best_E, double *trace, double *beta_sched, double *gamma_sched,
+                         double *s_sched, double *scan_s, double *scan_gamma, double *scan_chi, double *scalars) {
+    const int n = M->n;
+    const uint64_t key = seed + (uint64_t)read;
+    const double A0 = driver_A0 > 0.0 ? driver_A0 : gamma_start;
+    const double s_lo = A0 / (A0 + gamma_start), s_hi = A0 / (A0 + gamma_end);
+    for (int m = 0; m < scan_points; ++m) {
+        const double s_m = s_lo + (s_hi - s_lo) * (double)m / (double)(scan_points - 1);
+        const double g_m = chi_s_to_gamma(A0, s_m);
+        scan_s[m] = s_m;
+        scan_gamma[m] = g_m;
+        if (scan_chi_in) {
+            scan_chi[m] = scan_chi_in[m];
+        } else {
+            float B, T4;
+            step_consts(beta, g_m, P, &B, &T4);
+            scan_chi[m] = chi_pilot_point(M, P, K, key, m, B, T4, scan_sweeps, scan_burn);
+        }
+    }
+    or_chi_schedule(scan_points, scan_s, scan_gamma, scan_chi, beta, gamma_start, gamma_end, A0, P, num_steps,
+                    chi_floor_fraction, beta_ramp_fraction, beta_ramp_start, beta_sched, gamma_sched, s_sched, scalars);
+    scalars[4] = A0;
+    /* Stage 3: production on a fresh worldline */
+    ring_t R;
+    ring_alloc(&R, M, P, K, key);
+    ring_init(&R, DOM_PROD_INIT);
+    double *rbest = (double *)malloc(sizeof(double) * (size_t)K);
+    int *rstep = (int *)malloc(sizeof(int) * (size_t)K);
+    int8_t *rstate = (int8_t *)malloc((size_t)K * n);
+    double *rsum = (double *)malloc(sizeof(double) * (size_t)K);
+    for (int k = 0; k < K; ++k) { rbest[k] = INFINITY; rstep[k] = -1; }
+    for (int step = 0; step < num_steps; ++step) {
+        float B, T4;
+        step_consts(beta_sched[step], gamma_sched[step], P, &B, &T4);
+        for (int sw = 0; sw < spb; ++sw) slice_sweep(&R, (uint32_t)(step * spb + sw), DOM_PROD, B, T4, NULL);
+        for (int k = 0; k < K; ++k) {
+            double sum = 0.0, emin = INFINITY;
+            int tmin = 0;
+            for (int t = 0; t < P; ++t) {
+                double E = cell_energy(&R, k * P + t);
+                sum += E;
+                if (E < emin) { emin = E; tmin = t; }
+            }
+            rsum[k] = sum;
+            if (emin < rbest[k]) {
+                rbest[k] = emin; rstep[k] = step;
+                memcpy(rstate + (size_t)k * n, R.s + ((size_t)k * P + tmin) * n, (size_t)n);
+            }
+        }
+        double tot = 0.0;
+        for (int k = 0; k < K; ++k) tot += rsum[k];
+        trace[step] = tot / (double)(K * P);
+    }
+    int kb = 0;
+    for (int k = 1; k < K; ++k)
+        if (rbest[k] < rbest[kb] || (rbest[k] == rbest[kb] && rstep[k] < rstep[kb])) kb = k;
+    *best_E = rbest[kb];
+    memcpy(best_spins, rstate + (size_t)kb * n, (size_t)n);
+    free(rbest); free(rstep); free(rstate); free(rsum);
+    ring_free(&R);
+    return 0;
+}

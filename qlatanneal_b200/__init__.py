@@ -20,10 +20,12 @@ from .annealers import (  # noqa: F401
     AnnealResult,
     SQAResult,
     SQAParallelTemperingResult,
+    SQAChiResult,
     RunStats,
     Annealer,
     SQAAnnealer,
     SQAParallelTemperingAnnealer,
+    SQAChiAnnealer,
 )
 
 version_major, version_minor, version_patch = 2, 0, 0

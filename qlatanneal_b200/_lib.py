@@ -20,7 +20,7 @@ QA_OK, QA_ERR_ARG, QA_ERR_CUDA, QA_ERR_OOM, QA_ERR_TIMEOUT, QA_ERR_DRIFT, QA_ERR
 EXPORTED = [
     "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy",
     "qa_problem_dense", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
-    "qa_sa_run", "qa_sqa_run", "qa_sqapt_run",
+    "qa_sa_run", "qa_sqa_run", "qa_sqapt_run", "qa_chi_run",
 ]
 
 
@@ -60,6 +60,21 @@ class qa_sqapt_out(C.Structure):
                 ("swap_acceptance_trace", C.c_void_p)]
 
 
+class qa_chi_params(C.Structure):
+    _fields_ = [("trotter_slices", C.c_int), ("replicas", C.c_int), ("beta", C.c_double),
+                ("gamma_start", C.c_double), ("gamma_end", C.c_double), ("num_steps", C.c_int),
+                ("sweeps_per_step", C.c_int), ("scan_points", C.c_int), ("scan_sweeps", C.c_int),
+                ("scan_burn", C.c_int), ("chi_floor_fraction", C.c_double), ("driver_A0", C.c_double),
+                ("beta_ramp_fraction", C.c_double), ("beta_ramp_start", C.c_double), ("reads", C.c_int),
+                ("seed", C.c_uint64), ("scan_chi_in", C.c_void_p)]
+
+
+class qa_chi_out(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("best_spins", "best_energy", "energy_trace", "beta_schedule",
+                                         "gamma_schedule", "s_schedule", "scan_s", "scan_gamma", "scan_chi_B",
+                                         "scalars")]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -91,6 +106,8 @@ def load():
                                  C.POINTER(qa_stats)]
         L.qa_sqapt_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sqapt_params), C.POINTER(qa_sqapt_out),
                                    C.POINTER(qa_stats)]
+        L.qa_chi_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_chi_params), C.POINTER(qa_chi_out),
+                                 C.POINTER(qa_stats)]
         for name in list(EXPORTED):
             getattr(L, name)
         _lib = L

@@ -72,6 +72,25 @@ class SQAParallelTemperingResult:
 
 
 @dataclass
+class SQAChiResult:
+    """``qanneal.SQAChiResult`` (sqa_chi_annealer.hpp:18-36)."""
+    best_state: State
+    best_energy: float
+    energy_trace: List[float]
+    beta_schedule: List[float]
+    gamma_schedule: List[float]
+    s_schedule: List[float]
+    scan_s: List[float]
+    scan_gamma: List[float]
+    scan_chi_B: List[float]
+    s_star: float
+    gamma_star: float
+    j_perp_star: float
+    chi_floor: float
+    driver_A0: float
+
+
+@dataclass
 class RunStats:
     """Device-side totals of one batched call (qa_stats)."""
     slice_attempts: int = 0
@@ -257,3 +276,101 @@ class SQAParallelTemperingAnnealer(_Seeded):
         return [SQAParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
                                            float(bestE[r]), avg[r].tolist(), swp[r].tolist())
                 for r in range(reads)]
+
+
+class SQAChiAnnealer(_Seeded):
+    """``qanneal.SQAChiAnnealer(hamiltonian, trotter_slices, replicas, backend)``
+    (sqa_chi_annealer.cpp:146-438): pilot chi_B scan, chi-weighted schedule,
+    production anneal through the parity-phase kernel."""
+
+    def __init__(self, hamiltonian, trotter_slices: int, replicas: int = 1, backend: str = "cuda",
+                 device: Optional[int] = None):
+        super().__init__()
+        _check_backend(backend)
+        if hamiltonian is None:
+            raise ValueError("SQAChiAnnealer requires a backend.")
+        if trotter_slices <= 0:
+            raise ValueError("trotter_slices must be > 0.")
+        if replicas <= 0:
+            raise ValueError("replicas must be > 0.")
+        self.hamiltonian = hamiltonian
+        self.trotter_slices = int(trotter_slices)
+        self.replicas = int(replicas)
+        self.device = device
+        self.last_stats: Optional[RunStats] = None
+
+    def run_chi(self, beta: float, gamma_start: float, gamma_end: float, num_steps: int = 100,
+                sweeps_per_step: int = 20, scan_points: int = 16, scan_sweeps: int = 30, scan_burn: int = 10,
+                chi_floor_fraction: float = 1e-6, driver_A0: float = 0.0, beta_ramp_fraction: float = 0.3,
+                beta_ramp_start: float = 0.1, debug_csv_path: str = "") -> SQAChiResult:
+        res = self.run_chi_reads(beta, gamma_start, gamma_end, num_steps, sweeps_per_step, scan_points, scan_sweeps,
+                                 scan_burn, chi_floor_fraction, driver_A0, beta_ramp_fraction, beta_ramp_start,
+                                 reads=1)[0]
+        if debug_csv_path:
+            _write_chi_debug_csv(debug_csv_path, res, beta, self.trotter_slices, beta_ramp_fraction)
+        return res
+
+    def run_chi_reads(self, beta: float, gamma_start: float, gamma_end: float, num_steps: int = 100,
+                      sweeps_per_step: int = 20, scan_points: int = 16, scan_sweeps: int = 30, scan_burn: int = 10,
+                      chi_floor_fraction: float = 1e-6, driver_A0: float = 0.0, beta_ramp_fraction: float = 0.3,
+                      beta_ramp_start: float = 0.1, reads: int = 1, seed: Optional[int] = None,
+                      scan_chi: Optional[np.ndarray] = None) -> List[SQAChiResult]:
+        """Batched run_chi.  ``scan_chi`` ([reads][scan_points] or [scan_points])
+        replaces the pilot scan with a given chi_B curve (e.g. a predicted one)."""
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        seed = self._next_seed(reads) if seed is None else int(seed)
+        ov = None
+        if scan_chi is not None:
+            ov = np.ascontiguousarray(np.broadcast_to(np.asarray(scan_chi, np.float64), (reads, int(scan_points))))
+        prm = _lib.qa_chi_params(self.trotter_slices, self.replicas, float(beta), float(gamma_start),
+                                 float(gamma_end), int(num_steps), int(sweeps_per_step), int(scan_points),
+                                 int(scan_sweeps), int(scan_burn), float(chi_floor_fraction), float(driver_A0),
+                                 float(beta_ramp_fraction), float(beta_ramp_start), int(reads), seed,
+                                 None if ov is None else ov.ctypes.data)
+        n, S, Pt = self.hamiltonian.size(), max(int(num_steps), 1), max(int(scan_points), 1)
+        a = {"best_spins": np.zeros((reads, n), np.int8), "best_energy": np.zeros(reads)}
+        for k in ("energy_trace", "beta_schedule", "gamma_schedule", "s_schedule"):
+            a[k] = np.zeros((reads, S))
+        for k in ("scan_s", "scan_gamma", "scan_chi_B"):
+            a[k] = np.zeros((reads, Pt))
+        a["scalars"] = np.zeros((reads, 5))
+        o = _lib.qa_chi_out(*[a[f].ctypes.data for f, _ in _lib.qa_chi_out._fields_])
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_chi_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        out = []
+        for r in range(reads):
+            sc = a["scalars"][r]
+            out.append(SQAChiResult(State(a["best_spins"][r]), float(a["best_energy"][r]),
+                                    a["energy_trace"][r].tolist(), a["beta_schedule"][r].tolist(),
+                                    a["gamma_schedule"][r].tolist(), a["s_schedule"][r].tolist(),
+                                    a["scan_s"][r].tolist(), a["scan_gamma"][r].tolist(), a["scan_chi_B"][r].tolist(),
+                                    float(sc[0]), float(sc[1]), float(sc[2]), float(sc[3]), float(sc[4])))
+        return out
+
+
+def _trotter_coupling(beta: float, gamma: float, slices: int) -> float:
+    import math
+    x = max(beta * gamma / float(slices), 1e-12)
+    return 0.5 * math.log(1.0 / math.tanh(x))
+
+
+def _write_chi_debug_csv(path: str, res: SQAChiResult, beta: float, slices: int, ramp_fraction: float) -> None:
+    """The per-point and per-step rows run_chi writes (sqa_chi_annealer.cpp:201-212, 277-280, 380-387)."""
+    steps = len(res.s_schedule)
+    n1 = min(int(ramp_fraction * steps), steps - 2) if ramp_fraction > 0.0 else 0
+    try:
+        f = open(path, "w")
+    except OSError:
+        import sys
+        print(f"[qlatanneal_b200 run_chi] WARNING: could not open debug CSV '{path}'.", file=sys.stderr)
+        return
+    with f:
+        f.write("phase,index,s,gamma,j_perp,chi_B,beta\n")
+        for m, (s, g, c) in enumerate(zip(res.scan_s, res.scan_gamma, res.scan_chi_B)):
+            f.write(f"scan,{m},{s:.8e},{g:.8e},{_trotter_coupling(beta, g, slices):.8e},{c:.8e},{beta:.8e}\n")
+        for step, (s, g, b) in enumerate(zip(res.s_schedule, res.gamma_schedule, res.beta_schedule)):
+            phase = "beta_ramp" if step < n1 else "run"
+            f.write(f"{phase},{step},{s:.8e},{g:.8e},{_trotter_coupling(b, g, slices):.8e},,{b:.8e}\n")

@@ -11,6 +11,7 @@
 
 #include "qa_gpu.h"
 #include "qa_kernels.cuh"
+#include "qa_chi.cuh"
 #include "qa_pm1.cuh"
 #include "qa_pt.cuh"
 
@@ -163,26 +164,108 @@ struct Layout {
     int nw_max = 1;
 };
 
-void build_rings(Layout &L, const qa_problem *const *probs, int np, int reads, int K, int P, uint64_t seed) {
+// Rings ordered (problem, read, [scan point,] replica).  With points > 0 every
+// (read, point) probe gets its own K rings, schedule row `point` and the
+// domain-tag extension point << 8 (the chi pilot).
+void build_rings(Layout &L, const qa_problem *const *probs, int np, int reads, int K, int P, uint64_t seed,
+                 int points = 0) {
     L.rings.clear();
     L.spin_words = L.field_floats = 0;
     L.nw_max = 1;
     for (int p = 0; p < np; ++p) L.nw_max = std::max(L.nw_max, probs[p]->nw);
+    const int npt = points > 0 ? points : 1;
     for (int p = 0; p < np; ++p)
         for (int r = 0; r < reads; ++r)
-            for (int k = 0; k < K; ++k) {
-                RingDev R{};
-                R.prob = p;
-                R.out = p * reads + r;
-                R.k = k;
-                R.sched = 0;
-                R.key = seed + (uint64_t)r;
-                R.spin_off = L.spin_words;
-                R.field_off = L.field_floats;
-                L.spin_words += (long long)P * probs[p]->nw;
-                L.field_floats += (long long)P * pm1_npad(probs[p]->n);  // rows padded for ring_pm1_kernel
-                L.rings.push_back(R);
-            }
+            for (int m = 0; m < npt; ++m)
+                for (int k = 0; k < K; ++k) {
+                    RingDev R{};
+                    R.prob = p;
+                    R.out = p * reads + r;
+                    R.k = k;
+                    R.sched = points > 0 ? m : 0;
+                    R.tag_extra = points > 0 ? (uint32_t)m << 8 : 0u;
+                    R.key = seed + (uint64_t)r;
+                    R.spin_off = L.spin_words;
+                    R.field_off = L.field_floats;
+                    L.spin_words += (long long)P * probs[p]->nw;
+                    L.field_floats += (long long)P * pm1_npad(probs[p]->n);  // rows padded for ring_pm1_kernel
+                    L.rings.push_back(R);
+                }
+}
+
+double chi_s_to_gamma(double A0, double s) {
+    s = std::min(std::max(s, 1e-10), 1.0 - 1e-10);
+    return A0 * (1.0 - s) / s;
+}
+
+// Stage 2 of run_chi (sqa_chi_annealer.cpp:283-387), float64, same operation
+// order: the chi_B peak, floor, 4096-point trapezoid CDF of
+// w(s) = max(chi_B(s), floor), its inverse at uniform targets, the beta ramp.
+// scalars = {s*, Gamma*, J_perp*, floor}.
+void chi_schedule(int Pts, const double *xs, const double *gs, const double *ys, double beta, double gamma_start,
+                  double gamma_end, double A0, int slices, int num_steps, double floor_fraction, double ramp_fraction,
+                  double ramp_start, double *betas, double *gammas, double *s_sched, double *scalars) {
+    const int peak = (int)(std::max_element(ys, ys + Pts) - ys);
+    scalars[0] = xs[peak];
+    scalars[1] = gs[peak];
+    scalars[2] = trotter_coupling(beta, gs[peak], slices);
+    const double max_chi = ys[peak];
+    const bool degenerate = !(max_chi > 0.0) || !std::isfinite(max_chi);
+    if (degenerate)
+        std::fprintf(stderr, "[qlatanneal_b200 chi] WARNING: chi_B scan is flat/non-finite; "
+                             "falling back to a linear-in-s schedule.\n");
+    const double floor_ = degenerate ? 1.0 : std::max(floor_fraction * max_chi, 1e-12);
+    scalars[3] = floor_;
+    const double s_lo = A0 / (A0 + gamma_start), s_hi = A0 / (A0 + gamma_end);
+    auto weight_at = [&](double s) {
+        double chi;
+        if (s <= xs[0]) chi = ys[0];
+        else if (s >= xs[Pts - 1]) chi = ys[Pts - 1];
+        else {
+            int hi = 1;
+            while (hi < Pts && xs[hi] < s) ++hi;
+            const int lo = hi - 1;
+            const double t = (s - xs[lo]) / (xs[hi] - xs[lo]);
+            chi = ys[lo] + t * (ys[hi] - ys[lo]);
+        }
+        return std::max(chi, floor_);
+    };
+    int n1 = 0;
+    if (ramp_fraction > 0.0) {
+        n1 = (int)(size_t)(ramp_fraction * (double)num_steps);
+        if (n1 > num_steps - 2) n1 = num_steps - 2;
+    }
+    const int n2 = num_steps - n1;
+    const int GRID = 4096;
+    const double hs = (s_hi - s_lo) / (double)GRID;
+    std::vector<double> Wcum(GRID + 2, 0.0);
+    double prev_w = weight_at(s_lo);
+    for (int k = 1; k <= GRID; ++k) {
+        const double sk = s_lo + (double)k * hs;
+        const double cur_w = weight_at(sk);
+        Wcum[k] = Wcum[k - 1] + 0.5 * (prev_w + cur_w) * hs;
+        prev_w = cur_w;
+    }
+    const double W_total = Wcum[GRID];
+    for (int s = 0; s < num_steps; ++s) {
+        betas[s] = beta;
+        gammas[s] = gamma_start;
+        s_sched[s] = s_lo;
+    }
+    for (int step = 0; step < n1; ++step) {
+        const double frac = n1 > 1 ? (double)step / (double)(n1 - 1) : 1.0;
+        betas[step] = ramp_start + (beta - ramp_start) * frac;
+    }
+    int k_idx = 0;
+    for (int t = 0; t < n2; ++t) {
+        const double target = W_total > 0.0 ? ((double)t / (double)(n2 - 1)) * W_total : 0.0;
+        while (k_idx < GRID && Wcum[k_idx + 1] < target) ++k_idx;
+        const double w0 = Wcum[k_idx], w1 = Wcum[k_idx + 1];
+        const double frac = w1 > w0 ? (target - w0) / (w1 - w0) : 0.0;
+        const double s_t = s_lo + ((double)k_idx + frac) * hs;
+        s_sched[n1 + t] = s_t;
+        gammas[n1 + t] = std::min(std::max(chi_s_to_gamma(A0, s_t), gamma_end), gamma_start);
+    }
 }
 
 int upload_common(qa_ctx *ctx, const qa_problem *const *probs, int np, const Layout &L, ProbDev **d_probs,
@@ -983,6 +1066,236 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
                                      sizeof(int) * rin.size());
         stats->d2h_bytes = (int64_t)(sizeof(double) * (3 * nr + avg.size() + swp.size()) + 3 * sizeof(int) * nr +
                                      sizeof(int) * rin.size() + sizeof(uint32_t) * 2 * bits.size() + sizeof(cnt));
+    }
+    return QA_OK;
+}
+
+// ---------------------------------------------------------------------- SQA-Chi
+int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_chi_params *prm,
+               qa_chi_out *outs, qa_stats *stats) {
+    QA_TRY(begin(ctx));
+    if (!prm) return fail(QA_ERR_ARG, "null params");
+    // sqa_chi_annealer.cpp:159-179
+    if (prm->num_steps < 2) return fail(QA_ERR_ARG, "num_steps must be >= 2.");
+    if (prm->sweeps_per_step <= 0) return fail(QA_ERR_ARG, "sweeps_per_step must be > 0.");
+    if (!(prm->beta > 0.0)) return fail(QA_ERR_ARG, "beta must be > 0.");
+    if (!(prm->gamma_end > 0.0) || !(prm->gamma_start > prm->gamma_end))
+        return fail(QA_ERR_ARG, "Require gamma_start > gamma_end > 0.");
+    if (prm->scan_points < 4) return fail(QA_ERR_ARG, "scan_points must be >= 4.");
+    if (prm->scan_sweeps <= 0) return fail(QA_ERR_ARG, "scan_sweeps must be > 0.");
+    if (prm->scan_burn < 0) return fail(QA_ERR_ARG, "scan_burn must be >= 0.");
+    if (prm->chi_floor_fraction < 0.0) return fail(QA_ERR_ARG, "chi_floor_fraction must be >= 0.");
+    if (prm->trotter_slices <= 0) return fail(QA_ERR_ARG, "trotter_slices must be > 0.");
+    if (prm->replicas <= 0) return fail(QA_ERR_ARG, "replicas must be > 0.");
+    if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
+    int kind, n_max;
+    QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
+    const int P = prm->trotter_slices, K = prm->replicas, Pts = prm->scan_points, steps = prm->num_steps;
+    const int reads_total = n_problems * prm->reads;
+    const double A0 = prm->driver_A0 > 0.0 ? prm->driver_A0 : prm->gamma_start;
+    const double s_lo = A0 / (A0 + prm->gamma_start), s_hi = A0 / (A0 + prm->gamma_end);
+    std::vector<double> scan_s(Pts), scan_g(Pts), chi((size_t)reads_total * Pts);
+    for (int m = 0; m < Pts; ++m) {
+        scan_s[m] = s_lo + (s_hi - s_lo) * (double)m / (double)(Pts - 1);
+        scan_g[m] = chi_s_to_gamma(A0, scan_s[m]);
+    }
+    int64_t launches = 0, h2d = 0, d2h = 0;
+    unsigned long long cnt_total[4] = {0, 0, 0, 0};
+    float pilot_ms = 0.0f;
+    QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    Layout L;
+    ProbDev *d_probs;
+    RingDev *d_rings;
+    uint32_t *d_spins;
+    float *d_fields;
+    double *d_sum, *d_best, *d_exact;
+    int *d_bstep;
+    uint32_t *d_bits;
+    unsigned long long *d_cnt;
+    float *d_B, *d_T4;
+    if (prm->scan_chi_in) {
+        std::memcpy(chi.data(), prm->scan_chi_in, sizeof(double) * chi.size());
+    } else {
+        // ---- Stage 1: all (read, point) probes in one launch
+        build_rings(L, problems, n_problems, prm->reads, K, P, prm->seed, Pts);
+        const int nr = (int)L.rings.size();
+        const int sweeps_total = prm->scan_burn + prm->scan_sweeps;
+        QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
+        std::vector<float> B(Pts), T4(Pts);
+        for (int m = 0; m < Pts; ++m) {
+            B[m] = (float)(2.0 * (prm->beta / (double)P));
+            T4[m] = (float)(4.0 * trotter_coupling(prm->beta, scan_g[m], P));
+        }
+        int *d_mag, *d_nof;
+        double *d_chi;
+        QA_TRY(ws_array(ctx, W_A, Pts, &d_B));
+        QA_TRY(ws_array(ctx, W_T4, Pts, &d_T4));
+        QA_TRY(ws_array(ctx, W_SUM, nr, &d_sum));
+        QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
+        QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
+        QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
+        QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+        QA_TRY(ws_array(ctx, W_MAG, (size_t)nr * sweeps_total, &d_mag));
+        QA_TRY(ws_array(ctx, W_PROBOF, (size_t)reads_total * Pts, &d_nof));
+        QA_TRY(ws_array(ctx, W_EXACT, (size_t)reads_total * Pts, &d_chi));
+        std::vector<int> nof((size_t)reads_total * Pts);
+        for (int p = 0; p < n_problems; ++p)
+            for (int i = 0; i < prm->reads * Pts; ++i) nof[(size_t)p * prm->reads * Pts + i] = problems[p]->n;
+        std::vector<double> inf(nr, INFINITY);
+        QA_CK(cudaMemcpyAsync(d_B, B.data(), sizeof(float) * Pts, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * Pts, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_nof, nof.data(), sizeof(int) * nof.size(), cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+        h2d += (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * Pts +
+                         sizeof(int) * nof.size() + sizeof(double) * nr);
+        RingPlan pl;
+        QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
+        QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PILOT_INIT,
+                          !pl.pm1));
+        RingParams rp{};
+        rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
+        rp.P = P; rp.steps_total = 1; rp.spb = sweeps_total; rp.wls = 0; rp.slice_tag = DOM_PILOT;
+        rp.B = d_B; rp.T4 = d_T4; rp.ring_sum = d_sum; rp.rec_base = 0; rp.rec_stride = 1;
+        rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max;
+        rp.mag = d_mag; rp.counters = d_cnt; rp.step0 = 0; rp.step1 = 1; rp.init_fields = 1;
+        QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+        const int probes = reads_total * Pts;
+        chi_point_kernel<<<(probes + 127) / 128, 128, 0, ctx->stream>>>(d_mag, probes, K, sweeps_total,
+                                                                         prm->scan_burn, d_nof, P, d_chi);
+        QA_CK(cudaGetLastError());
+        launches += (pl.pm1 ? 1 : 2) + 2;
+        unsigned long long c[4];
+        QA_CK(cudaMemcpyAsync(chi.data(), d_chi, sizeof(double) * chi.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaMemcpyAsync(c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+        QA_CK(cudaStreamSynchronize(ctx->stream));
+        QA_CK(cudaEventElapsedTime(&pilot_ms, ctx->ev[0], ctx->ev[1]));
+        d2h += (int64_t)(sizeof(double) * chi.size() + sizeof(c));
+        for (int i = 0; i < 4; ++i) cnt_total[i] += c[i];
+    }
+
+    // ---- Stage 2 (host) per read
+    std::vector<double> bs((size_t)reads_total * steps), gsch((size_t)reads_total * steps),
+        ss((size_t)reads_total * steps), sc((size_t)reads_total * 5);
+    for (int q = 0; q < reads_total; ++q) {
+        chi_schedule(Pts, scan_s.data(), scan_g.data(), chi.data() + (size_t)q * Pts, prm->beta, prm->gamma_start,
+                     prm->gamma_end, A0, P, steps, prm->chi_floor_fraction, prm->beta_ramp_fraction,
+                     prm->beta_ramp_start, bs.data() + (size_t)q * steps, gsch.data() + (size_t)q * steps,
+                     ss.data() + (size_t)q * steps, sc.data() + (size_t)q * 5);
+        sc[(size_t)q * 5 + 4] = A0;
+    }
+
+    // ---- Stage 3: production on fresh worldlines, per-read schedules
+    build_rings(L, problems, n_problems, prm->reads, K, P, prm->seed);
+    for (auto &R : L.rings) R.sched = R.out * steps;
+    const int nr = (int)L.rings.size();
+    QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
+    std::vector<float> B((size_t)reads_total * steps), T4((size_t)reads_total * steps);
+    for (size_t i = 0; i < B.size(); ++i) {
+        B[i] = (float)(2.0 * (bs[i] / (double)P));
+        T4[i] = (float)(4.0 * trotter_coupling(bs[i], gsch[i], P));
+    }
+    QA_TRY(ws_array(ctx, W_A, B.size(), &d_B));
+    QA_TRY(ws_array(ctx, W_T4, T4.size(), &d_T4));
+    QA_TRY(ws_array(ctx, W_SUM, (size_t)nr * steps, &d_sum));
+    QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
+    QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
+    QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
+    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    QA_TRY(ws_array(ctx, W_EXACT, nr, &d_exact));
+    {
+        std::vector<double> inf(nr, INFINITY);
+        std::vector<int> neg(nr, -1);
+        QA_CK(cudaMemcpyAsync(d_B, B.data(), sizeof(float) * B.size(), cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * T4.size(), cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_bstep, neg.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+        QA_CK(cudaStreamSynchronize(ctx->stream));
+        h2d += (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * B.size() +
+                         (sizeof(double) + sizeof(int)) * nr);
+    }
+    RingPlan pl;
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
+    QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PROD_INIT, !pl.pm1));
+    RingParams rp{};
+    rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
+    rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_step; rp.wls = 0; rp.slice_tag = DOM_PROD;
+    rp.B = d_B; rp.T4 = d_T4; rp.ring_sum = d_sum; rp.rec_base = 0; rp.rec_stride = steps;
+    rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max; rp.counters = d_cnt;
+    int n_seg = 0;
+    for (int s0 = 0; s0 < steps; s0 += 256) {
+        rp.step0 = s0;
+        rp.step1 = std::min(steps, s0 + 256);
+        rp.init_fields = s0 == 0;
+        QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+        ++n_seg;
+    }
+    QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
+    QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    launches += (pl.pm1 ? 2 : 3) + n_seg;
+    std::vector<double> sums((size_t)nr * steps), bestE(nr), exact(nr);
+    std::vector<int> bstep(nr);
+    std::vector<uint32_t> bits((size_t)nr * L.nw_max);
+    unsigned long long cnt[4];
+    QA_CK(cudaMemcpyAsync(sums.data(), d_sum, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bstep.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    d2h += (int64_t)(sizeof(double) * (sums.size() + 2 * nr) + sizeof(int) * nr + sizeof(uint32_t) * bits.size() +
+                     sizeof(cnt));
+    for (int i = 0; i < 4; ++i) cnt_total[i] += cnt[i];
+
+    for (int p = 0; p < n_problems; ++p) {
+        const int n = problems[p]->n;
+        qa_chi_out &o = outs[p];
+        for (int r = 0; r < prm->reads; ++r) {
+            const int q = p * prm->reads + r, base = q * K;
+            if (o.energy_trace)
+                for (int s = 0; s < steps; ++s) {
+                    double tot = 0.0;
+                    for (int k = 0; k < K; ++k) tot += sums[(size_t)(base + k) * steps + s];
+                    o.energy_trace[(size_t)r * steps + s] = tot / (double)(K * P);
+                }
+            int kb = 0;
+            for (int k = 1; k < K; ++k) {
+                const int a = base + k, b = base + kb;
+                if (bestE[a] < bestE[b] || (bestE[a] == bestE[b] && bstep[a] < bstep[b])) kb = k;
+            }
+            if (o.best_spins) unpack_bits(bits.data() + (size_t)(base + kb) * L.nw_max, n, o.best_spins + (size_t)r * n);
+            if (o.best_energy) o.best_energy[r] = exact[base + kb];
+            auto cp = [&](double *dst, const double *src, size_t len) {
+                if (dst) std::memcpy(dst + (size_t)r * len, src, sizeof(double) * len);
+            };
+            cp(o.beta_schedule, bs.data() + (size_t)q * steps, steps);
+            cp(o.gamma_schedule, gsch.data() + (size_t)q * steps, steps);
+            cp(o.s_schedule, ss.data() + (size_t)q * steps, steps);
+            cp(o.scan_s, scan_s.data(), Pts);
+            cp(o.scan_gamma, scan_g.data(), Pts);
+            cp(o.scan_chi_B, chi.data() + (size_t)q * Pts, Pts);
+            cp(o.scalars, sc.data() + (size_t)q * 5, 5);
+        }
+    }
+    if (stats) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[3]);
+        stats->slice_attempts = (int64_t)cnt_total[0];
+        stats->slice_accepts = (int64_t)cnt_total[1];
+        stats->worldline_attempts = (int64_t)cnt_total[2];
+        stats->worldline_accepts = (int64_t)cnt_total[3];
+        stats->sweep_ms = a + pilot_ms;
+        stats->total_ms = b + pilot_ms;
+        stats->sweep_launches = n_seg + (prm->scan_chi_in ? 0 : 1);
+        stats->launches = launches;
+        stats->h2d_bytes = h2d;
+        stats->d2h_bytes = d2h;
     }
     return QA_OK;
 }

@@ -28,7 +28,8 @@ struct RingDev {
     int prob;            // problem index
     int out;             // result slot (problem, read)
     int k;               // replica index inside the read (slice-RNG cell base k*P)
-    int sched;           // offset into the per-step A/T4 tables
+    int sched;           // offset into the per-step B/T4 tables
+    uint32_t tag_extra;  // OR-ed into the domain tags of this ring (chi pilot: point << 8)
     uint64_t key;        // Philox key = seed + read
     long long spin_off;  // uint32 words, P * nw
     long long field_off; // floats, P * n
@@ -85,7 +86,7 @@ static __global__ void init_spins_kernel(const ProbDev *probs, const RingDev *ri
     const int t = blockIdx.y;
     const int ring_cell_base = R.k * P;
     for (int q = threadIdx.x; q < Pd.nw; q += blockDim.x) {
-        const U4 r = philox((uint32_t)(q >> 2), (uint32_t)(ring_cell_base + t), 0u, tag, R.key);
+        const U4 r = philox((uint32_t)(q >> 2), (uint32_t)(ring_cell_base + t), 0u, tag | R.tag_extra, R.key);
         uint32_t w = pick(r, q & 3);
         const int rem = Pd.n - 32 * q;
         if (rem < 32) w &= (1u << rem) - 1u;
@@ -309,7 +310,8 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                 for (int c = warp; c < cnt; c += W) {
                     const int t = phase_slice(NP, ph, c);
                     sweep_slice<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, B, T4, R.key,
-                                      (uint32_t)(slot * NP + t), sigma, p.slice_tag, lane, att_s, acc_s);
+                                      (uint32_t)(slot * NP + t), sigma, p.slice_tag | R.tag_extra, lane, att_s,
+                                      acc_s);
                 }
                 if (cnt) __syncthreads();
             }

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 for (int c = warp; c < cnt; c += W) {
                     const int t = phase_slice(NP, ph, c);
                     pm1_sweep_slice(Jw, S, G, Wc, h, n, nw, npad, NP, t, B, T4, R.key, (uint32_t)(slot * NP + t),
-                                    sigma, p.slice_tag, lane, att_s, acc_s);
+                                    sigma, p.slice_tag | R.tag_extra, lane, att_s, acc_s);
                 }
                 if (cnt) __syncthreads();
             }

@@ -79,6 +79,11 @@ class Oracle:
                                  C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i64p]
         L.or_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i8p, _f8p, _f8p, _i64p]
+        L.or_chi_schedule.argtypes = ([C.c_int, _f8p, _f8p, _f8p] + [C.c_double] * 4 + [C.c_int, C.c_int] +
+                                      [C.c_double] * 3 + [_f8p] * 4)
+        L.or_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 3 + [C.c_int] * 5 +
+                                 [C.c_double] * 4 + [C.c_uint64, C.c_int, C.c_void_p, _i8p, C.POINTER(C.c_double)] +
+                                 [_f8p] * 8)
 
     # ---- primitives
     def philox(self, ctr, key):
@@ -168,6 +173,29 @@ class Oracle:
         cnt = np.zeros(4, np.int64)
         self.L.or_sqa_run(m.h, betas, gammas, len(betas), P, K, spb, wls, seed, read, best, C.byref(E), trace, cnt)
         return best, E.value, trace, cnt
+
+    def chi_schedule(self, scan_s, scan_gamma, chi, beta, gamma_start, gamma_end, A0, slices, num_steps,
+                     floor_fraction=1e-6, ramp_fraction=0.3, ramp_start=0.1):
+        b, g, s = np.zeros(num_steps), np.zeros(num_steps), np.zeros(num_steps)
+        sc = np.zeros(5)
+        self.L.or_chi_schedule(len(chi), _c64(scan_s), _c64(scan_gamma), _c64(chi), beta, gamma_start, gamma_end, A0,
+                               slices, num_steps, floor_fraction, ramp_fraction, ramp_start, b, g, s, sc)
+        return b, g, s, sc
+
+    def chi_run(self, m, P, K, beta, gamma_start, gamma_end, num_steps, spb, points, sweeps, burn, seed, read=0,
+                floor_fraction=1e-6, A0=0.0, ramp_fraction=0.3, ramp_start=0.1, scan_chi_in=None):
+        best = np.zeros(m.n, np.int8)
+        E = C.c_double()
+        out = {k: np.zeros(num_steps) for k in ("trace", "beta", "gamma", "s")}
+        scan = {k: np.zeros(points) for k in ("s", "gamma", "chi")}
+        sc = np.zeros(5)
+        ov = None if scan_chi_in is None else _c64(scan_chi_in)
+        self.L.or_chi_run(m.h, P, K, beta, gamma_start, gamma_end, num_steps, spb, points, sweeps, burn,
+                          floor_fraction, A0, ramp_fraction, ramp_start, seed, read,
+                          None if ov is None else ov.ctypes.data, best, C.byref(E), out["trace"], out["beta"],
+                          out["gamma"], out["s"], scan["s"], scan["gamma"], scan["chi"], sc)
+        return dict(best=best, best_energy=E.value, scalars=sc, **{"scan_" + k: v for k, v in scan.items()},
+                    **out)
 
     def sqapt_run(self, m, betas, gammas, P, spb, wls, steps, swap_interval, seed, read=0):
         """Returns (best, best_E, final_E[R], final_spins[R][n], avg_trace, swap_trace, counters)."""
@@ -305,6 +333,21 @@ class RefModel:
         if self.ref.L.ref_sqa_run(self.h, betas, gammas, len(betas), P, K, spb, wls, seed, best, C.byref(E), tr) != 0:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return best, E.value, tr
+
+    def chi_run(self, P, K, beta, gamma_start, gamma_end, num_steps, spb, points, sweeps, burn, seed,
+                floor_fraction=1e-6, A0=0.0, ramp_fraction=0.3, ramp_start=0.1):
+        best = np.zeros(self.n, np.int8)
+        E = C.c_double()
+        arr = {k: np.zeros(points) for k in ("scan_s", "scan_gamma", "scan_chi")}
+        arr.update({k: np.zeros(num_steps) for k in ("beta", "gamma", "s", "trace")})
+        sc = np.zeros(5)
+        rc = self.ref.L.ref_chi_run(self.h, P, K, beta, gamma_start, gamma_end, num_steps, spb, points, sweeps, burn,
+                                    floor_fraction, A0, ramp_fraction, ramp_start, seed, best, C.byref(E),
+                                    arr["scan_s"], arr["scan_gamma"], arr["scan_chi"], arr["beta"], arr["gamma"],
+                                    arr["s"], arr["trace"], sc)
+        if rc != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return dict(best=best, best_energy=E.value, scalars=sc, **arr)
 
     def sqapt_run(self, betas, gammas, P, spb, wls, steps, swap_interval, seed):
         betas, gammas = _c64(betas), _c64(gammas)
