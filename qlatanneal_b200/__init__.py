@@ -28,6 +28,19 @@ from .annealers import (  # noqa: F401
     SQAChiAnnealer,
 )
 
+from .solver import (  # noqa: F401
+    SolveResult,
+    solve,
+    auto_schedule_sa,
+    auto_schedule_sqa,
+    auto_schedule_sa_tuned,
+    auto_schedule_sqa_tuned,
+    auto_ladder_sqa_tuned,
+    j_perp_from_beta_gamma,
+    optimal_j_perp_params,
+    j_rms_from_problem,
+)
+
 version_major, version_minor, version_patch = 2, 0, 0
 
 
