@@ -204,6 +204,32 @@ typedef struct {
 QA_API int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_chi_params *params,
                       qa_chi_out *outs, qa_stats *stats);
 
+/* Stage 1 alone (sqa_chi_annealer.cpp:217-281): scan_chi[(problem*reads + read)*scan_points + point]
+ * (the training curves of the chi_B MLP).  num_steps, sweeps_per_step and the
+ * schedule fields of params are ignored. */
+QA_API int qa_chi_pilot(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_chi_params *params,
+                        double *scan_chi, qa_stats *stats);
+
+/* ---- chi_B-curve MLP (no counterpart in the reference: it replaces Stage 1
+ * of run_chi, sqa_chi_annealer.cpp:217-281, with a predicted curve) --------
+ * dims[0] -> ... -> dims[n_dims-1], ReLU between layers; bfloat16 weights,
+ * float32 accumulation and float32 Adam masters.  The output holds M means and
+ * M log-variances (dims[last] = 2M) of a Gaussian over the M-point target; the
+ * loss is the mean Gaussian negative log-likelihood.  Inputs X [batch][dims[0]],
+ * targets T [batch][M], outputs Y [batch][2M] are host float32 arrays.
+ * Parameters: per layer W[d_l][d_l+1] row-major, then b[d_l+1]. */
+typedef struct qa_mlp qa_mlp;
+QA_API int qa_mlp_create(qa_ctx *ctx, const int *dims, int n_dims, uint64_t seed, qa_mlp **out);
+QA_API int qa_mlp_free(qa_mlp *m);
+QA_API int qa_mlp_num_params(const qa_mlp *m, int64_t *count);
+QA_API int qa_mlp_get_params(qa_mlp *m, float *params, int64_t count);
+QA_API int qa_mlp_set_params(qa_mlp *m, const float *params, int64_t count);  /* also resets Adam */
+QA_API int qa_mlp_forward(qa_mlp *m, const float *X, int batch, float *Y);
+/* loss of (X, T) and its gradient w.r.t. every parameter (grads may be NULL) */
+QA_API int qa_mlp_loss_grad(qa_mlp *m, const float *X, const float *T, int batch, float *loss, float *grads);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the batch; loss before the step */
+QA_API int qa_mlp_train_step(qa_mlp *m, const float *X, const float *T, int batch, float lr, float *loss);
+
 /* ---- SA on a dense model without any allocation by this library --------
  * No counterpart in the reference.  For callers that cannot let a library
  * call cudaMalloc/cudaFree: their device memory belongs to a framework

@@ -20,7 +20,9 @@ QA_OK, QA_ERR_ARG, QA_ERR_CUDA, QA_ERR_OOM, QA_ERR_TIMEOUT, QA_ERR_DRIFT, QA_ERR
 EXPORTED = [
     "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy",
     "qa_problem_dense", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
-    "qa_sa_run", "qa_sqa_run", "qa_sqapt_run", "qa_chi_run",
+    "qa_sa_run", "qa_sqa_run", "qa_sqapt_run", "qa_chi_run", "qa_chi_pilot",
+    "qa_mlp_create", "qa_mlp_free", "qa_mlp_num_params", "qa_mlp_get_params", "qa_mlp_set_params",
+    "qa_mlp_forward", "qa_mlp_loss_grad", "qa_mlp_train_step",
 ]
 
 
@@ -108,6 +110,15 @@ def load():
                                    C.POINTER(qa_stats)]
         L.qa_chi_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_chi_params), C.POINTER(qa_chi_out),
                                  C.POINTER(qa_stats)]
+        L.qa_chi_pilot.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_chi_params), vp, C.POINTER(qa_stats)]
+        L.qa_mlp_create.argtypes = [vp, C.POINTER(i), i, C.c_uint64, C.POINTER(vp)]
+        L.qa_mlp_free.argtypes = [vp]
+        L.qa_mlp_num_params.argtypes = [vp, C.POINTER(C.c_int64)]
+        L.qa_mlp_get_params.argtypes = [vp, vp, C.c_int64]
+        L.qa_mlp_set_params.argtypes = [vp, vp, C.c_int64]
+        L.qa_mlp_forward.argtypes = [vp, vp, i, vp]
+        L.qa_mlp_loss_grad.argtypes = [vp, vp, vp, i, C.POINTER(C.c_float), vp]
+        L.qa_mlp_train_step.argtypes = [vp, vp, vp, i, C.c_float, C.POINTER(C.c_float)]
         for name in list(EXPORTED):
             getattr(L, name)
         _lib = L

@@ -12,6 +12,7 @@
 #include "qa_gpu.h"
 #include "qa_kernels.cuh"
 #include "qa_chi.cuh"
+#include "qa_mlp.cuh"
 #include "qa_pm1.cuh"
 #include "qa_pt.cuh"
 
@@ -62,6 +63,20 @@ struct qa_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int smem_optin = 0;
     DevBuf ws[32];
+};
+
+struct qa_mlp {
+    qa_ctx *ctx = nullptr;
+    std::vector<int> dims;
+    long long nparams = 0, nw16 = 0;
+    std::vector<long long> woff, boff, w16off;
+    float *W = nullptr, *g = nullptr, *mo = nullptr, *vo = nullptr;  // masters, grads, Adam moments
+    __nv_bfloat16 *W16 = nullptr;
+    long long *wmap = nullptr;
+    int cap_B = 0;
+    std::vector<long long> aoff;  // per-layer activation offsets for the current batch
+    float *acts = nullptr, *dacts = nullptr, *T = nullptr, *rowloss = nullptr;
+    int step = 0;
 };
 
 struct qa_problem {
@@ -374,6 +389,69 @@ int ws_array(qa_ctx *ctx, int slot, size_t count, T **out) {
     void *v;
     QA_TRY(ws_get(ctx, slot, sizeof(T) * count, &v));
     *out = static_cast<T *>(v);
+    return QA_OK;
+}
+
+// Batch buffers of an MLP (grown on demand) and the inputs/targets copied in.
+int mlp_prepare(qa_mlp *m, int B, const float *X, const float *T) {
+    const int L = (int)m->dims.size() - 1;
+    if (B > m->cap_B) {
+        for (float **p : {&m->acts, &m->dacts, &m->T, &m->rowloss})
+            if (*p) { cudaFree(*p); *p = nullptr; }
+        long long per_row = 0;
+        for (int d : m->dims) per_row += d;
+        QA_CK(cudaMalloc(&m->acts, sizeof(float) * per_row * B));
+        QA_CK(cudaMalloc(&m->dacts, sizeof(float) * per_row * B));
+        QA_CK(cudaMalloc(&m->T, sizeof(float) * (size_t)B * (m->dims[L] / 2)));
+        QA_CK(cudaMalloc(&m->rowloss, sizeof(float) * B));
+        m->cap_B = B;
+    }
+    m->aoff.assign(L + 1, 0);
+    for (int l = 1; l <= L; ++l) m->aoff[l] = m->aoff[l - 1] + (long long)B * m->dims[l - 1];
+    QA_CK(cudaMemcpyAsync(m->acts, X, sizeof(float) * (size_t)B * m->dims[0], cudaMemcpyHostToDevice, m->ctx->stream));
+    if (T)
+        QA_CK(cudaMemcpyAsync(m->T, T, sizeof(float) * (size_t)B * (m->dims[L] / 2), cudaMemcpyHostToDevice,
+                              m->ctx->stream));
+    return QA_OK;
+}
+
+int mlp_forward_dev(qa_mlp *m, int B) {
+    const int L = (int)m->dims.size() - 1;
+    for (int l = 0; l < L; ++l) {
+        const int K = m->dims[l], N = m->dims[l + 1];
+        mlp_fwd_kernel<<<(B * N + 127) / 128, 128, 0, m->ctx->stream>>>(m->acts + m->aoff[l], B, K,
+                                                                        m->W16 + m->w16off[l], m->W + m->boff[l],
+                                                                        m->acts + m->aoff[l + 1], N, l + 1 < L);
+        QA_CK(cudaGetLastError());
+    }
+    return QA_OK;
+}
+
+// Loss and gradients (into m->g) of the last forward pass.
+int mlp_backward_dev(qa_mlp *m, int B, float *loss) {
+    const int L = (int)m->dims.size() - 1, M = m->dims[L] / 2;
+    mlp_loss_kernel<<<B, 128, 0, m->ctx->stream>>>(m->acts + m->aoff[L], m->T, B, M, m->dacts + m->aoff[L],
+                                                  m->rowloss);
+    QA_CK(cudaGetLastError());
+    for (int l = L - 1; l >= 0; --l) {
+        const int K = m->dims[l], N = m->dims[l + 1];
+        mlp_bwd_weight_kernel<<<(K * N + N + 127) / 128, 128, 0, m->ctx->stream>>>(
+            m->acts + m->aoff[l], m->dacts + m->aoff[l + 1], B, K, N, m->g + m->woff[l], m->g + m->boff[l]);
+        QA_CK(cudaGetLastError());
+        if (l > 0) {
+            mlp_bwd_input_kernel<<<(B * K + 127) / 128, 128, 0, m->ctx->stream>>>(
+                m->dacts + m->aoff[l + 1], m->W16 + m->w16off[l], m->acts + m->aoff[l], B, K, N, m->dacts + m->aoff[l]);
+            QA_CK(cudaGetLastError());
+        }
+    }
+    if (loss) {
+        std::vector<float> rl(B);
+        QA_CK(cudaMemcpyAsync(rl.data(), m->rowloss, sizeof(float) * B, cudaMemcpyDeviceToHost, m->ctx->stream));
+        QA_CK(cudaStreamSynchronize(m->ctx->stream));
+        double s = 0.0;
+        for (float x : rl) s += x;
+        *loss = (float)(s / ((double)B * M));
+    }
     return QA_OK;
 }
 
@@ -1070,6 +1148,258 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
     return QA_OK;
 }
 
+// ---------------------------------------------------------------------- MLP
+int qa_mlp_create(qa_ctx *ctx, const int *dims, int n_dims, uint64_t seed, qa_mlp **out) {
+    QA_TRY(begin(ctx));
+    if (!out || !dims || n_dims < 2) return fail(QA_ERR_ARG, "an MLP needs at least an input and an output size.");
+    for (int i = 0; i < n_dims; ++i)
+        if (dims[i] <= 0 || dims[i] > 4096) return fail(QA_ERR_ARG, "MLP layer sizes must be in [1, 4096].");
+    if (dims[n_dims - 1] % 2) return fail(QA_ERR_ARG, "the MLP output must hold M means and M log-variances.");
+    qa_mlp *m = new qa_mlp();
+    m->ctx = ctx;
+    m->dims.assign(dims, dims + n_dims);
+    const int L = n_dims - 1;
+    std::vector<long long> wmap;
+    for (int l = 0; l < L; ++l) {
+        const long long kn = (long long)dims[l] * dims[l + 1];
+        m->woff.push_back(m->nparams);
+        m->w16off.push_back(m->nw16);
+        for (long long i = 0; i < kn; ++i) wmap.push_back(m->nw16 + i);
+        m->nparams += kn;
+        m->nw16 += kn;
+        m->boff.push_back(m->nparams);
+        for (int i = 0; i < dims[l + 1]; ++i) wmap.push_back(-1);
+        m->nparams += dims[l + 1];
+    }
+    // He-uniform initial weights from a splitmix64 stream, zero biases
+    std::vector<float> W(m->nparams, 0.0f);
+    uint64_t s = seed;
+    auto next = [&s]() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    for (int l = 0; l < L; ++l) {
+        const double a = std::sqrt(6.0 / dims[l]);
+        for (long long i = 0; i < (long long)dims[l] * dims[l + 1]; ++i)
+            W[m->woff[l] + i] = (float)(a * (2.0 * ((next() >> 11) * (1.0 / 9007199254740992.0)) - 1.0));
+    }
+    cudaError_t e = cudaMalloc(&m->W, sizeof(float) * m->nparams);
+    if (e == cudaSuccess) e = cudaMalloc(&m->g, sizeof(float) * m->nparams);
+    if (e == cudaSuccess) e = cudaMalloc(&m->mo, sizeof(float) * m->nparams);
+    if (e == cudaSuccess) e = cudaMalloc(&m->vo, sizeof(float) * m->nparams);
+    if (e == cudaSuccess) e = cudaMalloc(&m->W16, sizeof(__nv_bfloat16) * m->nw16);
+    if (e == cudaSuccess) e = cudaMalloc(&m->wmap, sizeof(long long) * m->nparams);
+    if (e != cudaSuccess) {
+        qa_mlp_free(m);
+        return fail(e == cudaErrorMemoryAllocation ? QA_ERR_OOM : QA_ERR_CUDA, cudaGetErrorString(e));
+    }
+    QA_CK(cudaMemcpy(m->W, W.data(), sizeof(float) * m->nparams, cudaMemcpyHostToDevice));
+    QA_CK(cudaMemcpy(m->wmap, wmap.data(), sizeof(long long) * m->nparams, cudaMemcpyHostToDevice));
+    QA_CK(cudaMemset(m->mo, 0, sizeof(float) * m->nparams));
+    QA_CK(cudaMemset(m->vo, 0, sizeof(float) * m->nparams));
+    mlp_to_bf16_kernel<<<(unsigned)((m->nparams + 255) / 256), 256, 0, ctx->stream>>>(m->W, m->nparams, m->wmap, m->W16);
+    QA_CK(cudaGetLastError());
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    *out = m;
+    return QA_OK;
+}
+
+int qa_mlp_free(qa_mlp *m) {
+    if (!m) return QA_OK;
+    cudaSetDevice(m->ctx->device);
+    for (void *p : {(void *)m->W, (void *)m->g, (void *)m->mo, (void *)m->vo, (void *)m->W16, (void *)m->wmap,
+                    (void *)m->acts, (void *)m->dacts, (void *)m->T, (void *)m->rowloss})
+        if (p) cudaFree(p);
+    delete m;
+    return QA_OK;
+}
+
+int qa_mlp_num_params(const qa_mlp *m, int64_t *count) {
+    if (!m || !count) return fail(QA_ERR_ARG, "null argument");
+    *count = m->nparams;
+    return QA_OK;
+}
+
+int qa_mlp_get_params(qa_mlp *m, float *host, int64_t count) {
+    if (!m || !host || count != m->nparams) return fail(QA_ERR_ARG, "parameter buffer size mismatch");
+    QA_TRY(begin(m->ctx));
+    QA_CK(cudaMemcpy(host, m->W, sizeof(float) * count, cudaMemcpyDeviceToHost));
+    return QA_OK;
+}
+
+int qa_mlp_set_params(qa_mlp *m, const float *host, int64_t count) {
+    if (!m || !host || count != m->nparams) return fail(QA_ERR_ARG, "parameter buffer size mismatch");
+    QA_TRY(begin(m->ctx));
+    QA_CK(cudaMemcpy(m->W, host, sizeof(float) * count, cudaMemcpyHostToDevice));
+    QA_CK(cudaMemset(m->mo, 0, sizeof(float) * count));
+    QA_CK(cudaMemset(m->vo, 0, sizeof(float) * count));
+    m->step = 0;
+    mlp_to_bf16_kernel<<<(unsigned)((m->nparams + 255) / 256), 256, 0, m->ctx->stream>>>(m->W, m->nparams, m->wmap,
+                                                                                       m->W16);
+    QA_CK(cudaGetLastError());
+    QA_CK(cudaStreamSynchronize(m->ctx->stream));
+    return QA_OK;
+}
+
+int qa_mlp_forward(qa_mlp *m, const float *X, int batch, float *Y) {
+    if (!m || !X || !Y || batch <= 0) return fail(QA_ERR_ARG, "qa_mlp_forward: bad arguments");
+    QA_TRY(begin(m->ctx));
+    QA_TRY(mlp_prepare(m, batch, X, nullptr));
+    QA_TRY(mlp_forward_dev(m, batch));
+    const int L = (int)m->dims.size() - 1;
+    QA_CK(cudaMemcpyAsync(Y, m->acts + m->aoff[L], sizeof(float) * (size_t)batch * m->dims[L], cudaMemcpyDeviceToHost,
+                          m->ctx->stream));
+    QA_CK(cudaStreamSynchronize(m->ctx->stream));
+    return QA_OK;
+}
+
+int qa_mlp_loss_grad(qa_mlp *m, const float *X, const float *T, int batch, float *loss, float *grads) {
+    if (!m || !X || !T || batch <= 0) return fail(QA_ERR_ARG, "qa_mlp_loss_grad: bad arguments");
+    QA_TRY(begin(m->ctx));
+    QA_TRY(mlp_prepare(m, batch, X, T));
+    QA_TRY(mlp_forward_dev(m, batch));
+    QA_TRY(mlp_backward_dev(m, batch, loss));
+    if (grads) QA_CK(cudaMemcpy(grads, m->g, sizeof(float) * m->nparams, cudaMemcpyDeviceToHost));
+    return QA_OK;
+}
+
+int qa_mlp_train_step(qa_mlp *m, const float *X, const float *T, int batch, float lr, float *loss) {
+    if (!m || !X || !T || batch <= 0 || !(lr > 0.0f)) return fail(QA_ERR_ARG, "qa_mlp_train_step: bad arguments");
+    QA_TRY(begin(m->ctx));
+    QA_TRY(mlp_prepare(m, batch, X, T));
+    QA_TRY(mlp_forward_dev(m, batch));
+    QA_TRY(mlp_backward_dev(m, batch, loss));
+    m->step += 1;
+    const float c1 = (float)(1.0 - std::pow(0.9, m->step)), c2 = (float)(1.0 - std::pow(0.999, m->step));
+    mlp_adam_kernel<<<(unsigned)((m->nparams + 255) / 256), 256, 0, m->ctx->stream>>>(
+        m->W, m->g, m->mo, m->vo, m->nparams, lr, 0.9f, 0.999f, 1e-8f, c1, c2, m->wmap, m->W16);
+    QA_CK(cudaGetLastError());
+    QA_CK(cudaStreamSynchronize(m->ctx->stream));
+    return QA_OK;
+}
+
+// Stage 1 of run_chi: every (read, scan point) probe of the batch in one
+// ring-kernel launch; chi[(problem*reads + read)*points + point].
+static int chi_stage1(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_chi_params *prm,
+                      int kind, int n_max, const std::vector<double> &scan_g, std::vector<double> &chi,
+                      int64_t &launches, int64_t &h2d, int64_t &d2h, unsigned long long *cnt_total,
+                      float &pilot_ms) {
+    const int P = prm->trotter_slices, K = prm->replicas, Pts = prm->scan_points;
+    const int reads_total = n_problems * prm->reads;
+    Layout L;
+    ProbDev *d_probs;
+    RingDev *d_rings;
+    uint32_t *d_spins;
+    float *d_fields;
+    double *d_sum, *d_best;
+    int *d_bstep;
+    uint32_t *d_bits;
+    unsigned long long *d_cnt;
+    float *d_B, *d_T4;
+    QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    // ---- Stage 1: all (read, point) probes in one launch
+    build_rings(L, problems, n_problems, prm->reads, K, P, prm->seed, Pts);
+    const int nr = (int)L.rings.size();
+    const int sweeps_total = prm->scan_burn + prm->scan_sweeps;
+    QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
+    std::vector<float> B(Pts), T4(Pts);
+    for (int m = 0; m < Pts; ++m) {
+        B[m] = (float)(2.0 * (prm->beta / (double)P));
+        T4[m] = (float)(4.0 * trotter_coupling(prm->beta, scan_g[m], P));
+    }
+    int *d_mag, *d_nof;
+    double *d_chi;
+    QA_TRY(ws_array(ctx, W_A, Pts, &d_B));
+    QA_TRY(ws_array(ctx, W_T4, Pts, &d_T4));
+    QA_TRY(ws_array(ctx, W_SUM, nr, &d_sum));
+    QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
+    QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
+    QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
+    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    QA_TRY(ws_array(ctx, W_MAG, (size_t)nr * sweeps_total, &d_mag));
+    QA_TRY(ws_array(ctx, W_PROBOF, (size_t)reads_total * Pts, &d_nof));
+    QA_TRY(ws_array(ctx, W_EXACT, (size_t)reads_total * Pts, &d_chi));
+    std::vector<int> nof((size_t)reads_total * Pts);
+    for (int p = 0; p < n_problems; ++p)
+        for (int i = 0; i < prm->reads * Pts; ++i) nof[(size_t)p * prm->reads * Pts + i] = problems[p]->n;
+    std::vector<double> inf(nr, INFINITY);
+    QA_CK(cudaMemcpyAsync(d_B, B.data(), sizeof(float) * Pts, cudaMemcpyHostToDevice, ctx->stream));
+    QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * Pts, cudaMemcpyHostToDevice, ctx->stream));
+    QA_CK(cudaMemcpyAsync(d_nof, nof.data(), sizeof(int) * nof.size(), cudaMemcpyHostToDevice, ctx->stream));
+    QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+    h2d += (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * Pts +
+                     sizeof(int) * nof.size() + sizeof(double) * nr);
+    RingPlan pl;
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PILOT_INIT,
+                      !pl.pm1));
+    RingParams rp{};
+    rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
+    rp.P = P; rp.steps_total = 1; rp.spb = sweeps_total; rp.wls = 0; rp.slice_tag = DOM_PILOT;
+    rp.B = d_B; rp.T4 = d_T4; rp.ring_sum = d_sum; rp.rec_base = 0; rp.rec_stride = 1;
+    rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max;
+    rp.mag = d_mag; rp.counters = d_cnt; rp.step0 = 0; rp.step1 = 1; rp.init_fields = 1;
+    QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+    const int probes = reads_total * Pts;
+    chi_point_kernel<<<(probes + 127) / 128, 128, 0, ctx->stream>>>(d_mag, probes, K, sweeps_total,
+                                                                     prm->scan_burn, d_nof, P, d_chi);
+    QA_CK(cudaGetLastError());
+    launches += (pl.pm1 ? 1 : 2) + 2;
+    unsigned long long c[4];
+    QA_CK(cudaMemcpyAsync(chi.data(), d_chi, sizeof(double) * chi.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    QA_CK(cudaEventElapsedTime(&pilot_ms, ctx->ev[0], ctx->ev[1]));
+    d2h += (int64_t)(sizeof(double) * chi.size() + sizeof(c));
+    for (int i = 0; i < 4; ++i) cnt_total[i] += c[i];
+    return QA_OK;
+}
+
+// Stage 1 alone: the chi_B curves of every (problem, read).
+int qa_chi_pilot(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_chi_params *prm,
+                 double *scan_chi, qa_stats *stats) {
+    QA_TRY(begin(ctx));
+    if (!prm || !scan_chi) return fail(QA_ERR_ARG, "null argument");
+    if (!(prm->beta > 0.0)) return fail(QA_ERR_ARG, "beta must be > 0.");
+    if (!(prm->gamma_end > 0.0) || !(prm->gamma_start > prm->gamma_end))
+        return fail(QA_ERR_ARG, "Require gamma_start > gamma_end > 0.");
+    if (prm->scan_points < 4) return fail(QA_ERR_ARG, "scan_points must be >= 4.");
+    if (prm->scan_sweeps <= 0) return fail(QA_ERR_ARG, "scan_sweeps must be > 0.");
+    if (prm->scan_burn < 0) return fail(QA_ERR_ARG, "scan_burn must be >= 0.");
+    if (prm->trotter_slices <= 0) return fail(QA_ERR_ARG, "trotter_slices must be > 0.");
+    if (prm->replicas <= 0) return fail(QA_ERR_ARG, "replicas must be > 0.");
+    if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
+    int kind, n_max;
+    QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
+    const int Pts = prm->scan_points;
+    const double A0 = prm->driver_A0 > 0.0 ? prm->driver_A0 : prm->gamma_start;
+    const double s_lo = A0 / (A0 + prm->gamma_start), s_hi = A0 / (A0 + prm->gamma_end);
+    std::vector<double> scan_g(Pts), chi((size_t)n_problems * prm->reads * Pts);
+    for (int m = 0; m < Pts; ++m)
+        scan_g[m] = chi_s_to_gamma(A0, s_lo + (s_hi - s_lo) * (double)m / (double)(Pts - 1));
+    int64_t launches = 0, h2d = 0, d2h = 0;
+    unsigned long long cnt[4] = {0, 0, 0, 0};
+    float ms = 0.0f;
+    QA_TRY(chi_stage1(ctx, problems, n_problems, prm, kind, n_max, scan_g, chi, launches, h2d, d2h, cnt, ms));
+    std::memcpy(scan_chi, chi.data(), sizeof(double) * chi.size());
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->slice_attempts = (int64_t)cnt[0];
+        stats->slice_accepts = (int64_t)cnt[1];
+        stats->sweep_ms = ms;
+        stats->total_ms = ms;
+        stats->sweep_launches = 1;
+        stats->launches = launches;
+        stats->h2d_bytes = h2d;
+        stats->d2h_bytes = d2h;
+    }
+    return QA_OK;
+}
+
 // ---------------------------------------------------------------------- SQA-Chi
 int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_chi_params *prm,
                qa_chi_out *outs, qa_stats *stats) {
@@ -1116,63 +1446,8 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     if (prm->scan_chi_in) {
         std::memcpy(chi.data(), prm->scan_chi_in, sizeof(double) * chi.size());
     } else {
-        // ---- Stage 1: all (read, point) probes in one launch
-        build_rings(L, problems, n_problems, prm->reads, K, P, prm->seed, Pts);
-        const int nr = (int)L.rings.size();
-        const int sweeps_total = prm->scan_burn + prm->scan_sweeps;
-        QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
-        std::vector<float> B(Pts), T4(Pts);
-        for (int m = 0; m < Pts; ++m) {
-            B[m] = (float)(2.0 * (prm->beta / (double)P));
-            T4[m] = (float)(4.0 * trotter_coupling(prm->beta, scan_g[m], P));
-        }
-        int *d_mag, *d_nof;
-        double *d_chi;
-        QA_TRY(ws_array(ctx, W_A, Pts, &d_B));
-        QA_TRY(ws_array(ctx, W_T4, Pts, &d_T4));
-        QA_TRY(ws_array(ctx, W_SUM, nr, &d_sum));
-        QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
-        QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
-        QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
-        QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
-        QA_TRY(ws_array(ctx, W_MAG, (size_t)nr * sweeps_total, &d_mag));
-        QA_TRY(ws_array(ctx, W_PROBOF, (size_t)reads_total * Pts, &d_nof));
-        QA_TRY(ws_array(ctx, W_EXACT, (size_t)reads_total * Pts, &d_chi));
-        std::vector<int> nof((size_t)reads_total * Pts);
-        for (int p = 0; p < n_problems; ++p)
-            for (int i = 0; i < prm->reads * Pts; ++i) nof[(size_t)p * prm->reads * Pts + i] = problems[p]->n;
-        std::vector<double> inf(nr, INFINITY);
-        QA_CK(cudaMemcpyAsync(d_B, B.data(), sizeof(float) * Pts, cudaMemcpyHostToDevice, ctx->stream));
-        QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * Pts, cudaMemcpyHostToDevice, ctx->stream));
-        QA_CK(cudaMemcpyAsync(d_nof, nof.data(), sizeof(int) * nof.size(), cudaMemcpyHostToDevice, ctx->stream));
-        QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
-        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
-        h2d += (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * Pts +
-                         sizeof(int) * nof.size() + sizeof(double) * nr);
-        RingPlan pl;
-        QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
-        QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PILOT_INIT,
-                          !pl.pm1));
-        RingParams rp{};
-        rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
-        rp.P = P; rp.steps_total = 1; rp.spb = sweeps_total; rp.wls = 0; rp.slice_tag = DOM_PILOT;
-        rp.B = d_B; rp.T4 = d_T4; rp.ring_sum = d_sum; rp.rec_base = 0; rp.rec_stride = 1;
-        rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max;
-        rp.mag = d_mag; rp.counters = d_cnt; rp.step0 = 0; rp.step1 = 1; rp.init_fields = 1;
-        QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
-        const int probes = reads_total * Pts;
-        chi_point_kernel<<<(probes + 127) / 128, 128, 0, ctx->stream>>>(d_mag, probes, K, sweeps_total,
-                                                                         prm->scan_burn, d_nof, P, d_chi);
-        QA_CK(cudaGetLastError());
-        launches += (pl.pm1 ? 1 : 2) + 2;
-        unsigned long long c[4];
-        QA_CK(cudaMemcpyAsync(chi.data(), d_chi, sizeof(double) * chi.size(), cudaMemcpyDeviceToHost, ctx->stream));
-        QA_CK(cudaMemcpyAsync(c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
-        QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-        QA_CK(cudaStreamSynchronize(ctx->stream));
-        QA_CK(cudaEventElapsedTime(&pilot_ms, ctx->ev[0], ctx->ev[1]));
-        d2h += (int64_t)(sizeof(double) * chi.size() + sizeof(c));
-        for (int i = 0; i < 4; ++i) cnt_total[i] += c[i];
+        QA_TRY(chi_stage1(ctx, problems, n_problems, prm, kind, n_max, scan_g, chi, launches, h2d, d2h,
+                          cnt_total, pilot_ms));
     }
 
     // ---- Stage 2 (host) per read

@@ -320,7 +320,11 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
         if not (g0 > g1 > 0.0):
             raise ValueError(f"sqa_chi requires gamma_start > gamma_end > 0 (got {g0} and {g1}).")
         steps = int(optimal_num_steps) if optimal_num_steps is not None else max(100, len(sg) if sg else 100)
-        curve = chi_curve(ising) if callable(chi_curve) else chi_curve
+        if hasattr(chi_curve, "curve"):
+            curve = chi_curve.curve(ising, beta=beta, gamma_start=g0, gamma_end=g1, slices=trotter_slices,
+                                    points=chi_scan_points)
+        else:
+            curve = chi_curve(ising) if callable(chi_curve) else chi_curve
         ann = SQAChiAnnealer(ising, trotter_slices, replicas, backend=backend)
         res = ann.run_chi_reads(beta, g0, g1, steps, sweeps_per_beta, chi_scan_points, chi_scan_sweeps,
                                 chi_scan_burn, chi_floor_fraction, chi_driver_A0, optimal_beta_ramp_fraction,
