@@ -232,6 +232,7 @@ def main():
 
     import qlatanneal_b200 as qa
     from qlatanneal_b200 import _lib
+    from qlatanneal_b200.distributed import minloc_best, read_block
     _lib.Engine.get(local)
 
     n, P, reads = WL["n"], WL["P"], WL["reads"]
@@ -240,7 +241,8 @@ def main():
     sched = qa.SQASchedule.from_vectors(betas, gammas)
     model = qa.DenseIsing(h, J)
     ann = qa.SQAAnnealer(model, sched, P, 1, device=local)
-    seed = WL["run_seed"] + 1000003 * rank
+    # rank k anneals reads [k*reads, (k+1)*reads) of one job: read r keeps the key run_seed + r
+    seed = WL["run_seed"] + read_block(world * reads, rank, world).start
 
     def barrier():
         torch.cuda.synchronize()
@@ -300,10 +302,11 @@ def main():
     achieved = (bytes_step / launches) / (avg_launch_ms / 1e3) / 1e9
     traffic = load_traffic()
 
-    # best energy over all ranks (the MINLOC of qanneal's MPI reads helper)
-    be = torch.tensor([min(r.best_energy for r in res)], dtype=torch.float64, device=dev)
+    # best energy over all ranks (the MINLOC + broadcast of qanneal's MPI reads helper)
+    i_best = int(np.argmin([r.best_energy for r in res]))
+    best_E = float(res[i_best].best_energy)
     if world > 1:
-        dist.all_reduce(be, op=dist.ReduceOp.MIN)
+        best_E, _, _ = minloc_best(best_E, res[i_best].best_state.as_array())
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -327,7 +330,7 @@ def main():
             "config": {"workload": WORKLOAD_NAME, "n": n, "trotter_slices": P, "reads_per_gpu": reads,
                        "steps": WL["steps"], "sweeps_per_step": [WL["spb"], WL["wls"]],
                        "site_attempts_per_step": sites_step, "l2": "flushed (256 MiB write) between steps",
-                       "parallelism": f"replicas x{world}", "best_energy": float(be.item()),
+                       "parallelism": f"replicas x{world}", "best_energy": best_E,
                        "slice_accept_rate": st.slice_accepts / max(1, st.slice_attempts),
                        "worldline_accept_rate": st.worldline_accepts / max(1, st.worldline_attempts)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -1,0 +1,153 @@
+"""Reads sharded over ranks (gloo, world size 2, CPU): the partition, the
+MINLOC/broadcast exchange, a sharded solve equal read for read to the
+unsharded one (annealing by the oracle), and a rank that fails."""
+import json
+import os
+import socket
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from qlatanneal_b200.distributed import lpt_partition, read_block, sweep_cost  # noqa: E402
+
+
+def test_read_block_covers_reads():
+    for reads in (0, 1, 5, 64, 257):
+        for world in (1, 2, 3, 8):
+            blocks = [read_block(reads, r, world) for r in range(world)]
+            flat = [i for b in blocks for i in b]
+            assert flat == list(range(reads))
+            sizes = [len(b) for b in blocks]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        read_block(4, 2, 2)
+
+
+def test_lpt_partition():
+    costs = [sweep_cost(n, 16, 32, 2000, 25, 32) for n in (4096, 512, 2048, 1024, 3000, 700, 700)]
+    plan = lpt_partition(costs, 3)
+    assert sorted(i for p in plan for i in p) == list(range(len(costs)))
+    loads = [sum(costs[i] for i in p) for p in plan]
+    assert max(loads) <= 4 / 3 * (sum(costs) / 3) + max(costs)  # Graham's LPT bound, loosely
+    assert plan == lpt_partition(costs, 3)  # deterministic
+    assert lpt_partition([1.0, 1.0], 2) == [[0], [1]]
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, out_dir, mode):
+    import datetime
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=20))
+    try:
+        from qlatanneal_b200.distributed import minloc_best, solve_sharded
+        if mode == "solve":
+            res = solve_sharded(None, reads=7, seed=41, runner=_oracle_runner)
+            with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+                json.dump({"best": res.best_energy, "spins": res.best_sample.tolist(), "src": res.best_rank,
+                           "energies": res.energies.tolist(), "reads": list(res.reads)}, f)
+        elif mode == "tie":
+            e, s, src = minloc_best(-3.0, np.full(5, 1 if rank == 0 else -1, np.int8))
+            with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+                json.dump({"best": e, "spins": s.tolist(), "src": src}, f)
+        elif mode == "fail":
+            if rank == 1:
+                raise RuntimeError("rank 1 fails before the exchange")
+            try:
+                minloc_best(-1.0, np.ones(4, np.int8))
+                status = "returned"
+            except Exception as exc:  # the peer is gone: the collective errors out
+                status = "error: " + type(exc).__name__
+            with open(os.path.join(out_dir, "r0.json"), "w") as f:
+                json.dump({"status": status}, f)
+    finally:
+        try:
+            dist.destroy_process_group()
+        except Exception:
+            pass
+
+
+_INST = dict(n=24, seed=5)
+
+
+def _instance():
+    from qlatanneal_b200.instances import sk_dense
+    return sk_dense(_INST["n"], _INST["seed"])
+
+
+def _oracle_runner(problem, reads, seed):
+    """solve() stand-in that anneals on the CPU oracle: read r uses key seed + r."""
+    from oracle_lib import Oracle
+
+    class R:
+        pass
+
+    o = Oracle()
+    h, J = _instance()
+    m = o.dense(h, J)
+    betas = np.geomspace(0.1, 3.0, 20)
+    out = R()
+    out.energies, out.samples = [], []
+    for r in range(reads):
+        best, E, _, _ = o.sa_run(m, betas, 2, seed, read=r)
+        out.energies.append(E)
+        out.samples.append(best)
+    return out
+
+
+def _spawn(mode, out_dir):
+    import torch.multiprocessing as tmp
+    ctx = tmp.spawn(_worker, args=(2, _free_port(), out_dir, mode), nprocs=2, join=False)
+    ok = True
+    try:
+        while not ctx.join(timeout=120):
+            pass
+    except Exception:
+        ok = False
+    return ok
+
+
+def test_sharded_solve_equals_single_process():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    with tempfile.TemporaryDirectory() as d:
+        assert _spawn("solve", d)
+        r0 = json.load(open(os.path.join(d, "r0.json")))
+        r1 = json.load(open(os.path.join(d, "r1.json")))
+    ref = _oracle_runner(None, 7, 41)
+    assert r0["reads"] == [0, 1, 2, 3] and r1["reads"] == [4, 5, 6]
+    assert r0["energies"] == ref.energies and r1["energies"] == ref.energies
+    i = int(np.argmin(ref.energies))
+    assert r0["best"] == r1["best"] == ref.energies[i]
+    assert r0["spins"] == r1["spins"] == ref.samples[i].tolist()
+    assert r0["src"] == (0 if i < 4 else 1)
+
+
+def test_minloc_ties_go_to_lowest_rank():
+    with tempfile.TemporaryDirectory() as d:
+        assert _spawn("tie", d)
+        r0 = json.load(open(os.path.join(d, "r0.json")))
+        r1 = json.load(open(os.path.join(d, "r1.json")))
+    assert r0["src"] == r1["src"] == 0
+    assert r0["spins"] == r1["spins"] == [1] * 5
+
+
+def test_failed_rank_ends_the_exchange_with_an_error():
+    with tempfile.TemporaryDirectory() as d:
+        _spawn("fail", d)  # rank 1 exits with an exception
+        r0 = json.load(open(os.path.join(d, "r0.json")))
+    assert r0["status"].startswith("error")
