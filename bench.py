@@ -43,6 +43,12 @@ WORKLOAD_NAME = ("dense SQA, SK n=512 J=+-1, h~N(0,0.1^2) fp32, P=32, beta=0.5P,
                  "1000 steps, 1 slice + 1 worldline sweep per step, 256 reads")
 
 
+# SQA-Chi with a learned schedule: training set, pilot and production runs.
+CHI = dict(train=2000, n_min=256, n_max=2048, P=64, beta=4.0, gamma0=3.0, gamma1=0.01, points=64, sweeps=200,
+           burn=50, train_seed=7, prod_n=1024, reads=512, num_steps=100, sweeps_per_step=20, instances=3,
+           prod_seed=9001)
+
+
 def schedule(steps=None):
     steps = WL["steps"] if steps is None else steps
     P = WL["P"]
@@ -199,6 +205,89 @@ def run_reference_arm(args):
     return 0
 
 
+def tts99(t_call, reads, p):
+    """Time to reach the target with 99% probability, per-read time t/reads
+    repeated ln(0.01)/ln(1-p) times (one read when p >= 0.99)."""
+    if p <= 0.0:
+        return float("inf")
+    t = t_call / reads
+    return t if p >= 0.99 else t * np.log(0.01) / np.log(1.0 - p)
+
+
+def run_chi_ttt(args):
+    """Learned vs pilot-scan SQA-Chi: build the training set with the plain
+    pilot on the GPU, train the MLP with the library's kernels, then anneal
+    SK instances with both schedules and compare time-to-99%-of-best-known."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    import qlatanneal_b200 as qa
+    from qlatanneal_b200 import learned
+    from qlatanneal_b200.instances import sk_dense
+    c = CHI
+    run = dict(beta=c["beta"], gamma_start=c["gamma0"], gamma_end=c["gamma1"], slices=c["P"])
+    t0 = time.perf_counter()
+    X, Y, _ = learned.training_set(
+        learned.synthetic_instances(args.chi_train, c["n_min"], c["n_max"], c["train_seed"]), c["beta"], c["gamma0"],
+        c["gamma1"], c["P"], c["points"], c["sweeps"], c["burn"], seed=c["train_seed"])
+    t_data = time.perf_counter() - t0
+    model = learned.ChiCurveModel(seed=c["train_seed"])
+    t0 = time.perf_counter()
+    hist = model.fit(X, Y, epochs=300, batch=64, lr=2e-3, seed=1, run_params=dict(run, points=c["points"]))
+    t_fit = time.perf_counter() - t0
+    kw = dict(num_steps=c["num_steps"], sweeps_per_step=c["sweeps_per_step"], scan_points=c["points"],
+              scan_sweeps=c["sweeps"], scan_burn=c["burn"], reads=c["reads"])
+    rows = []
+    for k in range(args.chi_instances):
+        h, J = sk_dense(c["prod_n"], c["prod_seed"] + k)
+        m = qa.DenseIsing(h, J)
+        ann = qa.SQAChiAnnealer(m, c["P"], 1)
+        ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], num_steps=2, sweeps_per_step=1, scan_points=4,
+                          scan_sweeps=2, scan_burn=1, reads=2, seed=1)  # device copy + warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rp = ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], seed=1000 * k, **kw)
+        t_p = time.perf_counter() - t0
+        st_p = ann.last_stats
+        t0 = time.perf_counter()
+        curve = model.curve(m)
+        fallback = curve is None
+        rl = ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], seed=1000 * k + 500, scan_chi=curve, **kw)
+        t_l = time.perf_counter() - t0
+        st_l = ann.last_stats
+        ep = np.array([r.best_energy for r in rp])
+        el = np.array([r.best_energy for r in rl])
+        best = float(min(ep.min(), el.min()))
+        target = 0.99 * best
+        pp, pl = float(np.mean(ep <= target)), float(np.mean(el <= target))
+        rows.append(dict(instance_seed=c["prod_seed"] + k, best_known=best, p_pilot=pp, p_learned=pl,
+                         t_pilot_s=t_p, t_learned_s=t_l, gpu_ms_pilot=st_p.total_ms, gpu_ms_learned=st_l.total_ms,
+                         tts99_pilot_s=tts99(t_p, c["reads"], pp), tts99_learned_s=tts99(t_l, c["reads"], pl),
+                         mean_E_pilot=float(ep.mean()), mean_E_learned=float(el.mean()), fallback=fallback,
+                         predicted_std=model.last_std))
+        m.release()
+    tl = float(np.median([r["tts99_learned_s"] for r in rows]))
+    tp = float(np.median([r["tts99_pilot_s"] for r in rows]))
+    line = {
+        "metric": "time-to-target (99% of best-known energy, TTS99), SQA-Chi learned vs pilot-scan schedule",
+        "value": tl, "unit": "s", "higher_is_better": False, "n_gpus": 1, "pilot_value": tp,
+        "speedup_vs_pilot": tp / tl if tl > 0 else None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"SQA-Chi, SK n={c['prod_n']} J=+-1 h=0, P={c['P']}, beta={c['beta']}, Gamma "
+                               f"{c['gamma0']}->{c['gamma1']}, {c['num_steps']} steps x {c['sweeps_per_step']} "
+                               f"sweeps, {c['reads']} reads per call; pilot {c['points']} points x "
+                               f"({c['burn']} burn + {c['sweeps']}) sweeps per read",
+                   "training": {"instances": int(len(X)), "n_range": [c["n_min"], c["n_max"]],
+                                "kinds": "half dense SK +-1, half 3-regular +-1, h=0",
+                                "pilot_gpu_s": t_data, "fit_s": t_fit, "epochs_run": len(hist),
+                                "val_loss": model.val_loss, "max_std": model.max_std}},
+        "instances": rows,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def flush_l2(torch, dev):
     buf = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     buf.fill_(1)
@@ -212,11 +301,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="sqa", choices=["sqa", "chi-ttt"],
+                    help="sqa: the sweep-throughput line (default); chi-ttt: time-to-target of SQA-Chi with the "
+                         "learned vs the pilot-scan schedule, training set included")
+    ap.add_argument("--chi-train", type=int, default=CHI["train"], help="chi-ttt: training instances")
+    ap.add_argument("--chi-instances", type=int, default=CHI["instances"], help="chi-ttt: production instances")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "chi-ttt":
+        return run_chi_ttt(args)
 
     import torch
     import torch.distributed as dist

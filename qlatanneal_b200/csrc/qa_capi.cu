@@ -337,18 +337,36 @@ int exact_energies(qa_ctx *ctx, int kind, const ProbDev *d_probs, const Layout &
 // Which ring kernel a batch runs on, and with what launch shape.
 struct RingPlan {
     bool pm1 = false;
+    int gbytes = 4;       // pm1: bytes per field (4 int32, 2 int16)
+    bool jw_smem = true;  // pm1: J bits in shared memory
     int W = 1;
     size_t smem = 0;
     int smem_fields = 1;
 };
 
+// Dense +-1 batches run the bit-packed kernel, in the first of these forms
+// whose ring fits in shared memory: J bits + int32 fields, J bits + int16
+// fields, int16 fields with J read from L2.  P <= 64 (worldlines are 64-bit
+// columns) and n <= 2048.  Anything else runs ring_kernel.
 int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, int P, int n_max, RingPlan *pl) {
     pl->W = std::max(1, std::min(32, (P + 1) / 2));
-    pl->pm1 = kind == K_DENSE && P <= 64 && n_max <= 1024 &&
-              pm1_smem_bytes(P, n_max) <= (size_t)ctx->smem_optin && !std::getenv("QA_DISABLE_PM1");
+    pl->pm1 = kind == K_DENSE && P <= 64 && n_max <= 2048 && !std::getenv("QA_DISABLE_PM1");
     for (int p = 0; p < np && pl->pm1; ++p) pl->pm1 = probs[p]->dev.Jw != nullptr;
     if (pl->pm1) {
-        pl->smem = pm1_smem_bytes(P, n_max);
+        const size_t cap = (size_t)ctx->smem_optin;
+        const bool int32_only = std::getenv("QA_PM1_INT32_ONLY") != nullptr;
+        if (pm1_smem_bytes(P, n_max, 4, true) <= cap) {
+            pl->gbytes = 4; pl->jw_smem = true;
+        } else if (!int32_only && pm1_smem_bytes(P, n_max, 2, true) <= cap) {
+            pl->gbytes = 2; pl->jw_smem = true;
+        } else if (!int32_only && pm1_smem_bytes(P, n_max, 2, false) <= cap) {
+            pl->gbytes = 2; pl->jw_smem = false;
+        } else {
+            pl->pm1 = false;
+        }
+    }
+    if (pl->pm1) {
+        pl->smem = pm1_smem_bytes(P, n_max, pl->gbytes, pl->jw_smem);
         pl->smem_fields = 0;
         return QA_OK;
     }
@@ -367,9 +385,11 @@ int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n
     rp.W = pl.W;
     rp.smem_fields = pl.smem_fields;
     if (pl.pm1) {
+        auto kern = pl.gbytes == 4 ? ring_pm1_kernel<int, true>
+                                   : (pl.jw_smem ? ring_pm1_kernel<short, true> : ring_pm1_kernel<short, false>);
         if (pl.smem > 48 * 1024)
-            QA_CK(cudaFuncSetAttribute(ring_pm1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
-        ring_pm1_kernel<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
+            QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        kern<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
         QA_CK(cudaGetLastError());
         return QA_OK;
     }
@@ -845,59 +865,28 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     }
 
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    const int W = std::max(1, std::min(32, (P + 1) / 2));
-    // dense +-1 couplings: the bit-packed kernel (fields built in-kernel)
-    bool use_pm1 = kind == K_DENSE && P <= 64 && n_max <= 1024 &&
-                   pm1_smem_bytes(P, n_max) <= (size_t)ctx->smem_optin && !std::getenv("QA_DISABLE_PM1");
-    for (int p = 0; p < n_problems && use_pm1; ++p) use_pm1 = problems[p]->dev.Jw != nullptr;
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !use_pm1));
-    size_t smem = ring_smem_bytes(P, n_max, W, true);
-    int smem_fields = 1;
-    const size_t cap = (size_t)std::min(ctx->smem_optin, 200 * 1024);
-    if (smem > cap) {
-        smem_fields = 0;
-        smem = ring_smem_bytes(P, n_max, W, false);
-    }
-    if (smem > (size_t)ctx->smem_optin) return fail(QA_ERR_ARG, "ring state does not fit in shared memory.");
+    RingPlan pl;
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
+    // dense +-1 couplings: the bit-packed kernel builds its fields in-kernel
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.pm1));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
-    rp.P = P; rp.W = W; rp.steps_total = steps; rp.spb = prm->sweeps_per_beta; rp.wls = prm->worldline_sweeps;
+    rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_beta; rp.wls = prm->worldline_sweeps;
     rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.B = d_A; rp.T4 = d_T4; rp.per_slot_sched = 0;
-    rp.smem_fields = smem_fields; rp.ring_sum = d_sum; rp.ring_min = nullptr; rp.ring_bond = nullptr;
+    rp.ring_sum = d_sum; rp.ring_min = nullptr; rp.ring_bond = nullptr;
     rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max; rp.mag = nullptr;
     rp.counters = d_cnt;
     rp.rec_base = 0;
     rp.rec_stride = steps;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    int rc = QA_OK;
     const int seg = 256;
     const int n_seg = (steps + seg - 1) / seg;
-    if (use_pm1) {
-        const size_t sm1 = pm1_smem_bytes(P, n_max);
-        if (sm1 > 48 * 1024)
-            QA_CK(cudaFuncSetAttribute(ring_pm1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-        for (int s0 = 0; s0 < steps; s0 += seg) {
-            rp.step0 = s0;
-            rp.step1 = std::min(steps, s0 + seg);
-            rp.init_fields = s0 == 0;
-            ring_pm1_kernel<<<nr, 32 * W, sm1, ctx->stream>>>(rp);
-            QA_CK(cudaGetLastError());
-        }
-    } else {
-        dispatch_kind(kind, [&](auto Kd) {
-            auto kern = ring_kernel<decltype(Kd)::value>;
-            if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            for (int s0 = 0; s0 < steps && rc == QA_OK; s0 += seg) {
-                rp.step0 = s0;
-                rp.step1 = std::min(steps, s0 + seg);
-                kern<<<nr, 32 * W, smem, ctx->stream>>>(rp);
-                cudaError_t e = cudaGetLastError();
-                if (e != cudaSuccess)
-                    rc = fail(QA_ERR_CUDA, std::string("ring_kernel launch: ") + cudaGetErrorString(e));
-            }
-        });
+    for (int s0 = 0; s0 < steps; s0 += seg) {
+        rp.step0 = s0;
+        rp.step1 = std::min(steps, s0 + seg);
+        rp.init_fields = s0 == 0;
+        QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
     }
-    QA_TRY(rc);
     QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
     QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
@@ -949,7 +938,7 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
         stats->sweep_ms = a;
         stats->total_ms = b;
         stats->sweep_launches = n_seg;
-        stats->launches = (use_pm1 ? 2 : 3) + n_seg;
+        stats->launches = (pl.pm1 ? 2 : 3) + n_seg;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * steps +
                                      (sizeof(double) + sizeof(int)) * nr + sizeof(int) * nr);
         stats->d2h_bytes = (int64_t)(sizeof(double) * sums.size() + (2 * sizeof(double) + sizeof(int)) * nr +

@@ -25,17 +25,20 @@ namespace qa {
 
 __host__ __device__ inline int pm1_npad(int n) { return (n + 127) / 128 * 128; }
 
-__host__ __device__ inline size_t pm1_smem_bytes(int P, int n) {
+// Shared memory of one ring: gbytes = bytes per field (4: int32, 2: int16);
+// jw_smem = J bits staged in shared memory (else read through L1/L2).
+__host__ __device__ inline size_t pm1_smem_bytes(int P, int n, int gbytes = 4, bool jw_smem = true) {
     const int nw = (n + 31) / 32, np = pm1_npad(n);
-    size_t b = (size_t)nw * np * 4;                // Jw
+    size_t b = jw_smem ? (size_t)nw * np * 4 : 0;  // Jw
     b += align_up((size_t)P * nw * 4, 16);         // S
     b += (size_t)np * 4;                           // h
-    b += (size_t)P * np * 4;                       // G
+    b += align_up((size_t)P * np * gbytes, 16);    // G
     b += (size_t)np * 8;                           // W (worldline bits)
     b += (size_t)np * 4;                           // Gsum (worldline slice sums)
     b += (size_t)np * 4;                           // uw (worldline uniforms)
     b += align_up((size_t)P * 8, 16);              // cellE
-    b += 32 * 4 + 32 * 8 + 32 * 4 + 64;            // masks, old worldlines, partials, flags
+    b += (size_t)(np / 32) * 4;                    // worldline move masks, one per block (np/32 >= nw)
+    b += 32 * 8 + 32 * 4 + 64;                     // old worldlines, partials, flags
     return b + 64;
 }
 
@@ -71,9 +74,32 @@ __device__ __forceinline__ void pm1_block_update(int *Gt, const uint32_t *Jw, in
     }
 }
 
+// int16 fields (|g| <= n - 1 < 2^15): eight per lane per 128-bit access,
+// two per 32-bit word updated by a halfword-wise add (no carry between them).
+__device__ __forceinline__ uint32_t pack_delta2(int lo, int hi) {
+    return ((uint32_t)lo & 0xffffu) | ((uint32_t)hi << 16);
+}
+
+__device__ __forceinline__ void pm1_block_update(short *Gt, const uint32_t *Jw, int npad, int n, int q, uint32_t F,
+                                                 uint32_t sold, int lane) {
+    const uint32_t *Jq = Jw + q * npad;
+    for (int base = lane * 8; base < n; base += 256) {
+        const uint4 ja = *reinterpret_cast<const uint4 *>(Jq + base);
+        const uint4 jb = *reinterpret_cast<const uint4 *>(Jq + base + 4);
+        uint4 g = *reinterpret_cast<uint4 *>(Gt + base);
+        const uint32_t d = (base >> 5) == q ? (1u << (base & 31)) : 0u;
+        g.x = __vadd2(g.x, pack_delta2(flip_delta(ja.x, sold, F & ~d), flip_delta(ja.y, sold, F & ~(d << 1))));
+        g.y = __vadd2(g.y, pack_delta2(flip_delta(ja.z, sold, F & ~(d << 2)), flip_delta(ja.w, sold, F & ~(d << 3))));
+        g.z = __vadd2(g.z, pack_delta2(flip_delta(jb.x, sold, F & ~(d << 4)), flip_delta(jb.y, sold, F & ~(d << 5))));
+        g.w = __vadd2(g.w, pack_delta2(flip_delta(jb.z, sold, F & ~(d << 6)), flip_delta(jb.w, sold, F & ~(d << 7))));
+        *reinterpret_cast<uint4 *>(Gt + base) = g;
+    }
+}
+
 // One block of 32 spins (lane = spin) of slice t; rw is this lane's Philox word.
+template <typename GT>
 __device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, const uint32_t *Sp, const uint32_t *Sn,
-                                          int *Gt, unsigned long long *Wc, const float *h, int n, int npad, int q,
+                                          GT *Gt, unsigned long long *Wc, const float *h, int n, int npad, int q,
                                           int t, uint32_t rw, float B, float T4, int lane, unsigned long long &acc) {
     const int i = (q << 5) | lane;
     const bool valid = i < n;
@@ -84,7 +110,7 @@ __device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, cons
     const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
     const float u = u01(rw);
     const float hi = h[i];
-    const int gi = Gt[i];
+    const int gi = (int)Gt[i];
     bool ok = valid & metropolis_nb(
         __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gi)), sbit), B), tro), u);
     uint32_t m = __ballot_sync(FULL, ok);
@@ -111,7 +137,8 @@ __device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, cons
 }
 
 // One warp sweeps slice t; one Philox call per lane serves four blocks.
-__device__ __forceinline__ void pm1_sweep_slice(const uint32_t *Jw, uint32_t *S, int *G, unsigned long long *Wc,
+template <typename GT>
+__device__ __forceinline__ void pm1_sweep_slice(const uint32_t *Jw, uint32_t *S, GT *G, unsigned long long *Wc,
                                                 const float *h, int n, int nw, int npad, int NP, int t, float B,
                                                 float T4, uint64_t key, uint32_t rng_cell, uint32_t sigma,
                                                 uint32_t tag, int lane, unsigned long long &att,
@@ -119,7 +146,7 @@ __device__ __forceinline__ void pm1_sweep_slice(const uint32_t *Jw, uint32_t *S,
     uint32_t *St = S + t * nw;
     const uint32_t *Sp = S + (t == 0 ? NP - 1 : t - 1) * nw;
     const uint32_t *Sn = S + (t + 1 == NP ? 0 : t + 1) * nw;
-    int *Gt = G + t * npad;
+    GT *Gt = G + t * npad;
     att += (unsigned long long)n;
     for (int q4 = 0; q4 < nw; q4 += 4) {
         const U4 r = philox((uint32_t)(((q4 >> 2) << 5) | lane), rng_cell, sigma, tag, key);
@@ -137,6 +164,11 @@ __device__ __forceinline__ bool pm1_world_ok(const float *h, const int *Gs, cons
     return (i < n) & metropolis_nb(__fmul_rn(x, B), uw[i]);
 }
 
+// GT: field type (int: fields as int32; short: int16, for rings whose int32
+// fields would not fit).  JW_SMEM: J bits staged in shared memory, else read
+// from global memory (L2-resident: every ring of an instance reads the same
+// n^2/8 bytes).
+template <typename GT, bool JW_SMEM>
 __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const RingDev R = p.rings[blockIdx.x];
@@ -144,23 +176,26 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     const int NP = p.P, W = p.W, n = Pd.n, nw = Pd.nw, npad = pm1_npad(n);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char *ptr = smem;
-    uint32_t *Jw = reinterpret_cast<uint32_t *>(ptr); ptr += (size_t)nw * npad * 4;
+    uint32_t *Jw_s = reinterpret_cast<uint32_t *>(ptr);
+    if (JW_SMEM) ptr += (size_t)nw * npad * 4;
+    const uint32_t *Jw = JW_SMEM ? Jw_s : Pd.Jw;
     uint32_t *S = reinterpret_cast<uint32_t *>(ptr); ptr += align_up((size_t)NP * nw * 4, 16);
     float *h = reinterpret_cast<float *>(ptr); ptr += (size_t)npad * 4;
-    int *G = reinterpret_cast<int *>(ptr); ptr += (size_t)NP * npad * 4;
+    GT *G = reinterpret_cast<GT *>(ptr); ptr += align_up((size_t)NP * npad * sizeof(GT), 16);
     unsigned long long *Wc = reinterpret_cast<unsigned long long *>(ptr); ptr += (size_t)npad * 8;
     int *Gs = reinterpret_cast<int *>(ptr); ptr += (size_t)npad * 4;
     float *uw = reinterpret_cast<float *>(ptr); ptr += (size_t)npad * 4;
     double *cellE = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)NP * 8, 16);
-    uint32_t *mask = reinterpret_cast<uint32_t *>(ptr); ptr += 32 * 4;
+    uint32_t *mask = reinterpret_cast<uint32_t *>(ptr); ptr += (size_t)(npad / 32) * 4;
     unsigned long long *Wold = reinterpret_cast<unsigned long long *>(ptr); ptr += 32 * 8;
     int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
     int *flag = reinterpret_cast<int *>(ptr);  // [0]: best slice, [1]: block flips F, [2]: block index
 
-    for (int idx = threadIdx.x; idx < nw * npad; idx += blockDim.x) Jw[idx] = Pd.Jw[idx];
+    if (JW_SMEM)
+        for (int idx = threadIdx.x; idx < nw * npad; idx += blockDim.x) Jw_s[idx] = Pd.Jw[idx];
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) S[idx] = p.spins[R.spin_off + idx];
     for (int i = threadIdx.x; i < npad; i += blockDim.x) h[i] = i < n ? Pd.h32[i] : 0.0f;
-    int *Gg = reinterpret_cast<int *>(p.fields) + R.field_off;
+    GT *Gg = reinterpret_cast<GT *>(p.fields) + R.field_off;
     __syncthreads();
     if (p.init_fields) {
         // g_m = sum_{j != m} J_mj s_j by popcount over the packed rows
@@ -174,7 +209,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                     if (q == (mm >> 5)) vm &= ~(1u << (mm & 31));
                     g += 2 * __popc(~(Jw[q * npad + mm] ^ S[t * nw + q]) & vm) - __popc(vm);
                 }
-            G[idx] = g;
+            G[idx] = (GT)g;
         }
     } else {
         for (int idx = threadIdx.x; idx < NP * npad; idx += blockDim.x) G[idx] = Gg[idx];
@@ -232,7 +267,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 int gs = 0;
                 if (i < n)
                     for (int t = 0; t < NP; ++t) {
-                        const int g = G[t * npad + i];
+                        const int g = (int)G[t * npad + i];
                         gs += ((S[t * nw + q] >> lane) & 1u) ? g : -g;
                     }
                 Gs[i] = gs;
@@ -312,7 +347,8 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
             for (int i = lane; i < n; i += 32) {
                 const bool up = (S[t * nw + (i >> 5)] >> (i & 31)) & 1u;
                 ph = __dadd_rn(ph, up ? (double)h[i] : -(double)h[i]);
-                pg += up ? G[t * npad + i] : -G[t * npad + i];
+                const int g = (int)G[t * npad + i];
+                pg += up ? g : -g;
             }
             ph = warp_sum_d(ph);
             pg = warp_sum_i(pg);

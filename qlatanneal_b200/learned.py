@@ -34,17 +34,20 @@ FEATURE_NAMES = [
 ]
 
 
-def _pair_couplings(ising) -> Tuple[int, np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
-    """(n, rows, cols, values, h) of the two-body part (both directions)."""
+def _two_body(ising):
+    """(n, upper-triangle coupling values, degrees, h, matvec) of the two-body
+    part; matvec(x) = J x with the full symmetric J."""
     n = ising.size()
     if isinstance(ising, DenseIsing):
-        J = np.triu(ising.couplings(), 1)
-        r, c = np.nonzero(J)
-        v = J[r, c]
-        h = ising.fields()
-    elif isinstance(ising, SparseIsing):
+        J = np.array(ising.couplings(), dtype=np.float64)
+        np.fill_diagonal(J, 0.0)
+        nz = J != 0.0
+        deg = nz.sum(axis=1).astype(float)
+        v = J[np.triu(nz, 1)]
+        return n, v, deg, np.asarray(ising.fields(), float), (lambda x: J @ x)
+    if isinstance(ising, SparseIsing):
         r, c, v = ising._ei, ising._ej, ising._w
-        h = ising._h
+        h = np.asarray(ising._h, float)
     elif isinstance(ising, HigherOrderIsing):
         rs, cs, vs = [], [], []
         for k, w in ising.terms():
@@ -52,37 +55,41 @@ def _pair_couplings(ising) -> Tuple[int, np.ndarray, np.ndarray, np.ndarray, np.
                 for b in range(a + 1, len(k)):
                     rs.append(k[a]); cs.append(k[b]); vs.append(w)
         r, c, v = np.asarray(rs, int), np.asarray(cs, int), np.asarray(vs, float)
-        h = ising.h()
+        h = np.asarray(ising.h(), float)
     else:
         raise TypeError("unsupported model")
-    return n, np.concatenate([r, c]), np.concatenate([c, r]), np.concatenate([v, v]), np.asarray(h, float)
+    rows, cols, vals = np.concatenate([r, c]), np.concatenate([c, r]), np.concatenate([v, v])
+    deg = np.bincount(rows, minlength=n).astype(float)
+    return n, np.asarray(v, float), deg, h, (lambda x: np.bincount(rows, weights=vals * x[cols], minlength=n))
 
 
-def _top_eigenvalue(n: int, rows: np.ndarray, cols: np.ndarray, vals: np.ndarray, iters: int = 60) -> float:
-    """Largest-magnitude eigenvalue of the symmetric coupling matrix by power iteration."""
-    if vals.size == 0:
-        return 0.0
+def _top_eigenvalue(n: int, matvec, iters: int = 100) -> float:
+    """Largest |eigenvalue| of the symmetric coupling matrix by power
+    iteration; the estimate is |J x| for the unit iterate x, which tends to
+    |lambda_max| even when -lambda_max is (almost) as large, as in the
+    symmetric spectra of random +-1 couplings."""
     x = np.cos(np.arange(n) * 0.7 + 0.3)
     x /= np.linalg.norm(x)
-    lam = 0.0
+    nrm = 0.0
     for _ in range(iters):
-        y = np.bincount(rows, weights=vals * x[cols], minlength=n)
-        nrm = np.linalg.norm(y)
+        y = matvec(x)
+        nrm = float(np.linalg.norm(y))
         if nrm == 0.0:
             return 0.0
-        lam = float(x @ y)
         x = y / nrm
-    return abs(lam)
+    return nrm
 
 
 def instance_features(ising, beta: float, gamma_start: float, gamma_end: float, slices: int) -> np.ndarray:
-    n, r, c, v, h = _pair_couplings(ising)
-    deg = np.bincount(r, minlength=n).astype(float)
+    """The 16 inputs of the network: size, degree mean and spread, coupling
+    moments, field moments, the top eigenvalue of J (power iteration), and
+    the run parameters (beta, Gamma range, Trotter slices)."""
+    n, v, deg, h, matvec = _two_body(ising)
     mdeg = max(float(deg.mean()), 1e-9)
     av = np.abs(v)
     rms = float(np.sqrt(np.mean(v * v))) if v.size else 0.0
-    lam = _top_eigenvalue(n, r, c, v)
-    f = np.array([
+    lam = _top_eigenvalue(n, matvec) if v.size else 0.0
+    return np.array([
         math.log(n) / 8.0,
         mdeg / n,
         float(deg.std()) / mdeg,
@@ -100,7 +107,6 @@ def instance_features(ising, beta: float, gamma_start: float, gamma_end: float, 
         math.log(gamma_end),
         slices / 64.0,
     ])
-    return f
 
 
 def curve_target(chi: np.ndarray) -> np.ndarray:
@@ -322,3 +328,49 @@ class ChiCurveModel:
         return c
 
     __call__ = curve
+
+
+def synthetic_instances(count: int, n_min: int, n_max: int, seed: int, kinds=("sk", "regular3")):
+    """Seeded training instances: alternately dense Sherrington-Kirkpatrick
+    (J in {-1,+1}) and random 3-regular (J in {-1,+1}), h = 0, n uniform in
+    [n_min, n_max] (even)."""
+    from .instances import regular3, sk_dense
+    rng = np.random.default_rng(seed)
+    for i in range(count):
+        n = int(rng.integers(n_min // 2, n_max // 2 + 1)) * 2
+        s = int(rng.integers(1 << 31))
+        kind = kinds[i % len(kinds)]
+        if kind == "sk":
+            h, J = sk_dense(n, s)
+            yield DenseIsing(h, J)
+        else:
+            h, e = regular3(n, s, h_choices=(0.0,))
+            yield SparseIsing(h, e, n)
+
+
+def training_set(models, beta: float, gamma_start: float, gamma_end: float, slices: int, points: int = 64,
+                 sweeps: int = 200, burn: int = 50, reads: int = 1, seed: int = 0, chunk: int = 64,
+                 device: Optional[int] = None) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """(features [N][16], targets [N][points], pilot curves [N][points]) for a
+    stream of models, piloted ``chunk`` at a time (their device copies are
+    freed after each chunk)."""
+    X, chi = [], []
+    batch = []
+
+    def flush():
+        if not batch:
+            return
+        chi.append(pilot_curves(batch, beta, gamma_start, gamma_end, slices, points, sweeps, burn,
+                                reads=reads, seed=seed, device=device))
+        for m in batch:
+            X.append(instance_features(m, beta, gamma_start, gamma_end, slices))
+            m.release()
+        batch.clear()
+
+    for m in models:
+        batch.append(m)
+        if len(batch) >= chunk:
+            flush()
+    flush()
+    C_ = np.concatenate(chi) if chi else np.zeros((0, points))
+    return np.asarray(X), curve_target(C_), C_

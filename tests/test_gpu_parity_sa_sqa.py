@@ -81,6 +81,12 @@ SQA_CASES = [
     ("dense", 33, 3, 1, 2, 3, 0.1),
     ("dense", 256, 16, 1, 0, 3, 0.05),  # many accepted worldline moves
     ("dense_h", 70, 6, 2, 2, 1, 0.5),
+    # rings too large for int32 fields: int16 fields with J bits in shared
+    # memory (n=1024, P=32), then with J read from L2 (the rest)
+    ("dense", 1024, 32, 1, 1, 1, 1.0),
+    ("dense", 1024, 64, 1, 1, 1, 0.5),
+    ("dense_h", 1500, 20, 1, 1, 1, 0.5),
+    ("dense", 2048, 8, 1, 1, 2, 0.5),
     # the generic field-cache kernel
     ("dense_int", 80, 8, 2, 1, 1, 0.5),
     ("sparse", 128, 8, 1, 1, 1, 1.0),
