@@ -205,6 +205,167 @@ def run_reference_arm(args):
     return 0
 
 
+# The other workloads of the sweep engine (one call = one step; site-attempts/s).
+SIDE = {
+    "sa-dense": dict(desc="SA, SK n=256 J=+-1 h=0, 100 geometric betas 0.1->5 x 10 sweeps, 64 reads",
+                     method="sa", kind="sk", n=256, reads=64, steps=100, spb=10, b0=0.1, b1=5.0, seed=11),
+    "sqapt-sparse": dict(desc="SQA-PT, random 3-regular n=2048 J=+-1 h in {-0.5,0,0.5}, P=16, 32 rungs (beta "
+                              "geometric 0.2->4, Gamma linear 2.5->0.05), 100 pt steps x (20 slice + 5 worldline) "
+                              "sweeps, swap interval 10, 32 reads",
+                         method="sqapt", kind="regular3", n=2048, reads=32, steps=100, spb=20, wls=5, P=16,
+                         rungs=32, swap=10, seed=12),
+    "sqa-hubo": dict(desc="SQA, HUBO n=1024 (3n 3-body J=+-1, 2n 2-body J~U(-1,1), h~N(0,0.2^2)), P=16, beta "
+                          "linear 0.1->4, Gamma 2->0.02 over 500 steps, 1 slice + 1 worldline sweep, 128 reads",
+                     method="sqa", kind="hubo", n=1024, reads=128, steps=500, spb=1, wls=1, P=16, seed=13),
+}
+
+
+def _side_spec(w):
+    """The seeded instance data (generated once, outside every timed region)."""
+    from qlatanneal_b200.instances import hubo_random, regular3, sk_dense
+    if w["kind"] == "sk":
+        return ("dense",) + tuple(sk_dense(w["n"], w["seed"]))
+    if w["kind"] == "regular3":
+        return ("sparse",) + tuple(regular3(w["n"], w["seed"]))
+    return ("hubo", hubo_random(w["n"], w["seed"]), None)
+
+
+def _side_build(w, spec):
+    """The model through the public API, from host data."""
+    import qlatanneal_b200 as qa
+    kind, a, b = spec
+    if kind == "dense":
+        return qa.DenseIsing(a, b)
+    if kind == "sparse":
+        return qa.SparseIsing(a, b, w["n"])
+    return qa.HigherOrderIsing(a, w["n"])
+
+
+def _side_annealer(w, model):
+    import qlatanneal_b200 as qa
+    if w["method"] == "sa":
+        betas = w["b0"] * (w["b1"] / w["b0"]) ** (np.arange(w["steps"]) / (w["steps"] - 1))
+        ann = qa.Annealer(model, qa.AnnealSchedule.from_betas(betas))
+        return ann, (lambda seed: ann.run_reads(w["spb"], reads=w["reads"], seed=seed)), betas, None
+    if w["method"] == "sqapt":
+        R = w["rungs"]
+        betas = 0.2 * (4.0 / 0.2) ** (np.arange(R) / (R - 1))
+        gammas = np.linspace(2.5, 0.05, R)
+        ann = qa.SQAParallelTemperingAnnealer(model, betas, gammas, w["P"])
+        return ann, (lambda seed: ann.run_reads(w["spb"], w["wls"], w["steps"], w["swap"], reads=w["reads"],
+                                                seed=seed)), betas, gammas
+    betas = np.linspace(0.1, 4.0, w["steps"])
+    gammas = np.linspace(2.0, 0.02, w["steps"])
+    ann = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors(betas, gammas), w["P"], 1)
+    return ann, (lambda seed: ann.run_reads(w["spb"], w["wls"], reads=w["reads"], seed=seed)), betas, gammas
+
+
+def _side_sites(w, st):
+    P = w.get("P", 1)
+    return st.slice_attempts + st.worldline_attempts * P
+
+
+def _side_cpu(w, spec, target_s=10.0):
+    """qanneal on a bounded sample of the workload: SA/SQA reads over all host
+    threads (one annealer per thread), SQA-PT one ladder on one thread."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import REF_SO, Ref
+    if not os.path.exists(REF_SO):
+        return None
+    ref = Ref()
+    kind, a, b = spec
+    if kind == "dense":
+        rm = ref.dense(a, b)
+    elif kind == "sparse":
+        rm = ref.sparse(w["n"], a, b)
+    else:
+        rm = ref.hubo(w["n"], [(k, v) for k, v in a.items()])
+    threads = os.cpu_count() or 1
+    if w["method"] == "sqapt":
+        R = w["rungs"]
+        betas = 0.2 * (4.0 / 0.2) ** (np.arange(R) / (R - 1))
+        gammas = np.linspace(2.5, 0.05, R)
+        t0 = time.perf_counter()
+        rm.sqapt_run(betas, gammas, w["P"], w["spb"], w["wls"], 1, w["swap"], 3)
+        per_step = time.perf_counter() - t0
+        steps = int(max(1, min(w["steps"], target_s / max(per_step, 1e-6))))
+        t0 = time.perf_counter()
+        rm.sqapt_run(betas, gammas, w["P"], w["spb"], w["wls"], steps, w["swap"], 5)
+        dt = time.perf_counter() - t0
+        sites = steps * R * (w["spb"] + w["wls"]) * w["P"] * w["n"]
+        return {"value": sites / dt, "unit": "site-attempts/s", "cores": 1, "kind": "reference",
+                "sample": f"1 read x first {steps} of {w['steps']} pt steps ({sites:.3e} site-attempts, {dt:.1f} s)"}
+    method = 0 if w["method"] == "sa" else 1
+    if w["method"] == "sa":
+        betas = w["b0"] * (w["b1"] / w["b0"]) ** (np.arange(w["steps"]) / (w["steps"] - 1))
+        gammas, P, spb, wls, per_site = None, 1, w["spb"], 0, w["spb"]
+    else:
+        betas, gammas = np.linspace(0.1, 4.0, w["steps"]), np.linspace(2.0, 0.02, w["steps"])
+        P, spb, wls, per_site = w["P"], w["spb"], w["wls"], (w["spb"] + w["wls"]) * w["P"]
+    t0 = time.perf_counter()
+    rm.batch_run(method, betas[:5], None if gammas is None else gammas[:5], 5, P, 1, spb, wls, 1, 7, 1)
+    per_step = (time.perf_counter() - t0) / 5
+    steps = int(max(5, min(w["steps"], target_s / max(per_step, 1e-6))))
+    t0 = time.perf_counter()
+    rm.batch_run(method, betas[:steps], None if gammas is None else gammas[:steps], steps, P, 1, spb, wls,
+                 threads, 11, threads)
+    dt = time.perf_counter() - t0
+    sites = threads * steps * per_site * w["n"]
+    return {"value": sites / dt, "unit": "site-attempts/s", "cores": threads, "kind": "reference",
+            "sample": f"{threads} reads x first {steps} of {w['steps']} steps ({sites:.3e} site-attempts, "
+                      f"{dt:.1f} s, one annealer per thread)"}
+
+
+def run_side(args, w):
+    """Throughput of one of the other workloads on one GPU (device-timed)."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    spec = _side_spec(w)
+    model = _side_build(w, spec)
+    ann, call, _, _ = _side_annealer(w, model)
+    for _ in range(args.warmup):
+        call(w["seed"])
+    stats = []
+    with Clocks(0) as clk:
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush_l2(torch, dev)
+            torch.cuda.synchronize()
+            call(w["seed"])
+            stats.append(ann.last_stats)
+    dev_ms = sum(st.total_ms for st in stats)
+    sites = _side_sites(w, stats[0])
+    e2e = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m2 = _side_build(w, spec)
+        a2, c2, _, _ = _side_annealer(w, m2)
+        c2(w["seed"])
+        m2.release()
+        e2e.append(time.perf_counter() - t0)
+    cpu = None if args.no_cpu_baseline else _side_cpu(w, spec)
+    st = stats[0]
+    line = {"metric": "spin-flip attempts/s (site-attempts)", "workload": args.workload,
+            "value": sites * args.steps / (dev_ms / 1e3), "unit": "site-attempts/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["desc"], "site_attempts_per_step": sites,
+                       "l2": "flushed (256 MiB write) between steps",
+                       "slice_accept_rate": st.slice_accepts / max(1, st.slice_attempts),
+                       "worldline_accept_rate": st.worldline_accepts / max(1, st.worldline_attempts),
+                       "sweep_ms_per_step": sum(x.sweep_ms for x in stats) / args.steps},
+            "e2e": {"value": sites * args.steps / sum(e2e), "unit": "site-attempts/s",
+                    "ms_per_step": 1e3 * float(np.mean(e2e))},
+            "cpu_baseline": cpu, "gpu_launches": int(sum(x.launches for x in stats)), "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def tts99(t_call, reads, p):
     """Time to reach the target with 99% probability, per-read time t/reads
     repeated ln(0.01)/ln(1-p) times (one read when p >= 0.99)."""
@@ -301,9 +462,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="sqa", choices=["sqa", "chi-ttt"],
+    ap.add_argument("--workload", default="sqa", choices=["sqa", "chi-ttt"] + sorted(SIDE),
                     help="sqa: the sweep-throughput line (default); chi-ttt: time-to-target of SQA-Chi with the "
-                         "learned vs the pilot-scan schedule, training set included")
+                         "learned vs the pilot-scan schedule, training set included; " + "; ".join(
+                             f"{k}: {v['desc']}" for k, v in sorted(SIDE.items())))
     ap.add_argument("--chi-train", type=int, default=CHI["train"], help="chi-ttt: training instances")
     ap.add_argument("--chi-instances", type=int, default=CHI["instances"], help="chi-ttt: production instances")
     args = ap.parse_args()
@@ -313,6 +475,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "chi-ttt":
         return run_chi_ttt(args)
+    if args.workload in SIDE:
+        return run_side(args, SIDE[args.workload])
 
     import torch
     import torch.distributed as dist

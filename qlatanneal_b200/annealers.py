@@ -90,6 +90,34 @@ class SQAChiResult:
     driver_A0: float
 
 
+def _lazy_list(name: str) -> property:
+    """A result field that may be given as a numpy row and becomes a Python
+    list (the reference's std::vector -> list) on first access: building
+    hundreds of thousands of floats for traces nobody reads is most of the
+    host time of a large batched call."""
+    priv = "_lazy_" + name
+
+    def get(self):
+        v = self.__dict__[priv]
+        if isinstance(v, np.ndarray):
+            v = v.tolist()
+            self.__dict__[priv] = v
+        return v
+
+    def set(self, v):
+        self.__dict__[priv] = v
+
+    return property(get, set)
+
+
+for _cls, _names in ((AnnealResult, ("energy_trace",)), (SQAResult, ("energy_trace",)),
+                     (SQAParallelTemperingResult, ("average_energy_trace", "swap_acceptance_trace")),
+                     (SQAChiResult, ("energy_trace", "beta_schedule", "gamma_schedule", "s_schedule", "scan_s",
+                                     "scan_gamma", "scan_chi_B"))):
+    for _n in _names:
+        setattr(_cls, _n, _lazy_list(_n))
+
+
 @dataclass
 class RunStats:
     """Device-side totals of one batched call (qa_stats)."""
@@ -167,7 +195,7 @@ class Annealer(_Seeded):
         probs = (C.c_void_p * 1)(prob)
         _lib.check(eng.L.qa_sa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
-        return [AnnealResult(State(spins[r]), float(energies[r]), trace[r].tolist()) for r in range(reads)]
+        return [AnnealResult(State(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
 
 
 class SQAAnnealer(_Seeded):
@@ -217,7 +245,7 @@ class SQAAnnealer(_Seeded):
         probs = (C.c_void_p * 1)(prob)
         _lib.check(eng.L.qa_sqa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
-        return [SQAResult(State(spins[r]), float(energies[r]), trace[r].tolist()) for r in range(reads)]
+        return [SQAResult(State(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
 
 
 class SQAParallelTemperingAnnealer(_Seeded):
@@ -274,7 +302,7 @@ class SQAParallelTemperingAnnealer(_Seeded):
         _lib.check(eng.L.qa_sqapt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         return [SQAParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
-                                           float(bestE[r]), avg[r].tolist(), swp[r].tolist())
+                                           float(bestE[r]), avg[r], swp[r])
                 for r in range(reads)]
 
 
@@ -344,9 +372,8 @@ class SQAChiAnnealer(_Seeded):
         for r in range(reads):
             sc = a["scalars"][r]
             out.append(SQAChiResult(State(a["best_spins"][r]), float(a["best_energy"][r]),
-                                    a["energy_trace"][r].tolist(), a["beta_schedule"][r].tolist(),
-                                    a["gamma_schedule"][r].tolist(), a["s_schedule"][r].tolist(),
-                                    a["scan_s"][r].tolist(), a["scan_gamma"][r].tolist(), a["scan_chi_B"][r].tolist(),
+                                    a["energy_trace"][r], a["beta_schedule"][r], a["gamma_schedule"][r],
+                                    a["s_schedule"][r], a["scan_s"][r], a["scan_gamma"][r], a["scan_chi_B"][r],
                                     float(sc[0]), float(sc[1]), float(sc[2]), float(sc[3]), float(sc[4])))
         return out
 

@@ -678,6 +678,40 @@ int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int6
         for (int k = tptr[t]; k < tptr[t + 1]; ++k) incterm[incptr[tvars[k]] + fillc[tvars[k]]++] = t;
     std::vector<float> c32(n_terms);
     for (int t = 0; t < n_terms; ++t) c32[t] = (float)coeff[t];
+    // flip updates grouped by target (terms of degree <= 4 only)
+    bool small_terms = true;
+    for (int t = 0; t < n_terms && small_terms; ++t) small_terms = tptr[t + 1] - tptr[t] <= 4;
+    std::vector<int> upd_ptr, upd_run;
+    std::vector<int4> upd_rec;
+    if (small_terms) {
+        upd_ptr.assign(n + 1, 0);
+        struct U { int v, t, w1, w2; };
+        std::vector<U> u;
+        for (int j = 0; j < n; ++j) {
+            u.clear();
+            for (int q = incptr[j]; q < incptr[j + 1]; ++q) {
+                const int t = incterm[q];
+                for (int k = tptr[t]; k < tptr[t + 1]; ++k) {
+                    const int v = tvars[k];
+                    if (v == j) continue;
+                    int w[2] = {-1, -1}, nw_ = 0;
+                    for (int k2 = tptr[t]; k2 < tptr[t + 1]; ++k2)
+                        if (tvars[k2] != j && tvars[k2] != v) w[nw_++] = tvars[k2];
+                    u.push_back({v, t, w[0], w[1]});
+                }
+            }
+            std::stable_sort(u.begin(), u.end(), [](const U &a, const U &b) { return a.v != b.v ? a.v < b.v : a.t < b.t; });
+            for (size_t k = 0; k < u.size(); ++k) {
+                if (k == 0 || u[k].v != u[k - 1].v) upd_run.push_back((int)upd_rec.size());
+                const float two = 2.0f * c32[u[k].t];
+                int bits;
+                std::memcpy(&bits, &two, 4);
+                upd_rec.push_back(make_int4(u[k].v, u[k].w1, u[k].w2, bits));
+            }
+            upd_ptr[j + 1] = (int)upd_run.size();
+        }
+        upd_run.push_back((int)upd_rec.size());
+    }
     qa_problem *P = new qa_problem();
     P->ctx = ctx;
     P->kind = K_HUBO;
@@ -692,6 +726,11 @@ int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int6
     if (rc == QA_OK) rc = upload(P, incterm.data(), incterm.size(), &P->dev.incterm);
     if (rc == QA_OK) rc = upload(P, c32.data(), c32.size(), &P->dev.coef32);
     if (rc == QA_OK) rc = upload(P, coeff, (size_t)n_terms, &P->dev.coef64);
+    if (rc == QA_OK && small_terms) {
+        rc = upload(P, upd_ptr.data(), upd_ptr.size(), &P->dev.upd_ptr);
+        if (rc == QA_OK) rc = upload(P, upd_run.data(), upd_run.size(), &P->dev.upd_run);
+        if (rc == QA_OK) rc = upload(P, upd_rec.data(), upd_rec.size(), &P->dev.upd_rec);
+    }
     if (rc != QA_OK) {
         qa_problem_free(P);
         return rc;
@@ -739,8 +778,11 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
     double *d_exact = static_cast<double *>(v);
     QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
 
+    // dense +-1 couplings: bits and int32 fields in shared memory (fields built in-kernel)
+    bool pm1 = kind == K_DENSE && sa_pm1_smem_bytes(n_max) <= (size_t)ctx->smem_optin && !std::getenv("QA_DISABLE_PM1");
+    for (int p = 0; p < n_problems && pm1; ++p) pm1 = problems[p]->dev.Jw != nullptr;
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, 1, n_max, L.nw_max, DOM_INIT));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, 1, n_max, L.nw_max, DOM_INIT, !pm1));
     const int nwp = (L.nw_max + 3) & ~3, np4 = (n_max + 3) & ~3;
     size_t smem = (size_t)nwp * 4 + (size_t)np4 * 4;
     int smem_fields = (smem + (size_t)n_max * 4) <= (size_t)std::min(ctx->smem_optin, 160 * 1024) ? 1 : 0;
@@ -751,13 +793,21 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
     sp.trace = d_trace; sp.best_E = d_best; sp.best_bits = d_bits; sp.nw_max = L.nw_max; sp.counters = d_cnt;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     int rc = QA_OK;
-    dispatch_kind(kind, [&](auto K) {
-        auto kern = sa_kernel<decltype(K)::value>;
-        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<nr, 32, smem, ctx->stream>>>(sp);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, std::string("sa_kernel launch: ") + cudaGetErrorString(e));
-    });
+    if (pm1) {
+        const size_t sm1 = sa_pm1_smem_bytes(n_max);
+        if (sm1 > 48 * 1024)
+            QA_CK(cudaFuncSetAttribute(sa_pm1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+        sa_pm1_kernel<<<nr, 32, sm1, ctx->stream>>>(sp);
+        QA_CK(cudaGetLastError());
+    } else {
+        dispatch_kind(kind, [&](auto K) {
+            auto kern = sa_kernel<decltype(K)::value>;
+            if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            kern<<<nr, 32, smem, ctx->stream>>>(sp);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, std::string("sa_kernel launch: ") + cudaGetErrorString(e));
+        });
+    }
     QA_TRY(rc);
     QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
@@ -790,7 +840,7 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
         stats->worldline_attempts = stats->worldline_accepts = 0;
         stats->sweep_ms = a;
         stats->total_ms = b;
-        stats->launches = 4;
+        stats->launches = pm1 ? 3 : 4;
         stats->sweep_launches = 1;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + sizeof(float) * A.size() +
                                      sizeof(int) * nr);

@@ -124,6 +124,13 @@ struct ProbDev {
     // dense with every coupling in {-1,+1}: bit-packed rows, Jw[q*n + m] =
     // bits J[m][32q .. 32q+31] (1 = +1; diagonal and padding bits 0); else null
     const uint32_t *Jw;
+    // hubo with every term of degree <= 4: the field updates of a flip of
+    // spin j grouped by target.  Runs upd_run[upd_ptr[j] .. upd_ptr[j+1]) of
+    // j; run r = records upd_rec[upd_run[r] .. upd_run[r+1]), one target v,
+    // its terms in increasing term order; record = {v, w1, w2, bits(2 J_t)}
+    // with w1, w2 the term's other spins (-1: none).  Else null.
+    const int *upd_ptr, *upd_run;
+    const int4 *upd_rec;
 };
 
 __device__ __forceinline__ int spin_of(const uint32_t *S, int i) { return ((S[i >> 5] >> (i & 31)) & 1u) ? 1 : -1; }
@@ -145,6 +152,22 @@ __device__ __forceinline__ void apply_flip(const ProbDev &P, float *g, const uin
         for (int e = e0 + lane; e < e1; e += 32) {
             const int m = __ldg(P.col + e);
             g[m] = __fadd_rn(g[m], __fmul_rn(cf, __ldg(P.val32 + e)));
+        }
+    } else if (P.upd_rec) {
+        // one lane per target spin v, its terms in order: the same float
+        // additions, in the same order per field, as the term-by-term loop
+        const int sj = spin_of(S, j);  // S holds the new spin
+        const int r0 = __ldg(P.upd_ptr + j), r1 = __ldg(P.upd_ptr + j + 1);
+        for (int r = r0 + lane; r < r1; r += 32) {
+            const int a = __ldg(P.upd_run + r), b = __ldg(P.upd_run + r + 1);
+            for (int k = a; k < b; ++k) {
+                const int4 rc = __ldg(P.upd_rec + k);
+                int pr = sj;
+                if (rc.y >= 0) pr *= spin_of(S, rc.y);
+                if (rc.z >= 0) pr *= spin_of(S, rc.z);
+                const float two = __int_as_float(rc.w);
+                g[rc.x] = __fadd_rn(g[rc.x], pr > 0 ? two : -two);
+            }
         }
     } else {
         const int q0 = __ldg(P.incptr + j), q1 = __ldg(P.incptr + j + 1);

@@ -414,4 +414,111 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     }
 }
 
+// ------------------------------------------------------------------ SA, dense +-1
+// sa_kernel's run (annealer.cpp:50-67: fixed spin order, running energy, best
+// copied on every new minimum; one warp per read) with the couplings as bits
+// and exact int32 fields in shared memory: a flip of spin j updates the
+// fields from the bits of column j, g_m += -2 J_mj s_j(old), no global loads.
+__host__ __device__ inline size_t sa_pm1_smem_bytes(int n) {
+    const int nw = (n + 31) / 32, np = pm1_npad(n);
+    return (size_t)nw * np * 4 + (size_t)((nw + 3) & ~3) * 4 + (size_t)np * 4 + (size_t)np * 4;
+}
+
+__global__ void __launch_bounds__(32) sa_pm1_kernel(SAParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const RingDev R = p.rings[blockIdx.x];
+    const ProbDev Pd = p.probs[R.prob];
+    const int lane = threadIdx.x, n = Pd.n, nw = Pd.nw, npad = pm1_npad(n);
+    uint32_t *Jw = reinterpret_cast<uint32_t *>(smem);
+    uint32_t *S = Jw + (size_t)nw * npad;
+    float *h = reinterpret_cast<float *>(S + ((nw + 3) & ~3));
+    int *G = reinterpret_cast<int *>(h + npad);
+    for (int idx = lane * 4; idx < nw * npad; idx += 128)
+        *reinterpret_cast<uint4 *>(Jw + idx) = __ldg(reinterpret_cast<const uint4 *>(Pd.Jw + idx));
+    for (int q = lane; q < nw; q += 32) S[q] = p.spins[R.spin_off + q];
+    for (int i = lane; i < npad; i += 32) h[i] = i < n ? Pd.h32[i] : 0.0f;
+    __syncwarp();
+    for (int m = lane; m < npad; m += 32) {
+        int g = 0;
+        if (m < n)
+            for (int q = 0; q < nw; ++q) {
+                const int rem = n - 32 * q;
+                uint32_t vm = rem >= 32 ? FULL : ((1u << rem) - 1u);
+                if (q == (m >> 5)) vm &= ~(1u << (m & 31));
+                g += 2 * __popc(~(Jw[q * npad + m] ^ S[q]) & vm) - __popc(vm);
+            }
+        G[m] = g;
+    }
+    __syncwarp();
+    // E = c + (sum s h + (sum s g) / 2), sums in warp order (cell_energy)
+    double ph = 0.0;
+    int pg = 0;
+    for (int i = lane; i < n; i += 32) {
+        const bool up = (S[i >> 5] >> (i & 31)) & 1u;
+        ph = __dadd_rn(ph, up ? (double)h[i] : -(double)h[i]);
+        pg += up ? G[i] : -G[i];
+    }
+    double E = __dadd_rn(Pd.c, __dadd_rn(warp_sum_d(ph), __dmul_rn(0.5, (double)warp_sum_i(pg))));
+    uint32_t *bb = p.best_bits + (long long)blockIdx.x * p.nw_max;
+    double best = E;
+    for (int q = lane; q < nw; q += 32) bb[q] = S[q];
+    unsigned long long att = 0, acc = 0;
+    for (int step = 0; step < p.steps; ++step) {
+        const float B = p.B[step];
+        for (int sw = 0; sw < p.spb; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * p.spb + sw);
+            U4 rnd = {0, 0, 0, 0};
+            for (int q = 0; q < nw; ++q) {
+                if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), 0u, sigma, DOM_SA, R.key);
+                const int i = (q << 5) | lane;
+                const bool valid = i < n;
+                const uint32_t sword = S[q];
+                const uint32_t sbit = (sword >> lane) & 1u;
+                const float u = u01(pick(rnd, q & 3));
+                const float hi = h[i];
+                att += (unsigned long long)min(32, n - (q << 5));
+                uint32_t pending = FULL;
+                for (;;) {
+                    const float gi = __int2float_rn(G[i]);
+                    const float loc = __fadd_rn(hi, gi);
+                    const bool ok = valid & metropolis_nb(__fmul_rn(signed_by_bit(loc, sbit), B), u);
+                    const uint32_t m = __ballot_sync(FULL, ok) & pending;
+                    if (!m) break;
+                    const int j = __ffs(m) - 1;
+                    const double xd = sbit ? __dadd_rn((double)hi, (double)gi) : -__dadd_rn((double)hi, (double)gi);
+                    const double xj = __shfl_sync(FULL, xd, j);
+                    const uint32_t sj = (sword >> j) & 1u;  // old spin bit of j
+                    if (lane == 0) S[q] = S[q] ^ (1u << j);
+                    const int jj = (q << 5) | j;
+                    const uint32_t *Jq = Jw + q * npad;
+                    for (int base = lane * 4; base < n; base += 128) {
+                        const uint4 jw = *reinterpret_cast<const uint4 *>(Jq + base);
+                        int4 g = *reinterpret_cast<int4 *>(G + base);
+                        g.x += base + 0 == jj ? 0 : ((((jw.x >> j) & 1u) == sj) ? -2 : 2);
+                        g.y += base + 1 == jj ? 0 : ((((jw.y >> j) & 1u) == sj) ? -2 : 2);
+                        g.z += base + 2 == jj ? 0 : ((((jw.z >> j) & 1u) == sj) ? -2 : 2);
+                        g.w += base + 3 == jj ? 0 : ((((jw.w >> j) & 1u) == sj) ? -2 : 2);
+                        *reinterpret_cast<int4 *>(G + base) = g;
+                    }
+                    __syncwarp();
+                    ++acc;
+                    E = __dadd_rn(E, __dmul_rn(-2.0, xj));
+                    if (E < best) {
+                        best = E;
+                        for (int w = lane; w < nw; w += 32) bb[w] = S[w];
+                    }
+                    pending = j == 31 ? 0u : (FULL << (j + 1));
+                }
+            }
+        }
+        if (lane == 0) p.trace[(long long)blockIdx.x * p.steps + step] = E;
+    }
+    for (int q = lane; q < nw; q += 32) p.spins[R.spin_off + q] = S[q];
+    if (lane == 0) {
+        p.best_E[blockIdx.x] = best;
+        atomicAdd(p.counters + 0, att);
+        atomicAdd(p.counters + 1, acc);
+    }
+}
+
 }  // namespace qa

@@ -42,11 +42,32 @@ def make(kind, n, seed):
         return qa.SparseIsing(h, e, n, -2.0)
     if kind == "hubo":
         return qa.HigherOrderIsing(hubo_random(n, seed, integer=True), n)
+    if kind == "hubo_real":
+        return qa.HigherOrderIsing(hubo_random(n, seed, integer=False), n)
+    if kind == "hubo_deg5":
+        rng = np.random.default_rng(seed)
+        terms = {tuple(sorted(rng.choice(n, size=5, replace=False).tolist())): 1.0 for _ in range(n)}
+        terms.update({tuple(sorted(rng.choice(n, size=2, replace=False).tolist())): -1.0 for _ in range(n)})
+        return qa.HigherOrderIsing(terms, n)
     raise ValueError(kind)
 
 
+def _check_best_energy(oracle, om, kind, res, E_track, best):
+    """Integer couplings: the reported energy equals the tracked one bit for
+    bit.  Real couplings: the tracked energy uses the float32 couplings the
+    sweep runs on, the reported one is recomputed in float64 from the given
+    coefficients (as qanneal reports it); compare that with the oracle's
+    float64 energy of the same state."""
+    if kind in REAL_KINDS:
+        assert res.best_energy == pytest.approx(oracle.energy64(om, best), rel=1e-12, abs=1e-12)
+    else:
+        assert res.best_energy == E_track
+
+
+REAL_KINDS = ("hubo_real",)
+
 SA_CASES = [("dense", 64), ("dense", 100), ("dense", 256), ("dense_h", 96), ("sparse", 128), ("sparse", 70),
-            ("hubo", 60)]
+            ("hubo", 60), ("hubo_real", 64), ("hubo_deg5", 40)]
 
 
 @pytest.mark.parametrize("kind,n", SA_CASES)
@@ -62,7 +83,7 @@ def test_sa_bit_exact(oracle, kind, n):
         best, E, trace, cnt = oracle.sa_run(om, betas, spb, seed, r)
         tot_acc += cnt[1]
         np.testing.assert_array_equal(res[r].best_state.as_array(), best)
-        assert res[r].best_energy == E
+        _check_best_energy(oracle, om, kind, res[r], E, best)
         np.testing.assert_array_equal(np.asarray(res[r].energy_trace), trace)
         assert res[r].best_energy == pytest.approx(model.energy(res[r].best_state.spins), abs=1e-9)
     st = ann.last_stats
@@ -92,6 +113,10 @@ SQA_CASES = [
     ("sparse", 128, 8, 1, 1, 1, 1.0),
     ("sparse", 64, 7, 2, 2, 1, 1.0),
     ("hubo", 48, 4, 2, 1, 1, 1.0),
+    # real couplings: field updates in the same float order as the oracle's
+    ("hubo_real", 64, 6, 1, 2, 1, 1.0),
+    # a degree-5 term: the term-by-term update path
+    ("hubo_deg5", 40, 4, 1, 1, 1, 1.0),
 ]
 
 
@@ -122,7 +147,7 @@ def _sqa_case(oracle, kind, n, P, K, spb, wls, bscale):
         acc_s += cnt[1]
         acc_w += cnt[3]
         np.testing.assert_array_equal(res[r].best_state.as_array(), best)
-        assert res[r].best_energy == E
+        _check_best_energy(oracle, om, kind, res[r], E, best)
         np.testing.assert_array_equal(np.asarray(res[r].energy_trace), trace)
     st = ann.last_stats
     assert st.slice_attempts == reads * K * P * steps * spb * n
