@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <climits>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -13,6 +14,7 @@
 #include "qa_kernels.cuh"
 #include "qa_chi.cuh"
 #include "qa_mlp.cuh"
+#include "qa_sparse.cuh"
 #include "qa_pm1.cuh"
 #include "qa_pt.cuh"
 
@@ -85,6 +87,10 @@ struct qa_problem {
     double c = 0.0;
     std::vector<void *> allocs;
     ProbDev dev{};
+    // arrays staged on the host while the problem is built, then sent with
+    // one allocation and one copy; fix = (offset, device pointer to patch)
+    std::vector<unsigned char> stage;
+    std::vector<std::pair<size_t, const void **>> fix;
 };
 
 namespace {
@@ -109,12 +115,10 @@ int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
 
 template <class T>
 int upload(qa_problem *P, const T *host, size_t count, const T **dev) {
-    void *d = nullptr;
-    size_t bytes = std::max<size_t>(count * sizeof(T), 16);
-    QA_CK(cudaMalloc(&d, bytes));
-    P->allocs.push_back(d);
-    if (count) QA_CK(cudaMemcpy(d, host, count * sizeof(T), cudaMemcpyHostToDevice));
-    *dev = static_cast<const T *>(d);
+    const size_t off = (P->stage.size() + 255) & ~(size_t)255;
+    P->stage.resize(off + std::max<size_t>(count * sizeof(T), 16));
+    if (count) std::memcpy(P->stage.data() + off, host, count * sizeof(T));
+    P->fix.push_back({off, reinterpret_cast<const void **>(dev)});
     return QA_OK;
 }
 
@@ -124,13 +128,22 @@ int begin(qa_ctx *ctx) {
     return QA_OK;
 }
 
-void finish_problem(qa_problem *P) {
+// Sends the staged arrays (one allocation, one copy) and sets the scalars.
+int finish_problem(qa_problem *P) {
     P->dev.kind = P->kind;
     P->dev.n = P->n;
     P->dev.nw = P->nw;
     P->dev.T = P->T;
     P->dev.m = P->m;
     P->dev.c = P->c;
+    void *d = nullptr;
+    QA_CK(cudaMalloc(&d, std::max<size_t>(P->stage.size(), 16)));
+    P->allocs.push_back(d);
+    QA_CK(cudaMemcpy(d, P->stage.data(), P->stage.size(), cudaMemcpyHostToDevice));
+    for (auto &f : P->fix) *f.second = static_cast<unsigned char *>(d) + f.first;
+    std::vector<unsigned char>().swap(P->stage);
+    P->fix.clear();
+    return QA_OK;
 }
 
 int common_h(qa_problem *P, const double *h) {
@@ -336,7 +349,9 @@ int exact_energies(qa_ctx *ctx, int kind, const ProbDev *d_probs, const Layout &
 
 // Which ring kernel a batch runs on, and with what launch shape.
 struct RingPlan {
-    bool pm1 = false;
+    bool pm1 = false;     // ring_pm1_kernel
+    bool sparse = false;  // ring_sparse_kernel
+    bool own_fields() const { return pm1 || sparse; }  // no field cache to initialise
     int gbytes = 4;       // pm1: bytes per field (4 int32, 2 int16)
     bool jw_smem = true;  // pm1: J bits in shared memory
     int W = 1;
@@ -370,6 +385,15 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
         pl->smem_fields = 0;
         return QA_OK;
     }
+    // sparse integer couplings: fields on demand, worldline sums from bits
+    pl->sparse = kind == K_SPARSE && P <= 64 && sparse_smem_bytes(P, n_max) <= (size_t)ctx->smem_optin &&
+                 !std::getenv("QA_DISABLE_SPARSE_INT");
+    for (int p = 0; p < np && pl->sparse; ++p) pl->sparse = probs[p]->dev.spcv != nullptr;
+    if (pl->sparse) {
+        pl->smem = sparse_smem_bytes(P, n_max);
+        pl->smem_fields = 0;
+        return QA_OK;
+    }
     pl->smem = ring_smem_bytes(P, n_max, pl->W, true);
     pl->smem_fields = 1;
     if (pl->smem > (size_t)std::min(ctx->smem_optin, 200 * 1024)) {
@@ -390,6 +414,13 @@ int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n
         if (pl.smem > 48 * 1024)
             QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
         kern<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
+        QA_CK(cudaGetLastError());
+        return QA_OK;
+    }
+    if (pl.sparse) {
+        if (pl.smem > 48 * 1024)
+            QA_CK(cudaFuncSetAttribute(ring_sparse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        ring_sparse_kernel<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
         QA_CK(cudaGetLastError());
         return QA_OK;
     }
@@ -553,27 +584,29 @@ int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, doubl
     P->n = n;
     P->nw = (n + 31) / 32;
     P->c = c;
+    // the upper triangle defines J (DenseIsing::energy reads i < j), mirrored
     std::vector<float> J32((size_t)n * n, 0.0f);
+    bool pm1 = true;  // couplings all in {-1,+1}: bit-packed rows for ring_pm1_kernel
     for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) {
-            if (i == j) continue;
-            const int a = std::min(i, j), b = std::max(i, j);
-            J32[(size_t)i * n + j] = (float)J[(size_t)a * n + b];
-        }
-    // couplings all in {-1,+1}: bit-packed rows for ring_pm1_kernel
-    bool pm1 = true;
-    for (int i = 0; i < n && pm1; ++i)
         for (int j = i + 1; j < n; ++j) {
             const double v = J[(size_t)i * n + j];
-            if (v != 1.0 && v != -1.0) { pm1 = false; break; }
+            pm1 = pm1 && (v == 1.0 || v == -1.0);
+            J32[(size_t)i * n + j] = J32[(size_t)j * n + i] = (float)v;
         }
     std::vector<uint32_t> Jw;
     if (pm1) {
         const int nw = (n + 31) / 32, np = pm1_npad(n);
         Jw.assign((size_t)nw * np, 0u);
-        for (int m = 0; m < n; ++m)
-            for (int j = 0; j < n; ++j)
-                if (j != m && J32[(size_t)m * n + j] > 0.0f) Jw[(size_t)(j >> 5) * np + m] |= 1u << (j & 31);
+        for (int m = 0; m < n; ++m) {
+            const float *row = J32.data() + (size_t)m * n;
+            for (int q = 0; q < nw; ++q) {
+                uint32_t word = 0;
+                const int j1 = std::min(n, 32 * q + 32);
+                for (int j = 32 * q; j < j1; ++j)
+                    if (j != m && row[j] > 0.0f) word |= 1u << (j & 31);
+                Jw[(size_t)q * np + m] = word;
+            }
+        }
     }
     int rc = common_h(P, h);
     if (rc == QA_OK) rc = upload(P, J32.data(), J32.size(), &P->dev.J32);
@@ -583,7 +616,11 @@ int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, doubl
         qa_problem_free(P);
         return rc;
     }
-    finish_problem(P);
+    rc = finish_problem(P);
+    if (rc != QA_OK) {
+        qa_problem_free(P);
+        return rc;
+    }
     *out = P;
     return QA_OK;
 }
@@ -624,6 +661,23 @@ int qa_problem_sparse(qa_ctx *ctx, int n, const double *h, int m, const int64_t 
         }
     }
     rowptr[n] = (int)col.size();
+    // integer couplings (merged): (column, value) pairs for ring_sparse_kernel;
+    // every field then stays an exact integer (|g| <= 2^24 checked per row)
+    bool integer = true;
+    for (int i = 0; i < n && integer; ++i) {
+        double tot = 0.0;
+        for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+            const double v = (double)val[e];
+            integer = integer && v == std::nearbyint(v) && std::fabs(v) <= 32767.0;
+            tot += std::fabs(v);
+        }
+        integer = integer && tot < 16777216.0;
+    }
+    std::vector<int2> spcv;
+    if (integer) {
+        spcv.resize(col.size());
+        for (size_t e = 0; e < col.size(); ++e) spcv[e] = make_int2(col[e], (int)val[e]);
+    }
     std::vector<int> e_i(m), e_j(m);
     for (int e = 0; e < m; ++e) { e_i[e] = (int)ei[e]; e_j[e] = (int)ej[e]; }
     qa_problem *P = new qa_problem();
@@ -640,11 +694,16 @@ int qa_problem_sparse(qa_ctx *ctx, int n, const double *h, int m, const int64_t 
     if (rc == QA_OK) rc = upload(P, e_i.data(), e_i.size(), &P->dev.ei);
     if (rc == QA_OK) rc = upload(P, e_j.data(), e_j.size(), &P->dev.ej);
     if (rc == QA_OK) rc = upload(P, w, (size_t)m, &P->dev.ew);
+    if (rc == QA_OK && integer) rc = upload(P, spcv.data(), spcv.size(), &P->dev.spcv);
     if (rc != QA_OK) {
         qa_problem_free(P);
         return rc;
     }
-    finish_problem(P);
+    rc = finish_problem(P);
+    if (rc != QA_OK) {
+        qa_problem_free(P);
+        return rc;
+    }
     *out = P;
     return QA_OK;
 }
@@ -735,7 +794,11 @@ int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int6
         qa_problem_free(P);
         return rc;
     }
-    finish_problem(P);
+    rc = finish_problem(P);
+    if (rc != QA_OK) {
+        qa_problem_free(P);
+        return rc;
+    }
     *out = P;
     return QA_OK;
 }
@@ -918,7 +981,7 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     RingPlan pl;
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
     // dense +-1 couplings: the bit-packed kernel builds its fields in-kernel
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.pm1));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_beta; rp.wls = prm->worldline_sweeps;
@@ -988,7 +1051,7 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
         stats->sweep_ms = a;
         stats->total_ms = b;
         stats->sweep_launches = n_seg;
-        stats->launches = (pl.pm1 ? 2 : 3) + n_seg;
+        stats->launches = (pl.own_fields() ? 2 : 3) + n_seg;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * steps +
                                      (sizeof(double) + sizeof(int)) * nr + sizeof(int) * nr);
         stats->d2h_bytes = (int64_t)(sizeof(double) * sums.size() + (2 * sizeof(double) + sizeof(int)) * nr +
@@ -1079,7 +1142,7 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
     RingPlan pl;
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.pm1));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_step; rp.wls = prm->worldline_sweeps;
@@ -1177,7 +1240,7 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
         stats->sweep_ms = a;
         stats->total_ms = b;
         stats->sweep_launches = n_seg;
-        stats->launches = (pl.pm1 ? 2 : 3) + 2 * n_seg;
+        stats->launches = (pl.own_fields() ? 2 : 3) + 2 * n_seg;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * Rn +
                                      2 * sizeof(double) * Rn + (sizeof(double) + 3 * sizeof(int)) * nr +
                                      sizeof(int) * rin.size());
@@ -1374,7 +1437,7 @@ static int chi_stage1(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     RingPlan pl;
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PILOT_INIT,
-                      !pl.pm1));
+                      !pl.own_fields()));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = 1; rp.spb = sweeps_total; rp.wls = 0; rp.slice_tag = DOM_PILOT;
@@ -1386,7 +1449,7 @@ static int chi_stage1(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     chi_point_kernel<<<(probes + 127) / 128, 128, 0, ctx->stream>>>(d_mag, probes, K, sweeps_total,
                                                                      prm->scan_burn, d_nof, P, d_chi);
     QA_CK(cudaGetLastError());
-    launches += (pl.pm1 ? 1 : 2) + 2;
+    launches += (pl.own_fields() ? 1 : 2) + 2;
     unsigned long long c[4];
     QA_CK(cudaMemcpyAsync(chi.data(), d_chi, sizeof(double) * chi.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1533,7 +1596,7 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     RingPlan pl;
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PROD_INIT, !pl.pm1));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PROD_INIT, !pl.own_fields()));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_step; rp.wls = 0; rp.slice_tag = DOM_PROD;
@@ -1550,7 +1613,7 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
     QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-    launches += (pl.pm1 ? 2 : 3) + n_seg;
+    launches += (pl.own_fields() ? 2 : 3) + n_seg;
     std::vector<double> sums((size_t)nr * steps), bestE(nr), exact(nr);
     std::vector<int> bstep(nr);
     std::vector<uint32_t> bits((size_t)nr * L.nw_max);

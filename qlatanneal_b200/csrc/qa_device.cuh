@@ -131,6 +131,8 @@ struct ProbDev {
     // with w1, w2 the term's other spins (-1: none).  Else null.
     const int *upd_ptr, *upd_run;
     const int4 *upd_rec;
+    // sparse with integer couplings: CSR (column, value) pairs; else null
+    const int2 *spcv;
 };
 
 __device__ __forceinline__ int spin_of(const uint32_t *S, int i) { return ((S[i >> 5] >> (i & 31)) & 1u) ? 1 : -1; }

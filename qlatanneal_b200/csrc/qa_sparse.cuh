@@ -1,0 +1,260 @@
+// qa_sparse.cuh -- Trotter-ring sweep kernel for sparse models with integer
+// couplings (the random 3-regular +-1 instances of the benchmark set).
+//
+// Same replay semantics as ring_kernel<K_SPARSE> (qa_kernels.cuh); different
+// data path.  With integer couplings every local field g = J.s is an exact
+// integer, so the kernel keeps no field cache at all:
+//  * slice moves read the field on demand from the CSR row and the
+//    neighbours' spin bits (deg loads; a flip only toggles a bit);
+//  * worldline moves (sqa_annealer.cpp:294-315) need the slice sum
+//    G_i = sum_t s_t,i g_t,i = sum_j J_ij (P - 2 popc(W_i ^ W_j)), where W_i
+//    is spin i's worldline (its bits over the P <= 64 slices): deg popcounts.
+// Both equal the maintained float fields of the generic kernel bit for bit
+// (integer sums below 2^24 are exact in float32), so results are identical.
+#pragma once
+#include "qa_pm1.cuh"
+
+namespace qa {
+
+__host__ __device__ inline size_t sparse_smem_bytes(int P, int n) {
+    const int nw = (n + 31) / 32, n32 = nw * 32;
+    size_t b = align_up((size_t)P * nw * 4, 16);  // S
+    b += (size_t)n32 * 8;                          // W (worldline bits)
+    b += (size_t)n32 * 4;                          // h
+    b += align_up((size_t)P * 8, 16);              // cellE
+    b += 32 * 4 + 64;                              // partials, flags
+    return b + 64;
+}
+
+// Local field of spin i in slice St (its spin bits), from the CSR row.
+__device__ __forceinline__ int sp_field(const int2 *cv, const int *rowptr, const uint32_t *St, int i) {
+    const int e0 = __ldg(rowptr + i), e1 = __ldg(rowptr + i + 1);
+    int g = 0;
+    for (int e = e0; e < e1; ++e) {
+        const int2 c = __ldg(cv + e);
+        g += ((St[c.x >> 5] >> (c.x & 31)) & 1u) ? c.y : -c.y;
+    }
+    return g;
+}
+
+// Slice sum over the worldlines: sum_t s_t,i g_t,i.
+__device__ __forceinline__ int sp_world_sum(const int2 *cv, const int *rowptr, const unsigned long long *Wc,
+                                            unsigned long long pmask, int NP, int i) {
+    const int e0 = __ldg(rowptr + i), e1 = __ldg(rowptr + i + 1);
+    const unsigned long long wi = Wc[i];
+    int g = 0;
+    for (int e = e0; e < e1; ++e) {
+        const int2 c = __ldg(cv + e);
+        g += c.y * (NP - 2 * __popcll((wi ^ Wc[c.x]) & pmask));
+    }
+    return g;
+}
+
+__device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, unsigned long long *Wc,
+                                               const float *h, int NP, int t, float B, float T4, uint64_t key,
+                                               uint32_t rng_cell, uint32_t sigma, uint32_t tag, int lane,
+                                               unsigned long long &att, unsigned long long &acc) {
+    const int n = Pd.n, nw = Pd.nw;
+    uint32_t *St = S + t * nw;
+    const uint32_t *Sp = S + (t == 0 ? NP - 1 : t - 1) * nw;
+    const uint32_t *Sn = S + (t + 1 == NP ? 0 : t + 1) * nw;
+    U4 rnd = {0, 0, 0, 0};
+    att += (unsigned long long)n;
+    for (int q = 0; q < nw; ++q) {
+        if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), rng_cell, sigma, tag, key);
+        const int i = (q << 5) | lane;
+        const bool valid = i < n;
+        const uint32_t sw = St[q];
+        const uint32_t sbit = (sw >> lane) & 1u;
+        const int d = (int)(((sw ^ Sp[q]) >> lane) & 1u) + (int)(((sw ^ Sn[q]) >> lane) & 1u);
+        const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
+        const float u = u01(pick(rnd, q & 3));
+        const float hi = h[i];
+        uint32_t pending = FULL;
+        for (;;) {
+            const int g = valid ? sp_field(Pd.spcv, Pd.rowptr, St, i) : 0;
+            const float loc = __fadd_rn(hi, __int2float_rn(g));
+            const bool ok = valid & metropolis_nb(__fsub_rn(__fmul_rn(signed_by_bit(loc, sbit), B), tro), u);
+            const uint32_t m = __ballot_sync(FULL, ok) & pending;
+            if (!m) break;
+            const int j = __ffs(m) - 1;
+            if (lane == 0) St[q] = St[q] ^ (1u << j);
+            if (lane == j) atomicXor(Wc + i, 1ull << t);
+            __syncwarp();
+            ++acc;
+            pending = j == 31 ? 0u : (FULL << (j + 1));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const RingDev R = p.rings[blockIdx.x];
+    const ProbDev Pd = p.probs[R.prob];
+    const int NP = p.P, W = p.W, n = Pd.n, nw = Pd.nw, n32 = nw * 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char *ptr = smem;
+    uint32_t *S = reinterpret_cast<uint32_t *>(ptr); ptr += align_up((size_t)NP * nw * 4, 16);
+    unsigned long long *Wc = reinterpret_cast<unsigned long long *>(ptr); ptr += (size_t)n32 * 8;
+    float *h = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * 4;
+    double *cellE = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)NP * 8, 16);
+    int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
+    int *flag = reinterpret_cast<int *>(ptr);  // [0]: best slice, [3]: lowest slice (final state)
+
+    for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) S[idx] = p.spins[R.spin_off + idx];
+    for (int i = threadIdx.x; i < n32; i += blockDim.x) h[i] = i < n ? Pd.h32[i] : 0.0f;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n32; i += blockDim.x) {
+        unsigned long long wc = 0;
+        if (i < n)
+            for (int t = 0; t < NP; ++t) wc |= (unsigned long long)((S[t * nw + (i >> 5)] >> (i & 31)) & 1u) << t;
+        Wc[i] = wc;
+    }
+    __syncthreads();
+
+    const unsigned long long pmask = NP == 64 ? ~0ull : ((1ull << NP) - 1ull);
+    const int slot = p.slot ? p.slot[blockIdx.x] : R.k;
+    unsigned long long att_s = 0, acc_s = 0, att_w = 0, acc_w = 0;
+    double bestE = p.best_E[blockIdx.x];
+    int bestStep = p.best_step[blockIdx.x];
+
+    for (int step = p.step0 - (p.init_scan ? 1 : 0); step < p.step1; ++step) {
+        // step -1 (init_scan) only scores the starting state
+        const int spb = step >= 0 ? p.spb : 0, wls = step >= 0 ? p.wls : 0;
+        const int si_tab = R.sched + (p.per_slot_sched ? slot : max(step, 0));
+        const float B = p.B[si_tab], T4 = p.T4[si_tab];
+        for (int sw = 0; sw < spb; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * p.spb + sw);
+            for (int ph = 0; ph < 3; ++ph) {
+                const int cnt = phase_count(NP, ph);
+                for (int c = warp; c < cnt; c += W) {
+                    const int t = phase_slice(NP, ph, c);
+                    sp_sweep_slice(Pd, S, Wc, h, NP, t, B, T4, R.key, (uint32_t)(slot * NP + t), sigma,
+                                   p.slice_tag | R.tag_extra, lane, att_s, acc_s);
+                }
+                if (cnt) __syncthreads();
+            }
+            if (p.mag) {
+                int ps = 0;
+                for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) ps += __popc(S[idx]);
+                ps = warp_sum_i(ps);
+                if (lane == 0) wpart[warp] = ps;
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    long long tot = 0;
+                    for (int w = 0; w < W; ++w) tot += wpart[w];
+                    p.mag[(long long)blockIdx.x * (p.steps_total * p.spb) + sigma] = (int)(2 * tot - (long long)NP * n);
+                }
+                __syncthreads();
+            }
+        }
+        // worldline sweeps: one warp, spins in order, sums from the worldline bits
+        for (int sw = 0; sw < wls; ++sw) {
+            if (warp == 0) {
+                const uint32_t sigma = (uint32_t)(step * p.wls + sw);
+                U4 rnd = {0, 0, 0, 0};
+                for (int q = 0; q < nw; ++q) {
+                    if ((q & 3) == 0)
+                        rnd = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
+                    const int i = (q << 5) | lane;
+                    const bool valid = i < n;
+                    const float u = u01(pick(rnd, q & 3));
+                    const double hi = (double)h[i];
+                    att_w += (unsigned long long)min(32, n - (q << 5));
+                    uint32_t pending = FULL;
+                    for (;;) {
+                        bool ok = false;
+                        if (valid) {
+                            const int sh = 2 * __popcll(Wc[i] & pmask) - NP;
+                            const int gs = sp_world_sum(Pd.spcv, Pd.rowptr, Wc, pmask, NP, i);
+                            const float x = __double2float_rn(__dadd_rn(__dmul_rn(hi, (double)sh), (double)gs));
+                            ok = metropolis_nb(__fmul_rn(x, B), u);
+                        }
+                        const uint32_t m = __ballot_sync(FULL, ok) & pending;
+                        if (!m) break;
+                        const int j = __ffs(m) - 1;
+                        for (int t = lane; t < NP; t += 32) S[t * nw + q] ^= 1u << j;
+                        if (lane == j) Wc[i] ^= pmask;
+                        __syncwarp();
+                        ++acc_w;
+                        pending = j == 31 ? 0u : (FULL << (j + 1));
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // ---- step end: slice energies E = c + (sum s h + (sum s g)/2), ring sum, best
+        for (int t = warp; t < NP; t += W) {
+            const uint32_t *St = S + t * nw;
+            double ph = 0.0;
+            int pg = 0;
+            for (int i = lane; i < n; i += 32) {
+                const bool up = (St[i >> 5] >> (i & 31)) & 1u;
+                ph = __dadd_rn(ph, up ? (double)h[i] : -(double)h[i]);
+                const int g = sp_field(Pd.spcv, Pd.rowptr, St, i);
+                pg += up ? g : -g;
+            }
+            ph = warp_sum_d(ph);
+            pg = warp_sum_i(pg);
+            if (lane == 0) cellE[t] = __dadd_rn(Pd.c, __dadd_rn(ph, __dmul_rn(0.5, (double)pg)));
+        }
+        if (p.ring_bond) {
+            int b = 0;
+            for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) {
+                const int t = idx / nw, q = idx - t * nw;
+                const int tn = t + 1 == NP ? 0 : t + 1;
+                const int rem = n - 32 * q;
+                const uint32_t vm = rem >= 32 ? FULL : ((1u << rem) - 1u);
+                b += 2 * __popc(~(S[idx] ^ S[tn * nw + q]) & vm) - __popc(vm);
+            }
+            b = warp_sum_i(b);
+            if (lane == 0) wpart[warp] = b;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sum = 0.0, emin = __longlong_as_double(0x7ff0000000000000LL);
+            int tmin = 0;
+            for (int t = 0; t < NP; ++t) {
+                const double E = cellE[t];
+                sum = __dadd_rn(sum, E);
+                if (E < emin) { emin = E; tmin = t; }
+            }
+            const long long ro = (long long)blockIdx.x * p.rec_stride + p.rec_base + step;
+            if (p.ring_sum) p.ring_sum[ro] = sum;
+            if (p.ring_min) p.ring_min[ro] = emin;
+            if (p.ring_bond) {
+                long long tb = 0;
+                for (int w = 0; w < W; ++w) tb += wpart[w];
+                p.ring_bond[ro] = tb;
+            }
+            flag[0] = emin < bestE ? tmin : -1;
+            flag[3] = tmin;
+        }
+        __syncthreads();
+        const int tb = flag[0];
+        if (tb >= 0) {
+            bestE = cellE[tb];
+            bestStep = step;
+            if (threadIdx.x == 0 && p.best_slot) p.best_slot[blockIdx.x] = slot;
+            for (int q = threadIdx.x; q < nw; q += blockDim.x)
+                p.best_bits[(long long)blockIdx.x * p.nw_max + q] = S[tb * nw + q];
+        }
+        if (p.final_bits && step == p.steps_total - 1)
+            for (int q = threadIdx.x; q < nw; q += blockDim.x)
+                p.final_bits[(long long)blockIdx.x * p.nw_max + q] = S[flag[3] * nw + q];
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) p.spins[R.spin_off + idx] = S[idx];
+    if (lane == 0) {
+        atomicAdd(p.counters + 0, att_s);
+        atomicAdd(p.counters + 1, acc_s);
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(p.counters + 2, att_w);
+        atomicAdd(p.counters + 3, acc_w);
+        p.best_E[blockIdx.x] = bestE;
+        p.best_step[blockIdx.x] = bestStep;
+    }
+}
+
+}  // namespace qa

@@ -94,7 +94,13 @@ class DenseIsing(_DeviceModel):
         if n == 0:
             raise ValueError("DenseIsing size must be > 0.")
         self._h, self._J, self._c, self._n = h, J, float(c), n
-        self._upper = np.triu(J, 1)
+        self._upper_cache = None
+
+    @property
+    def _upper(self) -> np.ndarray:
+        if self._upper_cache is None:
+            self._upper_cache = np.triu(self._J, 1)
+        return self._upper_cache
 
     def size(self) -> int:
         return self._n

@@ -33,6 +33,13 @@ def make(kind, n, seed):
         h, J = sk_dense(n, seed)
         h = rng.choice([-0.5, 0.0, 0.25, 0.5], size=n)
         return qa.DenseIsing(h, J, 1.5)
+    if kind == "dense_hwide":
+        # fields whose float64 sums round (h spans 2^-100 .. 2^3): energies summed, not tracked
+        rng = np.random.default_rng(seed + 9)
+        h, J = sk_dense(n, seed)
+        h = rng.normal(0.0, 2.0, size=n)
+        h[::7] = 1e-30
+        return qa.DenseIsing(h, J)
     if kind == "dense_int":
         rng = np.random.default_rng(seed)
         J = np.triu(rng.choice([-2.0, -1.0, 1.0, 2.0], size=(n, n)), 1)
@@ -40,6 +47,10 @@ def make(kind, n, seed):
     if kind == "sparse":
         h, e = regular3(n, seed)
         return qa.SparseIsing(h, e, n, -2.0)
+    if kind == "sparse_real":
+        h, e = regular3(n, seed)
+        rng = np.random.default_rng(seed + 3)
+        return qa.SparseIsing(h, [(a, b, float(w) * rng.uniform(0.2, 1.3)) for a, b, w in e], n, 0.5)
     if kind == "hubo":
         return qa.HigherOrderIsing(hubo_random(n, seed, integer=True), n)
     if kind == "hubo_real":
@@ -64,7 +75,7 @@ def _check_best_energy(oracle, om, kind, res, E_track, best):
         assert res.best_energy == E_track
 
 
-REAL_KINDS = ("hubo_real",)
+REAL_KINDS = ("hubo_real", "sparse_real", "dense_hwide")
 
 SA_CASES = [("dense", 64), ("dense", 100), ("dense", 256), ("dense_h", 96), ("sparse", 128), ("sparse", 70),
             ("hubo", 60), ("hubo_real", 64), ("hubo_deg5", 40)]
@@ -102,6 +113,7 @@ SQA_CASES = [
     ("dense", 33, 3, 1, 2, 3, 0.1),
     ("dense", 256, 16, 1, 0, 3, 0.05),  # many accepted worldline moves
     ("dense_h", 70, 6, 2, 2, 1, 0.5),
+    ("dense_hwide", 96, 8, 1, 1, 1, 0.5),
     # rings too large for int32 fields: int16 fields with J bits in shared
     # memory (n=1024, P=32), then with J read from L2 (the rest)
     ("dense", 1024, 32, 1, 1, 1, 1.0),
@@ -112,6 +124,9 @@ SQA_CASES = [
     ("dense_int", 80, 8, 2, 1, 1, 0.5),
     ("sparse", 128, 8, 1, 1, 1, 1.0),
     ("sparse", 64, 7, 2, 2, 1, 1.0),
+    ("sparse", 2048, 16, 1, 1, 2, 0.5),  # integer couplings: on-demand fields
+    ("sparse", 150, 64, 1, 1, 1, 1.0),
+    ("sparse_real", 96, 6, 1, 1, 1, 1.0),  # real couplings: the field cache
     ("hubo", 48, 4, 2, 1, 1, 1.0),
     # real couplings: field updates in the same float order as the oracle's
     ("hubo_real", 64, 6, 1, 2, 1, 1.0),
@@ -129,6 +144,13 @@ def test_sqa_bit_exact(oracle, kind, n, P, K, spb, wls, bscale):
 def test_sqa_generic_kernel_on_pm1_models(oracle, monkeypatch, kind, n, P, K, spb, wls, bscale):
     """The generic field-cache kernel gives the same bits as the +-1 kernel."""
     monkeypatch.setenv("QA_DISABLE_PM1", "1")
+    _sqa_case(oracle, kind, n, P, K, spb, wls, bscale)
+
+
+@pytest.mark.parametrize("kind,n,P,K,spb,wls,bscale", [("sparse", 128, 8, 1, 1, 1, 1.0), ("sparse", 64, 7, 2, 2, 1, 1.0)])
+def test_sqa_cached_field_kernel_on_integer_sparse(oracle, monkeypatch, kind, n, P, K, spb, wls, bscale):
+    """The field-cache kernel gives the same bits as the on-demand one."""
+    monkeypatch.setenv("QA_DISABLE_SPARSE_INT", "1")
     _sqa_case(oracle, kind, n, P, K, spb, wls, bscale)
 
 
