@@ -6,6 +6,8 @@
 #include <cstdio>
 #include <climits>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -49,6 +51,44 @@ struct DevBuf {
     size_t cap = 0;
 };
 
+// Device blocks of freed problems, kept for the next problem of about the
+// same size (a model rebuilt per call then costs no cudaMalloc / cudaFree).
+// Shared by a context and its problems, so it outlives whichever goes last.
+struct BlockPool {
+    int device = 0;
+    std::mutex mu;
+    std::vector<std::pair<size_t, void *>> free_blocks;
+    size_t pooled = 0;
+    static constexpr size_t kCap = (size_t)1 << 30;
+    ~BlockPool() {
+        cudaSetDevice(device);
+        for (auto &b : free_blocks) cudaFree(b.second);
+    }
+    void *take(size_t bytes, size_t *got) {
+        std::lock_guard<std::mutex> lk(mu);
+        int best = -1;
+        for (int k = 0; k < (int)free_blocks.size(); ++k) {
+            const size_t c = free_blocks[k].first;
+            if (c >= bytes && c <= 2 * bytes + ((size_t)1 << 20) && (best < 0 || c < free_blocks[best].first)) best = k;
+        }
+        if (best < 0) return nullptr;
+        void *p = free_blocks[best].second;
+        *got = free_blocks[best].first;
+        pooled -= *got;
+        free_blocks.erase(free_blocks.begin() + best);
+        return p;
+    }
+    void give(void *p, size_t bytes) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (pooled + bytes > kCap) {
+            cudaFree(p);
+            return;
+        }
+        free_blocks.push_back({bytes, p});
+        pooled += bytes;
+    }
+};
+
 }  // namespace
 
 namespace qa {
@@ -61,6 +101,8 @@ int set_last_error(int code, const char *msg) {
 
 struct qa_ctx {
     int device = 0;
+    std::shared_ptr<BlockPool> pool;
+    std::vector<unsigned char> stage;  // host staging of problem arrays, reused across problems
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int smem_optin = 0;
@@ -87,10 +129,13 @@ struct qa_problem {
     double c = 0.0;
     std::vector<void *> allocs;
     ProbDev dev{};
-    // arrays staged on the host while the problem is built, then sent with
-    // one allocation and one copy; fix = (offset, device pointer to patch)
-    std::vector<unsigned char> stage;
+    // arrays staged on the host (the context's buffer) while the problem is
+    // built, then sent with one copy into one device block; fix = (offset,
+    // device pointer to patch)
     std::vector<std::pair<size_t, const void **>> fix;
+    std::shared_ptr<BlockPool> pool;  // where the block goes back
+    void *block = nullptr;
+    size_t block_bytes = 0;
 };
 
 namespace {
@@ -113,12 +158,22 @@ int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
     return QA_OK;
 }
 
+// Space for `count` T in the staging buffer, to be filled before the next
+// staging call (which may move the buffer); *dev is set by finish_problem.
+template <class T>
+T *stage_array(qa_problem *P, size_t count, const T **dev) {
+    std::vector<unsigned char> &st = P->ctx->stage;
+    if (P->fix.empty()) st.clear();  // first array of this problem
+    const size_t off = (st.size() + 255) & ~(size_t)255;
+    st.resize(off + std::max<size_t>(count * sizeof(T), 16));
+    P->fix.push_back({off, reinterpret_cast<const void **>(dev)});
+    return reinterpret_cast<T *>(st.data() + off);
+}
+
 template <class T>
 int upload(qa_problem *P, const T *host, size_t count, const T **dev) {
-    const size_t off = (P->stage.size() + 255) & ~(size_t)255;
-    P->stage.resize(off + std::max<size_t>(count * sizeof(T), 16));
-    if (count) std::memcpy(P->stage.data() + off, host, count * sizeof(T));
-    P->fix.push_back({off, reinterpret_cast<const void **>(dev)});
+    T *dst = stage_array(P, count, dev);
+    if (count) std::memcpy(dst, host, count * sizeof(T));
     return QA_OK;
 }
 
@@ -136,12 +191,29 @@ int finish_problem(qa_problem *P) {
     P->dev.T = P->T;
     P->dev.m = P->m;
     P->dev.c = P->c;
-    void *d = nullptr;
-    QA_CK(cudaMalloc(&d, std::max<size_t>(P->stage.size(), 16)));
-    P->allocs.push_back(d);
-    QA_CK(cudaMemcpy(d, P->stage.data(), P->stage.size(), cudaMemcpyHostToDevice));
+    std::vector<unsigned char> &st = P->ctx->stage;
+    const size_t bytes = std::max<size_t>(st.size(), 16);
+    P->pool = P->ctx->pool;
+    size_t got = 0;
+    void *d = P->pool->take(bytes, &got);
+    if (!d) {
+        const cudaError_t e = cudaMalloc(&d, bytes);
+        if (e != cudaSuccess) {
+            st.clear();
+            P->fix.clear();
+            return fail(e == cudaErrorMemoryAllocation ? QA_ERR_OOM : QA_ERR_CUDA, cudaGetErrorString(e));
+        }
+        got = bytes;
+    }
+    P->block = d;
+    P->block_bytes = got;
+    const cudaError_t e = cudaMemcpy(d, st.data(), st.size(), cudaMemcpyHostToDevice);
+    st.clear();
+    if (e != cudaSuccess) {
+        P->fix.clear();
+        return fail(QA_ERR_CUDA, cudaGetErrorString(e));
+    }
     for (auto &f : P->fix) *f.second = static_cast<unsigned char *>(d) + f.first;
-    std::vector<unsigned char>().swap(P->stage);
     P->fix.clear();
     return QA_OK;
 }
@@ -534,6 +606,8 @@ int qa_create(qa_ctx **out, int device) {
     QA_CK(cudaSetDevice(device));
     qa_ctx *ctx = new qa_ctx();
     ctx->device = device;
+    ctx->pool = std::make_shared<BlockPool>();
+    ctx->pool->device = device;
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -560,8 +634,9 @@ int qa_destroy(qa_ctx *ctx) {
 
 int qa_problem_free(qa_problem *p) {
     if (!p) return QA_OK;
-    if (p->ctx) cudaSetDevice(p->ctx->device);
+    if (p->pool) cudaSetDevice(p->pool->device);
     for (void *d : p->allocs) cudaFree(d);
+    if (p->block) p->pool->give(p->block, p->block_bytes);
     delete p;
     return QA_OK;
 }
@@ -585,20 +660,25 @@ int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, doubl
     P->nw = (n + 31) / 32;
     P->c = c;
     // the upper triangle defines J (DenseIsing::energy reads i < j), mirrored
-    std::vector<float> J32((size_t)n * n, 0.0f);
+    int rc = common_h(P, h);
+    if (rc == QA_OK) rc = upload(P, J, (size_t)n * n, &P->dev.J64);
+    // J32 is written straight into the staging buffer: the upper triangle
+    // defines J (DenseIsing::energy reads i < j), mirrored, zero diagonal
+    float *J32 = stage_array(P, (size_t)n * n, &P->dev.J32);
     bool pm1 = true;  // couplings all in {-1,+1}: bit-packed rows for ring_pm1_kernel
-    for (int i = 0; i < n; ++i)
+    for (int i = 0; i < n; ++i) {
+        J32[(size_t)i * n + i] = 0.0f;
         for (int j = i + 1; j < n; ++j) {
             const double v = J[(size_t)i * n + j];
             pm1 = pm1 && (v == 1.0 || v == -1.0);
             J32[(size_t)i * n + j] = J32[(size_t)j * n + i] = (float)v;
         }
-    std::vector<uint32_t> Jw;
+    }
     if (pm1) {
         const int nw = (n + 31) / 32, np = pm1_npad(n);
-        Jw.assign((size_t)nw * np, 0u);
+        std::vector<uint32_t> Jw((size_t)nw * np, 0u);
         for (int m = 0; m < n; ++m) {
-            const float *row = J32.data() + (size_t)m * n;
+            const float *row = J32 + (size_t)m * n;  // read before the next staging call moves the buffer
             for (int q = 0; q < nw; ++q) {
                 uint32_t word = 0;
                 const int j1 = std::min(n, 32 * q + 32);
@@ -607,11 +687,8 @@ int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, doubl
                 Jw[(size_t)q * np + m] = word;
             }
         }
+        if (rc == QA_OK) rc = upload(P, Jw.data(), Jw.size(), &P->dev.Jw);
     }
-    int rc = common_h(P, h);
-    if (rc == QA_OK) rc = upload(P, J32.data(), J32.size(), &P->dev.J32);
-    if (rc == QA_OK) rc = upload(P, J, (size_t)n * n, &P->dev.J64);
-    if (rc == QA_OK && pm1) rc = upload(P, Jw.data(), Jw.size(), &P->dev.Jw);
     if (rc != QA_OK) {
         qa_problem_free(P);
         return rc;
