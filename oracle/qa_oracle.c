@@ -76,7 +76,7 @@ OR_EXPORT void or_philox(const uint32_t ctr_in[4], const uint32_t key_in[2], uin
 /* Domain tags (counter word 3, low byte). */
 enum {
     DOM_INIT = 1, DOM_SA = 2, DOM_SLICE = 3, DOM_WORLD = 4, DOM_SWAP = 5,
-    DOM_PILOT_INIT = 6, DOM_PILOT = 7, DOM_PROD_INIT = 8, DOM_PROD = 9
+    DOM_PILOT_INIT = 6, DOM_PILOT = 7, DOM_PROD_INIT = 8, DOM_PROD = 9, DOM_CSPIN = 10, DOM_CBOND = 11
 };
 
 static inline uint32_t spin_slot(int i) { return (uint32_t)(((i >> 7) << 5) | (i & 31)); }
@@ -667,6 +667,77 @@ static void worldline_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma,
     }
 }
 
+/* Cluster move of spin i of replica k along imaginary time, the
+   Swendsen-Wang step of sqa_annealer.cpp:215-288 (and
+   sqa_parallel_tempering.cpp:224-278) in the replay form:
+   - seed slice t0 = floor(u * P) from word 0 of philox(0, ring, sweep,
+     CSPIN | i << 8); the acceptance uniform is word 1 of the same call;
+   - bond b joins slices b and b+1 (mod P) when both carry the seed's spin and
+     its uniform (word b & 3 of philox(b >> 2, ring, sweep, CBOND | i << 8))
+     is below JP = 1 - exp(-2 J_perp); the cluster is the run of joined bonds
+     through t0, grown right then left (every slice when the run closes the
+     ring, as the reference's growth does with P - 1 joined bonds);
+   - y = x B - k T4 / 2 with x = h s0 |C| + sum_{t in C} s0 g_t (the sum in
+     warp order over t) and k = s0 (s_left + s_right) over the two slices
+     just outside the cluster (none when it is the whole ring). */
+static int cluster_move(ring_t *R, int k, int i, uint32_t rng_ring, uint32_t sigma, float B, float T4, float JP) {
+    const or_model *M = R->M;
+    const int n = R->n, P = R->P;
+    int8_t *s = R->s + (size_t)k * P * n;
+    float *g = R->g + (size_t)k * P * n;
+    const uint32_t c3s = DOM_CSPIN | ((uint32_t)i << 8), c3b = DOM_CBOND | ((uint32_t)i << 8);
+    const int t0 = (int)(((uint64_t)(draw(R->key, 0u, rng_ring, sigma, c3s, 0) >> 8) * (uint64_t)P) >> 24);
+    const float u = u01(draw(R->key, 0u, rng_ring, sigma, c3s, 1));
+    const int s0 = s[(size_t)t0 * n + i];
+    int act[64];
+    int all = 1;
+    for (int b = 0; b < P; ++b) {
+        const int b1 = b + 1 == P ? 0 : b + 1;
+        act[b] = s[(size_t)b * n + i] == s0 && s[(size_t)b1 * n + i] == s0 &&
+                 u01(draw(R->key, (uint32_t)(b >> 2), rng_ring, sigma, c3b, b & 3)) < JP;
+        all &= act[b];
+    }
+    int inC[64] = {0};
+    int kb = 0, r = 0, l = 0;
+    if (!all) {
+        while (act[(t0 + r) % P]) ++r;
+        while (act[((t0 - 1 - l) % P + P) % P]) ++l;
+        all = l + r + 1 >= P;  /* the arc closes on itself: every slice, no boundary */
+    }
+    if (all) {
+        for (int t = 0; t < P; ++t) inC[t] = 1;
+    } else {
+        for (int d = -l; d <= r; ++d) inC[((t0 + d) % P + P) % P] = 1;
+        const int tl = ((t0 - l - 1) % P + P) % P, tr = (t0 + r + 1) % P;
+        kb = s0 * s[(size_t)tl * n + i] + s0 * s[(size_t)tr * n + i];
+    }
+    double c[64];
+    int size = 0;
+    for (int t = 0; t < P; ++t) {
+        c[t] = inC[t] ? (double)s0 * (double)g[(size_t)t * n + i] : 0.0;
+        size += inC[t];
+    }
+    const double G = wsum(c, P);
+    const float x = (float)((double)M->h32[i] * (double)(s0 * size) + G);
+    const float y = (x * B) - ((float)kb * (0.5f * T4));
+    if (!metropolis(y, u)) return 0;
+    for (int t = 0; t < P; ++t)
+        if (inC[t]) {
+            int8_t *st = s + (size_t)t * n;
+            st[i] = (int8_t)-s0;
+            apply_flip(M, st, g + (size_t)t * n, i, s0);
+        }
+    return 1;
+}
+
+static void cluster_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma, float B, float T4, float JP) {
+    for (int i = 0; i < R->n; ++i) cluster_move(R, k, i, rng_ring, sigma, B, T4, JP);
+}
+
+static float join_prob(double beta, double gamma, int P) {
+    return (float)(1.0 - exp(-2.0 * trotter_coupling(beta, gamma, P)));
+}
+
 static double cell_energy(ring_t *R, int c) {
     return energy_track(R->M, R->s + (size_t)c * R->n, R->g + (size_t)c * R->n, R->sc);
 }
@@ -683,7 +754,7 @@ static void step_consts(double beta, double gamma, int P, float *B, float *T4) {
 /* ------------------------------------------------------------------ */
 OR_EXPORT int or_sqa_run(const or_model *M, const double *betas, const double *gammas, int steps, int P, int K,
                          int spb, int wls, uint64_t seed, int read, int8_t *best_spins, double *best_E,
-                         double *trace, int64_t *counters) {
+                         double *trace, int64_t *counters, int cls) {
     const int n = M->n;
     ring_t R;
     ring_alloc(&R, M, P, K, seed + (uint64_t)read);
@@ -697,6 +768,11 @@ OR_EXPORT int or_sqa_run(const or_model *M, const double *betas, const double *g
         float B, T4;
         step_consts(betas[step], gammas[step], P, &B, &T4);
         for (int sw = 0; sw < spb; ++sw) slice_sweep(&R, (uint32_t)(step * spb + sw), DOM_SLICE, B, T4, NULL);
+        if (cls > 0) {
+            const float JP = join_prob(betas[step], gammas[step], P);
+            for (int sw = 0; sw < cls; ++sw)
+                for (int k = 0; k < K; ++k) cluster_sweep(&R, k, (uint32_t)k, (uint32_t)(step * cls + sw), B, T4, JP);
+        }
         for (int sw = 0; sw < wls; ++sw)
             for (int k = 0; k < K; ++k) worldline_sweep(&R, k, (uint32_t)k, (uint32_t)(step * wls + sw), B);
         for (int k = 0; k < K; ++k) {
@@ -761,7 +837,7 @@ static void ring_scan(ring_t *R, int k, double *sum, double *emin, int *tmin, lo
 OR_EXPORT int or_sqapt_run(const or_model *M, const double *betas, const double *gammas, int Rn, int P, int spb,
                            int wls, int steps, int swap_interval, uint64_t seed, int read, int8_t *best_spins,
                            double *best_E, double *final_E, int8_t *final_spins, double *avg_trace,
-                           double *swap_trace, int64_t *counters) {
+                           double *swap_trace, int64_t *counters, int cls) {
     const int n = M->n;
     ring_t R;
     ring_alloc(&R, M, P, Rn, seed + (uint64_t)read);
@@ -798,6 +874,12 @@ OR_EXPORT int or_sqapt_run(const or_model *M, const double *betas, const double 
                         sweep_cell(&R, k, t, (uint32_t)(sl * P + t), sigma, DOM_SLICE, B[sl], T4[sl]);
                     }
         }
+        for (int sw = 0; sw < cls; ++sw)
+            for (int k = 0; k < Rn; ++k) {
+                const int sl = slot_of[k];
+                cluster_sweep(&R, k, (uint32_t)sl, (uint32_t)(step * cls + sw), B[sl], T4[sl],
+                              join_prob(betas[sl], gammas[sl], P));
+            }
         for (int sw = 0; sw < wls; ++sw)
             for (int k = 0; k < Rn; ++k)
                 worldline_sweep(&R, k, (uint32_t)slot_of[k], (uint32_t)(step * wls + sw), B[slot_of[k]]);

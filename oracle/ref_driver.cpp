@@ -151,14 +151,14 @@ int ref_sa_run(void *p, const double *betas, int steps, int spb, uint64_t seed, 
 
 // SQAAnnealer::run, one read (sqa_annealer.cpp:87-477).
 int ref_sqa_run(void *p, const double *betas, const double *gammas, int steps, int P, int K, int spb, int wls,
-                uint64_t seed, int8_t *best_spins, double *best_E, double *trace) {
+                uint64_t seed, int8_t *best_spins, double *best_E, double *trace, int cls) {
     return guarded([&] {
         auto *m = static_cast<RefModel *>(p);
         auto sched = SQASchedule::from_vectors(std::vector<double>(betas, betas + steps),
                                                std::vector<double>(gammas, gammas + steps));
         SQAAnnealer a(make_backend(BackendKind::CPU, m->ham), sched, (size_t)P, (size_t)K);
         a.set_seed(seed);
-        SQAResult r = a.run((size_t)spb, (size_t)wls);
+        SQAResult r = a.run((size_t)spb, (size_t)wls, (size_t)cls);
         std::memcpy(best_spins, r.best_state.spins.data(), r.best_state.size());
         *best_E = r.best_energy;
         if (trace) std::memcpy(trace, r.energy_trace.data(), sizeof(double) * r.energy_trace.size());
@@ -168,13 +168,13 @@ int ref_sqa_run(void *p, const double *betas, const double *gammas, int steps, i
 // SQAParallelTemperingAnnealer::run, one read (sqa_parallel_tempering.cpp:81-346).
 int ref_sqapt_run(void *p, const double *betas, const double *gammas, int R, int P, int spb, int wls, int steps,
                   int swap_interval, uint64_t seed, int8_t *best_spins, double *best_E, double *final_E,
-                  double *avg_trace, double *swap_trace) {
+                  double *avg_trace, double *swap_trace, int cls) {
     return guarded([&] {
         auto *m = static_cast<RefModel *>(p);
         SQAParallelTemperingAnnealer a(make_backend(BackendKind::CPU, m->ham), std::vector<double>(betas, betas + R),
                                        std::vector<double>(gammas, gammas + R), (size_t)P);
         a.set_seed(seed);
-        auto r = a.run((size_t)spb, (size_t)wls, (size_t)steps, (size_t)swap_interval);
+        auto r = a.run((size_t)spb, (size_t)wls, (size_t)steps, (size_t)swap_interval, (size_t)cls);
         std::memcpy(best_spins, r.best_state.spins.data(), r.best_state.size());
         *best_E = r.best_energy;
         if (final_E) std::memcpy(final_E, r.final_energies.data(), sizeof(double) * r.final_energies.size());

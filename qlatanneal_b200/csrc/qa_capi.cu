@@ -141,7 +141,7 @@ struct qa_problem {
 namespace {
 
 enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
-              W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP };
+              W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP, W_JP };
 
 int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
     DevBuf &b = ctx->ws[slot];
@@ -435,9 +435,11 @@ struct RingPlan {
 // whose ring fits in shared memory: J bits + int32 fields, J bits + int16
 // fields, int16 fields with J read from L2.  P <= 64 (worldlines are 64-bit
 // columns) and n <= 2048.  Anything else runs ring_kernel.
-int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, int P, int n_max, RingPlan *pl) {
+int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, int P, int n_max, RingPlan *pl,
+               bool clusters = false) {
     pl->W = std::max(1, std::min(32, (P + 1) / 2));
-    pl->pm1 = kind == K_DENSE && P <= 64 && n_max <= 2048 && !std::getenv("QA_DISABLE_PM1");
+    // cluster moves are in ring_kernel only
+    pl->pm1 = !clusters && kind == K_DENSE && P <= 64 && n_max <= 2048 && !std::getenv("QA_DISABLE_PM1");
     for (int p = 0; p < np && pl->pm1; ++p) pl->pm1 = probs[p]->dev.Jw != nullptr;
     if (pl->pm1) {
         const size_t cap = (size_t)ctx->smem_optin;
@@ -458,7 +460,7 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
         return QA_OK;
     }
     // sparse integer couplings: fields on demand, worldline sums from bits
-    pl->sparse = kind == K_SPARSE && P <= 64 && sparse_smem_bytes(P, n_max) <= (size_t)ctx->smem_optin &&
+    pl->sparse = !clusters && kind == K_SPARSE && P <= 64 && sparse_smem_bytes(P, n_max) <= (size_t)ctx->smem_optin &&
                  !std::getenv("QA_DISABLE_SPARSE_INT");
     for (int p = 0; p < np && pl->sparse; ++p) pl->sparse = probs[p]->dev.spcv != nullptr;
     if (pl->sparse) {
@@ -1003,8 +1005,6 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     if (prm->sweeps_per_beta == 0 && prm->worldline_sweeps == 0 && prm->cluster_sweeps == 0)
         return fail(QA_ERR_ARG,
                     "At least one of sweeps_per_beta, worldline_sweeps, or cluster_sweeps must be > 0.");
-    if (prm->cluster_sweeps > 0)
-        return fail(QA_ERR_UNSUPPORTED, "cluster_sweeps > 0 is not supported by the CUDA sweep engine.");
     if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
     int kind, n_max;
     QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
@@ -1012,6 +1012,8 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
                       ? prm->continuous_time_slices
                       : prm->trotter_slices;
     const int K = prm->replicas, steps = prm->steps;
+    if (prm->cluster_sweeps > 0 && P > 64)
+        return fail(QA_ERR_UNSUPPORTED, "cluster_sweeps > 0 runs with at most 64 Trotter slices on the GPU.");
     Layout L;
     build_rings(L, problems, n_problems, prm->reads, K, P, prm->seed);
     const int nr = (int)L.rings.size();
@@ -1033,6 +1035,12 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     float *d_T4 = static_cast<float *>(v);
     QA_CK(cudaMemcpyAsync(d_A, A.data(), sizeof(float) * steps, cudaMemcpyHostToDevice, ctx->stream));
     QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * steps, cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<float> JP(steps);  // join probability of the cluster moves (sqa_annealer.cpp:158)
+    for (int s = 0; s < steps; ++s)
+        JP[s] = (float)(1.0 - std::exp(-2.0 * trotter_coupling(prm->betas[s], prm->gammas[s], P)));
+    QA_TRY(ws_get(ctx, W_JP, sizeof(float) * steps, &v));
+    float *d_JP = static_cast<float *>(v);
+    QA_CK(cudaMemcpyAsync(d_JP, JP.data(), sizeof(float) * steps, cudaMemcpyHostToDevice, ctx->stream));
     QA_TRY(ws_get(ctx, W_SUM, sizeof(double) * (size_t)nr * steps, &v));
     double *d_sum = static_cast<double *>(v);
     QA_TRY(ws_get(ctx, W_BESTE, sizeof(double) * nr, &v));
@@ -1056,13 +1064,14 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
 
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     RingPlan pl;
-    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0));
     // dense +-1 couplings: the bit-packed kernel builds its fields in-kernel
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_beta; rp.wls = prm->worldline_sweeps;
     rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.B = d_A; rp.T4 = d_T4; rp.per_slot_sched = 0;
+    rp.cls = prm->cluster_sweeps; rp.JP = d_JP;
     rp.ring_sum = d_sum; rp.ring_min = nullptr; rp.ring_bond = nullptr;
     rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max; rp.mag = nullptr;
     rp.counters = d_cnt;
@@ -1151,14 +1160,14 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
         return fail(QA_ERR_ARG, "sweep counts must be >= 0.");
     if (prm->sweeps_per_step == 0 && prm->worldline_sweeps == 0 && prm->cluster_sweeps == 0)
         return fail(QA_ERR_ARG, "At least one of sweeps_per_step/worldline_sweeps/cluster_sweeps must be > 0.");
-    if (prm->cluster_sweeps > 0)
-        return fail(QA_ERR_UNSUPPORTED, "cluster_sweeps > 0 is not supported by the CUDA sweep engine.");
     if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
     int kind, n_max;
     QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
     const int P = (prm->continuous_time_slices > 0 && prm->continuous_time_slices > prm->trotter_slices)
                       ? prm->continuous_time_slices
                       : prm->trotter_slices;
+    if (prm->cluster_sweeps > 0 && P > 64)
+        return fail(QA_ERR_UNSUPPORTED, "cluster_sweeps > 0 runs with at most 64 Trotter slices on the GPU.");
     const int Rn = prm->rungs, steps = prm->steps, reads_total = n_problems * prm->reads;
     Layout L;
     build_rings(L, problems, n_problems, prm->reads, Rn, P, prm->seed);
@@ -1168,13 +1177,14 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
     uint32_t *d_spins;
     float *d_fields;
     QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
-    std::vector<float> B(Rn), T4(Rn);
+    std::vector<float> B(Rn), T4(Rn), JP(Rn);
     std::vector<double> bpjp(2 * Rn);
     for (int r = 0; r < Rn; ++r) {
         B[r] = (float)(2.0 * (prm->betas[r] / (double)P));
         T4[r] = (float)(4.0 * trotter_coupling(prm->betas[r], prm->gammas[r], P));
         bpjp[r] = prm->betas[r] / (double)P;
         bpjp[Rn + r] = trotter_coupling(prm->betas[r], prm->gammas[r], P);
+        JP[r] = (float)(1.0 - std::exp(-2.0 * bpjp[Rn + r]));  // sqa_parallel_tempering.cpp:201
     }
     float *d_B, *d_T4;
     double *d_bpjp, *d_sum, *d_min, *d_best, *d_exact, *d_avg, *d_swp;
@@ -1185,6 +1195,8 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
     const size_t rec = (size_t)nr * (steps + 1);
     QA_TRY(ws_array(ctx, W_A, Rn, &d_B));
     QA_TRY(ws_array(ctx, W_T4, Rn, &d_T4));
+    float *d_JP;
+    QA_TRY(ws_array(ctx, W_JP, Rn, &d_JP));
     QA_TRY(ws_array(ctx, W_BPJP, 2 * Rn, &d_bpjp));
     QA_TRY(ws_array(ctx, W_SUM, rec, &d_sum));
     QA_TRY(ws_array(ctx, W_MIN, rec, &d_min));
@@ -1207,6 +1219,7 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
         for (size_t i = 0; i < rin.size(); ++i) rin[i] = (int)(i % Rn);
         QA_CK(cudaMemcpyAsync(d_B, B.data(), sizeof(float) * Rn, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * Rn, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_JP, JP.data(), sizeof(float) * Rn, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_bpjp, bpjp.data(), sizeof(double) * 2 * Rn, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_bstep, neg.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
@@ -1217,13 +1230,14 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
         QA_CK(cudaStreamSynchronize(ctx->stream));
     }
     RingPlan pl;
-    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0));
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_step; rp.wls = prm->worldline_sweeps;
     rp.slice_tag = DOM_SLICE; rp.slot = d_slot; rp.B = d_B; rp.T4 = d_T4; rp.per_slot_sched = 1;
+    rp.cls = prm->cluster_sweeps; rp.JP = d_JP;
     rp.ring_sum = d_sum; rp.ring_min = d_min; rp.ring_bond = d_bond; rp.rec_base = 1; rp.rec_stride = steps + 1;
     rp.best_E = d_best; rp.best_step = d_bstep; rp.best_slot = d_bslot; rp.best_bits = d_bits;
     rp.final_bits = d_fbits; rp.nw_max = L.nw_max; rp.counters = d_cnt;

@@ -47,6 +47,8 @@ struct RingParams {
     uint32_t slice_tag;   // DOM_SLICE, DOM_PROD or DOM_PILOT|(point<<8)
     const int *slot;      // PT: rung slot of each ring (null: slot = k)
     const float *B, *T4;  // [sched + step] (PT: [sched + slot]): B = 2 beta/P, T4 = 4 J_perp
+    int cls;              // cluster sweeps per step (ring_kernel only; P <= 64)
+    const float *JP;      // like B: bond probability 1 - exp(-2 J_perp) of the cluster moves
     int per_slot_sched;   // 1: index A/T4 by slot instead of step
     int smem_fields;
     int init_fields;      // ring_pm1_kernel: build the int32 fields from the spins first
@@ -269,6 +271,86 @@ __host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fiel
     return b;
 }
 
+// Cluster move of spin i along imaginary time (sqa_annealer.cpp:215-288,
+// sqa_parallel_tempering.cpp:224-278), one warp.  Seed slice and acceptance
+// uniform from philox(0, ring, sweep, CSPIN | i << 8); bond b (slices b and
+// b+1) joins when both carry the seed's spin and its uniform, word b & 3 of
+// philox(b >> 2, ring, sweep, CBOND | i << 8), is below JP.  The cluster is
+// the run of joined bonds through the seed (every slice when the run closes
+// the ring); y = x B - k T4/2 with x = h s0 |C| + sum_{t in C} s0 g_t (warp
+// order over t = lane, lane + 32) and k the seed spin times the two spins just
+// outside the cluster.  Lane t holds slices t and t + 32 (P <= 64).
+template <int KIND>
+__device__ __forceinline__ void cluster_move(const ProbDev &Pd, uint32_t *S, float *gbase, const float *h, int NP,
+                                             int i, uint32_t ring, uint32_t sigma, float B, float T4, float JP,
+                                             uint64_t key, int lane) {
+    const int n = Pd.n, nw = Pd.nw;
+    const uint32_t c3s = DOM_CSPIN | ((uint32_t)i << 8), c3b = DOM_CBOND | ((uint32_t)i << 8);
+    const U4 w = philox(0u, ring, sigma, c3s, key);
+    const int t0 = (int)(((unsigned long long)(w.x >> 8) * (unsigned long long)NP) >> 24);
+    const float u = u01(w.y);
+    const int q = i >> 5;
+    const uint32_t bit = 1u << (i & 31);
+    const int ta = lane, tb = lane + 32;
+    const bool upa = ta < NP && (S[ta * nw + q] & bit), upb = tb < NP && (S[tb * nw + q] & bit);
+    const unsigned long long Wi =
+        (unsigned long long)__ballot_sync(FULL, upa) | ((unsigned long long)__ballot_sync(FULL, upb) << 32);
+    const unsigned long long pmask = NP == 64 ? ~0ull : ((1ull << NP) - 1ull);
+    const bool s0up = (Wi >> t0) & 1ull;
+    const int s0 = s0up ? 1 : -1;
+    const unsigned long long same = (s0up ? Wi : ~Wi) & pmask;
+    // bond uniforms: lane l draws bonds 4l .. 4l+3; bond b takes its word from lane b >> 2
+    U4 bw = {0u, 0u, 0u, 0u};
+    if (4 * lane < NP) bw = philox((uint32_t)lane, ring, sigma, c3b, key);
+    bool act[2];
+#pragma unroll
+    for (int h2 = 0; h2 < 2; ++h2) {
+        const int b = lane + 32 * h2;
+        const int src = b >> 2;
+        const uint32_t x0 = __shfl_sync(FULL, bw.x, src), x1 = __shfl_sync(FULL, bw.y, src);
+        const uint32_t x2 = __shfl_sync(FULL, bw.z, src), x3 = __shfl_sync(FULL, bw.w, src);
+        const uint32_t wb = (b & 3) == 0 ? x0 : ((b & 3) == 1 ? x1 : ((b & 3) == 2 ? x2 : x3));
+        const int b1 = b + 1 == NP ? 0 : b + 1;
+        act[h2] = b < NP && ((same >> b) & 1ull) && ((same >> b1) & 1ull) && u01(wb) < JP;
+    }
+    const unsigned long long A0 =
+        (unsigned long long)__ballot_sync(FULL, act[0]) | ((unsigned long long)__ballot_sync(FULL, act[1]) << 32);
+    bool all = (A0 & pmask) == pmask;
+    int r = 0, l = 0;
+    if (!all) {
+        const unsigned long long A = t0 == 0 ? A0 : (((A0 >> t0) | (A0 << (NP - t0))) & pmask);
+        r = __ffsll((long long)~A) - 1;                         // joined bonds right of the seed
+        l = NP - 1 - (63 - __clzll((long long)(~A & pmask)));  // joined bonds left of it
+        all = l + r + 1 >= NP;
+    }
+    unsigned long long Cm = pmask;
+    int kb = 0, size = NP;
+    if (!all) {
+        unsigned long long Cr = (r >= 63 ? ~0ull : ((2ull << r) - 1ull));
+        if (l > 0) Cr |= pmask & ~((1ull << (NP - l)) - 1ull);
+        Cr &= pmask;
+        Cm = t0 == 0 ? Cr : (((Cr << t0) | (Cr >> (NP - t0))) & pmask);
+        const int tl = (t0 - l - 1 + NP) % NP, tr = (t0 + r + 1) % NP;
+        kb = s0 * ((((Wi >> tl) & 1ull) ? 1 : -1) + (((Wi >> tr) & 1ull) ? 1 : -1));
+        size = l + r + 1;
+    }
+    double acc = 0.0;
+    if (ta < NP && ((Cm >> ta) & 1ull)) acc = __dadd_rn(acc, (double)s0 * (double)gbase[(long long)ta * n + i]);
+    if (tb < NP && ((Cm >> tb) & 1ull)) acc = __dadd_rn(acc, (double)s0 * (double)gbase[(long long)tb * n + i]);
+    const double G = warp_sum_d(acc);
+    const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)h[i], (double)(s0 * size)), G));
+    const float y = __fsub_rn(__fmul_rn(x, B), __fmul_rn(__int2float_rn(kb), __fmul_rn(0.5f, T4)));
+    if (!metropolis_nb(y, u)) return;
+    if (ta < NP && ((Cm >> ta) & 1ull)) S[ta * nw + q] ^= bit;
+    if (tb < NP && ((Cm >> tb) & 1ull)) S[tb * nw + q] ^= bit;
+    __syncwarp();
+    for (unsigned long long c = Cm; c; c &= c - 1ull) {
+        const int t = __ffsll((long long)c) - 1;
+        apply_flip<KIND>(Pd, gbase + (long long)t * n, S + t * nw, i, s0, lane);
+    }
+    __syncwarp();
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -328,6 +410,17 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                 }
                 __syncthreads();
             }
+        }
+        // cluster sweeps: one warp, spins in order
+        const int cls = step >= 0 ? p.cls : 0;
+        for (int sw = 0; sw < cls; ++sw) {
+            if (warp == 0) {
+                const uint32_t sigma = (uint32_t)(step * p.cls + sw);
+                const float JPv = p.JP[si_tab];
+                for (int i = 0; i < n; ++i)
+                    cluster_move<KIND>(Pd, sm.S, gbase, sm.h, NP, i, (uint32_t)slot, sigma, B, T4, JPv, R.key, lane);
+            }
+            __syncthreads();
         }
         for (int sw = 0; sw < wls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);

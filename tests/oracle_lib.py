@@ -76,9 +76,10 @@ class Oracle:
         L.or_sa_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double),
                                 _f8p, _i64p]
         L.or_sqa_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
-                                 C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i64p]
+                                 C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i64p, C.c_int]
         L.or_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                   C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i8p, _f8p, _f8p, _i64p]
+                                   C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i8p, _f8p, _f8p, _i64p,
+                                   C.c_int]
         L.or_chi_schedule.argtypes = ([C.c_int, _f8p, _f8p, _f8p] + [C.c_double] * 4 + [C.c_int, C.c_int] +
                                       [C.c_double] * 3 + [_f8p] * 4)
         L.or_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 3 + [C.c_int] * 5 +
@@ -165,13 +166,14 @@ class Oracle:
         self.L.or_sa_run(m.h, betas, len(betas), sweeps_per_beta, seed, read, best, C.byref(E), trace, cnt)
         return best, E.value, trace, cnt
 
-    def sqa_run(self, m, betas, gammas, P, K, spb, wls, seed, read=0):
+    def sqa_run(self, m, betas, gammas, P, K, spb, wls, seed, read=0, cls=0):
         betas, gammas = _c64(betas), _c64(gammas)
         best = np.zeros(m.n, np.int8)
         E = C.c_double()
         trace = np.zeros(len(betas), np.float64)
         cnt = np.zeros(4, np.int64)
-        self.L.or_sqa_run(m.h, betas, gammas, len(betas), P, K, spb, wls, seed, read, best, C.byref(E), trace, cnt)
+        self.L.or_sqa_run(m.h, betas, gammas, len(betas), P, K, spb, wls, seed, read, best, C.byref(E), trace, cnt,
+                          cls)
         return best, E.value, trace, cnt
 
     def chi_schedule(self, scan_s, scan_gamma, chi, beta, gamma_start, gamma_end, A0, slices, num_steps,
@@ -197,7 +199,7 @@ class Oracle:
         return dict(best=best, best_energy=E.value, scalars=sc, **{"scan_" + k: v for k, v in scan.items()},
                     **out)
 
-    def sqapt_run(self, m, betas, gammas, P, spb, wls, steps, swap_interval, seed, read=0):
+    def sqapt_run(self, m, betas, gammas, P, spb, wls, steps, swap_interval, seed, read=0, cls=0):
         """Returns (best, best_E, final_E[R], final_spins[R][n], avg_trace, swap_trace, counters)."""
         betas, gammas = _c64(betas), _c64(gammas)
         R = len(betas)
@@ -209,7 +211,7 @@ class Oracle:
         swp = np.zeros(steps)
         cnt = np.zeros(4, np.int64)
         self.L.or_sqapt_run(m.h, betas, gammas, R, P, spb, wls, steps, swap_interval, seed, read, best, C.byref(E),
-                            fE, fs, avg, swp, cnt)
+                            fE, fs, avg, swp, cnt, cls)
         return best, E.value, fE, fs.reshape(R, m.n), avg, swp, cnt
 
 
@@ -239,9 +241,9 @@ class Ref:
         L.ref_update_fields.argtypes = [C.c_void_p, _f8p, _i8p, C.c_int, C.c_int, C.c_int]
         L.ref_sa_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p]
         L.ref_sqa_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
-                                  _i8p, C.POINTER(C.c_double), _f8p]
+                                  _i8p, C.POINTER(C.c_double), _f8p, C.c_int]
         L.ref_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                    C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p, _f8p, _f8p]
+                                    C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p, _f8p, _f8p, C.c_int]
         L.ref_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                    C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                    C.c_uint64, _i8p, C.POINTER(C.c_double)] + [_f8p] * 8)
@@ -325,12 +327,13 @@ class RefModel:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return best, E.value, tr
 
-    def sqa_run(self, betas, gammas, P, K, spb, wls, seed):
+    def sqa_run(self, betas, gammas, P, K, spb, wls, seed, cls=0):
         betas, gammas = _c64(betas), _c64(gammas)
         best = np.zeros(self.n, np.int8)
         E = C.c_double()
         tr = np.zeros(len(betas))
-        if self.ref.L.ref_sqa_run(self.h, betas, gammas, len(betas), P, K, spb, wls, seed, best, C.byref(E), tr) != 0:
+        if self.ref.L.ref_sqa_run(self.h, betas, gammas, len(betas), P, K, spb, wls, seed, best, C.byref(E), tr,
+                                  cls) != 0:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return best, E.value, tr
 
@@ -349,14 +352,14 @@ class RefModel:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return dict(best=best, best_energy=E.value, scalars=sc, **arr)
 
-    def sqapt_run(self, betas, gammas, P, spb, wls, steps, swap_interval, seed):
+    def sqapt_run(self, betas, gammas, P, spb, wls, steps, swap_interval, seed, cls=0):
         betas, gammas = _c64(betas), _c64(gammas)
         R = len(betas)
         best = np.zeros(self.n, np.int8)
         E = C.c_double()
         fE, avg, swp = np.zeros(R), np.zeros(steps), np.zeros(steps)
         rc = self.ref.L.ref_sqapt_run(self.h, betas, gammas, R, P, spb, wls, steps, swap_interval, seed, best,
-                                      C.byref(E), fE, avg, swp)
+                                      C.byref(E), fE, avg, swp, cls)
         if rc != 0:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return best, E.value, fE, avg, swp

@@ -69,5 +69,29 @@ def test_sqapt_argument_errors():
         ann.run(1, 1, 0)
     with pytest.raises(ValueError):
         ann.run(1, 1, 5, 0)
-    with pytest.raises(NotImplementedError):
-        ann.run(1, 1, 5, 1, cluster_sweeps=1)
+    with pytest.raises(NotImplementedError):  # cluster moves keep a slice's worldline in 64 bits
+        qa.SQAParallelTemperingAnnealer(m, [1.0, 2.0], [1.0, 0.5], 65).run(1, 1, 5, 1, cluster_sweeps=1)
+
+
+@pytest.mark.parametrize("kind,n,P,R,spb,wls,cls,steps,swap", [
+    ("dense", 64, 8, 4, 1, 0, 1, 10, 1),
+    ("sparse", 100, 6, 3, 0, 1, 2, 8, 2),
+    ("hubo", 40, 4, 3, 1, 1, 1, 7, 1),
+])
+def test_sqapt_cluster_bit_exact(oracle, kind, n, P, R, spb, wls, cls, steps, swap):
+    """SQA-PT with cluster sweeps (SQAPT+SW, sqa_parallel_tempering.cpp:222-278)."""
+    model = make(kind, n, 33)
+    om = oracle_model(oracle, model)
+    betas = np.geomspace(0.3, 3.0, R) * P / 8.0
+    gammas = np.linspace(2.5, 0.05, R)
+    reads, seed = 3, 1357
+    ann = qa.SQAParallelTemperingAnnealer(model, betas, gammas, P)
+    res = ann.run_reads(spb, wls, steps, swap, cls, reads=reads, seed=seed)
+    for r in range(reads):
+        best, E, fE, fs, avg, swp, cnt = oracle.sqapt_run(om, betas, gammas, P, spb, wls, steps, swap, seed, r,
+                                                          cls=cls)
+        np.testing.assert_array_equal(res[r].best_state.as_array(), best)
+        assert res[r].best_energy == E
+        np.testing.assert_array_equal(np.asarray(res[r].final_energies), fE)
+        np.testing.assert_array_equal(np.asarray(res[r].average_energy_trace), avg)
+        np.testing.assert_array_equal(np.asarray(res[r].swap_acceptance_trace), swp)

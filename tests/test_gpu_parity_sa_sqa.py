@@ -154,7 +154,29 @@ def test_sqa_cached_field_kernel_on_integer_sparse(oracle, monkeypatch, kind, n,
     _sqa_case(oracle, kind, n, P, K, spb, wls, bscale)
 
 
-def _sqa_case(oracle, kind, n, P, K, spb, wls, bscale):
+CLUSTER_CASES = [
+    # kind, n, P, K, spb, wls, cluster sweeps, beta scale
+    ("dense", 64, 8, 2, 1, 1, 1, 1.0),
+    ("dense", 40, 1, 1, 1, 0, 2, 1.0),
+    ("dense", 40, 2, 1, 0, 1, 2, 1.0),
+    ("dense", 33, 5, 1, 1, 0, 1, 0.5),
+    ("dense", 100, 64, 1, 0, 1, 1, 0.25),
+    ("dense_h", 70, 6, 2, 0, 0, 3, 0.5),
+    ("dense_int", 48, 12, 1, 1, 1, 1, 0.5),
+    ("sparse", 128, 8, 1, 1, 1, 1, 1.0),
+    ("sparse_real", 96, 6, 1, 0, 1, 2, 1.0),
+    ("hubo", 48, 4, 2, 1, 1, 1, 1.0),
+    ("hubo_real", 64, 6, 1, 1, 0, 1, 1.0),
+]
+
+
+@pytest.mark.parametrize("kind,n,P,K,spb,wls,cls,bscale", CLUSTER_CASES)
+def test_sqa_cluster_bit_exact(oracle, kind, n, P, K, spb, wls, cls, bscale):
+    """Imaginary-time cluster moves (sqa_annealer.cpp:215-288) on the GPU equal the oracle's."""
+    _sqa_case(oracle, kind, n, P, K, spb, wls, bscale, cls)
+
+
+def _sqa_case(oracle, kind, n, P, K, spb, wls, bscale, cls=0):
     model = make(kind, n, 21)
     om = oracle_model(oracle, model)
     steps = 25
@@ -162,10 +184,10 @@ def _sqa_case(oracle, kind, n, P, K, spb, wls, bscale):
     gammas = np.linspace(3.0, 0.05, steps)
     reads, seed = 3, 777
     ann = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors(betas, gammas), P, K)
-    res = ann.run_reads(spb, wls, reads=reads, seed=seed)
+    res = ann.run_reads(spb, wls, cls, reads=reads, seed=seed)
     acc_s = acc_w = 0
     for r in range(reads):
-        best, E, trace, cnt = oracle.sqa_run(om, betas, gammas, P, K, spb, wls, seed, r)
+        best, E, trace, cnt = oracle.sqa_run(om, betas, gammas, P, K, spb, wls, seed, r, cls=cls)
         acc_s += cnt[1]
         acc_w += cnt[3]
         np.testing.assert_array_equal(res[r].best_state.as_array(), best)
@@ -226,5 +248,5 @@ def test_argument_errors():
         qa.Annealer(m, qa.AnnealSchedule.from_betas([1.0])).run(0)
     with pytest.raises(ValueError):
         qa.SQAAnnealer(m, qa.SQASchedule.from_vectors([1.0], [1.0]), 4).run(0, 0)
-    with pytest.raises(NotImplementedError):
-        qa.SQAAnnealer(m, qa.SQASchedule.from_vectors([1.0], [1.0]), 4).run(1, 1, cluster_sweeps=1)
+    with pytest.raises(NotImplementedError):  # cluster moves keep a slice's worldline in 64 bits
+        qa.SQAAnnealer(m, qa.SQASchedule.from_vectors([1.0], [1.0]), 65).run(1, 1, cluster_sweeps=1)
