@@ -114,6 +114,23 @@ typedef struct {
 QA_API int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *params,
               qa_run_out *outs, qa_stats *stats);
 
+/* ---- SA replicas: ReplicaAnnealer::run (replica_annealer.cpp:46-142) -------
+ * params->reads = replicas; replica r is SA read r (keyed seed + r).  Besides
+ * qa_sa_run's outputs: the magnetisation after each step and the step whose
+ * sweeps last lowered each replica's best energy (-1: the starting state),
+ * from which the caller picks the global best as the reference does (lowest
+ * energy, then earliest step, then lowest replica). */
+typedef struct {
+    int8_t *best_spins;              /* [replicas][n] */
+    double *best_energy;             /* [replicas] */
+    double *energy_trace;            /* [replicas][steps] */
+    double *magnetization_trace;     /* [replicas][steps] */
+    int32_t *best_step;              /* [replicas] */
+} qa_replica_out;
+
+QA_API int qa_replica_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
+                          const qa_sa_params *params, qa_replica_out *outs, qa_stats *stats);
+
 /* ---- SQA: SQAAnnealer::run (sqa_annealer.cpp:87-477) ---------------------- */
 typedef struct {
     const double *betas;     /* [steps]  SQASchedule */
@@ -123,7 +140,7 @@ typedef struct {
     int replicas;            /* K > 0 rings per read */
     int sweeps_per_beta;     /* slice sweeps per step */
     int worldline_sweeps;    /* worldline sweeps per step */
-    int cluster_sweeps;      /* must be 0 (QA_ERR_UNSUPPORTED otherwise) */
+    int cluster_sweeps;      /* imaginary-time cluster sweeps per step (P <= 64) */
     int continuous_time_slices; /* slices = max(P, this) when larger, as in the reference */
     int reads;
     uint64_t seed;
@@ -145,7 +162,7 @@ typedef struct {
     int worldline_sweeps;
     int steps;               /* pt_steps */
     int swap_interval;       /* > 0 */
-    int cluster_sweeps;      /* must be 0 */
+    int cluster_sweeps;      /* imaginary-time cluster sweeps per step (P <= 64) */
     int continuous_time_slices;
     int reads;
     uint64_t seed;
@@ -162,6 +179,24 @@ typedef struct {
 
 QA_API int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
                         const qa_sqapt_params *params, qa_sqapt_out *outs, qa_stats *stats);
+
+/* ---- classical parallel tempering: ParallelTemperingAnnealer::run
+ *      (parallel_tempering.cpp:36-122) --------------------------------------
+ * One replica per beta, Metropolis sweeps, swaps of neighbouring replicas
+ * every swap_interval steps.  Outputs as qa_sqapt_out (final energies are the
+ * replicas' energies). */
+typedef struct {
+    const double *betas;     /* [rungs] */
+    int rungs;               /* >= 2 */
+    int sweeps_per_step;     /* > 0 */
+    int steps;               /* > 0 */
+    int swap_interval;       /* > 0 */
+    int reads;
+    uint64_t seed;
+} qa_pt_params;
+
+QA_API int qa_pt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_pt_params *params,
+                     qa_sqapt_out *outs, qa_stats *stats);
 
 /* ---- SQA-Chi: SQAChiAnnealer::run_chi (sqa_chi_annealer.cpp:146-438) -----
  * Stage 1, the pilot chi_B scan (scan_points fresh worldlines per read, all

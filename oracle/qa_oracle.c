@@ -16,6 +16,9 @@
  *                    per-step energy scan and best tracking)
  *   SQA-PT run()     src/sqa_parallel_tempering.cpp:81-346
  *   SQA-Chi run_chi  src/sqa_chi_annealer.cpp:81-438
+ *   cluster moves    src/sqa_annealer.cpp:215-288, src/sqa_parallel_tempering.cpp:222-278
+ *   classical PT     src/parallel_tempering.cpp:36-122 (the SQA-PT core, one slice)
+ *   replicas         src/replica_annealer.cpp:46-142 (SA reads + magnetisation)
  *
  * The "replay model".  The qanneal loops draw from std::mt19937_64 through
  * libstdc++ distributions and visit spins in std::shuffle order, which no GPU
@@ -528,8 +531,12 @@ static double trotter_coupling(double beta, double gamma, int P) {
 /* ------------------------------------------------------------------ */
 /* SA (annealer.cpp:33-75)                                              */
 /* ------------------------------------------------------------------ */
+/* mag_trace (nullable): magnetisation after each step (ReplicaAnnealer,
+   replica_annealer.cpp:119-131); best_step (nullable): the step whose sweeps
+   last lowered the best energy, -1 for the starting state. */
 OR_EXPORT int or_sa_run(const or_model *M, const double *betas, int steps, int spb, uint64_t seed, int read,
-                        int8_t *best_spins, double *best_E, double *trace, int64_t *counters) {
+                        int8_t *best_spins, double *best_E, double *trace, int64_t *counters, double *mag_trace,
+                        int *best_step) {
     const int n = M->n;
     const uint64_t key = seed + (uint64_t)read;
     int8_t *s = (int8_t *)malloc((size_t)n);
@@ -539,6 +546,7 @@ OR_EXPORT int or_sa_run(const or_model *M, const double *betas, int steps, int s
     fields_init(M, s, g);
     double E = energy_track(M, s, g, sc);
     double best = E;
+    int bstep = -1;
     memcpy(best_spins, s, (size_t)n);
     int64_t att = 0, acc = 0;
     for (int step = 0; step < steps; ++step) {
@@ -557,13 +565,19 @@ OR_EXPORT int or_sa_run(const or_model *M, const double *betas, int steps, int s
                     s[i] = (int8_t)-so;
                     apply_flip(M, s, g, i, so);
                     E += -2.0 * xd;
-                    if (E < best) { best = E; memcpy(best_spins, s, (size_t)n); }
+                    if (E < best) { best = E; bstep = step; memcpy(best_spins, s, (size_t)n); }
                 }
             }
         }
         trace[step] = E;
+        if (mag_trace) {
+            long long m = 0;
+            for (int i = 0; i < n; ++i) m += s[i];
+            mag_trace[step] = (double)m / (double)n;
+        }
     }
     *best_E = best;
+    if (best_step) *best_step = bstep;
     if (counters) { counters[0] = att; counters[1] = acc; }
     free(s); free(g); free(sc);
     return 0;
@@ -834,10 +848,35 @@ static void ring_scan(ring_t *R, int k, double *sum, double *emin, int *tmin, lo
 /* swaps exchange which ring sits in which slot, pairs r = 0..R-2 in     */
 /* order (cascading), every swap_interval steps.                         */
 /* ------------------------------------------------------------------ */
+static int sqapt_core(const or_model *M, const double *betas, const double *gammas, int Rn, int P, int spb, int wls,
+                      int steps, int swap_interval, uint64_t seed, int read, int8_t *best_spins, double *best_E,
+                      double *final_E, int8_t *final_spins, double *avg_trace, double *swap_trace,
+                      int64_t *counters, int cls, int classical);
+
 OR_EXPORT int or_sqapt_run(const or_model *M, const double *betas, const double *gammas, int Rn, int P, int spb,
                            int wls, int steps, int swap_interval, uint64_t seed, int read, int8_t *best_spins,
                            double *best_E, double *final_E, int8_t *final_spins, double *avg_trace,
                            double *swap_trace, int64_t *counters, int cls) {
+    return sqapt_core(M, betas, gammas, Rn, P, spb, wls, steps, swap_interval, seed, read, best_spins, best_E,
+                      final_E, final_spins, avg_trace, swap_trace, counters, cls, 0);
+}
+
+/* Classical parallel tempering (parallel_tempering.cpp:36-122): the SQA-PT
+   core with one slice per rung and no transverse field -- B = 2 beta, no
+   Trotter term, the swap action beta E, so a swap of rungs i, i+1 is
+   accepted on -(beta_i - beta_{i+1}) (E_{i+1} - E_i) -- and no worldline or
+   cluster moves. */
+OR_EXPORT int or_pt_run(const or_model *M, const double *betas, int Rn, int spb, int steps, int swap_interval,
+                        uint64_t seed, int read, int8_t *best_spins, double *best_E, double *final_E,
+                        int8_t *final_spins, double *avg_trace, double *swap_trace, int64_t *counters) {
+    return sqapt_core(M, betas, betas, Rn, 1, spb, 0, steps, swap_interval, seed, read, best_spins, best_E, final_E,
+                      final_spins, avg_trace, swap_trace, counters, 0, 1);
+}
+
+static int sqapt_core(const or_model *M, const double *betas, const double *gammas, int Rn, int P, int spb, int wls,
+                      int steps, int swap_interval, uint64_t seed, int read, int8_t *best_spins, double *best_E,
+                      double *final_E, int8_t *final_spins, double *avg_trace, double *swap_trace,
+                      int64_t *counters, int cls, int classical) {
     const int n = M->n;
     ring_t R;
     ring_alloc(&R, M, P, Rn, seed + (uint64_t)read);
@@ -853,6 +892,7 @@ OR_EXPORT int or_sqapt_run(const or_model *M, const double *betas, const double 
         step_consts(betas[k], gammas[k], P, &B[k], &T4[k]);
         bp[k] = betas[k] / (double)P;
         jp[k] = trotter_coupling(betas[k], gammas[k], P);
+        if (classical) { T4[k] = 0.0f; jp[k] = 0.0; }
     }
     double best = INFINITY;
     for (int k = 0; k < Rn; ++k) ring_scan(&R, k, &Esum[k], &Emin[k], &tmin[k], &bond[k]);

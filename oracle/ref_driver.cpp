@@ -17,6 +17,8 @@
 #include <vector>
 
 #include "qanneal/annealer.hpp"
+#include "qanneal/parallel_tempering.hpp"
+#include "qanneal/replica_annealer.hpp"
 #include "qanneal/backend.hpp"
 #include "qanneal/dense_ising.hpp"
 #include "qanneal/higher_order_ising.hpp"
@@ -162,6 +164,38 @@ int ref_sqa_run(void *p, const double *betas, const double *gammas, int steps, i
         std::memcpy(best_spins, r.best_state.spins.data(), r.best_state.size());
         *best_E = r.best_energy;
         if (trace) std::memcpy(trace, r.energy_trace.data(), sizeof(double) * r.energy_trace.size());
+    });
+}
+
+// ParallelTemperingAnnealer::run (parallel_tempering.cpp:36-122).
+int ref_pt_run(void *p, const double *betas, int R, int spb, int steps, int swap_interval, uint64_t seed,
+               int8_t *best_spins, double *best_E, double *final_E, double *avg_trace, double *swap_trace) {
+    return guarded([&] {
+        auto *m = static_cast<RefModel *>(p);
+        ParallelTemperingAnnealer a(make_backend(BackendKind::CPU, m->ham), std::vector<double>(betas, betas + R));
+        a.set_seed(seed);
+        auto r = a.run((size_t)spb, (size_t)steps, (size_t)swap_interval);
+        std::memcpy(best_spins, r.best_state.spins.data(), r.best_state.size());
+        *best_E = r.best_energy;
+        if (final_E) std::memcpy(final_E, r.final_energies.data(), sizeof(double) * r.final_energies.size());
+        if (avg_trace) std::memcpy(avg_trace, r.average_energy_trace.data(), sizeof(double) * steps);
+        if (swap_trace) std::memcpy(swap_trace, r.swap_acceptance_trace.data(), sizeof(double) * steps);
+    });
+}
+
+// ReplicaAnnealer::run (replica_annealer.cpp:46-142): global best and the average traces.
+int ref_replica_run(void *p, const double *betas, int steps, int spb, int R, uint64_t seed, double *best_E,
+                    double *avg_energy, double *avg_mag) {
+    return guarded([&] {
+        auto *m = static_cast<RefModel *>(p);
+        AnnealSchedule sched;
+        sched.betas.assign(betas, betas + steps);
+        ReplicaAnnealer a(make_backend(BackendKind::CPU, m->ham), sched, (size_t)R);
+        a.set_seed(seed);
+        auto r = a.run((size_t)spb);
+        *best_E = r.global_best_energy;
+        std::memcpy(avg_energy, r.average_energy_trace.data(), sizeof(double) * steps);
+        std::memcpy(avg_mag, r.average_magnetization_trace.data(), sizeof(double) * steps);
     });
 }
 

@@ -21,8 +21,13 @@ from .annealers import (  # noqa: F401
     SQAResult,
     SQAParallelTemperingResult,
     SQAChiResult,
+    ReplicaResult,
+    MultiAnnealResult,
+    ParallelTemperingResult,
     RunStats,
     Annealer,
+    ReplicaAnnealer,
+    ParallelTemperingAnnealer,
     SQAAnnealer,
     SQAParallelTemperingAnnealer,
     SQAChiAnnealer,

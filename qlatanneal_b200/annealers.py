@@ -90,6 +90,36 @@ class SQAChiResult:
     driver_A0: float
 
 
+@dataclass
+class ReplicaResult:
+    """``qanneal.ReplicaResult`` (replica_annealer.hpp:15-20)."""
+    best_state: State
+    best_energy: float
+    energy_trace: List[float]
+    magnetization_trace: List[float]
+
+
+@dataclass
+class MultiAnnealResult:
+    """``qanneal.MultiAnnealResult`` (replica_annealer.hpp:22-28)."""
+    replicas: List[ReplicaResult]
+    global_best_state: State
+    global_best_energy: float
+    average_energy_trace: List[float]
+    average_magnetization_trace: List[float]
+
+
+@dataclass
+class ParallelTemperingResult:
+    """``qanneal.ParallelTemperingResult`` (parallel_tempering.hpp:13-20)."""
+    final_states: List[State]
+    final_energies: List[float]
+    best_state: State
+    best_energy: float
+    average_energy_trace: List[float]
+    swap_acceptance_trace: List[float]
+
+
 def _lazy_list(name: str) -> property:
     """A result field that may be given as a numpy row and becomes a Python
     list (the reference's std::vector -> list) on first access: building
@@ -111,6 +141,9 @@ def _lazy_list(name: str) -> property:
 
 
 for _cls, _names in ((AnnealResult, ("energy_trace",)), (SQAResult, ("energy_trace",)),
+                     (ReplicaResult, ("energy_trace", "magnetization_trace")),
+                     (MultiAnnealResult, ("average_energy_trace", "average_magnetization_trace")),
+                     (ParallelTemperingResult, ("average_energy_trace", "swap_acceptance_trace")),
                      (SQAParallelTemperingResult, ("average_energy_trace", "swap_acceptance_trace")),
                      (SQAChiResult, ("energy_trace", "beta_schedule", "gamma_schedule", "s_schedule", "scan_s",
                                      "scan_gamma", "scan_chi_B"))):
@@ -196,6 +229,105 @@ class Annealer(_Seeded):
         _lib.check(eng.L.qa_sa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         return [AnnealResult(State(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
+
+
+class ReplicaAnnealer(_Seeded):
+    """``qanneal.ReplicaAnnealer(hamiltonian, schedule, replicas, backend)``
+    (replica_annealer.cpp:46-142): independent SA replicas in one launch
+    (replica r is the SA read keyed seed + r), with the magnetisation traces
+    and the global best the reference reports."""
+
+    def __init__(self, hamiltonian, schedule: AnnealSchedule, replicas: int, backend: str = "cuda",
+                 device: Optional[int] = None):
+        super().__init__()
+        _check_backend(backend)
+        if hamiltonian is None:
+            raise ValueError("ReplicaAnnealer requires a backend.")
+        if len(schedule.betas) == 0:
+            raise ValueError("Schedule must contain at least one beta.")
+        if replicas <= 0:
+            raise ValueError("replicas must be > 0.")
+        self.hamiltonian = hamiltonian
+        self.schedule = schedule
+        self.replicas = int(replicas)
+        self.device = device
+        self.last_stats: Optional[RunStats] = None
+
+    def run(self, sweeps_per_beta: int, seed: Optional[int] = None) -> MultiAnnealResult:
+        if sweeps_per_beta <= 0:
+            raise ValueError("sweeps_per_beta must be > 0.")
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        betas = np.ascontiguousarray(self.schedule.betas, dtype=np.float64)
+        R, S, n = self.replicas, len(betas), self.hamiltonian.size()
+        seed = self._next_seed(R) if seed is None else int(seed)
+        prm = _lib.qa_sa_params(betas.ctypes.data, S, int(sweeps_per_beta), R, seed)
+        spins = np.zeros((R, n), np.int8)
+        best = np.zeros(R)
+        trace = np.zeros((R, S))
+        mag = np.zeros((R, S))
+        bstep = np.zeros(R, np.int32)
+        o = _lib.qa_replica_out(spins.ctypes.data, best.ctypes.data, trace.ctypes.data, mag.ctypes.data,
+                                bstep.ctypes.data)
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_replica_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        reps = [ReplicaResult(State(spins[r]), float(best[r]), trace[r], mag[r]) for r in range(R)]
+        # replica_annealer.cpp:75-81, 112-117: the lowest energy, first reached (earliest step, then replica)
+        g = min(range(R), key=lambda r: (best[r], int(bstep[r]), r))
+        return MultiAnnealResult(reps, State(spins[g]), float(best[g]), trace.mean(axis=0), mag.mean(axis=0))
+
+
+class ParallelTemperingAnnealer(_Seeded):
+    """``qanneal.ParallelTemperingAnnealer(hamiltonian, betas, backend)``
+    (parallel_tempering.cpp:36-122): one replica per beta, Metropolis sweeps
+    and neighbour swaps, ``run_reads`` batching independent ladders."""
+
+    def __init__(self, hamiltonian, betas: Sequence[float], backend: str = "cuda", device: Optional[int] = None):
+        super().__init__()
+        _check_backend(backend)
+        if hamiltonian is None:
+            raise ValueError("ParallelTemperingAnnealer requires a backend.")
+        if len(betas) < 2:
+            raise ValueError("Parallel tempering requires at least two betas.")
+        self.hamiltonian = hamiltonian
+        self.betas = [float(b) for b in betas]
+        self.device = device
+        self.last_stats: Optional[RunStats] = None
+
+    def run(self, sweeps_per_step: int, steps: int, swap_interval: int = 1) -> ParallelTemperingResult:
+        return self.run_reads(sweeps_per_step, steps, swap_interval, reads=1)[0]
+
+    def run_reads(self, sweeps_per_step: int, steps: int, swap_interval: int = 1, reads: int = 1,
+                  seed: Optional[int] = None) -> List[ParallelTemperingResult]:
+        if sweeps_per_step <= 0:
+            raise ValueError("sweeps_per_step must be > 0.")
+        if steps <= 0:
+            raise ValueError("steps must be > 0.")
+        if swap_interval <= 0:
+            raise ValueError("swap_interval must be > 0.")
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        betas = np.ascontiguousarray(self.betas, dtype=np.float64)
+        R, n = len(betas), self.hamiltonian.size()
+        seed = self._next_seed(reads) if seed is None else int(seed)
+        prm = _lib.qa_pt_params(betas.ctypes.data, R, int(sweeps_per_step), int(steps), int(swap_interval),
+                                int(reads), seed)
+        best = np.zeros((reads, n), np.int8)
+        bestE = np.zeros(reads)
+        fin = np.zeros((reads, R, n), np.int8)
+        finE = np.zeros((reads, R))
+        avg = np.zeros((reads, steps))
+        swp = np.zeros((reads, steps))
+        o = _lib.qa_sqapt_out(best.ctypes.data, bestE.ctypes.data, fin.ctypes.data, finE.ctypes.data,
+                              avg.ctypes.data, swp.ctypes.data)
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_pt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        return [ParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
+                                        float(bestE[r]), avg[r], swp[r]) for r in range(reads)]
 
 
 class SQAAnnealer(_Seeded):

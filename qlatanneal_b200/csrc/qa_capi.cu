@@ -883,8 +883,10 @@ int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int6
 }
 
 // ---------------------------------------------------------------------- SA
-int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *prm,
-              qa_run_out *outs, qa_stats *stats) {
+// SA reads (qa_sa_run) and SA replicas (qa_replica_run, which adds the
+// magnetisation trace and the step of each replica's best).
+static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *prm,
+                   qa_run_out *outs, qa_stats *stats, double *const *mag_out, int32_t *const *bstep_out) {
     QA_TRY(begin(ctx));
     if (!prm) return fail(QA_ERR_ARG, "null params");
     if (prm->steps <= 0 || !prm->betas) return fail(QA_ERR_ARG, "Schedule must contain at least one beta.");
@@ -919,6 +921,14 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
     QA_TRY(ws_get(ctx, W_EXACT, sizeof(double) * nr, &v));
     double *d_exact = static_cast<double *>(v);
     QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+    double *d_mag = nullptr;
+    int *d_bstep = nullptr;
+    if (mag_out) {
+        QA_TRY(ws_get(ctx, W_MAG, sizeof(double) * (size_t)nr * prm->steps, &v));
+        d_mag = static_cast<double *>(v);
+        QA_TRY(ws_get(ctx, W_BESTSTEP, sizeof(int) * nr, &v));
+        d_bstep = static_cast<int *>(v);
+    }
 
     // dense +-1 couplings: bits and int32 fields in shared memory (fields built in-kernel)
     bool pm1 = kind == K_DENSE && sa_pm1_smem_bytes(n_max) <= (size_t)ctx->smem_optin && !std::getenv("QA_DISABLE_PM1");
@@ -933,6 +943,7 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
     sp.probs = d_probs; sp.rings = d_rings; sp.spins = d_spins; sp.fields = d_fields; sp.B = d_A;
     sp.steps = prm->steps; sp.spb = prm->sweeps_per_beta; sp.smem_fields = smem_fields;
     sp.trace = d_trace; sp.best_E = d_best; sp.best_bits = d_bits; sp.nw_max = L.nw_max; sp.counters = d_cnt;
+    sp.mag_trace = d_mag; sp.best_step = d_bstep;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     int rc = QA_OK;
     if (pm1) {
@@ -962,6 +973,12 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
     QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<double> mag(mag_out ? (size_t)nr * prm->steps : 0);
+    std::vector<int> bst(mag_out ? nr : 0);
+    if (mag_out) {
+        QA_CK(cudaMemcpyAsync(mag.data(), d_mag, sizeof(double) * mag.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaMemcpyAsync(bst.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    }
     QA_CK(cudaStreamSynchronize(ctx->stream));
     for (int i = 0; i < nr; ++i) {
         const RingDev &R = L.rings[i];
@@ -972,6 +989,10 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
         if (o.energy_trace)
             std::memcpy(o.energy_trace + (size_t)r * prm->steps, trace.data() + (size_t)i * prm->steps,
                         sizeof(double) * prm->steps);
+        if (mag_out && mag_out[p])
+            std::memcpy(mag_out[p] + (size_t)r * prm->steps, mag.data() + (size_t)i * prm->steps,
+                        sizeof(double) * prm->steps);
+        if (bstep_out && bstep_out[p]) bstep_out[p][r] = bst[i];
     }
     if (stats) {
         float a = 0, b = 0;
@@ -990,6 +1011,26 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
                                      sizeof(uint32_t) * bits.size() + sizeof(cnt));
     }
     return QA_OK;
+}
+
+int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *prm,
+              qa_run_out *outs, qa_stats *stats) {
+    return sa_impl(ctx, problems, n_problems, prm, outs, stats, nullptr, nullptr);
+}
+
+int qa_replica_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *prm,
+                   qa_replica_out *outs, qa_stats *stats) {
+    if (!outs || n_problems <= 0) return fail(QA_ERR_ARG, "null outputs or empty batch");
+    if (prm && prm->reads <= 0) return fail(QA_ERR_ARG, "replicas must be > 0.");
+    std::vector<qa_run_out> ro(n_problems);
+    std::vector<double *> mag(n_problems);
+    std::vector<int32_t *> bst(n_problems);
+    for (int p = 0; p < n_problems; ++p) {
+        ro[p] = qa_run_out{outs[p].best_spins, outs[p].best_energy, outs[p].energy_trace};
+        mag[p] = outs[p].magnetization_trace;
+        bst[p] = outs[p].best_step;
+    }
+    return sa_impl(ctx, problems, n_problems, prm, ro.data(), stats, mag.data(), bst.data());
 }
 
 // ---------------------------------------------------------------------- SQA
@@ -1147,8 +1188,11 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
 }
 
 // ---------------------------------------------------------------------- SQA-PT
-int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqapt_params *prm,
-                 qa_sqapt_out *outs, qa_stats *stats) {
+// SQA-PT (qa_sqapt_run) and, with `classical`, the classical parallel
+// tempering of qa_pt_run: one slice, B = 2 beta, no Trotter term (T4 = 0,
+// J_perp = 0 in the swap action).
+static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqapt_params *prm,
+                      qa_sqapt_out *outs, qa_stats *stats, bool classical) {
     QA_TRY(begin(ctx));
     if (!prm) return fail(QA_ERR_ARG, "null params");
     if (prm->rungs < 2 || !prm->betas || !prm->gammas)
@@ -1185,6 +1229,10 @@ int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
         bpjp[r] = prm->betas[r] / (double)P;
         bpjp[Rn + r] = trotter_coupling(prm->betas[r], prm->gammas[r], P);
         JP[r] = (float)(1.0 - std::exp(-2.0 * bpjp[Rn + r]));  // sqa_parallel_tempering.cpp:201
+        if (classical) {
+            T4[r] = 0.0f;
+            bpjp[Rn + r] = 0.0;
+        }
     }
     float *d_B, *d_T4;
     double *d_bpjp, *d_sum, *d_min, *d_best, *d_exact, *d_avg, *d_swp;
@@ -1591,6 +1639,35 @@ int qa_chi_pilot(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
         stats->d2h_bytes = d2h;
     }
     return QA_OK;
+}
+
+int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqapt_params *prm,
+                 qa_sqapt_out *outs, qa_stats *stats) {
+    return sqapt_impl(ctx, problems, n_problems, prm, outs, stats, false);
+}
+
+int qa_pt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_pt_params *prm,
+              qa_sqapt_out *outs, qa_stats *stats) {
+    if (!prm) return fail(QA_ERR_ARG, "null params");
+    // parallel_tempering.cpp:15-17, 39-47
+    if (prm->rungs < 2 || !prm->betas) return fail(QA_ERR_ARG, "Parallel tempering requires at least two betas.");
+    if (prm->sweeps_per_step <= 0) return fail(QA_ERR_ARG, "sweeps_per_step must be > 0.");
+    if (prm->steps <= 0) return fail(QA_ERR_ARG, "steps must be > 0.");
+    if (prm->swap_interval <= 0) return fail(QA_ERR_ARG, "swap_interval must be > 0.");
+    qa_sqapt_params q{};
+    q.betas = prm->betas;
+    q.gammas = prm->betas;  // unused: no transverse field
+    q.rungs = prm->rungs;
+    q.trotter_slices = 1;
+    q.sweeps_per_step = prm->sweeps_per_step;
+    q.worldline_sweeps = 0;
+    q.steps = prm->steps;
+    q.swap_interval = prm->swap_interval;
+    q.cluster_sweeps = 0;
+    q.continuous_time_slices = 0;
+    q.reads = prm->reads;
+    q.seed = prm->seed;
+    return sqapt_impl(ctx, problems, n_problems, &q, outs, stats, true);
 }
 
 // ---------------------------------------------------------------------- SQA-Chi

@@ -170,7 +170,19 @@ struct SAParams {
     uint32_t *best_bits;    // [ring][nw_max]
     int nw_max;
     unsigned long long *counters;
+    double *mag_trace;      // [ring][steps] magnetisation after each step, or null
+    int *best_step;         // [ring] step of the last best improvement (-1: start), or null
 };
+
+// Magnetisation sum(s) / n of the current state (metrics.hpp:11-20), exact.
+__device__ __forceinline__ void sa_record_mag(const SAParams &p, const uint32_t *S, int n, int nw, int step,
+                                              int lane) {
+    int up = 0;
+    for (int q = lane; q < nw; q += 32) up += __popc(S[q]);
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) up += __shfl_xor_sync(FULL, up, off);
+    if (lane == 0) p.mag_trace[(long long)blockIdx.x * p.steps + step] = (double)(2 * up - n) / (double)n;
+}
 
 // annealer.cpp:50-67: spins in fixed order, running energy, best copied on
 // every new minimum.  One warp per read.
@@ -192,6 +204,7 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
     uint32_t *bb = p.best_bits + (long long)blockIdx.x * p.nw_max;
     double E = cell_energy<KIND>(Pd, S, g, h, lane);
     double best = E;
+    int bstep = -1;
     for (int q = lane; q < nw; q += 32) bb[q] = S[q];
     unsigned long long att = 0, acc = 0;
     for (int step = 0; step < p.steps; ++step) {
@@ -227,6 +240,7 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
                     E = __dadd_rn(E, __dmul_rn(-2.0, xj));
                     if (E < best) {
                         best = E;
+                        bstep = step;
                         for (int w = lane; w < nw; w += 32) bb[w] = S[w];
                     }
                     pending = j == 31 ? 0u : (FULL << (j + 1));
@@ -234,12 +248,14 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
             }
         }
         if (lane == 0) p.trace[(long long)blockIdx.x * p.steps + step] = E;
+        if (p.mag_trace) sa_record_mag(p, S, n, nw, step, lane);
     }
     for (int q = lane; q < nw; q += 32) p.spins[R.spin_off + q] = S[q];
     if (p.smem_fields)
         for (int i = lane; i < n; i += 32) p.fields[R.field_off + i] = g[i];
     if (lane == 0) {
         p.best_E[blockIdx.x] = best;
+        if (p.best_step) p.best_step[blockIdx.x] = bstep;
         atomicAdd(p.counters + 0, att);
         atomicAdd(p.counters + 1, acc);
     }

@@ -461,6 +461,7 @@ __global__ void __launch_bounds__(32) sa_pm1_kernel(SAParams p) {
     double E = __dadd_rn(Pd.c, __dadd_rn(warp_sum_d(ph), __dmul_rn(0.5, (double)warp_sum_i(pg))));
     uint32_t *bb = p.best_bits + (long long)blockIdx.x * p.nw_max;
     double best = E;
+    int bstep = -1;
     for (int q = lane; q < nw; q += 32) bb[q] = S[q];
     unsigned long long att = 0, acc = 0;
     for (int step = 0; step < p.steps; ++step) {
@@ -505,6 +506,7 @@ __global__ void __launch_bounds__(32) sa_pm1_kernel(SAParams p) {
                     E = __dadd_rn(E, __dmul_rn(-2.0, xj));
                     if (E < best) {
                         best = E;
+                        bstep = step;
                         for (int w = lane; w < nw; w += 32) bb[w] = S[w];
                     }
                     pending = j == 31 ? 0u : (FULL << (j + 1));
@@ -512,10 +514,12 @@ __global__ void __launch_bounds__(32) sa_pm1_kernel(SAParams p) {
             }
         }
         if (lane == 0) p.trace[(long long)blockIdx.x * p.steps + step] = E;
+        if (p.mag_trace) sa_record_mag(p, S, n, nw, step, lane);
     }
     for (int q = lane; q < nw; q += 32) p.spins[R.spin_off + q] = S[q];
     if (lane == 0) {
         p.best_E[blockIdx.x] = best;
+        if (p.best_step) p.best_step[blockIdx.x] = bstep;
         atomicAdd(p.counters + 0, att);
         atomicAdd(p.counters + 1, acc);
     }

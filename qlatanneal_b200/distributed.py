@@ -155,3 +155,40 @@ def _sample_len(local: Any, group=None) -> int:
     t = torch.tensor([n], dtype=torch.int64, device=_device_for(group))
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return int(t.item())
+
+
+@dataclass
+class MPIReplicaSummary:
+    """``qanneal.mpi.MPIReplicaSummary`` (mpi_replica.hpp:13-20)."""
+    rank: int
+    size: int
+    local_best_energy: float
+    local_best_state: np.ndarray
+    global_best_energy: float
+    global_best_state: np.ndarray
+
+
+def run_replica_anneal(hamiltonian: Any, schedule: Any, sweeps_per_beta: int, replicas_per_rank: int, seed: int,
+                       group=None, runner: Optional[Callable[..., Any]] = None) -> MPIReplicaSummary:
+    """``mpi::run_replica_anneal`` (mpi_replica.cpp:8-52) over
+    torch.distributed: every rank runs a ReplicaAnnealer of
+    ``replicas_per_rank`` replicas, then the global best is the MINLOC of the
+    ranks' bests, broadcast from its rank.  Rank k's replicas use the read keys
+    seed + k * replicas_per_rank + r, so no two replicas of the job share a
+    random stream.  ``runner(hamiltonian, schedule, sweeps_per_beta,
+    replicas, seed)`` defaults to the GPU ReplicaAnnealer and must return an
+    object with ``global_best_energy`` and ``global_best_state``."""
+    import torch.distributed as dist
+    if replicas_per_rank <= 0:
+        raise ValueError("replicas must be > 0.")
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    if runner is None:
+        def runner(h, sch, spb, reps, s):
+            from .annealers import ReplicaAnnealer
+            return ReplicaAnnealer(h, sch, reps).run(spb, seed=s)
+    res = runner(hamiltonian, schedule, int(sweeps_per_beta), int(replicas_per_rank),
+                 int(seed) + rank * int(replicas_per_rank))
+    state = res.global_best_state
+    local = np.asarray(state.as_array() if hasattr(state, "as_array") else state, np.int8)
+    e, s, _ = minloc_best(float(res.global_best_energy), local, group)
+    return MPIReplicaSummary(rank, world, float(res.global_best_energy), local, e, s)

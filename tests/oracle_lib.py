@@ -74,7 +74,9 @@ class Oracle:
         L.or_fields_init.argtypes = [C.c_void_p, _i8p, _f4p]
         L.or_init_spins.argtypes = [_i8p, C.c_int, C.c_uint64, C.c_uint32, C.c_uint32]
         L.or_sa_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double),
-                                _f8p, _i64p]
+                                _f8p, _i64p, C.c_void_p, C.c_void_p]
+        L.or_pt_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p,
+                                C.POINTER(C.c_double), _f8p, _i8p, _f8p, _f8p, _i64p]
         L.or_sqa_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
                                  C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i64p, C.c_int]
         L.or_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -163,8 +165,35 @@ class Oracle:
         E = C.c_double()
         trace = np.zeros(len(betas), np.float64)
         cnt = np.zeros(4, np.int64)
-        self.L.or_sa_run(m.h, betas, len(betas), sweeps_per_beta, seed, read, best, C.byref(E), trace, cnt)
+        self.L.or_sa_run(m.h, betas, len(betas), sweeps_per_beta, seed, read, best, C.byref(E), trace, cnt, None, None)
         return best, E.value, trace, cnt
+
+    def replica_run(self, m, betas, sweeps_per_beta, seed, read=0):
+        """SA read with the magnetisation trace and the step of the last best
+        improvement: (best, best_E, trace, mag_trace, best_step)."""
+        betas = _c64(betas)
+        best = np.zeros(m.n, np.int8)
+        E = C.c_double()
+        trace = np.zeros(len(betas))
+        mag = np.zeros(len(betas))
+        bstep = C.c_int()
+        cnt = np.zeros(4, np.int64)
+        self.L.or_sa_run(m.h, betas, len(betas), sweeps_per_beta, seed, read, best, C.byref(E), trace, cnt,
+                         mag.ctypes.data, C.addressof(bstep))
+        return best, E.value, trace, mag, bstep.value
+
+    def pt_run(self, m, betas, spb, steps, swap_interval, seed, read=0):
+        """Classical PT read: (best, best_E, final_E[R], final_spins[R][n], avg_trace, swap_trace)."""
+        betas = _c64(betas)
+        R = len(betas)
+        best = np.zeros(m.n, np.int8)
+        E = C.c_double()
+        fE, fs = np.zeros(R), np.zeros(R * m.n, np.int8)
+        avg, swp = np.zeros(steps), np.zeros(steps)
+        cnt = np.zeros(4, np.int64)
+        self.L.or_pt_run(m.h, betas, R, spb, steps, swap_interval, seed, read, best, C.byref(E), fE, fs, avg, swp,
+                         cnt)
+        return best, E.value, fE, fs.reshape(R, m.n), avg, swp
 
     def sqa_run(self, m, betas, gammas, P, K, spb, wls, seed, read=0, cls=0):
         betas, gammas = _c64(betas), _c64(gammas)
@@ -242,6 +271,10 @@ class Ref:
         L.ref_sa_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p]
         L.ref_sqa_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
                                   _i8p, C.POINTER(C.c_double), _f8p, C.c_int]
+        L.ref_pt_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, _i8p,
+                                 C.POINTER(C.c_double), _f8p, _f8p, _f8p]
+        L.ref_replica_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_double),
+                                      _f8p, _f8p]
         L.ref_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                     C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p, _f8p, _f8p, C.c_int]
         L.ref_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
@@ -351,6 +384,25 @@ class RefModel:
         if rc != 0:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return dict(best=best, best_energy=E.value, scalars=sc, **arr)
+
+    def pt_run(self, betas, spb, steps, swap_interval, seed):
+        betas = _c64(betas)
+        R = len(betas)
+        best = np.zeros(self.n, np.int8)
+        E = C.c_double()
+        fE, avg, swp = np.zeros(R), np.zeros(steps), np.zeros(steps)
+        if self.ref.L.ref_pt_run(self.h, betas, R, spb, steps, swap_interval, seed, best, C.byref(E), fE, avg,
+                                 swp) != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return best, E.value, fE, avg, swp
+
+    def replica_run(self, betas, spb, R, seed):
+        betas = _c64(betas)
+        E = C.c_double()
+        avg, mag = np.zeros(len(betas)), np.zeros(len(betas))
+        if self.ref.L.ref_replica_run(self.h, betas, len(betas), spb, R, seed, C.byref(E), avg, mag) != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return E.value, avg, mag
 
     def sqapt_run(self, betas, gammas, P, spb, wls, steps, swap_interval, seed, cls=0):
         betas, gammas = _c64(betas), _c64(gammas)

@@ -65,6 +65,12 @@ def _worker(rank, world, port, out_dir, mode):
             e, s, src = minloc_best(-3.0, np.full(5, 1 if rank == 0 else -1, np.int8))
             with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
                 json.dump({"best": e, "spins": s.tolist(), "src": src}, f)
+        elif mode == "replica":
+            from qlatanneal_b200.distributed import run_replica_anneal
+            res = run_replica_anneal(None, None, 2, 3, 61, runner=_oracle_replicas)
+            with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+                json.dump({"local": res.local_best_energy, "best": res.global_best_energy,
+                           "spins": res.global_best_state.tolist(), "size": res.size}, f)
         elif mode == "fail":
             if rank == 1:
                 raise RuntimeError("rank 1 fails before the exchange")
@@ -110,6 +116,25 @@ def _oracle_runner(problem, reads, seed):
     return out
 
 
+def _oracle_replicas(h_, sched_, spb, reps, seed):
+    """ReplicaAnnealer stand-in on the CPU oracle: replica r keyed seed + r,
+    global best = lowest energy, earliest step, lowest replica."""
+    from oracle_lib import Oracle
+
+    class R:
+        pass
+
+    o = Oracle()
+    h, J = _instance()
+    m = o.dense(h, J)
+    betas = np.geomspace(0.1, 3.0, 15)
+    runs = [o.replica_run(m, betas, spb, seed, r) for r in range(reps)]
+    g = min(range(reps), key=lambda r: (runs[r][1], runs[r][4], r))
+    out = R()
+    out.global_best_energy, out.global_best_state = runs[g][1], runs[g][0]
+    return out
+
+
 def _spawn(mode, out_dir):
     import torch.multiprocessing as tmp
     ctx = tmp.spawn(_worker, args=(2, _free_port(), out_dir, mode), nprocs=2, join=False)
@@ -151,3 +176,18 @@ def test_failed_rank_ends_the_exchange_with_an_error():
         _spawn("fail", d)  # rank 1 exits with an exception
         r0 = json.load(open(os.path.join(d, "r0.json")))
     assert r0["status"].startswith("error")
+
+
+def test_replica_anneal_over_ranks():
+    """mpi::run_replica_anneal (mpi_replica.cpp:8-52): each rank's replicas,
+    then the MINLOC of the ranks' bests, on every rank; equal to one process
+    running all 6 replicas."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    with tempfile.TemporaryDirectory() as d:
+        assert _spawn("replica", d)
+        r0 = json.load(open(os.path.join(d, "r0.json")))
+        r1 = json.load(open(os.path.join(d, "r1.json")))
+    allr = _oracle_replicas(None, None, 2, 6, 61)
+    assert r0["best"] == r1["best"] == allr.global_best_energy
+    assert r0["spins"] == r1["spins"]
+    assert min(r0["local"], r1["local"]) == r0["best"] and r0["size"] == 2

@@ -205,3 +205,42 @@ def test_cluster_sqapt_restatement_matches_reference_statistics(oracle, ref):
         er.append(rm.sqapt_run(betas, gammas, P, 0, 0, steps, 2, 7000 + k, cls=2)[3][-20:].mean())
     (ma, ca), (mb, cb) = _ci95(eo), _ci95(er)
     assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
+
+
+def test_classical_pt_restatement_matches_reference_statistics(oracle, ref):
+    """Classical parallel tempering (parallel_tempering.cpp:36-122): at
+    equilibrium the replay form and qanneal's ParallelTemperingAnnealer have
+    the same average energy and swap acceptance (95% CIs, 300 reads)."""
+    h, J = sk_dense(20, 13)
+    m, rm = oracle.dense(h, J), ref.dense(h, J)
+    betas = np.geomspace(0.2, 2.0, 4)
+    steps = 60
+    eo, er, so, sr = [], [], [], []
+    for k in range(300):
+        o = oracle.pt_run(m, betas, 1, steps, 2, 100, k)
+        r = rm.pt_run(betas, 1, steps, 2, 7000 + k)
+        eo.append(o[4][-20:].mean()); er.append(r[3][-20:].mean())
+        so.append(o[5][1::2].mean()); sr.append(r[4][1::2].mean())
+    for a, b in ((eo, er), (so, sr)):
+        (ma, ca), (mb, cb) = _ci95(a), _ci95(b)
+        assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
+
+
+def test_replica_restatement_matches_reference_statistics(oracle, ref):
+    """ReplicaAnnealer (replica_annealer.cpp:46-142) is independent SA
+    replicas; its average energy and magnetisation traces match qanneal's."""
+    rng = np.random.default_rng(3)
+    h, J = sk_dense(24, 14)
+    h = rng.choice([0.5, 1.0, 0.0], size=24)
+    m, rm = oracle.dense(h, J), ref.dense(h, J)
+    betas = geometric_betas(0.1, 2.0, 10)
+    R = 8
+    eo, mo, er, mr = [], [], [], []
+    for k in range(60):
+        runs = [oracle.replica_run(m, betas, 2, 500 + 100 * k, r) for r in range(R)]
+        eo.append(np.mean([x[2][-1] for x in runs])); mo.append(np.mean([x[3][-1] for x in runs]))
+        _, avg, mag = rm.replica_run(betas, 2, R, 9000 + k)
+        er.append(avg[-1]); mr.append(mag[-1])
+    for a, b in ((eo, er), (mo, mr)):
+        (ma, ca), (mb, cb) = _ci95(a), _ci95(b)
+        assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
