@@ -149,6 +149,48 @@ typedef struct {
 QA_API int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *params,
                qa_run_out *outs, qa_stats *stats);
 
+/* ---- SQA with the calibrated chi_B schedule: SQAAnnealer::run_optimal
+ *      (sqa_annealer.cpp:499-952) ---------------------------------------------
+ * Phase 1: beta ramped from beta_ramp_start to beta over beta_ramp_fraction
+ * of the steps at J_perp = j_perp_start.  Then, when eps_tilde <= 0, a
+ * calibration pilot (calib_probes probes of calib_sweeps sweeps from the
+ * post-ramp state, which is restored afterwards) measures chi_B(J_perp) =
+ * Var(bond sum) and sets the J_perp trajectory of phase 2 (inverse of the
+ * integral of chi_B^alpha); with eps_tilde > 0, J_perp advances online by
+ * eps_tilde * chi_B^-alpha after every step.  Phase 2 runs at the cold beta.
+ * The slices' Trotter coupling is J_perp itself (no Gamma). */
+typedef struct {
+    int trotter_slices;
+    int replicas;
+    double beta;
+    double j_perp_start;
+    double j_perp_end;             /* > j_perp_start */
+    double eps_tilde;              /* <= 0: calibrate */
+    double alpha;
+    int num_steps;
+    int sweeps_per_step;
+    int worldline_sweeps;
+    int cluster_sweeps;            /* P <= 64 when > 0 */
+    int calib_probes;
+    int calib_sweeps;
+    double beta_ramp_fraction;
+    double beta_ramp_start;
+    int reads;
+    uint64_t seed;
+} qa_sqaopt_params;
+
+typedef struct {
+    int8_t *best_spins;        /* [reads][n] */
+    double *best_energy;       /* [reads] */
+    double *energy_trace;      /* [reads][num_steps] average energy over replicas and slices */
+    double *j_perp_trace;      /* [reads][num_steps] */
+    double *chi_B_trace;       /* [reads][num_steps] the chi_B that drove each step */
+    double *scalars;           /* [reads][4] calibrated_eps_tilde, j_perp_start, resolved_j_perp_end, final_j_perp */
+} qa_sqaopt_out;
+
+QA_API int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
+                          const qa_sqaopt_params *params, qa_sqaopt_out *outs, qa_stats *stats);
+
 /* ---- SQA parallel tempering: SQAParallelTemperingAnnealer::run
  *      (sqa_parallel_tempering.cpp:81-346) ----------------------------------
  * rungs (beta_r, Gamma_r) pairs, one Trotter ring per rung, swaps of

@@ -79,7 +79,8 @@ OR_EXPORT void or_philox(const uint32_t ctr_in[4], const uint32_t key_in[2], uin
 /* Domain tags (counter word 3, low byte). */
 enum {
     DOM_INIT = 1, DOM_SA = 2, DOM_SLICE = 3, DOM_WORLD = 4, DOM_SWAP = 5,
-    DOM_PILOT_INIT = 6, DOM_PILOT = 7, DOM_PROD_INIT = 8, DOM_PROD = 9, DOM_CSPIN = 10, DOM_CBOND = 11
+    DOM_PILOT_INIT = 6, DOM_PILOT = 7, DOM_PROD_INIT = 8, DOM_PROD = 9, DOM_CSPIN = 10, DOM_CBOND = 11,
+    DOM_OPTCAL = 12
 };
 
 static inline uint32_t spin_slot(int i) { return (uint32_t)(((i >> 7) << 5) | (i & 31)); }
@@ -1156,6 +1157,246 @@ OR_EXPORT int or_chi_run(const or_model *M, int P, int K, double beta, double ga
     *best_E = rbest[kb];
     memcpy(best_spins, rstate + (size_t)kb * n, (size_t)n);
     free(rbest); free(rstep); free(rstate); free(rsum);
+    ring_free(&R);
+    return 0;
+}
+
+
+/* ------------------------------------------------------------------ */
+/* SQAAnnealer::run_optimal (sqa_annealer.cpp:499-952), one read         */
+/* ------------------------------------------------------------------ */
+/* Imaginary-time bond sum B = sum_{t,i} s_t,i s_t+1,i of ring k (exact). */
+static long long bond_sum(const ring_t *R, int k) {
+    const int n = R->n, P = R->P;
+    long long b = 0;
+    for (int t = 0; t < P; ++t) {
+        const int8_t *a = R->s + ((size_t)k * P + t) * n, *c = R->s + ((size_t)k * P + (t + 1) % P) * n;
+        for (int i = 0; i < n; ++i) b += a[i] * c[i];
+    }
+    return b;
+}
+
+/* chi_B = Var(B) over the step's samples of every replica
+   (sqa_annealer.cpp:711-739): samples [K][ns], last_bond[K] the bond sum after
+   the step (for the one-sample fallback). */
+static double opt_chi_raw(const long long *samp, int K, int ns, const long long *last_bond, double nM) {
+    double bs = 0.0, b2 = 0.0;
+    long long total = 0;
+    for (int k = 0; k < K; ++k)
+        for (int j = 0; j < ns; ++j) {
+            const double b = (double)samp[(size_t)k * ns + j];
+            bs += b;
+            b2 += b * b;
+            ++total;
+        }
+    double var;
+    if (total >= 2) {
+        const double bm = bs / (double)total, b2m = b2 / (double)total;
+        var = b2m - bm * bm;
+    } else {
+        const double ba = (double)last_bond[0] / nM;
+        var = nM * (1.0 - ba * ba);
+    }
+    if (K == 1 && ns > 0) {
+        const double ba = (double)samp[ns - 1] / nM;
+        const double g = nM * (1.0 - ba * ba);
+        if (g > var) var = g;
+    }
+    return var;
+}
+
+/* One step of sweeps at (B, T4, JP) with bond samples after every slice and
+   cluster sweep; step index s drives the sweep counters. */
+static void opt_sweep(ring_t *R, int s, int spb, int cls, int wls, float B, float T4, float JP, uint32_t slice_tag,
+                      long long *samp) {
+    const int K = R->K, ns = spb + cls;
+    for (int sw = 0; sw < spb; ++sw) {
+        slice_sweep(R, (uint32_t)(s * spb + sw), slice_tag, B, T4, NULL);
+        for (int k = 0; k < K; ++k) samp[(size_t)k * ns + sw] = bond_sum(R, k);
+    }
+    for (int sw = 0; sw < cls; ++sw) {
+        for (int k = 0; k < K; ++k) {
+            cluster_sweep(R, k, (uint32_t)k, (uint32_t)(s * cls + sw), B, T4, JP);
+            samp[(size_t)k * ns + spb + sw] = bond_sum(R, k);
+        }
+    }
+    for (int sw = 0; sw < wls; ++sw)
+        for (int k = 0; k < K; ++k) worldline_sweep(R, k, (uint32_t)k, (uint32_t)(s * wls + sw), B);
+}
+
+/* Linear interpolation of the calibration profile (sqa_annealer.cpp:832-843). */
+static double opt_profile(const double *pj, const double *pc, int M, double J) {
+    if (M == 0) return -1.0;
+    if (J <= pj[0]) return pc[0];
+    if (J >= pj[M - 1]) return pc[M - 1];
+    int hi = 1;
+    while (hi < M && pj[hi] < J) ++hi;
+    const int lo = hi - 1;
+    const double t = (J - pj[lo]) / (pj[hi] - pj[lo]);
+    return pc[lo] + t * (pc[hi] - pc[lo]);
+}
+
+/* Replay form: phase-1 steps s = 0..n1-1 and phase-2 steps s = n1..num_steps-1
+   use the sweep counters of step s; calibration probe m runs as step
+   num_steps + m with slice tag OPTCAL (cs slice sweeps, max(cls, 1) cluster
+   sweeps when cls > 0).  B = 2 beta_t / P, T4 = 4 J_perp, JP = 1 - e^{-2 J_perp}.
+   scalars: calibrated eps_tilde, J_start, J_end, final J.  Returns 1 when
+   run_optimal would reject its arguments. */
+OR_EXPORT int or_sqa_opt_run(const or_model *M, int P, int K, double beta, double js, double je, double eps_tilde,
+                             double alpha, int num_steps, int spb, int wls, int cls, int probes, int csweeps,
+                             double ramp_fraction, double ramp_start, uint64_t seed, int read, int8_t *best_spins,
+                             double *best_E, double *trace, double *jtrace, double *chitrace, double *scalars) {
+    if (num_steps <= 0 || (spb == 0 && wls == 0 && cls == 0) || !(je > js)) return 1;
+    const int n = M->n;
+    const int calibrate = eps_tilde <= 0.0;
+    const double nM = (double)n * (double)P;
+    double min_chi = 1e-4 * nM;
+    ring_t R;
+    ring_alloc(&R, M, P, K, seed + (uint64_t)read);
+    ring_init(&R, DOM_INIT);
+    const int ns = spb + cls;
+    long long *samp = (long long *)malloc(sizeof(long long) * (size_t)K * (size_t)(ns > 0 ? ns : 1) * 2 + 16);
+    long long *lastb = (long long *)malloc(sizeof(long long) * (size_t)K);
+    double *rbest = (double *)malloc(sizeof(double) * (size_t)K);
+    int *rstep = (int *)malloc(sizeof(int) * (size_t)K);
+    int8_t *rstate = (int8_t *)malloc((size_t)K * n);
+    for (int k = 0; k < K; ++k) { rbest[k] = INFINITY; rstep[k] = -1; }
+    const float Bc = (float)(2.0 * (beta / (double)P));
+    int n1 = 0;
+    if (ramp_fraction > 0.0) {
+        n1 = (int)(ramp_fraction * (double)num_steps);
+        if (n1 >= num_steps) n1 = num_steps - 1;
+    }
+    const int n2 = num_steps - n1;
+
+#define OPT_RECORD(STEP, JV, CHIV)                                                                  \
+    do {                                                                                            \
+        double tot_ = 0.0;                                                                          \
+        for (int k = 0; k < K; ++k) {                                                               \
+            double sum_ = 0.0, emin_ = INFINITY;                                                    \
+            int tmin_ = 0;                                                                          \
+            for (int t = 0; t < P; ++t) {                                                           \
+                const double E_ = cell_energy(&R, k * P + t);                                       \
+                sum_ += E_;                                                                         \
+                if (E_ < emin_) { emin_ = E_; tmin_ = t; }                                          \
+            }                                                                                       \
+            tot_ += sum_;                                                                           \
+            if (emin_ < rbest[k]) {                                                                 \
+                rbest[k] = emin_; rstep[k] = (STEP);                                                \
+                memcpy(rstate + (size_t)k * n, R.s + ((size_t)k * P + tmin_) * n, (size_t)n);      \
+            }                                                                                       \
+        }                                                                                           \
+        trace[(STEP)] = tot_ / (double)(K * P);                                                     \
+        jtrace[(STEP)] = (JV);                                                                      \
+        chitrace[(STEP)] = (CHIV);                                                                  \
+    } while (0)
+
+    /* phase 1: beta ramp at J_start */
+    for (int s = 0; s < n1; ++s) {
+        const double frac = n1 > 1 ? (double)s / (double)(n1 - 1) : 1.0;
+        const double bt = ramp_start + (beta - ramp_start) * frac;
+        opt_sweep(&R, s, spb, cls, wls, (float)(2.0 * (bt / (double)P)), (float)(4.0 * js),
+                  (float)(1.0 - exp(-2.0 * js)), DOM_SLICE, samp);
+        for (int k = 0; k < K; ++k) lastb[k] = bond_sum(&R, k);
+        double chi = opt_chi_raw(samp, K, ns, lastb, nM);
+        if (chi < 0.0) chi = 0.0;
+        OPT_RECORD(s, js, chi);
+    }
+    /* calibration pre-pass */
+    const int Mp = probes > 2 ? probes : 2;
+    const int cs = csweeps > 1 ? csweeps : 1;
+    const int pc = cls > 0 ? cls : 0;
+    double *pj = (double *)malloc(sizeof(double) * (size_t)Mp), *pcv = (double *)malloc(sizeof(double) * (size_t)Mp);
+    int have_profile = 0;
+    const double dJ = je - js;
+    if (calibrate) {
+        int8_t *ss = (int8_t *)malloc((size_t)K * P * n);
+        float *sg = (float *)malloc(sizeof(float) * (size_t)K * P * n);
+        memcpy(ss, R.s, (size_t)K * P * n);
+        memcpy(sg, R.g, sizeof(float) * (size_t)K * P * n);
+        const int nsc = cs + pc;
+        long long *csamp = (long long *)malloc(sizeof(long long) * (size_t)K * (size_t)nsc + 16);
+        const double dJp = dJ / (double)Mp;
+        double integral = 0.0, maxc = 0.0;
+        for (int m = 0; m < Mp; ++m) {
+            const double Jm = js + ((double)m + 0.5) * dJp;
+            opt_sweep(&R, num_steps + m, cs, pc, 0, Bc, (float)(4.0 * Jm), (float)(1.0 - exp(-2.0 * Jm)), DOM_OPTCAL,
+                      csamp);
+            for (int k = 0; k < K; ++k) lastb[k] = bond_sum(&R, k);
+            double chi = opt_chi_raw(csamp, K, nsc, lastb, nM);
+            if (!(chi > 0.0)) chi = 0.0;
+            pj[m] = Jm;
+            pcv[m] = chi;
+            integral += pow(chi > 1e-12 ? chi : 1e-12, alpha) * dJp;
+            if (chi > maxc) maxc = chi;
+        }
+        memcpy(R.s, ss, (size_t)K * P * n);
+        memcpy(R.g, sg, sizeof(float) * (size_t)K * P * n);
+        free(ss); free(sg); free(csamp);
+        eps_tilde = integral / (double)n2;
+        if (!(eps_tilde > 0.0) || !isfinite(eps_tilde)) {
+            eps_tilde = (dJ > 0.0 ? dJ : 0.0) / (double)num_steps;
+            if (!(eps_tilde > 0.0)) eps_tilde = 1e-9;
+        }
+        min_chi = 1e-4 * maxc > 1e-12 ? 1e-4 * maxc : 1e-12;
+        have_profile = 1;
+    }
+    scalars[0] = eps_tilde;
+    scalars[1] = js;
+    scalars[2] = je;
+    /* the J trajectory: inverse of G(J) = int chi(J')^alpha dJ' on a 4096 grid */
+    double *jt = NULL;
+    if (calibrate && have_profile && je > js) {
+        const int GRID = 4096;
+        const double h = (je - js) / (double)GRID;
+        double *G = (double *)calloc((size_t)GRID + 1, sizeof(double));
+        double c0 = opt_profile(pj, pcv, Mp, js);
+        double prev = pow(c0 > min_chi ? c0 : min_chi, alpha);
+        for (int k = 1; k <= GRID; ++k) {
+            const double Jk = js + (double)k * h;
+            const double ck = opt_profile(pj, pcv, Mp, Jk);
+            const double cur = pow(ck > min_chi ? ck : min_chi, alpha);
+            G[k] = G[k - 1] + 0.5 * (prev + cur) * h;
+            prev = cur;
+        }
+        const double Gt = G[GRID];
+        jt = (double *)malloc(sizeof(double) * (size_t)n2);
+        int k = 0;
+        const double den = n2 > 1 ? (double)(n2 - 1) : 1.0;
+        for (int t = 0; t < n2; ++t) {
+            const double target = Gt > 0.0 ? ((double)t / den) * Gt : 0.0;
+            while (k < GRID && G[k + 1] < target) ++k;
+            const double g0 = G[k], g1 = G[k + 1];
+            const double fr = g1 > g0 ? (target - g0) / (g1 - g0) : 0.0;
+            jt[t] = js + ((double)k + fr) * h;
+        }
+        free(G);
+    }
+    /* phase 2: fixed cold beta, J from the trajectory (or online) */
+    double J = js;
+    for (int t = 0; t < n2; ++t) {
+        const int s = n1 + t;
+        if (jt) J = jt[t];
+        opt_sweep(&R, s, spb, cls, wls, Bc, (float)(4.0 * J), (float)(1.0 - exp(-2.0 * J)), DOM_SLICE, samp);
+        for (int k = 0; k < K; ++k) lastb[k] = bond_sum(&R, k);
+        const double chi_on = opt_chi_raw(samp, K, ns, lastb, nM);
+        const double cp = have_profile ? opt_profile(pj, pcv, Mp, J) : -1.0;
+        const double raw = cp >= 0.0 ? cp : chi_on;
+        const double drive = raw > min_chi ? raw : min_chi;
+        OPT_RECORD(s, J, drive);
+        if (!jt) {
+            const double nj = J + eps_tilde * pow(drive, -alpha);
+            J = nj < je ? nj : je;
+        }
+    }
+#undef OPT_RECORD
+    scalars[3] = J;
+    int kb = 0;
+    for (int k = 1; k < K; ++k)
+        if (rbest[k] < rbest[kb] || (rbest[k] == rbest[kb] && rstep[k] < rstep[kb])) kb = k;
+    *best_E = rbest[kb];
+    memcpy(best_spins, rstate + (size_t)kb * n, (size_t)n);
+    free(jt); free(pj); free(pcv); free(samp); free(lastb); free(rbest); free(rstep); free(rstate);
     ring_free(&R);
     return 0;
 }

@@ -199,6 +199,29 @@ int ref_replica_run(void *p, const double *betas, int steps, int spb, int R, uin
     });
 }
 
+// SQAAnnealer::run_optimal, one read (sqa_annealer.cpp:499-952).
+int ref_sqa_opt_run(void *p, int P, int K, double beta, double js, double je, double eps_tilde, double alpha,
+                    int num_steps, int spb, int wls, int cls, int probes, int csweeps, double ramp_fraction,
+                    double ramp_start, uint64_t seed, double *best_E, double *trace, double *jtrace, double *chitrace,
+                    double *scalars) {
+    return guarded([&] {
+        auto *m = static_cast<RefModel *>(p);
+        SQAAnnealer a(make_backend(BackendKind::CPU, m->ham), SQASchedule::from_vectors({1.0}, {1.0}), (size_t)P,
+                      (size_t)K);
+        a.set_seed(seed);
+        SQAResult r = a.run_optimal(beta, js, je, eps_tilde, alpha, (size_t)num_steps, (size_t)spb, (size_t)wls,
+                                    (size_t)cls, (size_t)probes, (size_t)csweeps, "", ramp_fraction, ramp_start);
+        *best_E = r.best_energy;
+        std::memcpy(trace, r.energy_trace.data(), sizeof(double) * num_steps);
+        std::memcpy(jtrace, r.j_perp_trace.data(), sizeof(double) * num_steps);
+        std::memcpy(chitrace, r.chi_B_trace.data(), sizeof(double) * num_steps);
+        scalars[0] = r.calibrated_eps_tilde;
+        scalars[1] = r.j_perp_start;
+        scalars[2] = r.resolved_j_perp_end;
+        scalars[3] = r.final_j_perp;
+    });
+}
+
 // SQAParallelTemperingAnnealer::run, one read (sqa_parallel_tempering.cpp:81-346).
 int ref_sqapt_run(void *p, const double *betas, const double *gammas, int R, int P, int spb, int wls, int steps,
                   int swap_interval, uint64_t seed, int8_t *best_spins, double *best_E, double *final_E,

@@ -380,6 +380,72 @@ class SQAAnnealer(_Seeded):
         return [SQAResult(State(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
 
 
+def _write_opt_debug_csv(path: str, res: "SQAResult", beta_ramp_steps: int, alpha: float) -> None:
+    """The per-step rows of run_optimal's diagnostic CSV (sqa_annealer.cpp:777-787,
+    914-918): phase, step, J_perp, chi_B, the step delta_J = eps chi^-alpha."""
+    try:
+        f = open(path, "w")
+    except OSError:
+        import sys
+        print(f"[qlatanneal_b200 SQA run_optimal] WARNING: could not open debug CSV '{path}'.", file=sys.stderr)
+        return
+    with f:
+        f.write("phase,step_index,j_perp,chi_B,delta_j,eps_tilde,alpha,floor_hit,chi_B_online\n")
+        eps = res.calibrated_eps_tilde
+        for k, (j, chi) in enumerate(zip(res.j_perp_trace, res.chi_B_trace)):
+            if k < beta_ramp_steps:
+                f.write(f"beta_ramp,{k},{j:.8e},{chi:.8e},0,0,{alpha:.8e},0,\n")
+            else:
+                dj = eps * chi ** (-alpha) if chi > 0 else 0.0
+                f.write(f"run,{k},{j:.8e},{chi:.8e},{dj:.8e},{eps:.8e},{alpha:.8e},,\n")
+
+
+def _sqa_run_optimal_reads(self, beta: float, j_perp_start: float, j_perp_end: float, eps_tilde: float,
+                           alpha: float = 15.0 / 14.0, num_steps: int = 100, sweeps_per_step: int = 20,
+                           worldline_sweeps: int = 0, cluster_sweeps: int = 0, calib_probes: int = 12,
+                           calib_sweeps: int = 10, beta_ramp_fraction: float = 0.3, beta_ramp_start: float = 0.1,
+                           reads: int = 1, seed: Optional[int] = None) -> List["SQAResult"]:
+    """Batched ``run_optimal``: read r keyed seed + r, all reads in one call."""
+    eng = _lib.Engine.get(self.device)
+    prob = self.hamiltonian._device_problem(eng)
+    seed = self._next_seed(reads) if seed is None else int(seed)
+    prm = _lib.qa_sqaopt_params(self.trotter_slices, self.replicas, float(beta), float(j_perp_start),
+                                float(j_perp_end), float(eps_tilde), float(alpha), int(num_steps),
+                                int(sweeps_per_step), int(worldline_sweeps), int(cluster_sweeps), int(calib_probes),
+                                int(calib_sweeps), float(beta_ramp_fraction), float(beta_ramp_start), int(reads),
+                                seed)
+    n, S = self.hamiltonian.size(), max(int(num_steps), 1)
+    spins = np.zeros((reads, n), np.int8)
+    best = np.zeros(reads)
+    tr, jt, ct = np.zeros((reads, S)), np.zeros((reads, S)), np.zeros((reads, S))
+    sc = np.zeros((reads, 4))
+    o = _lib.qa_sqaopt_out(spins.ctypes.data, best.ctypes.data, tr.ctypes.data, jt.ctypes.data, ct.ctypes.data,
+                           sc.ctypes.data)
+    st = _lib.qa_stats()
+    probs = (C.c_void_p * 1)(prob)
+    _lib.check(eng.L.qa_sqa_opt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
+    self.last_stats = RunStats.from_c(st)
+    return [SQAResult(State(spins[r]), float(best[r]), tr[r], jt[r].tolist(), ct[r].tolist(), float(sc[r, 0]),
+                      float(sc[r, 1]), float(sc[r, 2]), float(sc[r, 3])) for r in range(reads)]
+
+
+def _sqa_run_optimal(self, beta: float, j_perp_start: float, j_perp_end: float, eps_tilde: float,
+                     alpha: float = 15.0 / 14.0, num_steps: int = 100, sweeps_per_step: int = 20,
+                     worldline_sweeps: int = 0, cluster_sweeps: int = 0, calib_probes: int = 12,
+                     calib_sweeps: int = 10, debug_csv_path: str = "", beta_ramp_fraction: float = 0.3,
+                     beta_ramp_start: float = 0.1) -> "SQAResult":
+    """``SQAAnnealer.run_optimal`` (sqa_annealer.cpp:499-952), one read."""
+    res = self.run_optimal_reads(beta, j_perp_start, j_perp_end, eps_tilde, alpha, num_steps, sweeps_per_step,
+                                 worldline_sweeps, cluster_sweeps, calib_probes, calib_sweeps, beta_ramp_fraction,
+                                 beta_ramp_start, reads=1)[0]
+    if debug_csv_path:
+        n1 = 0
+        if beta_ramp_fraction > 0.0:
+            n1 = min(int(beta_ramp_fraction * num_steps), num_steps - 1)
+        _write_opt_debug_csv(debug_csv_path, res, n1, alpha)
+    return res
+
+
 class SQAParallelTemperingAnnealer(_Seeded):
     """``qanneal.SQAParallelTemperingAnnealer(hamiltonian, betas, gammas, trotter_slices, backend)``
     (sqa_parallel_tempering.cpp:81-346): one Trotter ring per (beta, Gamma) rung,
@@ -533,3 +599,7 @@ def _write_chi_debug_csv(path: str, res: SQAChiResult, beta: float, slices: int,
         for step, (s, g, b) in enumerate(zip(res.s_schedule, res.gamma_schedule, res.beta_schedule)):
             phase = "beta_ramp" if step < n1 else "run"
             f.write(f"{phase},{step},{s:.8e},{g:.8e},{_trotter_coupling(b, g, slices):.8e},,{b:.8e}\n")
+
+
+SQAAnnealer.run_optimal = _sqa_run_optimal
+SQAAnnealer.run_optimal_reads = _sqa_run_optimal_reads

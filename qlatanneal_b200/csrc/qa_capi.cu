@@ -141,7 +141,8 @@ struct qa_problem {
 namespace {
 
 enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
-              W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP, W_JP };
+              W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP, W_JP,
+              W_BSAMP, W_SSAVE, W_FSAVE, W_CBESTE, W_CBSTEP, W_CBITS, W_CBOND };
 
 int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
     DevBuf &b = ctx->ws[slot];
@@ -1183,6 +1184,389 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
                                      (sizeof(double) + sizeof(int)) * nr + sizeof(int) * nr);
         stats->d2h_bytes = (int64_t)(sizeof(double) * sums.size() + (2 * sizeof(double) + sizeof(int)) * nr +
                                      sizeof(uint32_t) * bits.size() + sizeof(cnt));
+    }
+    return QA_OK;
+}
+
+// ---------------------------------------------------------------------- SQA run_optimal
+namespace {
+
+// chi_B = Var(B) over one step's bond-sum samples of a read's K rings
+// (sqa_annealer.cpp:711-739); last_bond: the first ring's bond sum after the
+// step (the one-sample fallback).
+double opt_chi_raw(const long long *samp, int K, int ns, size_t ring_stride, long long last_bond, double nM) {
+    double bs = 0.0, b2 = 0.0;
+    long long total = 0;
+    for (int k = 0; k < K; ++k)
+        for (int j = 0; j < ns; ++j) {
+            const double b = (double)samp[(size_t)k * ring_stride + j];
+            bs += b;
+            b2 += b * b;
+            ++total;
+        }
+    double var;
+    if (total >= 2) {
+        const double bm = bs / (double)total, b2m = b2 / (double)total;
+        var = b2m - bm * bm;
+    } else {
+        const double ba = (double)last_bond / nM;
+        var = nM * (1.0 - ba * ba);
+    }
+    if (K == 1 && ns > 0) {
+        const double ba = (double)samp[ns - 1] / nM;
+        var = std::max(var, nM * (1.0 - ba * ba));
+    }
+    return var;
+}
+
+double opt_profile(const std::vector<double> &pj, const std::vector<double> &pc, double J) {
+    const size_t M = pj.size();
+    if (M == 0) return -1.0;
+    if (J <= pj.front()) return pc.front();
+    if (J >= pj.back()) return pc.back();
+    size_t hi = 1;
+    while (hi < M && pj[hi] < J) ++hi;
+    const size_t lo = hi - 1;
+    const double t = (J - pj[lo]) / (pj[hi] - pj[lo]);
+    return pc[lo] + t * (pc[hi] - pc[lo]);
+}
+
+}  // namespace
+
+int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqaopt_params *prm,
+                   qa_sqaopt_out *outs, qa_stats *stats) {
+    QA_TRY(begin(ctx));
+    if (!prm || !outs) return fail(QA_ERR_ARG, "null params");
+    // sqa_annealer.cpp:513-521
+    if (prm->num_steps <= 0) return fail(QA_ERR_ARG, "num_steps must be > 0.");
+    if (prm->sweeps_per_step < 0 || prm->worldline_sweeps < 0 || prm->cluster_sweeps < 0)
+        return fail(QA_ERR_ARG, "sweep counts must be >= 0.");
+    if (prm->sweeps_per_step == 0 && prm->worldline_sweeps == 0 && prm->cluster_sweeps == 0)
+        return fail(QA_ERR_ARG,
+                    "At least one of sweeps_per_step, worldline_sweeps, or cluster_sweeps must be > 0.");
+    if (!(prm->j_perp_end > prm->j_perp_start)) return fail(QA_ERR_ARG, "j_perp_end must be > j_perp_start.");
+    if (prm->trotter_slices <= 0) return fail(QA_ERR_ARG, "trotter_slices must be > 0.");
+    if (prm->replicas <= 0) return fail(QA_ERR_ARG, "replicas must be > 0.");
+    if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
+    int kind, n_max;
+    QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
+    const int P = prm->trotter_slices, K = prm->replicas, S = prm->num_steps;
+    const int spb = prm->sweeps_per_step, wls = prm->worldline_sweeps, cls = prm->cluster_sweeps;
+    if (cls > 0 && P > 64)
+        return fail(QA_ERR_UNSUPPORTED, "cluster_sweeps > 0 runs with at most 64 Trotter slices on the GPU.");
+    const bool calibrate = prm->eps_tilde <= 0.0;
+    const int Mp = std::max(prm->calib_probes, 2), cs = std::max(prm->calib_sweeps, 1), pc = cls;
+    const double beta = prm->beta, js = prm->j_perp_start, je = prm->j_perp_end, alpha = prm->alpha;
+    int n1 = 0;
+    if (prm->beta_ramp_fraction > 0.0) {
+        n1 = (int)(prm->beta_ramp_fraction * (double)S);
+        if (n1 >= S) n1 = S - 1;
+    }
+    const int n2 = S - n1, S_all = S + Mp, ns = spb + cls, nsc = cs + pc;
+    const int reads_total = n_problems * prm->reads;
+
+    Layout L;
+    build_rings(L, problems, n_problems, prm->reads, K, P, prm->seed);
+    for (auto &R : L.rings) R.sched = R.out * S_all;  // one schedule row per read
+    const int nr = (int)L.rings.size();
+    ProbDev *d_probs;
+    RingDev *d_rings;
+    uint32_t *d_spins;
+    float *d_fields;
+    QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
+    std::vector<float> A((size_t)reads_total * S_all, 0.0f), T4(A.size(), 0.0f), JP(A.size(), 0.0f);
+    auto set_col = [&](int rd, int col, double bscale, double J) {
+        const size_t i = (size_t)rd * S_all + col;
+        A[i] = (float)(2.0 * bscale);
+        T4[i] = (float)(4.0 * J);
+        JP[i] = (float)(1.0 - std::exp(-2.0 * J));
+    };
+    for (int rd = 0; rd < reads_total; ++rd)
+        for (int s = 0; s < n1; ++s) {
+            const double frac = n1 > 1 ? (double)s / (double)(n1 - 1) : 1.0;
+            const double bt = prm->beta_ramp_start + (beta - prm->beta_ramp_start) * frac;
+            set_col(rd, s, bt / (double)P, js);
+        }
+    float *d_A, *d_T4, *d_JP;
+    double *d_sum, *d_best, *d_exact, *d_cbest;
+    long long *d_bond, *d_bsamp, *d_cbond;
+    int *d_bstep, *d_cbstep;
+    uint32_t *d_bits, *d_cbits, *d_ssave;
+    float *d_fsave;
+    unsigned long long *d_cnt;
+    const size_t samp_per_ring = (size_t)std::max({n1 * ns, Mp * nsc, ns, 1});
+    QA_TRY(ws_array(ctx, W_A, A.size(), &d_A));
+    QA_TRY(ws_array(ctx, W_T4, A.size(), &d_T4));
+    QA_TRY(ws_array(ctx, W_JP, A.size(), &d_JP));
+    QA_TRY(ws_array(ctx, W_SUM, (size_t)nr * S, &d_sum));
+    QA_TRY(ws_array(ctx, W_BOND, (size_t)nr * S, &d_bond));
+    QA_TRY(ws_array(ctx, W_BSAMP, (size_t)nr * samp_per_ring, &d_bsamp));
+    QA_TRY(ws_array(ctx, W_CBOND, (size_t)nr * Mp, &d_cbond));
+    QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
+    QA_TRY(ws_array(ctx, W_CBESTE, nr, &d_cbest));
+    QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
+    QA_TRY(ws_array(ctx, W_CBSTEP, nr, &d_cbstep));
+    QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
+    QA_TRY(ws_array(ctx, W_CBITS, (size_t)nr * L.nw_max, &d_cbits));
+    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    QA_TRY(ws_array(ctx, W_EXACT, nr, &d_exact));
+    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+    auto upload_tables = [&]() -> int {
+        QA_CK(cudaMemcpyAsync(d_A, A.data(), sizeof(float) * A.size(), cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * A.size(), cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_JP, JP.data(), sizeof(float) * A.size(), cudaMemcpyHostToDevice, ctx->stream));
+        return QA_OK;
+    };
+    QA_TRY(upload_tables());
+    {
+        std::vector<double> inf(nr, INFINITY);
+        std::vector<int> neg(nr, -1);
+        QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_bstep, neg.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+    }
+
+    QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    RingPlan pl;
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, cls > 0));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
+                      !pl.own_fields()));
+    RingParams rp{};
+    rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
+    rp.P = P; rp.steps_total = S; rp.spb = spb; rp.wls = wls; rp.cls = cls;
+    rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.B = d_A; rp.T4 = d_T4; rp.JP = d_JP; rp.per_slot_sched = 0;
+    rp.ring_sum = d_sum; rp.ring_min = nullptr; rp.ring_bond = d_bond; rp.rec_base = 0; rp.rec_stride = S;
+    rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max; rp.mag = nullptr;
+    rp.counters = d_cnt;
+    QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    bool fresh = true;  // the next launch builds its fields from the spins (own-field kernels)
+    int n_launch = 0;
+    auto run_steps = [&](int s0, int s1, long long *bsamp, int bstride) -> int {
+        for (int a = s0; a < s1; a += 256) {
+            rp.step0 = a;
+            rp.step1 = std::min(s1, a + 256);
+            rp.init_fields = fresh;
+            rp.bsamp = bsamp ? bsamp + (size_t)(a - s0) * (rp.spb + rp.cls) : nullptr;
+            rp.bstride = bstride;
+            QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+            fresh = false;
+            ++n_launch;
+        }
+        return QA_OK;
+    };
+    std::vector<double> jtr((size_t)reads_total * S), chitr((size_t)reads_total * S);
+    std::vector<double> eps(reads_total, prm->eps_tilde), minchi(reads_total, 1e-4 * (double)n_max * P);
+    std::vector<double> Jcur(reads_total, js);
+    std::vector<long long> hs, hb;
+    // ---- phase 1: beta ramp at J_start (chi from the per-sweep bond sums)
+    if (n1 > 0) {
+        QA_TRY(run_steps(0, n1, ns > 0 ? d_bsamp : nullptr, (int)samp_per_ring));
+        hs.resize((size_t)nr * samp_per_ring);
+        hb.resize((size_t)nr * S);
+        QA_CK(cudaMemcpyAsync(hs.data(), d_bsamp, sizeof(long long) * hs.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaMemcpyAsync(hb.data(), d_bond, sizeof(long long) * hb.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaStreamSynchronize(ctx->stream));
+        for (int rd = 0; rd < reads_total; ++rd) {
+            const int p = rd / prm->reads, base = rd * K;
+            const double nM = (double)problems[p]->n * (double)P;
+            for (int s = 0; s < n1; ++s) {
+                const double chi = opt_chi_raw(hs.data() + (size_t)base * samp_per_ring + (size_t)s * ns, K, ns,
+                                               samp_per_ring, hb[(size_t)base * S + s], nM);
+                jtr[(size_t)rd * S + s] = js;
+                chitr[(size_t)rd * S + s] = std::max(chi, 0.0);
+            }
+        }
+    }
+    // ---- calibration pilot: M probes from the post-ramp state, then restored
+    std::vector<std::vector<double>> pj(reads_total), pcv(reads_total);
+    std::vector<std::vector<double>> jtraj(reads_total);
+    if (calibrate) {
+        QA_TRY(ws_array(ctx, W_SSAVE, (size_t)std::max<long long>(L.spin_words, 1), &d_ssave));
+        QA_TRY(ws_array(ctx, W_FSAVE, (size_t)std::max<long long>(L.field_floats, 1), &d_fsave));
+        QA_CK(cudaMemcpyAsync(d_ssave, d_spins, sizeof(uint32_t) * L.spin_words, cudaMemcpyDeviceToDevice, ctx->stream));
+        // field caches are valid unless an own-field kernel has not run yet (it then builds them from the spins)
+        const bool fields_valid = !fresh || !pl.own_fields();
+        if (fields_valid)
+            QA_CK(cudaMemcpyAsync(d_fsave, d_fields, sizeof(float) * L.field_floats, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+        const bool fresh_before = fresh;
+        const double dJp = (je - js) / (double)Mp;
+        const double bcold = beta / (double)P;
+        for (int rd = 0; rd < reads_total; ++rd)
+            for (int m = 0; m < Mp; ++m) set_col(rd, S + m, bcold, js + ((double)m + 0.5) * dJp);
+        QA_TRY(upload_tables());
+        {
+            std::vector<double> inf(nr, INFINITY);
+            QA_CK(cudaMemcpyAsync(d_cbest, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        }
+        RingParams keep = rp;
+        rp.spb = cs; rp.cls = pc; rp.wls = 0; rp.slice_tag = DOM_OPTCAL;
+        rp.ring_sum = nullptr; rp.ring_bond = d_cbond; rp.rec_stride = 1; rp.rec_base = -S;
+        rp.best_E = d_cbest; rp.best_step = d_cbstep; rp.best_bits = d_cbits;
+        // ring_bond index = ring * rec_stride + rec_base + step: one slot per (ring, probe) via rec_base per launch
+        std::vector<long long> cb((size_t)nr * Mp);
+        hs.assign((size_t)nr * samp_per_ring, 0);
+        for (int m = 0; m < Mp; ++m) {
+            // the bond record of probe m lands at d_cbond[ring * Mp + m]
+            rp.rec_stride = Mp;
+            rp.rec_base = m - (S + m);
+            QA_TRY(run_steps(S + m, S + m + 1, nsc > 0 ? d_bsamp + (size_t)m * nsc : nullptr, (int)samp_per_ring));
+        }
+        rp = keep;
+        QA_CK(cudaMemcpyAsync(hs.data(), d_bsamp, sizeof(long long) * hs.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaMemcpyAsync(cb.data(), d_cbond, sizeof(long long) * cb.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        // restore the post-ramp state (own-field kernels rebuild their exact fields from it)
+        QA_CK(cudaMemcpyAsync(d_spins, d_ssave, sizeof(uint32_t) * L.spin_words, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (fields_valid)
+            QA_CK(cudaMemcpyAsync(d_fields, d_fsave, sizeof(float) * L.field_floats, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+        fresh = fresh_before || pl.own_fields();
+        QA_CK(cudaStreamSynchronize(ctx->stream));
+        for (int rd = 0; rd < reads_total; ++rd) {
+            const int p = rd / prm->reads, base = rd * K;
+            const double nM = (double)problems[p]->n * (double)P;
+            pj[rd].resize(Mp);
+            pcv[rd].resize(Mp);
+            double integral = 0.0, maxc = 0.0;
+            for (int m = 0; m < Mp; ++m) {
+                double chi = opt_chi_raw(hs.data() + (size_t)base * samp_per_ring + (size_t)m * nsc, K, nsc,
+                                         samp_per_ring, cb[(size_t)base * Mp + m], nM);
+                if (!(chi > 0.0)) chi = 0.0;
+                pj[rd][m] = js + ((double)m + 0.5) * dJp;
+                pcv[rd][m] = chi;
+                integral += std::pow(std::max(chi, 1e-12), alpha) * dJp;
+                maxc = std::max(maxc, chi);
+            }
+            double e = integral / (double)n2;
+            if (!(e > 0.0) || !std::isfinite(e)) {
+                e = std::max(je - js, 0.0) / (double)S;
+                if (!(e > 0.0)) e = 1e-9;
+            }
+            eps[rd] = e;
+            minchi[rd] = std::max(1e-4 * maxc, 1e-12);
+            // J trajectory: inverse of G(J) = int chi(J')^alpha dJ' on a 4096 grid (sqa_annealer.cpp:848-872)
+            const int GRID = 4096;
+            const double h = (je - js) / (double)GRID;
+            std::vector<double> G(GRID + 1, 0.0);
+            double prev = std::pow(std::max(opt_profile(pj[rd], pcv[rd], js), minchi[rd]), alpha);
+            for (int k = 1; k <= GRID; ++k) {
+                const double Jk = js + (double)k * h;
+                const double cur = std::pow(std::max(opt_profile(pj[rd], pcv[rd], Jk), minchi[rd]), alpha);
+                G[k] = G[k - 1] + 0.5 * (prev + cur) * h;
+                prev = cur;
+            }
+            const double Gt = G[GRID];
+            jtraj[rd].resize(n2);
+            int k = 0;
+            const double den = n2 > 1 ? (double)(n2 - 1) : 1.0;
+            for (int t = 0; t < n2; ++t) {
+                const double target = Gt > 0.0 ? ((double)t / den) * Gt : 0.0;
+                while (k < GRID && G[k + 1] < target) ++k;
+                const double g0 = G[k], g1 = G[k + 1];
+                const double fr = g1 > g0 ? (target - g0) / (g1 - g0) : 0.0;
+                jtraj[rd][t] = js + ((double)k + fr) * h;
+            }
+        }
+    } else {
+        for (int rd = 0; rd < reads_total; ++rd) minchi[rd] = 1e-4 * (double)problems[rd / prm->reads]->n * P;
+    }
+    // ---- phase 2 at the cold beta
+    const double bcold = beta / (double)P;
+    if (calibrate) {
+        for (int rd = 0; rd < reads_total; ++rd)
+            for (int t = 0; t < n2; ++t) {
+                const double J = jtraj[rd][t];
+                set_col(rd, n1 + t, bcold, J);
+                const double cp = opt_profile(pj[rd], pcv[rd], J);
+                jtr[(size_t)rd * S + n1 + t] = J;
+                chitr[(size_t)rd * S + n1 + t] = std::max(cp, minchi[rd]);
+            }
+        for (int rd = 0; rd < reads_total; ++rd) Jcur[rd] = n2 > 0 ? jtraj[rd][n2 - 1] : js;
+        QA_TRY(upload_tables());
+        QA_TRY(run_steps(n1, S, nullptr, 0));
+    } else {
+        hs.assign((size_t)nr * samp_per_ring, 0);
+        std::vector<long long> bnow((size_t)nr * S);
+        for (int t = 0; t < n2; ++t) {
+            const int s = n1 + t;
+            for (int rd = 0; rd < reads_total; ++rd) set_col(rd, s, bcold, Jcur[rd]);
+            QA_TRY(upload_tables());
+            QA_TRY(run_steps(s, s + 1, ns > 0 ? d_bsamp : nullptr, (int)samp_per_ring));
+            if (ns > 0)
+                QA_CK(cudaMemcpyAsync(hs.data(), d_bsamp, sizeof(long long) * hs.size(), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+            QA_CK(cudaMemcpyAsync(bnow.data(), d_bond, sizeof(long long) * bnow.size(), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+            QA_CK(cudaStreamSynchronize(ctx->stream));
+            for (int rd = 0; rd < reads_total; ++rd) {
+                const int p = rd / prm->reads, base = rd * K;
+                const double nM = (double)problems[p]->n * (double)P;
+                const double on = opt_chi_raw(hs.data() + (size_t)base * samp_per_ring, K, ns, samp_per_ring,
+                                              bnow[(size_t)base * S + s], nM);
+                const double drive = std::max(on, minchi[rd]);
+                jtr[(size_t)rd * S + s] = Jcur[rd];
+                chitr[(size_t)rd * S + s] = drive;
+                Jcur[rd] = std::min(Jcur[rd] + eps[rd] * std::pow(drive, -alpha), je);
+            }
+        }
+    }
+    QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
+    QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+
+    std::vector<double> sums((size_t)nr * S), bestE(nr), exact(nr);
+    std::vector<int> bstep(nr);
+    std::vector<uint32_t> bits((size_t)nr * L.nw_max);
+    unsigned long long cnt[4];
+    QA_CK(cudaMemcpyAsync(sums.data(), d_sum, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bstep.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    for (int p = 0; p < n_problems; ++p) {
+        const int n = problems[p]->n;
+        qa_sqaopt_out &o = outs[p];
+        for (int r = 0; r < prm->reads; ++r) {
+            const int rd = p * prm->reads + r, base = rd * K;
+            for (int s = 0; s < S; ++s) {
+                double tot = 0.0;
+                for (int k = 0; k < K; ++k) tot += sums[(size_t)(base + k) * S + s];
+                if (o.energy_trace) o.energy_trace[(size_t)r * S + s] = tot / (double)(K * P);
+                if (o.j_perp_trace) o.j_perp_trace[(size_t)r * S + s] = jtr[(size_t)rd * S + s];
+                if (o.chi_B_trace) o.chi_B_trace[(size_t)r * S + s] = chitr[(size_t)rd * S + s];
+            }
+            int kb = 0;
+            for (int k = 1; k < K; ++k) {
+                const int a = base + k, b = base + kb;
+                if (bestE[a] < bestE[b] || (bestE[a] == bestE[b] && bstep[a] < bstep[b])) kb = k;
+            }
+            const int ib = base + kb;
+            if (o.best_spins) unpack_bits(bits.data() + (size_t)ib * L.nw_max, n, o.best_spins + (size_t)r * n);
+            if (o.best_energy) o.best_energy[r] = exact[ib];
+            if (o.scalars) {
+                double *sc = o.scalars + (size_t)r * 4;
+                sc[0] = eps[rd];
+                sc[1] = js;
+                sc[2] = je;
+                sc[3] = Jcur[rd];
+            }
+        }
+    }
+    if (stats) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]);
+        stats->slice_attempts = (int64_t)cnt[0];
+        stats->slice_accepts = (int64_t)cnt[1];
+        stats->worldline_attempts = (int64_t)cnt[2];
+        stats->worldline_accepts = (int64_t)cnt[3];
+        stats->sweep_ms = a;
+        stats->total_ms = b;
+        stats->sweep_launches = n_launch;
+        stats->launches = (pl.own_fields() ? 2 : 3) + n_launch;
+        stats->h2d_bytes = 0;
+        stats->d2h_bytes = (int64_t)(sizeof(double) * sums.size());
     }
     return QA_OK;
 }

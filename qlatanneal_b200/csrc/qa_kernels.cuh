@@ -49,6 +49,8 @@ struct RingParams {
     const float *B, *T4;  // [sched + step] (PT: [sched + slot]): B = 2 beta/P, T4 = 4 J_perp
     int cls;              // cluster sweeps per step (ring_kernel only; P <= 64)
     const float *JP;      // like B: bond probability 1 - exp(-2 J_perp) of the cluster moves
+    long long *bsamp;     // bond sum after every slice and cluster sweep, or null:
+    int bstride;          //   [ring * bstride + (step - step0) * (spb + cls) + sweep]
     int per_slot_sched;   // 1: index A/T4 by slot instead of step
     int smem_fields;
     int init_fields;      // ring_pm1_kernel: build the int32 fields from the spins first
@@ -275,6 +277,35 @@ struct RingSmem {
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Imaginary-time bond sum of the ring, sum_{t,i} s_t,i s_t+1,i (whole CTA;
+// the total is valid on thread 0).  part: one int per warp.
+__device__ __forceinline__ long long ring_bond_total(const uint32_t *S, int NP, int nw, int n, int *part, int W) {
+    int b = 0;
+    for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) {
+        const int t = idx / nw, q = idx - t * nw;
+        const int tn = t + 1 == NP ? 0 : t + 1;
+        const int rem = n - 32 * q;
+        const uint32_t vm = rem >= 32 ? FULL : ((1u << rem) - 1u);
+        b += 2 * __popc(~(S[idx] ^ S[tn * nw + q]) & vm) - __popc(vm);
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) b += __shfl_xor_sync(FULL, b, off);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = b;
+    __syncthreads();
+    long long tb = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < W; ++w) tb += part[w];
+    __syncthreads();
+    return tb;
+}
+
+__device__ __forceinline__ void record_bond_sample(const RingParams &p, const uint32_t *S, int NP, int nw, int n,
+                                                   int *part, int W, int step, int j) {
+    const long long tb = ring_bond_total(S, NP, nw, n, part, W);
+    if (threadIdx.x == 0)
+        p.bsamp[(long long)blockIdx.x * p.bstride + (long long)(step - p.step0) * (p.spb + p.cls) + j] = tb;
+}
+
 __host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fields) {
     const int nw = (n + 31) / 32;
     size_t b = align_up((size_t)P * nw * 4, 16);
@@ -426,6 +457,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                 }
                 __syncthreads();
             }
+            if (p.bsamp) record_bond_sample(p, sm.S, NP, nw, n, sm.wl_sh, W, step, sw);
         }
         // cluster sweeps: one warp, spins in order
         const int cls = step >= 0 ? p.cls : 0;
@@ -437,6 +469,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                     cluster_move<KIND>(Pd, sm.S, gbase, sm.h, NP, i, (uint32_t)slot, sigma, B, T4, JPv, R.key, lane);
             }
             __syncthreads();
+            if (p.bsamp) record_bond_sample(p, sm.S, NP, nw, n, sm.wl_sh, W, step, p.spb + sw);
         }
         for (int sw = 0; sw < wls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);

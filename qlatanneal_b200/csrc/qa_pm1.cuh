@@ -257,6 +257,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 }
                 __syncthreads();
             }
+            if (p.bsamp) record_bond_sample(p, S, NP, nw, n, wpart, W, step, sw);
         }
         for (int sw = 0; sw < wls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);

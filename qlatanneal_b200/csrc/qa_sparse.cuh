@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
                 }
                 __syncthreads();
             }
+            if (p.bsamp) record_bond_sample(p, S, NP, nw, n, wpart, W, step, sw);
         }
         // worldline sweeps: one warp, spins in order, sums from the worldline bits
         for (int sw = 0; sw < wls; ++sw) {

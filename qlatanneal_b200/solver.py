@@ -267,8 +267,9 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
                          "leave schedule_type='standard' and use the chi_* parameters.")
     if method == "ctpimc":
         raise NotImplementedError("method='ctpimc' stays on qanneal's CPU path (not part of the sweep engine).")
-    if schedule_type == "optimal":
-        raise NotImplementedError("schedule_type='optimal' (run_optimal) is not part of the CUDA sweep engine.")
+    if schedule_type == "optimal" and method == "sqapt":
+        raise NotImplementedError("schedule_type='optimal' with method='sqapt' (SQAParallelTemperingAnnealer."
+                                  "run_optimal) is not part of the CUDA sweep engine.")
     if logger is None:
         logger = logging.getLogger("qlatanneal_b200.solve")
     if reads <= 0:
@@ -291,7 +292,32 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
     if progress and reads > 1:
         logger.info("Running %d reads in one batched GPU call...", reads)
 
-    if method == "sqa":
+    if method == "sqa" and schedule_type == "optimal":
+        # solver.py:616-645 and 686-702: beta / J_perp range resolved once, then
+        # run_optimal per read (read r keyed seed + r).
+        auto_beta, auto_jps, auto_jpe = optimal_j_perp_params(ising, trotter_slices=trotter_slices)
+        beta = float(optimal_beta) if optimal_beta is not None else auto_beta
+        jps = float(optimal_j_perp_start) if optimal_j_perp_start is not None else auto_jps
+        if optimal_j_perp_end is not None:
+            jpe = float(optimal_j_perp_end)
+        else:
+            jrms = j_rms_from_problem(problem, n=n)
+            if jrms is not None and jrms > 0.0:
+                jpe = max(jps, 5.0 * jrms)
+                if jpe <= jps:
+                    logger.warning("optimal schedule: 5*j_rms=%.4g <= j_perp_start=%.4g; the system starts past "
+                                   "criticality and the adaptive schedule has little range to traverse. Consider "
+                                   "a problem with larger j_rms.", 5.0 * jrms, jps)
+            else:
+                jpe = auto_jpe
+        steps = int(optimal_num_steps) if optimal_num_steps is not None else max(100, len(schedule.betas))
+        ann = SQAAnnealer(ising, schedule, trotter_slices, replicas, backend=backend)
+        res = ann.run_optimal_reads(beta, jps, jpe, optimal_eps_tilde, optimal_alpha, steps, sweeps_per_beta,
+                                    worldline_sweeps, cluster_sweeps, int(optimal_calib_probes),
+                                    int(optimal_calib_sweeps), float(optimal_beta_ramp_fraction), reads=reads,
+                                    seed=seed)
+        traces = [r.energy_trace for r in res]
+    elif method == "sqa":
         ann = SQAAnnealer(ising, schedule, trotter_slices, replicas, backend=backend)
         res = ann.run_reads(sweeps_per_beta, worldline_sweeps, cluster_sweeps, continuous_time_slices, reads=reads,
                             seed=seed)

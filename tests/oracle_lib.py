@@ -75,6 +75,9 @@ class Oracle:
         L.or_init_spins.argtypes = [_i8p, C.c_int, C.c_uint64, C.c_uint32, C.c_uint32]
         L.or_sa_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double),
                                 _f8p, _i64p, C.c_void_p, C.c_void_p]
+        L.or_sqa_opt_run.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 5 + [C.c_int] * 6 +
+                                     [C.c_double, C.c_double, C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double),
+                                      _f8p, _f8p, _f8p, _f8p])
         L.or_pt_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p,
                                 C.POINTER(C.c_double), _f8p, _i8p, _f8p, _f8p, _i64p]
         L.or_sqa_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
@@ -182,6 +185,17 @@ class Oracle:
                          mag.ctypes.data, C.addressof(bstep))
         return best, E.value, trace, mag, bstep.value
 
+    def sqa_opt_run(self, m, P, K, beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps, ramp_fraction,
+                    ramp_start, seed, read=0):
+        best = np.zeros(m.n, np.int8)
+        E = C.c_double()
+        tr, jt, ct, sc = np.zeros(steps), np.zeros(steps), np.zeros(steps), np.zeros(4)
+        rc = self.L.or_sqa_opt_run(m.h, P, K, beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps,
+                                   ramp_fraction, ramp_start, seed, read, best, C.byref(E), tr, jt, ct, sc)
+        if rc != 0:
+            raise ValueError("run_optimal arguments rejected")
+        return dict(best=best, best_energy=E.value, trace=tr, j_perp=jt, chi=ct, scalars=sc)
+
     def pt_run(self, m, betas, spb, steps, swap_interval, seed, read=0):
         """Classical PT read: (best, best_E, final_E[R], final_spins[R][n], avg_trace, swap_trace)."""
         betas = _c64(betas)
@@ -275,6 +289,9 @@ class Ref:
                                  C.POINTER(C.c_double), _f8p, _f8p, _f8p]
         L.ref_replica_run.argtypes = [C.c_void_p, _f8p, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_double),
                                       _f8p, _f8p]
+        L.ref_sqa_opt_run.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 5 +
+                                      [C.c_int] * 6 + [C.c_double, C.c_double, C.c_uint64, C.POINTER(C.c_double),
+                                                       _f8p, _f8p, _f8p, _f8p])
         L.ref_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                     C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p, _f8p, _f8p, C.c_int]
         L.ref_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
@@ -403,6 +420,15 @@ class RefModel:
         if self.ref.L.ref_replica_run(self.h, betas, len(betas), spb, R, seed, C.byref(E), avg, mag) != 0:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return E.value, avg, mag
+
+    def sqa_opt_run(self, P, K, beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps, ramp_fraction,
+                    ramp_start, seed):
+        E = C.c_double()
+        tr, jt, ct, sc = np.zeros(steps), np.zeros(steps), np.zeros(steps), np.zeros(4)
+        if self.ref.L.ref_sqa_opt_run(self.h, P, K, beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps,
+                                      ramp_fraction, ramp_start, seed, C.byref(E), tr, jt, ct, sc) != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return dict(best_energy=E.value, trace=tr, j_perp=jt, chi=ct, scalars=sc)
 
     def sqapt_run(self, betas, gammas, P, spb, wls, steps, swap_interval, seed, cls=0):
         betas, gammas = _c64(betas), _c64(gammas)

@@ -244,3 +244,23 @@ def test_replica_restatement_matches_reference_statistics(oracle, ref):
     for a, b in ((eo, er), (mo, mr)):
         (ma, ca), (mb, cb) = _ci95(a), _ci95(b)
         assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
+
+
+@pytest.mark.parametrize("eps", [0.0, 0.02])
+def test_run_optimal_restatement_matches_reference_statistics(oracle, ref, eps):
+    """SQAAnnealer::run_optimal (sqa_annealer.cpp:499-952): beta ramp,
+    calibration pilot (eps_tilde <= 0) or online J_perp updates (eps_tilde > 0),
+    chi_B from bond-sum samples.  Final energy, the J_perp reached mid-run and
+    the calibrated budget agree with qanneal within 95% CIs (200 reads)."""
+    h, J = sk_dense(24, 17)
+    m, rm = oracle.dense(h, J), ref.dense(h, J)
+    a = (8, 2, 2.0, 0.05, 2.0, eps, 15 / 14, 30, 2, 1, 1, 8, 4, 0.3, 0.1)
+    A = [oracle.sqa_opt_run(m, *a, seed=100, read=k) for k in range(200)]
+    B = [rm.sqa_opt_run(*a, seed=5000 + k) for k in range(200)]
+    for f in (lambda d: d["trace"][-1], lambda d: d["j_perp"][20], lambda d: d["scalars"][0],
+              lambda d: d["best_energy"]):
+        (ma, ca), (mb, cb) = _ci95([f(d) for d in A]), _ci95([f(d) for d in B])
+        assert abs(ma - mb) <= 1.5 * (ca + cb) + 1e-12, (ma, ca, mb, cb)
+    d = A[0]
+    assert d["scalars"][1] == 0.05 and d["scalars"][2] == 2.0
+    assert np.all(np.diff(d["j_perp"][9:]) >= 0) and d["j_perp"][-1] <= 2.0 + 1e-12

@@ -42,7 +42,7 @@ def test_normalize_problem_forms():
     with pytest.raises(NotImplementedError):
         qa.solve(Q, method="ctpimc")
     with pytest.raises(NotImplementedError):
-        qa.solve(Q, method="sqa", schedule_type="optimal")
+        qa.solve(Q, method="sqapt", schedule_type="optimal")
 
 
 @pytest.mark.gpu
