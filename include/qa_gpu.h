@@ -222,6 +222,44 @@ typedef struct {
 QA_API int qa_sqapt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
                         const qa_sqapt_params *params, qa_sqapt_out *outs, qa_stats *stats);
 
+/* ---- SQA-PT adaptive schedule: SQAParallelTemperingAnnealer::run_optimal
+ *      (sqa_parallel_tempering.cpp:348-882) ----------------------------------
+ * Every rung keeps its beta_r and runs at one schedule J_perp per step,
+ * starting at the hottest rung's coupling J(beta_0, Gamma_0).  eps_tilde <= 0:
+ * calib_probes chi_B probes from the starting states fix eps_tilde and a
+ * J_perp trajectory spanning num_steps; eps_tilde > 0: J += eps_tilde *
+ * chi_B^-alpha after every step.  Swaps use the classical action (the shared
+ * Trotter terms cancel).  Outputs as qa_sqapt_out plus the schedule traces. */
+typedef struct {
+    const double *betas;     /* [rungs] */
+    const double *gammas;    /* [rungs] (J_start and the default J_end only) */
+    int rungs;               /* >= 2 */
+    int trotter_slices;
+    int continuous_time_slices;
+    int sweeps_per_step;
+    int worldline_sweeps;
+    int cluster_sweeps;      /* P <= 64 when > 0 */
+    int num_steps;           /* > 0 */
+    int swap_interval;       /* > 0 */
+    double eps_tilde;        /* <= 0: calibrate */
+    double alpha;
+    double j_perp_end;       /* <= 0: the coldest rung's coupling */
+    int calib_probes;
+    int calib_sweeps;
+    int reads;
+    uint64_t seed;
+} qa_sqaptopt_params;
+
+typedef struct {
+    qa_sqapt_out pt;           /* best / final states and energies, average energy and swap traces */
+    double *j_perp_trace;      /* [reads][num_steps] */
+    double *chi_B_trace;       /* [reads][num_steps] */
+    double *scalars;           /* [reads][4] calibrated_eps_tilde, j_perp_start, resolved_j_perp_end, final_j_perp */
+} qa_sqaptopt_out;
+
+QA_API int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
+                            const qa_sqaptopt_params *params, qa_sqaptopt_out *outs, qa_stats *stats);
+
 /* ---- classical parallel tempering: ParallelTemperingAnnealer::run
  *      (parallel_tempering.cpp:36-122) --------------------------------------
  * One replica per beta, Metropolis sweeps, swaps of neighbouring replicas

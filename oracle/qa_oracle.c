@@ -19,6 +19,8 @@
  *   cluster moves    src/sqa_annealer.cpp:215-288, src/sqa_parallel_tempering.cpp:222-278
  *   classical PT     src/parallel_tempering.cpp:36-122 (the SQA-PT core, one slice)
  *   replicas         src/replica_annealer.cpp:46-142 (SA reads + magnetisation)
+ *   SQA run_optimal  src/sqa_annealer.cpp:499-952 (beta ramp, chi_B calibration, J_perp trajectory)
+ *   SQA-PT run_optimal src/sqa_parallel_tempering.cpp:348-882
  *
  * The "replay model".  The qanneal loops draw from std::mt19937_64 through
  * libstdc++ distributions and visit spins in std::shuffle order, which no GPU
@@ -1236,6 +1238,37 @@ static double opt_profile(const double *pj, const double *pc, int M, double J) {
     return pc[lo] + t * (pc[hi] - pc[lo]);
 }
 
+/* The J trajectory of a calibrated run: step t of nt sits where
+   G(J) = int_{js}^{J} max(chi(J'), min_chi)^alpha dJ' (trapezoids on a 4096 grid)
+   reaches t/(nt-1) of G(je) (sqa_annealer.cpp:848-872,
+   sqa_parallel_tempering.cpp:768-794). */
+static void opt_trajectory(const double *pj, const double *pc, int Mp, double js, double je, double min_chi,
+                           double alpha, int nt, double *jt) {
+    const int GRID = 4096;
+    const double h = (je - js) / (double)GRID;
+    double *G = (double *)calloc((size_t)GRID + 1, sizeof(double));
+    double c0 = opt_profile(pj, pc, Mp, js);
+    double prev = pow(c0 > min_chi ? c0 : min_chi, alpha);
+    for (int k = 1; k <= GRID; ++k) {
+        const double Jk = js + (double)k * h;
+        const double ck = opt_profile(pj, pc, Mp, Jk);
+        const double cur = pow(ck > min_chi ? ck : min_chi, alpha);
+        G[k] = G[k - 1] + 0.5 * (prev + cur) * h;
+        prev = cur;
+    }
+    const double Gt = G[GRID];
+    int k = 0;
+    const double den = nt > 1 ? (double)(nt - 1) : 1.0;
+    for (int t = 0; t < nt; ++t) {
+        const double target = Gt > 0.0 ? ((double)t / den) * Gt : 0.0;
+        while (k < GRID && G[k + 1] < target) ++k;
+        const double g0 = G[k], g1 = G[k + 1];
+        const double fr = g1 > g0 ? (target - g0) / (g1 - g0) : 0.0;
+        jt[t] = js + ((double)k + fr) * h;
+    }
+    free(G);
+}
+
 /* Replay form: phase-1 steps s = 0..n1-1 and phase-2 steps s = n1..num_steps-1
    use the sweep counters of step s; calibration probe m runs as step
    num_steps + m with slice tag OPTCAL (cs slice sweeps, max(cls, 1) cluster
@@ -1347,30 +1380,8 @@ OR_EXPORT int or_sqa_opt_run(const or_model *M, int P, int K, double beta, doubl
     /* the J trajectory: inverse of G(J) = int chi(J')^alpha dJ' on a 4096 grid */
     double *jt = NULL;
     if (calibrate && have_profile && je > js) {
-        const int GRID = 4096;
-        const double h = (je - js) / (double)GRID;
-        double *G = (double *)calloc((size_t)GRID + 1, sizeof(double));
-        double c0 = opt_profile(pj, pcv, Mp, js);
-        double prev = pow(c0 > min_chi ? c0 : min_chi, alpha);
-        for (int k = 1; k <= GRID; ++k) {
-            const double Jk = js + (double)k * h;
-            const double ck = opt_profile(pj, pcv, Mp, Jk);
-            const double cur = pow(ck > min_chi ? ck : min_chi, alpha);
-            G[k] = G[k - 1] + 0.5 * (prev + cur) * h;
-            prev = cur;
-        }
-        const double Gt = G[GRID];
         jt = (double *)malloc(sizeof(double) * (size_t)n2);
-        int k = 0;
-        const double den = n2 > 1 ? (double)(n2 - 1) : 1.0;
-        for (int t = 0; t < n2; ++t) {
-            const double target = Gt > 0.0 ? ((double)t / den) * Gt : 0.0;
-            while (k < GRID && G[k + 1] < target) ++k;
-            const double g0 = G[k], g1 = G[k + 1];
-            const double fr = g1 > g0 ? (target - g0) / (g1 - g0) : 0.0;
-            jt[t] = js + ((double)k + fr) * h;
-        }
-        free(G);
+        opt_trajectory(pj, pcv, Mp, js, je, min_chi, alpha, n2, jt);
     }
     /* phase 2: fixed cold beta, J from the trajectory (or online) */
     double J = js;
@@ -1397,6 +1408,189 @@ OR_EXPORT int or_sqa_opt_run(const or_model *M, int P, int K, double beta, doubl
     *best_E = rbest[kb];
     memcpy(best_spins, rstate + (size_t)kb * n, (size_t)n);
     free(jt); free(pj); free(pcv); free(samp); free(lastb); free(rbest); free(rstep); free(rstate);
+    ring_free(&R);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* SQAParallelTemperingAnnealer::run_optimal                            */
+/* (sqa_parallel_tempering.cpp:348-882), one read                       */
+/* ------------------------------------------------------------------ */
+/* One step of every rung at the shared J_perp: slice sweeps (bond sample of
+   each ring after each), cluster sweeps (likewise), worldline sweeps.  Rung
+   slot sl keeps its own B = 2 beta_sl / P and its random streams. */
+static void ptopt_sweep(ring_t *R, const int *slot_of, const float *B, int step, int spb, int cls, int wls, float T4,
+                        float JP, uint32_t slice_tag, long long *samp) {
+    const int Rn = R->K, P = R->P, ns = spb + cls;
+    for (int sw = 0; sw < spb; ++sw) {
+        const uint32_t sigma = (uint32_t)(step * spb + sw);
+        for (int ph = 0; ph < 3; ++ph)
+            for (int k = 0; k < Rn; ++k)
+                for (int t = 0; t < P; ++t) {
+                    if (phase_of(t, P) != ph) continue;
+                    const int sl = slot_of[k];
+                    sweep_cell(R, k, t, (uint32_t)(sl * P + t), sigma, slice_tag, B[sl], T4);
+                }
+        for (int k = 0; k < Rn; ++k) samp[(size_t)k * ns + sw] = bond_sum(R, k);
+    }
+    for (int sw = 0; sw < cls; ++sw)
+        for (int k = 0; k < Rn; ++k) {
+            const int sl = slot_of[k];
+            cluster_sweep(R, k, (uint32_t)sl, (uint32_t)(step * cls + sw), B[sl], T4, JP);
+            samp[(size_t)k * ns + spb + sw] = bond_sum(R, k);
+        }
+    for (int sw = 0; sw < wls; ++sw)
+        for (int k = 0; k < Rn; ++k)
+            worldline_sweep(R, k, (uint32_t)slot_of[k], (uint32_t)(step * wls + sw), B[slot_of[k]]);
+}
+
+/* Replay form: every rung runs at the one schedule J_perp of the step
+   (T4 = 4 J, JP = 1 - e^{-2J}) and its own B; J starts at the hottest rung's
+   coupling.  Calibration (eps_tilde <= 0) probes M points from the starting
+   state, probe m as step num_steps + m with slice tag OPTCAL, then restores
+   it; eps = sum_m chi_m^alpha dJ/M / num_steps and the trajectory spans all
+   num_steps.  Swaps: the rung action with J_perp = 0, (beta_r/P) sum_t E_t --
+   the shared Trotter terms cancel (sqa_parallel_tempering.cpp:846-861).
+   P is the resolved slice count.  scalars: calibrated eps_tilde, J_start,
+   resolved J_end, final J.  Returns 1 when run_optimal rejects its
+   arguments. */
+OR_EXPORT int or_sqapt_opt_run(const or_model *M, const double *betas, const double *gammas, int Rn, int P, int spb,
+                               int wls, int cls, int steps, int swap_interval, double eps_tilde, double alpha,
+                               double je, int probes, int csweeps, uint64_t seed, int read, int8_t *best_spins,
+                               double *best_E, double *final_E, int8_t *final_spins, double *avg_trace,
+                               double *swap_trace, double *jtrace, double *chitrace, double *scalars) {
+    if (steps <= 0 || swap_interval <= 0 || (spb == 0 && wls == 0 && cls == 0) || Rn < 2) return 1;
+    const int n = M->n;
+    const int calibrate = eps_tilde <= 0.0;
+    const double nM = (double)n * (double)P;
+    const double js = trotter_coupling(betas[0], gammas[0], P);
+    if (je <= 0.0) je = trotter_coupling(betas[Rn - 1], gammas[Rn - 1], P);
+    if (je <= js) je = js + 1e6;
+    ring_t R;
+    ring_alloc(&R, M, P, Rn, seed + (uint64_t)read);
+    ring_init(&R, DOM_INIT);
+    int *slot_of = (int *)malloc(sizeof(int) * (size_t)Rn), *ring_in = (int *)malloc(sizeof(int) * (size_t)Rn);
+    float *B = (float *)malloc(sizeof(float) * (size_t)Rn);
+    double *bp = (double *)malloc(sizeof(double) * (size_t)Rn);
+    double *Esum = (double *)malloc(sizeof(double) * (size_t)Rn), *Emin = (double *)malloc(sizeof(double) * (size_t)Rn);
+    int *tmin = (int *)malloc(sizeof(int) * (size_t)Rn);
+    long long *bond = (long long *)malloc(sizeof(long long) * (size_t)Rn);
+    for (int k = 0; k < Rn; ++k) {
+        slot_of[k] = ring_in[k] = k;
+        B[k] = (float)(2.0 * (betas[k] / (double)P));
+        bp[k] = betas[k] / (double)P;
+    }
+    double best = INFINITY;
+    for (int k = 0; k < Rn; ++k) ring_scan(&R, k, &Esum[k], &Emin[k], &tmin[k], &bond[k]);
+    for (int r = 0; r < Rn; ++r) {
+        const int k = ring_in[r];
+        if (Emin[k] < best) {
+            best = Emin[k];
+            memcpy(best_spins, R.s + ((size_t)k * P + tmin[k]) * n, (size_t)n);
+        }
+    }
+    const int ns = spb + cls;
+    const int Mp = probes > 2 ? probes : 2, cs = csweeps > 1 ? csweeps : 1, pc = cls > 0 ? cls : 0;
+    const int nsc = cs + pc;
+    long long *samp = (long long *)malloc(sizeof(long long) * (size_t)Rn * (size_t)(ns > nsc ? ns : nsc) + 16);
+    long long lastb[1];
+    double min_chi = 1e-4 * nM;
+    double *pj = (double *)malloc(sizeof(double) * (size_t)Mp), *pcv = (double *)malloc(sizeof(double) * (size_t)Mp);
+    double *jt = NULL;
+    const double dJ = je - js;
+    if (calibrate) {
+        int8_t *ss = (int8_t *)malloc((size_t)Rn * P * n);
+        float *sg = (float *)malloc(sizeof(float) * (size_t)Rn * P * n);
+        memcpy(ss, R.s, (size_t)Rn * P * n);
+        memcpy(sg, R.g, sizeof(float) * (size_t)Rn * P * n);
+        const double dJp = dJ / (double)Mp;
+        double integral = 0.0, maxc = 0.0;
+        for (int m = 0; m < Mp; ++m) {
+            const double Jm = js + ((double)m + 0.5) * dJp;
+            ptopt_sweep(&R, slot_of, B, steps + m, cs, pc, 0, (float)(4.0 * Jm), (float)(1.0 - exp(-2.0 * Jm)),
+                        DOM_OPTCAL, samp);
+            lastb[0] = bond_sum(&R, ring_in[0]);
+            double chi = opt_chi_raw(samp, Rn, nsc, lastb, nM);
+            if (!(chi > 0.0)) chi = 0.0;
+            pj[m] = Jm;
+            pcv[m] = chi;
+            integral += pow(chi > 1e-12 ? chi : 1e-12, alpha) * dJp;
+            if (chi > maxc) maxc = chi;
+        }
+        memcpy(R.s, ss, (size_t)Rn * P * n);
+        memcpy(R.g, sg, sizeof(float) * (size_t)Rn * P * n);
+        free(ss); free(sg);
+        eps_tilde = integral / (double)steps;
+        if (!(eps_tilde > 0.0) || !isfinite(eps_tilde)) {
+            eps_tilde = (dJ > 0.0 ? dJ : 0.0) / (double)steps;
+            if (!(eps_tilde > 0.0)) eps_tilde = 1e-9;
+        }
+        min_chi = 1e-4 * maxc > 1e-12 ? 1e-4 * maxc : 1e-12;
+        jt = (double *)malloc(sizeof(double) * (size_t)steps);
+        opt_trajectory(pj, pcv, Mp, js, je, min_chi, alpha, steps, jt);
+    }
+    scalars[0] = eps_tilde;
+    scalars[1] = js;
+    scalars[2] = je;
+    double J = js;
+    for (int step = 0; step < steps; ++step) {
+        if (jt) J = jt[step];
+        ptopt_sweep(&R, slot_of, B, step, spb, cls, wls, (float)(4.0 * J), (float)(1.0 - exp(-2.0 * J)), DOM_SLICE,
+                    samp);
+        for (int k = 0; k < Rn; ++k) ring_scan(&R, k, &Esum[k], &Emin[k], &tmin[k], &bond[k]);
+        for (int r = 0; r < Rn; ++r) {
+            const int k = ring_in[r];
+            if (Emin[k] < best) {
+                best = Emin[k];
+                memcpy(best_spins, R.s + ((size_t)k * P + tmin[k]) * n, (size_t)n);
+            }
+        }
+        lastb[0] = bond[ring_in[0]];
+        const double chi_on = opt_chi_raw(samp, Rn, ns, lastb, nM);
+        const double cp = jt ? opt_profile(pj, pcv, Mp, J) : -1.0;
+        const double raw = cp >= 0.0 ? cp : chi_on;
+        const double drive = raw > min_chi ? raw : min_chi;
+        jtrace[step] = J;
+        chitrace[step] = drive;
+        if (!jt) {
+            const double nj = J + eps_tilde * pow(drive, -alpha);
+            J = nj < je ? nj : je;
+        }
+        double acc = 0.0, att = 0.0;
+        if ((step + 1) % swap_interval == 0) {
+            const uint32_t w = (uint32_t)((step + 1) / swap_interval - 1);
+            for (int r = 0; r + 1 < Rn; ++r) {
+                const int a = ring_in[r], b = ring_in[r + 1];
+                const double e_aa = bp[r] * Esum[a];
+                const double e_bb = bp[r + 1] * Esum[b];
+                const double e_ab = bp[r] * Esum[b];
+                const double e_ba = bp[r + 1] * Esum[a];
+                const double delta = (e_ab + e_ba) - (e_aa + e_bb);
+                att += 1.0;
+                const float u = u01(draw(R.key, (uint32_t)r, 0u, w, DOM_SWAP, 0));
+                if (metropolis((float)(-delta), u)) {
+                    ring_in[r] = b;
+                    ring_in[r + 1] = a;
+                    slot_of[b] = r;
+                    slot_of[a] = r + 1;
+                    acc += 1.0;
+                }
+            }
+        }
+        double avg = 0.0;
+        for (int r = 0; r < Rn; ++r) avg += Emin[ring_in[r]];
+        avg_trace[step] = avg / (double)Rn;
+        swap_trace[step] = att > 0.0 ? acc / att : 0.0;
+    }
+    scalars[3] = J;
+    for (int r = 0; r < Rn; ++r) {
+        const int k = ring_in[r];
+        final_E[r] = Emin[k];
+        memcpy(final_spins + (size_t)r * n, R.s + ((size_t)k * P + tmin[k]) * n, (size_t)n);
+    }
+    *best_E = best;
+    free(jt); free(pj); free(pcv); free(samp); free(slot_of); free(ring_in); free(B); free(bp); free(Esum);
+    free(Emin); free(tmin); free(bond);
     ring_free(&R);
     return 0;
 }

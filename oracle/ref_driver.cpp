@@ -240,6 +240,31 @@ int ref_sqapt_run(void *p, const double *betas, const double *gammas, int R, int
     });
 }
 
+// SQAParallelTemperingAnnealer::run_optimal, one read (sqa_parallel_tempering.cpp:348-882).
+int ref_sqapt_opt_run(void *p, const double *betas, const double *gammas, int R, int P, int spb, int wls, int cls,
+                      int steps, int swap_interval, double eps_tilde, double alpha, double je, int probes,
+                      int csweeps, uint64_t seed, double *best_E, double *final_E, double *avg_trace,
+                      double *swap_trace, double *jtrace, double *chitrace, double *scalars) {
+    return guarded([&] {
+        auto *m = static_cast<RefModel *>(p);
+        SQAParallelTemperingAnnealer a(make_backend(BackendKind::CPU, m->ham), std::vector<double>(betas, betas + R),
+                                       std::vector<double>(gammas, gammas + R), (size_t)P);
+        a.set_seed(seed);
+        auto r = a.run_optimal((size_t)steps, (size_t)spb, (size_t)wls, eps_tilde, alpha, je, (size_t)cls,
+                               (size_t)swap_interval, 0, (size_t)probes, (size_t)csweeps, "");
+        *best_E = r.best_energy;
+        std::memcpy(final_E, r.final_energies.data(), sizeof(double) * r.final_energies.size());
+        std::memcpy(avg_trace, r.average_energy_trace.data(), sizeof(double) * steps);
+        std::memcpy(swap_trace, r.swap_acceptance_trace.data(), sizeof(double) * steps);
+        std::memcpy(jtrace, r.j_perp_trace.data(), sizeof(double) * steps);
+        std::memcpy(chitrace, r.chi_B_trace.data(), sizeof(double) * steps);
+        scalars[0] = r.calibrated_eps_tilde;
+        scalars[1] = r.j_perp_start;
+        scalars[2] = r.resolved_j_perp_end;
+        scalars[3] = r.final_j_perp;
+    });
+}
+
 // SQAChiAnnealer::run_chi, one read (sqa_chi_annealer.cpp:146-438).
 int ref_chi_run(void *p, int P, int K, double beta, double gamma_start, double gamma_end, int num_steps, int spb,
                 int scan_points, int scan_sweeps, int scan_burn, double chi_floor_fraction, double driver_A0,

@@ -20,8 +20,8 @@ QA_OK, QA_ERR_ARG, QA_ERR_CUDA, QA_ERR_OOM, QA_ERR_TIMEOUT, QA_ERR_DRIFT, QA_ERR
 EXPORTED = [
     "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy",
     "qa_problem_dense", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
-    "qa_sa_run", "qa_replica_run", "qa_sqa_run", "qa_sqa_opt_run", "qa_sqapt_run", "qa_pt_run", "qa_chi_run",
-    "qa_chi_pilot",
+    "qa_sa_run", "qa_replica_run", "qa_sqa_run", "qa_sqa_opt_run", "qa_sqapt_run", "qa_sqapt_opt_run", "qa_pt_run",
+    "qa_chi_run", "qa_chi_pilot",
     "qa_mlp_create", "qa_mlp_free", "qa_mlp_num_params", "qa_mlp_get_params", "qa_mlp_set_params",
     "qa_mlp_forward", "qa_mlp_loss_grad", "qa_mlp_train_step",
 ]
@@ -87,6 +87,19 @@ class qa_sqapt_out(C.Structure):
                 ("swap_acceptance_trace", C.c_void_p)]
 
 
+class qa_sqaptopt_params(C.Structure):
+    _fields_ = [("betas", C.c_void_p), ("gammas", C.c_void_p), ("rungs", C.c_int), ("trotter_slices", C.c_int),
+                ("continuous_time_slices", C.c_int), ("sweeps_per_step", C.c_int), ("worldline_sweeps", C.c_int),
+                ("cluster_sweeps", C.c_int), ("num_steps", C.c_int), ("swap_interval", C.c_int),
+                ("eps_tilde", C.c_double), ("alpha", C.c_double), ("j_perp_end", C.c_double),
+                ("calib_probes", C.c_int), ("calib_sweeps", C.c_int), ("reads", C.c_int), ("seed", C.c_uint64)]
+
+
+class qa_sqaptopt_out(C.Structure):
+    _fields_ = [("pt", qa_sqapt_out), ("j_perp_trace", C.c_void_p), ("chi_B_trace", C.c_void_p),
+                ("scalars", C.c_void_p)]
+
+
 class qa_chi_params(C.Structure):
     _fields_ = [("trotter_slices", C.c_int), ("replicas", C.c_int), ("beta", C.c_double),
                 ("gamma_start", C.c_double), ("gamma_end", C.c_double), ("num_steps", C.c_int),
@@ -139,6 +152,8 @@ def load():
                                      C.POINTER(qa_stats)]
         L.qa_sqapt_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sqapt_params), C.POINTER(qa_sqapt_out),
                                    C.POINTER(qa_stats)]
+        L.qa_sqapt_opt_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sqaptopt_params),
+                                       C.POINTER(qa_sqaptopt_out), C.POINTER(qa_stats)]
         L.qa_chi_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_chi_params), C.POINTER(qa_chi_out),
                                  C.POINTER(qa_stats)]
         L.qa_chi_pilot.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_chi_params), vp, C.POINTER(qa_stats)]

@@ -41,7 +41,7 @@ class AnnealResult:
 
 @dataclass
 class SQAResult:
-    """``qanneal.SQAResult`` (sqa_annealer.hpp:18-29); the run_optimal diagnostics stay empty."""
+    """``qanneal.SQAResult`` (sqa_annealer.hpp:18-29); the schedule diagnostics are filled by ``run_optimal``."""
     best_state: State
     best_energy: float
     energy_trace: List[float]
@@ -56,7 +56,7 @@ class SQAResult:
 @dataclass
 class SQAParallelTemperingResult:
     """``qanneal.SQAParallelTemperingResult`` (sqa_parallel_tempering.hpp:15-29);
-    the run_optimal diagnostics stay empty."""
+    the schedule diagnostics are filled by ``run_optimal``."""
     final_states: List[State]
     final_energies: List[float]
     best_state: State
@@ -501,6 +501,56 @@ class SQAParallelTemperingAnnealer(_Seeded):
         self.last_stats = RunStats.from_c(st)
         return [SQAParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
                                            float(bestE[r]), avg[r], swp[r])
+                for r in range(reads)]
+
+    def run_optimal(self, num_steps: int, sweeps_per_step: int, worldline_sweeps: int = 0, eps_tilde: float = 0.0,
+                    alpha: float = 15.0 / 14.0, j_perp_end: float = 0.0, cluster_sweeps: int = 0,
+                    swap_interval: int = 1, continuous_time_slices: int = 0, calib_probes: int = 12,
+                    calib_sweeps: int = 10, debug_csv_path: str = "") -> SQAParallelTemperingResult:
+        """``run_optimal`` (sqa_parallel_tempering.cpp:348-882), one read: every rung
+        at one adaptive J_perp per step, from the hottest rung's coupling to
+        ``j_perp_end`` (<= 0: the coldest rung's coupling)."""
+        res = self.run_optimal_reads(num_steps, sweeps_per_step, worldline_sweeps, eps_tilde, alpha, j_perp_end,
+                                     cluster_sweeps, swap_interval, continuous_time_slices, calib_probes,
+                                     calib_sweeps, reads=1)[0]
+        if debug_csv_path:
+            _write_opt_debug_csv(debug_csv_path, res, 0, alpha)
+        return res
+
+    def run_optimal_reads(self, num_steps: int, sweeps_per_step: int, worldline_sweeps: int = 0,
+                          eps_tilde: float = 0.0, alpha: float = 15.0 / 14.0, j_perp_end: float = 0.0,
+                          cluster_sweeps: int = 0, swap_interval: int = 1, continuous_time_slices: int = 0,
+                          calib_probes: int = 12, calib_sweeps: int = 10, reads: int = 1,
+                          seed: Optional[int] = None) -> List[SQAParallelTemperingResult]:
+        """Batched ``run_optimal``: read r keyed seed + r, all reads in one call."""
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        betas = np.ascontiguousarray(self.betas, dtype=np.float64)
+        gammas = np.ascontiguousarray(self.gammas, dtype=np.float64)
+        R = len(betas)
+        seed = self._next_seed(reads) if seed is None else int(seed)
+        prm = _lib.qa_sqaptopt_params(betas.ctypes.data, gammas.ctypes.data, R, self.trotter_slices,
+                                      int(continuous_time_slices), int(sweeps_per_step), int(worldline_sweeps),
+                                      int(cluster_sweeps), int(num_steps), int(swap_interval), float(eps_tilde),
+                                      float(alpha), float(j_perp_end), int(calib_probes), int(calib_sweeps),
+                                      int(reads), seed)
+        n, S = self.hamiltonian.size(), max(int(num_steps), 1)
+        best = np.zeros((reads, n), np.int8)
+        bestE = np.zeros(reads)
+        fin = np.zeros((reads, R, n), np.int8)
+        finE = np.zeros((reads, R))
+        avg, swp, jt, ct = np.zeros((reads, S)), np.zeros((reads, S)), np.zeros((reads, S)), np.zeros((reads, S))
+        sc = np.zeros((reads, 4))
+        pt = _lib.qa_sqapt_out(best.ctypes.data, bestE.ctypes.data, fin.ctypes.data, finE.ctypes.data,
+                               avg.ctypes.data, swp.ctypes.data)
+        o = _lib.qa_sqaptopt_out(pt, jt.ctypes.data, ct.ctypes.data, sc.ctypes.data)
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_sqapt_opt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        return [SQAParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
+                                           float(bestE[r]), avg[r], swp[r], jt[r].tolist(), ct[r].tolist(),
+                                           float(sc[r, 0]), float(sc[r, 1]), float(sc[r, 2]), float(sc[r, 3]))
                 for r in range(reads)]
 
 

@@ -1231,6 +1231,35 @@ double opt_profile(const std::vector<double> &pj, const std::vector<double> &pc,
     return pc[lo] + t * (pc[hi] - pc[lo]);
 }
 
+// The calibrated J_perp trajectory: step t of nt sits where
+// G(J) = int_js^J max(chi(J'), min_chi)^alpha dJ' (trapezoids on a 4096 grid)
+// reaches t/(nt-1) of G(je) (sqa_annealer.cpp:848-872,
+// sqa_parallel_tempering.cpp:768-794).
+std::vector<double> opt_trajectory(const std::vector<double> &pj, const std::vector<double> &pc, double js, double je,
+                                   double min_chi, double alpha, int nt) {
+    const int GRID = 4096;
+    const double h = (je - js) / (double)GRID;
+    std::vector<double> G(GRID + 1, 0.0), jt(nt);
+    double prev = std::pow(std::max(opt_profile(pj, pc, js), min_chi), alpha);
+    for (int k = 1; k <= GRID; ++k) {
+        const double Jk = js + (double)k * h;
+        const double cur = std::pow(std::max(opt_profile(pj, pc, Jk), min_chi), alpha);
+        G[k] = G[k - 1] + 0.5 * (prev + cur) * h;
+        prev = cur;
+    }
+    const double Gt = G[GRID];
+    int k = 0;
+    const double den = nt > 1 ? (double)(nt - 1) : 1.0;
+    for (int t = 0; t < nt; ++t) {
+        const double target = Gt > 0.0 ? ((double)t / den) * Gt : 0.0;
+        while (k < GRID && G[k + 1] < target) ++k;
+        const double g0 = G[k], g1 = G[k + 1];
+        const double fr = g1 > g0 ? (target - g0) / (g1 - g0) : 0.0;
+        jt[t] = js + ((double)k + fr) * h;
+    }
+    return jt;
+}
+
 }  // namespace
 
 int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqaopt_params *prm,
@@ -1443,28 +1472,7 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
             }
             eps[rd] = e;
             minchi[rd] = std::max(1e-4 * maxc, 1e-12);
-            // J trajectory: inverse of G(J) = int chi(J')^alpha dJ' on a 4096 grid (sqa_annealer.cpp:848-872)
-            const int GRID = 4096;
-            const double h = (je - js) / (double)GRID;
-            std::vector<double> G(GRID + 1, 0.0);
-            double prev = std::pow(std::max(opt_profile(pj[rd], pcv[rd], js), minchi[rd]), alpha);
-            for (int k = 1; k <= GRID; ++k) {
-                const double Jk = js + (double)k * h;
-                const double cur = std::pow(std::max(opt_profile(pj[rd], pcv[rd], Jk), minchi[rd]), alpha);
-                G[k] = G[k - 1] + 0.5 * (prev + cur) * h;
-                prev = cur;
-            }
-            const double Gt = G[GRID];
-            jtraj[rd].resize(n2);
-            int k = 0;
-            const double den = n2 > 1 ? (double)(n2 - 1) : 1.0;
-            for (int t = 0; t < n2; ++t) {
-                const double target = Gt > 0.0 ? ((double)t / den) * Gt : 0.0;
-                while (k < GRID && G[k + 1] < target) ++k;
-                const double g0 = G[k], g1 = G[k + 1];
-                const double fr = g1 > g0 ? (target - g0) / (g1 - g0) : 0.0;
-                jtraj[rd][t] = js + ((double)k + fr) * h;
-            }
+            jtraj[rd] = opt_trajectory(pj[rd], pcv[rd], js, je, minchi[rd], alpha, n2);
         }
     } else {
         for (int rd = 0; rd < reads_total; ++rd) minchi[rd] = 1e-4 * (double)problems[rd / prm->reads]->n * P;
@@ -1572,6 +1580,85 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
 }
 
 // ---------------------------------------------------------------------- SQA-PT
+// Device records of a parallel-tempering run (rec_base 1, rec_stride steps + 1).
+struct PTDev {
+    double *best, *exact, *min, *avg, *swp;
+    int *bstep, *bslot, *rin;
+    uint32_t *bits, *fbits;
+    unsigned long long *cnt;
+};
+
+// Downloads of a parallel-tempering run and the per-read outputs: the best
+// state of a read is the lowest energy, then the earliest step (the starting
+// state is step -1), then the lowest slot -- the (step, slot) scan order of
+// sqa_parallel_tempering.cpp:177-185, 299-306; final states per slot; the
+// average-energy and swap traces.  Fills the counters and times of stats.
+static int pt_collect(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, int reads, int Rn, int steps,
+                      const Layout &L, const PTDev &d, qa_sqapt_out *const *outs, qa_stats *stats, int64_t *d2h) {
+    const int nr = (int)L.rings.size(), reads_total = n_problems * reads;
+    std::vector<double> bestE(nr), exact(nr), lastmin(nr), avg((size_t)reads_total * steps),
+        swp((size_t)reads_total * steps);
+    std::vector<int> bstep(nr), bslot(nr), rin((size_t)reads_total * Rn);
+    std::vector<uint32_t> bits((size_t)nr * L.nw_max), fbits((size_t)nr * L.nw_max);
+    unsigned long long cnt[4];
+    QA_CK(cudaMemcpyAsync(bestE.data(), d.best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(exact.data(), d.exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpy2DAsync(lastmin.data(), sizeof(double), d.min + steps, sizeof(double) * (steps + 1),
+                            sizeof(double), nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(avg.data(), d.avg, sizeof(double) * avg.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(swp.data(), d.swp, sizeof(double) * swp.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bstep.data(), d.bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bslot.data(), d.bslot, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(rin.data(), d.rin, sizeof(int) * rin.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(bits.data(), d.bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(fbits.data(), d.fbits, sizeof(uint32_t) * fbits.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(cnt, d.cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    for (int p = 0; p < n_problems; ++p) {
+        const int n = problems[p]->n;
+        qa_sqapt_out &o = *outs[p];
+        for (int r = 0; r < reads; ++r) {
+            const int q = p * reads + r, base = q * Rn;
+            int kb = 0;
+            for (int k = 1; k < Rn; ++k) {
+                const int a = base + k, b = base + kb;
+                if (bestE[a] < bestE[b] || (bestE[a] == bestE[b] && (bstep[a] < bstep[b] ||
+                                                                     (bstep[a] == bstep[b] && bslot[a] < bslot[b]))))
+                    kb = k;
+            }
+            if (o.best_spins) unpack_bits(bits.data() + (size_t)(base + kb) * L.nw_max, n, o.best_spins + (size_t)r * n);
+            if (o.best_energy) o.best_energy[r] = exact[base + kb];
+            for (int s = 0; s < Rn; ++s) {
+                const int k = rin[(size_t)q * Rn + s];
+                if (o.final_energies) o.final_energies[(size_t)r * Rn + s] = lastmin[base + k];
+                if (o.final_spins)
+                    unpack_bits(fbits.data() + (size_t)(base + k) * L.nw_max, n,
+                                o.final_spins + ((size_t)r * Rn + s) * n);
+            }
+            if (o.average_energy_trace)
+                std::memcpy(o.average_energy_trace + (size_t)r * steps, avg.data() + (size_t)q * steps,
+                            sizeof(double) * steps);
+            if (o.swap_acceptance_trace)
+                std::memcpy(o.swap_acceptance_trace + (size_t)r * steps, swp.data() + (size_t)q * steps,
+                            sizeof(double) * steps);
+        }
+    }
+    if (stats) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]);
+        stats->slice_attempts = (int64_t)cnt[0];
+        stats->slice_accepts = (int64_t)cnt[1];
+        stats->worldline_attempts = (int64_t)cnt[2];
+        stats->worldline_accepts = (int64_t)cnt[3];
+        stats->sweep_ms = a;
+        stats->total_ms = b;
+    }
+    *d2h = (int64_t)(sizeof(double) * (3 * (size_t)nr + avg.size() + swp.size()) + 3 * sizeof(int) * (size_t)nr +
+                     sizeof(int) * rin.size() + sizeof(uint32_t) * 2 * bits.size() + sizeof(cnt));
+    return QA_OK;
+}
+
 // SQA-PT (qa_sqapt_run) and, with `classical`, the classical parallel
 // tempering of qa_pt_run: one slice, B = 2 beta, no Trotter term (T4 = 0,
 // J_perp = 0 in the swap action).
@@ -1700,75 +1787,354 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
     QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     (void)ring_ms;
-
-    std::vector<double> bestE(nr), exact(nr), lastmin(nr), avg((size_t)reads_total * steps),
-        swp((size_t)reads_total * steps);
-    std::vector<int> bstep(nr), bslot(nr), rin((size_t)reads_total * Rn);
-    std::vector<uint32_t> bits((size_t)nr * L.nw_max), fbits((size_t)nr * L.nw_max);
-    unsigned long long cnt[4];
-    QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpy2DAsync(lastmin.data(), sizeof(double), d_min + steps, sizeof(double) * (steps + 1),
-                            sizeof(double), nr, cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(avg.data(), d_avg, sizeof(double) * avg.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(swp.data(), d_swp, sizeof(double) * swp.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(bstep.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(bslot.data(), d_bslot, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(rin.data(), d_rin, sizeof(int) * rin.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(fbits.data(), d_fbits, sizeof(uint32_t) * fbits.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
-    QA_CK(cudaStreamSynchronize(ctx->stream));
-
-    // best of a read: lowest energy, then earliest step (the starting state is
-    // step -1), then lowest slot -- the (step, slot) scan order of
-    // sqa_parallel_tempering.cpp:177-185, 299-306
-    for (int p = 0; p < n_problems; ++p) {
-        const int n = problems[p]->n;
-        qa_sqapt_out &o = outs[p];
-        for (int r = 0; r < prm->reads; ++r) {
-            const int q = p * prm->reads + r, base = q * Rn;
-            int kb = 0;
-            for (int k = 1; k < Rn; ++k) {
-                const int a = base + k, b = base + kb;
-                if (bestE[a] < bestE[b] || (bestE[a] == bestE[b] && (bstep[a] < bstep[b] ||
-                                                                     (bstep[a] == bstep[b] && bslot[a] < bslot[b]))))
-                    kb = k;
-            }
-            if (o.best_spins) unpack_bits(bits.data() + (size_t)(base + kb) * L.nw_max, n, o.best_spins + (size_t)r * n);
-            if (o.best_energy) o.best_energy[r] = exact[base + kb];
-            for (int s = 0; s < Rn; ++s) {
-                const int k = rin[(size_t)q * Rn + s];
-                if (o.final_energies) o.final_energies[(size_t)r * Rn + s] = lastmin[base + k];
-                if (o.final_spins)
-                    unpack_bits(fbits.data() + (size_t)(base + k) * L.nw_max, n,
-                                o.final_spins + ((size_t)r * Rn + s) * n);
-            }
-            if (o.average_energy_trace)
-                std::memcpy(o.average_energy_trace + (size_t)r * steps, avg.data() + (size_t)q * steps,
-                            sizeof(double) * steps);
-            if (o.swap_acceptance_trace)
-                std::memcpy(o.swap_acceptance_trace + (size_t)r * steps, swp.data() + (size_t)q * steps,
-                            sizeof(double) * steps);
-        }
-    }
+    std::vector<qa_sqapt_out *> po(n_problems);
+    for (int p = 0; p < n_problems; ++p) po[p] = outs + p;
+    const PTDev dv{d_best, d_exact, d_min, d_avg, d_swp, d_bstep, d_bslot, d_rin, d_bits, d_fbits, d_cnt};
+    int64_t d2h = 0;
+    QA_TRY(pt_collect(ctx, problems, n_problems, prm->reads, Rn, steps, L, dv, po.data(), stats, &d2h));
     if (stats) {
-        float a = 0, b = 0;
-        cudaEventElapsedTime(&a, ctx->ev[1], ctx->ev[2]);
-        cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[3]);
-        stats->slice_attempts = (int64_t)cnt[0];
-        stats->slice_accepts = (int64_t)cnt[1];
-        stats->worldline_attempts = (int64_t)cnt[2];
-        stats->worldline_accepts = (int64_t)cnt[3];
-        stats->sweep_ms = a;
-        stats->total_ms = b;
         stats->sweep_launches = n_seg;
         stats->launches = (pl.own_fields() ? 2 : 3) + 2 * n_seg;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * Rn +
                                      2 * sizeof(double) * Rn + (sizeof(double) + 3 * sizeof(int)) * nr +
-                                     sizeof(int) * rin.size());
-        stats->d2h_bytes = (int64_t)(sizeof(double) * (3 * nr + avg.size() + swp.size()) + 3 * sizeof(int) * nr +
-                                     sizeof(int) * rin.size() + sizeof(uint32_t) * 2 * bits.size() + sizeof(cnt));
+                                     sizeof(int) * (size_t)reads_total * Rn);
+        stats->d2h_bytes = d2h;
+    }
+    return QA_OK;
+}
+
+// ---------------------------------------------------------------------- SQA-PT run_optimal
+// SQAParallelTemperingAnnealer::run_optimal (sqa_parallel_tempering.cpp:348-882).
+// Schedule tables are [read][step][slot]: rung slot r keeps B = 2 beta_r / P,
+// every slot of a step shares T4 = 4 J and JP = 1 - e^{-2J}.  Calibration
+// probes run as steps num_steps + m (slice tag OPTCAL) from the starting
+// states, which are restored afterwards; the calibrated production runs in
+// swap segments like qa_sqapt_run, the online one (eps_tilde > 0) a step per
+// launch with chi_B reduced on the host.  Swaps use the rung action with
+// J_perp = 0: the shared Trotter terms cancel (sqa_parallel_tempering.cpp:846-861).
+int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqaptopt_params *prm,
+                     qa_sqaptopt_out *outs, qa_stats *stats) {
+    QA_TRY(begin(ctx));
+    if (!prm || !outs) return fail(QA_ERR_ARG, "null params");
+    // sqa_parallel_tempering.cpp:361-366
+    if (prm->num_steps <= 0) return fail(QA_ERR_ARG, "num_steps must be > 0.");
+    if (prm->swap_interval <= 0) return fail(QA_ERR_ARG, "swap_interval must be > 0.");
+    if (prm->sweeps_per_step < 0 || prm->worldline_sweeps < 0 || prm->cluster_sweeps < 0)
+        return fail(QA_ERR_ARG, "sweep counts must be >= 0.");
+    if (prm->sweeps_per_step == 0 && prm->worldline_sweeps == 0 && prm->cluster_sweeps == 0)
+        return fail(QA_ERR_ARG, "At least one of sweeps_per_step/worldline_sweeps/cluster_sweeps must be > 0.");
+    if (prm->rungs < 2 || !prm->betas || !prm->gammas)
+        return fail(QA_ERR_ARG, "SQA parallel tempering requires >=2 beta/gamma pairs.");
+    if (prm->trotter_slices <= 0) return fail(QA_ERR_ARG, "trotter_slices must be > 0.");
+    if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
+    int kind, n_max;
+    QA_TRY(check_batch(problems, n_problems, &kind, &n_max));
+    const int P = (prm->continuous_time_slices > 0 && prm->continuous_time_slices > prm->trotter_slices)
+                      ? prm->continuous_time_slices
+                      : prm->trotter_slices;
+    const int Rn = prm->rungs, S = prm->num_steps, spb = prm->sweeps_per_step, wls = prm->worldline_sweeps,
+              cls = prm->cluster_sweeps;
+    if (cls > 0 && P > 64)
+        return fail(QA_ERR_UNSUPPORTED, "cluster_sweeps > 0 runs with at most 64 Trotter slices on the GPU.");
+    const bool calibrate = prm->eps_tilde <= 0.0;
+    const int Mp = std::max(prm->calib_probes, 2), cs = std::max(prm->calib_sweeps, 1), pc = cls;
+    const int ns = spb + cls, nsc = cs + pc, S_all = S + Mp, reads_total = n_problems * prm->reads;
+    const double alpha = prm->alpha;
+    // J_start: the hottest rung's coupling; J_end <= 0: the coldest rung's (sqa_parallel_tempering.cpp:377-398)
+    const double js = trotter_coupling(prm->betas[0], prm->gammas[0], P);
+    double je = prm->j_perp_end;
+    if (je <= 0.0) {
+        je = trotter_coupling(prm->betas[Rn - 1], prm->gammas[Rn - 1], P);
+        std::fprintf(stderr,
+                     "[qanneal run_optimal] WARNING: j_perp_end not specified; defaulted to coldest-replica "
+                     "trotter_coupling = %g (j_perp_start = %g). For benchmark runs pass an explicit j_perp_end "
+                     "(e.g. 5*j_rms).\n", je, js);
+    }
+    if (je <= js) {
+        std::fprintf(stderr,
+                     "[qanneal run_optimal] WARNING: resolved j_perp_end (%g) <= j_perp_start (%g). The adaptive "
+                     "schedule has no range to traverse and will not anneal. Installing finite ceiling "
+                     "j_perp_start + 1e6 so the run terminates by num_steps.\n", je, js);
+        je = js + 1e6;
+    }
+
+    Layout L;
+    build_rings(L, problems, n_problems, prm->reads, Rn, P, prm->seed);
+    for (auto &R : L.rings) R.sched = R.out * S_all * Rn;  // [read][step][slot]
+    const int nr = (int)L.rings.size();
+    ProbDev *d_probs;
+    RingDev *d_rings;
+    uint32_t *d_spins;
+    float *d_fields;
+    QA_TRY(upload_common(ctx, problems, n_problems, L, &d_probs, &d_rings, &d_spins, &d_fields));
+    const size_t tab = (size_t)reads_total * S_all * Rn;
+    std::vector<float> Bt(tab), T4t(tab), JPt(tab);
+    auto set_step = [&](int rd, int step, double J) {
+        const float t4 = (float)(4.0 * J), jp = (float)(1.0 - std::exp(-2.0 * J));
+        for (int r = 0; r < Rn; ++r) {
+            const size_t i = ((size_t)rd * S_all + step) * Rn + r;
+            Bt[i] = (float)(2.0 * (prm->betas[r] / (double)P));
+            T4t[i] = t4;
+            JPt[i] = jp;
+        }
+    };
+    std::vector<double> bpjp(2 * Rn, 0.0);
+    for (int r = 0; r < Rn; ++r) bpjp[r] = prm->betas[r] / (double)P;
+    float *d_B, *d_T4, *d_JP;
+    double *d_bpjp, *d_sum, *d_min, *d_best, *d_cbest, *d_exact, *d_avg, *d_swp;
+    long long *d_bond, *d_bsamp;
+    int *d_bstep, *d_cbstep, *d_bslot, *d_slot, *d_rin;
+    uint32_t *d_bits, *d_cbits, *d_fbits, *d_ssave;
+    float *d_fsave;
+    unsigned long long *d_cnt;
+    const size_t rec = (size_t)nr * (S + 1);
+    const size_t samp_per_ring = (size_t)std::max({calibrate ? Mp * nsc : 0, ns, 1});
+    QA_TRY(ws_array(ctx, W_A, tab, &d_B));
+    QA_TRY(ws_array(ctx, W_T4, tab, &d_T4));
+    QA_TRY(ws_array(ctx, W_JP, tab, &d_JP));
+    QA_TRY(ws_array(ctx, W_BPJP, 2 * Rn, &d_bpjp));
+    QA_TRY(ws_array(ctx, W_SUM, rec, &d_sum));
+    QA_TRY(ws_array(ctx, W_MIN, rec, &d_min));
+    QA_TRY(ws_array(ctx, W_BOND, rec, &d_bond));
+    QA_TRY(ws_array(ctx, W_BSAMP, (size_t)nr * samp_per_ring, &d_bsamp));
+    QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
+    QA_TRY(ws_array(ctx, W_CBESTE, nr, &d_cbest));
+    QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
+    QA_TRY(ws_array(ctx, W_CBSTEP, nr, &d_cbstep));
+    QA_TRY(ws_array(ctx, W_BSLOT, nr, &d_bslot));
+    QA_TRY(ws_array(ctx, W_SLOT, nr, &d_slot));
+    QA_TRY(ws_array(ctx, W_RIN, (size_t)reads_total * Rn, &d_rin));
+    QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
+    QA_TRY(ws_array(ctx, W_CBITS, (size_t)nr * L.nw_max, &d_cbits));
+    QA_TRY(ws_array(ctx, W_FBITS, (size_t)nr * L.nw_max, &d_fbits));
+    QA_TRY(ws_array(ctx, W_EXACT, nr, &d_exact));
+    QA_TRY(ws_array(ctx, W_AVG, (size_t)reads_total * S, &d_avg));
+    QA_TRY(ws_array(ctx, W_SWP, (size_t)reads_total * S, &d_swp));
+    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    auto upload_tables = [&]() -> int {
+        QA_CK(cudaMemcpyAsync(d_B, Bt.data(), sizeof(float) * tab, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_T4, T4t.data(), sizeof(float) * tab, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_JP, JPt.data(), sizeof(float) * tab, cudaMemcpyHostToDevice, ctx->stream));
+        return QA_OK;
+    };
+    // the rows of one step, [read] x [slot] at a pitch of S_all * Rn entries
+    auto upload_step = [&](int step) -> int {
+        const size_t pitch = sizeof(float) * S_all * Rn, off = (size_t)step * Rn, w = sizeof(float) * Rn;
+        QA_CK(cudaMemcpy2DAsync(d_B + off, pitch, Bt.data() + off, pitch, w, reads_total, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        QA_CK(cudaMemcpy2DAsync(d_T4 + off, pitch, T4t.data() + off, pitch, w, reads_total, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        QA_CK(cudaMemcpy2DAsync(d_JP + off, pitch, JPt.data() + off, pitch, w, reads_total, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        return QA_OK;
+    };
+    {
+        std::vector<double> inf(nr, INFINITY);
+        std::vector<int> neg(nr, -2), slot(nr), rin((size_t)reads_total * Rn);
+        for (int i = 0; i < nr; ++i) slot[i] = L.rings[i].k;
+        for (size_t i = 0; i < rin.size(); ++i) rin[i] = (int)(i % Rn);
+        QA_CK(cudaMemcpyAsync(d_bpjp, bpjp.data(), sizeof(double) * 2 * Rn, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_cbest, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_bstep, neg.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_cbstep, neg.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_bslot, slot.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_slot, slot.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_rin, rin.data(), sizeof(int) * rin.size(), cudaMemcpyHostToDevice, ctx->stream));
+        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+        QA_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    RingPlan pl;
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, cls > 0));
+    QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
+                      !pl.own_fields()));
+    RingParams rp{};
+    rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
+    rp.P = P; rp.steps_total = S; rp.spb = spb; rp.wls = wls; rp.cls = cls;
+    rp.slice_tag = DOM_SLICE; rp.slot = d_slot; rp.B = d_B; rp.T4 = d_T4; rp.JP = d_JP;
+    rp.per_slot_sched = 1; rp.slot_step = Rn;
+    rp.ring_sum = d_sum; rp.ring_min = d_min; rp.ring_bond = d_bond; rp.rec_base = 1; rp.rec_stride = S + 1;
+    rp.best_E = d_best; rp.best_step = d_bstep; rp.best_slot = d_bslot; rp.best_bits = d_bits;
+    rp.final_bits = d_fbits; rp.nw_max = L.nw_max; rp.counters = d_cnt;
+    PTSegParams sp{};
+    sp.rings = d_rings; sp.reads = reads_total; sp.R = Rn; sp.bp = d_bpjp; sp.jp = d_bpjp + Rn;
+    sp.ring_sum = d_sum; sp.ring_min = d_min; sp.ring_bond = d_bond; sp.rec_base = 1; sp.rec_stride = S + 1;
+    sp.ring_in = d_rin; sp.slot_of = d_slot; sp.avg_trace = d_avg; sp.swap_trace = d_swp; sp.steps_total = S;
+    QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    bool fresh = true;  // the next launch builds its fields from the spins (own-field kernels)
+    int n_launch = 0, n_seg = 0;
+    std::vector<double> jtr((size_t)reads_total * S), chitr((size_t)reads_total * S), eps(reads_total, prm->eps_tilde),
+        minchi(reads_total), Jcur(reads_total, js);
+    std::vector<std::vector<double>> pj(reads_total), pcv(reads_total), jtraj(reads_total);
+    for (int rd = 0; rd < reads_total; ++rd) minchi[rd] = 1e-4 * (double)problems[rd / prm->reads]->n * P;
+    // ---- calibration probes from the starting states, which are then restored
+    if (calibrate) {
+        QA_TRY(ws_array(ctx, W_SSAVE, (size_t)std::max<long long>(L.spin_words, 1), &d_ssave));
+        QA_TRY(ws_array(ctx, W_FSAVE, (size_t)std::max<long long>(L.field_floats, 1), &d_fsave));
+        QA_CK(cudaMemcpyAsync(d_ssave, d_spins, sizeof(uint32_t) * L.spin_words, cudaMemcpyDeviceToDevice, ctx->stream));
+        const bool fields_valid = !pl.own_fields();  // own-field kernels build theirs on their first launch
+        if (fields_valid)
+            QA_CK(cudaMemcpyAsync(d_fsave, d_fields, sizeof(float) * L.field_floats, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+        const double dJp = (je - js) / (double)Mp;
+        for (int rd = 0; rd < reads_total; ++rd)
+            for (int m = 0; m < Mp; ++m) set_step(rd, S + m, js + ((double)m + 0.5) * dJp);
+        QA_TRY(upload_tables());
+        RingParams keep = rp;
+        rp.spb = cs; rp.cls = pc; rp.wls = 0; rp.slice_tag = DOM_OPTCAL; rp.init_scan = 0;
+        rp.ring_sum = nullptr; rp.ring_min = nullptr; rp.ring_bond = nullptr;
+        rp.best_E = d_cbest; rp.best_step = d_cbstep; rp.best_slot = nullptr; rp.best_bits = d_cbits;
+        rp.final_bits = nullptr; rp.bstride = (int)samp_per_ring;
+        for (int m = 0; m < Mp; ++m) {
+            rp.step0 = S + m;
+            rp.step1 = S + m + 1;
+            rp.init_fields = fresh;
+            rp.bsamp = d_bsamp + (size_t)m * nsc;
+            QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+            fresh = false;
+            ++n_launch;
+        }
+        rp = keep;
+        std::vector<long long> hs((size_t)nr * samp_per_ring);
+        QA_CK(cudaMemcpyAsync(hs.data(), d_bsamp, sizeof(long long) * hs.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaMemcpyAsync(d_spins, d_ssave, sizeof(uint32_t) * L.spin_words, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (fields_valid)
+            QA_CK(cudaMemcpyAsync(d_fields, d_fsave, sizeof(float) * L.field_floats, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+        fresh = true;
+        QA_CK(cudaStreamSynchronize(ctx->stream));
+        for (int rd = 0; rd < reads_total; ++rd) {
+            const double nM = (double)problems[rd / prm->reads]->n * (double)P;
+            pj[rd].resize(Mp);
+            pcv[rd].resize(Mp);
+            double integral = 0.0, maxc = 0.0;
+            for (int m = 0; m < Mp; ++m) {
+                // Rn >= 2 rings and nsc >= 1 samples each: the one-sample fallback never applies
+                double chi = opt_chi_raw(hs.data() + (size_t)rd * Rn * samp_per_ring + (size_t)m * nsc, Rn, nsc,
+                                         samp_per_ring, 0, nM);
+                if (!(chi > 0.0)) chi = 0.0;
+                pj[rd][m] = js + ((double)m + 0.5) * dJp;
+                pcv[rd][m] = chi;
+                integral += std::pow(std::max(chi, 1e-12), alpha) * dJp;
+                maxc = std::max(maxc, chi);
+            }
+            double e = integral / (double)S;
+            if (!(e > 0.0) || !std::isfinite(e)) {
+                e = std::max(je - js, 0.0) / (double)S;
+                if (!(e > 0.0)) e = 1e-9;
+            }
+            eps[rd] = e;
+            minchi[rd] = std::max(1e-4 * maxc, 1e-12);
+            jtraj[rd] = opt_trajectory(pj[rd], pcv[rd], js, je, minchi[rd], alpha, S);
+        }
+    }
+    // ---- production
+    if (calibrate) {
+        for (int rd = 0; rd < reads_total; ++rd) {
+            for (int s = 0; s < S; ++s) {
+                const double J = jtraj[rd][s];
+                set_step(rd, s, J);
+                jtr[(size_t)rd * S + s] = J;
+                chitr[(size_t)rd * S + s] = std::max(opt_profile(pj[rd], pcv[rd], J), minchi[rd]);
+            }
+            Jcur[rd] = jtraj[rd][S - 1];
+        }
+        QA_TRY(upload_tables());
+        for (int s0 = 0; s0 < S;) {
+            const int s1 = std::min({S, (s0 / prm->swap_interval + 1) * prm->swap_interval, s0 + 256});
+            rp.step0 = s0;
+            rp.step1 = s1;
+            rp.init_scan = s0 == 0;
+            rp.init_fields = fresh;
+            QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+            fresh = false;
+            ++n_launch;
+            sp.s0 = s0;
+            sp.s1 = s1;
+            sp.swap = s1 % prm->swap_interval == 0;
+            sp.round = (uint32_t)(s1 / prm->swap_interval - 1);
+            pt_segment_kernel<<<(reads_total + 127) / 128, 128, 0, ctx->stream>>>(sp);
+            QA_CK(cudaGetLastError());
+            ++n_seg;
+            s0 = s1;
+        }
+    } else {
+        std::vector<long long> hs((size_t)nr * std::max(ns, 1)), hb(nr);
+        std::vector<int> rin_prev((size_t)reads_total * Rn);
+        for (size_t i = 0; i < rin_prev.size(); ++i) rin_prev[i] = (int)(i % Rn);
+        rp.bstride = (int)samp_per_ring;
+        for (int s = 0; s < S; ++s) {
+            for (int rd = 0; rd < reads_total; ++rd) set_step(rd, s, Jcur[rd]);
+            QA_TRY(upload_step(s));
+            rp.step0 = s;
+            rp.step1 = s + 1;
+            rp.init_scan = s == 0;
+            rp.init_fields = fresh;
+            rp.bsamp = ns > 0 ? d_bsamp : nullptr;
+            QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+            fresh = false;
+            ++n_launch;
+            if (ns > 0)
+                QA_CK(cudaMemcpy2DAsync(hs.data(), sizeof(long long) * ns, d_bsamp, sizeof(long long) * samp_per_ring,
+                                        sizeof(long long) * ns, nr, cudaMemcpyDeviceToHost, ctx->stream));
+            else
+                QA_CK(cudaMemcpy2DAsync(hb.data(), sizeof(long long), d_bond + 1 + s, sizeof(long long) * (S + 1),
+                                        sizeof(long long), nr, cudaMemcpyDeviceToHost, ctx->stream));
+            sp.s0 = s;
+            sp.s1 = s + 1;
+            sp.swap = (s + 1) % prm->swap_interval == 0;
+            sp.round = (uint32_t)((s + 1) / prm->swap_interval - 1);
+            pt_segment_kernel<<<(reads_total + 127) / 128, 128, 0, ctx->stream>>>(sp);
+            QA_CK(cudaGetLastError());
+            ++n_seg;
+            QA_CK(cudaStreamSynchronize(ctx->stream));
+            for (int rd = 0; rd < reads_total; ++rd) {
+                const double nM = (double)problems[rd / prm->reads]->n * (double)P;
+                // the fallback reads the bond sum of the ring in slot 0 before this step's swaps
+                const long long b0 = ns > 0 ? 0 : hb[(size_t)rd * Rn + rin_prev[(size_t)rd * Rn]];
+                const double on = opt_chi_raw(hs.data() + (size_t)rd * Rn * std::max(ns, 1), Rn, ns,
+                                              (size_t)std::max(ns, 1), b0, nM);
+                const double drive = std::max(on, minchi[rd]);
+                jtr[(size_t)rd * S + s] = Jcur[rd];
+                chitr[(size_t)rd * S + s] = drive;
+                Jcur[rd] = std::min(Jcur[rd] + eps[rd] * std::pow(drive, -alpha), je);
+            }
+            if (ns == 0) {
+                QA_CK(cudaMemcpyAsync(rin_prev.data(), d_rin, sizeof(int) * rin_prev.size(), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+                QA_CK(cudaStreamSynchronize(ctx->stream));
+            }
+        }
+    }
+    QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
+    QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    std::vector<qa_sqapt_out *> po(n_problems);
+    for (int p = 0; p < n_problems; ++p) po[p] = &outs[p].pt;
+    const PTDev dv{d_best, d_exact, d_min, d_avg, d_swp, d_bstep, d_bslot, d_rin, d_bits, d_fbits, d_cnt};
+    int64_t d2h = 0;
+    QA_TRY(pt_collect(ctx, problems, n_problems, prm->reads, Rn, S, L, dv, po.data(), stats, &d2h));
+    for (int p = 0; p < n_problems; ++p) {
+        qa_sqaptopt_out &o = outs[p];
+        for (int r = 0; r < prm->reads; ++r) {
+            const int rd = p * prm->reads + r;
+            if (o.j_perp_trace) std::memcpy(o.j_perp_trace + (size_t)r * S, jtr.data() + (size_t)rd * S, sizeof(double) * S);
+            if (o.chi_B_trace) std::memcpy(o.chi_B_trace + (size_t)r * S, chitr.data() + (size_t)rd * S, sizeof(double) * S);
+            if (o.scalars) {
+                double *sc = o.scalars + (size_t)r * 4;
+                sc[0] = eps[rd];
+                sc[1] = js;
+                sc[2] = je;
+                sc[3] = Jcur[rd];
+            }
+        }
+    }
+    if (stats) {
+        stats->sweep_launches = n_launch;
+        stats->launches = (pl.own_fields() ? 2 : 3) + n_launch + n_seg;
+        stats->h2d_bytes = 0;
+        stats->d2h_bytes = d2h;
     }
     return QA_OK;
 }

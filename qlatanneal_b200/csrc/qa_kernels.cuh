@@ -46,12 +46,13 @@ struct RingParams {
     int spb, wls;         // slice / worldline sweeps per step
     uint32_t slice_tag;   // DOM_SLICE, DOM_PROD or DOM_PILOT|(point<<8)
     const int *slot;      // PT: rung slot of each ring (null: slot = k)
-    const float *B, *T4;  // [sched + step] (PT: [sched + slot]): B = 2 beta/P, T4 = 4 J_perp
+    const float *B, *T4;  // [sched + step] (PT: [sched + slot + step * slot_step]): B = 2 beta/P, T4 = 4 J_perp
     int cls;              // cluster sweeps per step (ring_kernel only; P <= 64)
     const float *JP;      // like B: bond probability 1 - exp(-2 J_perp) of the cluster moves
     long long *bsamp;     // bond sum after every slice and cluster sweep, or null:
     int bstride;          //   [ring * bstride + (step - step0) * (spb + cls) + sweep]
-    int per_slot_sched;   // 1: index A/T4 by slot instead of step
+    int per_slot_sched;   // 1: index B/T4/JP by slot (+ step * slot_step) instead of step
+    int slot_step;        //   0: one entry per slot; R: a row of R slots per step (one J_perp per step)
     int smem_fields;
     int init_fields;      // ring_pm1_kernel: build the int32 fields from the spins first
     int init_scan;        // score the starting state as "step -1" before step0 (PT)
@@ -430,7 +431,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     for (int step = p.step0 - (p.init_scan ? 1 : 0); step < p.step1; ++step) {
         // step -1 (init_scan) only scores the starting state
         const int spb = step >= 0 ? p.spb : 0, wls = step >= 0 ? p.wls : 0;
-        const int si_tab = R.sched + (p.per_slot_sched ? slot : max(step, 0));
+        const int si_tab = R.sched + (p.per_slot_sched ? slot + max(step, 0) * p.slot_step : max(step, 0));
         const float B = p.B[si_tab], T4 = p.T4[si_tab];
         for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);

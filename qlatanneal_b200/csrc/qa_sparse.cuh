@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
     for (int step = p.step0 - (p.init_scan ? 1 : 0); step < p.step1; ++step) {
         // step -1 (init_scan) only scores the starting state
         const int spb = step >= 0 ? p.spb : 0, wls = step >= 0 ? p.wls : 0;
-        const int si_tab = R.sched + (p.per_slot_sched ? slot : max(step, 0));
+        const int si_tab = R.sched + (p.per_slot_sched ? slot + max(step, 0) * p.slot_step : max(step, 0));
         const float B = p.B[si_tab], T4 = p.T4[si_tab];
         for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);

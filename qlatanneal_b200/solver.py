@@ -16,7 +16,7 @@ from typing import Any, Iterable, List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from .annealers import Annealer, SQAAnnealer, SQAChiAnnealer, SQAParallelTemperingAnnealer
+from .annealers import Annealer, SQAAnnealer, SQAChiAnnealer, SQAParallelTemperingAnnealer, _write_opt_debug_csv
 from .models import AnnealSchedule, DenseIsing, HigherOrderIsing, QUBO, SparseIsing, SQASchedule
 
 try:
@@ -267,9 +267,6 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
                          "leave schedule_type='standard' and use the chi_* parameters.")
     if method == "ctpimc":
         raise NotImplementedError("method='ctpimc' stays on qanneal's CPU path (not part of the sweep engine).")
-    if schedule_type == "optimal" and method == "sqapt":
-        raise NotImplementedError("schedule_type='optimal' with method='sqapt' (SQAParallelTemperingAnnealer."
-                                  "run_optimal) is not part of the CUDA sweep engine.")
     if logger is None:
         logger = logging.getLogger("qlatanneal_b200.solve")
     if reads <= 0:
@@ -292,9 +289,8 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
     if progress and reads > 1:
         logger.info("Running %d reads in one batched GPU call...", reads)
 
-    if method == "sqa" and schedule_type == "optimal":
-        # solver.py:616-645 and 686-702: beta / J_perp range resolved once, then
-        # run_optimal per read (read r keyed seed + r).
+    if schedule_type == "optimal" and method in ("sqa", "sqapt"):
+        # solver.py:616-645: beta / J_perp range / step budget resolved once
         auto_beta, auto_jps, auto_jpe = optimal_j_perp_params(ising, trotter_slices=trotter_slices)
         beta = float(optimal_beta) if optimal_beta is not None else auto_beta
         jps = float(optimal_j_perp_start) if optimal_j_perp_start is not None else auto_jps
@@ -310,9 +306,12 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
                                    "a problem with larger j_rms.", 5.0 * jrms, jps)
             else:
                 jpe = auto_jpe
-        steps = int(optimal_num_steps) if optimal_num_steps is not None else max(100, len(schedule.betas))
+        opt_steps = int(optimal_num_steps) if optimal_num_steps is not None else max(100, len(schedule.betas))
+
+    if method == "sqa" and schedule_type == "optimal":
+        # solver.py:686-702: run_optimal per read (read r keyed seed + r)
         ann = SQAAnnealer(ising, schedule, trotter_slices, replicas, backend=backend)
-        res = ann.run_optimal_reads(beta, jps, jpe, optimal_eps_tilde, optimal_alpha, steps, sweeps_per_beta,
+        res = ann.run_optimal_reads(beta, jps, jpe, optimal_eps_tilde, optimal_alpha, opt_steps, sweeps_per_beta,
                                     worldline_sweeps, cluster_sweeps, int(optimal_calib_probes),
                                     int(optimal_calib_sweeps), float(optimal_beta_ramp_fraction), reads=reads,
                                     seed=seed)
@@ -334,8 +333,14 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
             ladder = auto_ladder_sqa_tuned(ising, replicas=max(2, replicas))
             lb, lg = ladder.betas, ladder.gammas
         ann = SQAParallelTemperingAnnealer(ising, lb, lg, trotter_slices, backend=backend)
-        res = ann.run_reads(sweeps_per_beta, worldline_sweeps, pt_steps, swap_interval, cluster_sweeps,
-                            continuous_time_slices, reads=reads, seed=seed)
+        if schedule_type == "optimal":
+            # solver.py:718-735: J_perp runs from the ladder's hottest coupling to jpe
+            res = ann.run_optimal_reads(opt_steps, sweeps_per_beta, worldline_sweeps, optimal_eps_tilde,
+                                        optimal_alpha, jpe, cluster_sweeps, swap_interval, continuous_time_slices,
+                                        int(optimal_calib_probes), int(optimal_calib_sweeps), reads=reads, seed=seed)
+        else:
+            res = ann.run_reads(sweeps_per_beta, worldline_sweeps, pt_steps, swap_interval, cluster_sweeps,
+                                continuous_time_slices, reads=reads, seed=seed)
         traces = [r.average_energy_trace for r in res]
     elif method == "sqa_chi":
         beta = float(optimal_beta) if optimal_beta is not None else optimal_j_perp_params(
@@ -361,6 +366,12 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
         res = ann.run_reads(sweeps_per_beta, reads=reads, seed=seed)
         traces = [r.energy_trace for r in res]
 
+    if optimal_debug_csv and schedule_type == "optimal" and method in ("sqa", "sqapt"):
+        # each read of the reference rewrites the file: the last read's rows remain
+        n1 = 0
+        if method == "sqa" and optimal_beta_ramp_fraction > 0.0:
+            n1 = min(int(optimal_beta_ramp_fraction * opt_steps), opt_steps - 1)
+        _write_opt_debug_csv(optimal_debug_csv, res[-1], n1, optimal_alpha)
     samples, energies = [], []
     for r in res:
         spins = r.best_state.as_array().astype(int)

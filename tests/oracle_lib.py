@@ -85,6 +85,9 @@ class Oracle:
         L.or_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double), _f8p, _i8p, _f8p, _f8p, _i64p,
                                    C.c_int]
+        L.or_sqapt_opt_run.argtypes = ([C.c_void_p, _f8p, _f8p] + [C.c_int] * 7 + [C.c_double] * 3 +
+                                       [C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double), _f8p,
+                                        _i8p] + [_f8p] * 5)
         L.or_chi_schedule.argtypes = ([C.c_int, _f8p, _f8p, _f8p] + [C.c_double] * 4 + [C.c_int, C.c_int] +
                                       [C.c_double] * 3 + [_f8p] * 4)
         L.or_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 3 + [C.c_int] * 5 +
@@ -257,6 +260,22 @@ class Oracle:
                             fE, fs, avg, swp, cnt, cls)
         return best, E.value, fE, fs.reshape(R, m.n), avg, swp, cnt
 
+    def sqapt_opt_run(self, m, betas, gammas, P, spb, wls, cls, steps, swap_interval, eps, alpha, je, probes,
+                      csweeps, seed, read=0):
+        """SQA-PT run_optimal read (P = resolved slice count)."""
+        betas, gammas = _c64(betas), _c64(gammas)
+        R = len(betas)
+        best = np.zeros(m.n, np.int8)
+        E = C.c_double()
+        fE, fs = np.zeros(R), np.zeros(R * m.n, np.int8)
+        avg, swp, jt, ct, sc = np.zeros(steps), np.zeros(steps), np.zeros(steps), np.zeros(steps), np.zeros(4)
+        rc = self.L.or_sqapt_opt_run(m.h, betas, gammas, R, P, spb, wls, cls, steps, swap_interval, eps, alpha, je,
+                                     probes, csweeps, seed, read, best, C.byref(E), fE, fs, avg, swp, jt, ct, sc)
+        if rc != 0:
+            raise ValueError("run_optimal arguments rejected")
+        return dict(best=best, best_energy=E.value, final_E=fE, final_spins=fs.reshape(R, m.n), avg=avg, swap=swp,
+                    j_perp=jt, chi=ct, scalars=sc)
+
 
 class Ref:
     """The unmodified qanneal classes (compiled from the reference sources)."""
@@ -294,6 +313,8 @@ class Ref:
                                                        _f8p, _f8p, _f8p, _f8p])
         L.ref_sqapt_run.argtypes = [C.c_void_p, _f8p, _f8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                     C.c_uint64, _i8p, C.POINTER(C.c_double), _f8p, _f8p, _f8p, C.c_int]
+        L.ref_sqapt_opt_run.argtypes = ([C.c_void_p, _f8p, _f8p] + [C.c_int] * 7 + [C.c_double] * 3 +
+                                        [C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_double)] + [_f8p] * 6)
         L.ref_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                    C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                    C.c_uint64, _i8p, C.POINTER(C.c_double)] + [_f8p] * 8)
@@ -441,6 +462,19 @@ class RefModel:
         if rc != 0:
             raise ValueError(self.ref.L.ref_last_error().decode())
         return best, E.value, fE, avg, swp
+
+    def sqapt_opt_run(self, betas, gammas, P, spb, wls, cls, steps, swap_interval, eps, alpha, je, probes, csweeps,
+                      seed):
+        betas, gammas = _c64(betas), _c64(gammas)
+        R = len(betas)
+        E = C.c_double()
+        fE, avg, swp, jt, ct, sc = (np.zeros(R), np.zeros(steps), np.zeros(steps), np.zeros(steps), np.zeros(steps),
+                                    np.zeros(4))
+        rc = self.ref.L.ref_sqapt_opt_run(self.h, betas, gammas, R, P, spb, wls, cls, steps, swap_interval, eps, alpha,
+                                          je, probes, csweeps, seed, C.byref(E), fE, avg, swp, jt, ct, sc)
+        if rc != 0:
+            raise ValueError(self.ref.L.ref_last_error().decode())
+        return dict(best_energy=E.value, final_E=fE, avg=avg, swap=swp, j_perp=jt, chi=ct, scalars=sc)
 
     def batch_run(self, method, betas, gammas, steps, P, K, spb, wls, reads, seed, threads):
         out = np.zeros(reads)

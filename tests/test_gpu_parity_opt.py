@@ -102,3 +102,76 @@ def test_solve_optimal_sqa():
     assert len(r.trace) == 30
     one = qa.solve(d, method="sqa", schedule_type="optimal", reads=1, seed=12, **kw)
     assert one.energies[0] == r.energies[1]
+
+
+PTOPT_CASES = [
+    # kind, n, rungs, P, sweeps/step, worldline, cluster, steps, swap interval, eps_tilde, J_end, continuous slices
+    ("dense", 64, 4, 8, 2, 1, 0, 24, 1, 0.0, 2.0, 0),
+    ("dense", 48, 3, 16, 1, 1, 1, 20, 2, 0.0, 2.5, 0),
+    ("dense", 40, 3, 4, 1, 0, 0, 12, 1, 0.0, 0.0, 10),
+    ("dense", 40, 3, 8, 0, 2, 0, 12, 1, 0.05, 2.0, 0),
+    ("dense", 40, 3, 8, 1, 0, 0, 10, 1, 0.0, 0.5, 0),
+    ("dense_h", 70, 4, 6, 1, 0, 0, 18, 3, 0.03, 2.0, 0),
+    ("sparse", 128, 4, 8, 1, 1, 0, 20, 1, 0.0, 0.0, 0),
+    ("sparse_real", 96, 3, 6, 1, 1, 1, 16, 2, 0.02, 2.0, 0),
+    ("hubo", 48, 3, 4, 1, 1, 1, 16, 2, 0.0, 2.0, 0),
+    ("hubo_real", 40, 3, 6, 1, 0, 0, 14, 1, 0.0, 2.0, 0),
+]
+
+
+@pytest.mark.parametrize("kind,n,R,P,spb,wls,cls,steps,swap,eps,je,cts", PTOPT_CASES)
+def test_sqapt_run_optimal_bit_exact(oracle, kind, n, R, P, spb, wls, cls, steps, swap, eps, je, cts):
+    """SQAParallelTemperingAnnealer.run_optimal (sqa_parallel_tempering.cpp:348-882)
+    on the GPU equals the oracle: best and final states, traces, J_perp and chi_B."""
+    model = make(kind, n, 67)
+    om = oracle_model(oracle, model)
+    betas, gammas = np.geomspace(0.5, 3.0, R), np.geomspace(2.0, 0.3, R)
+    alpha, probes, csweeps = 15.0 / 14.0, 5, 3
+    reads, seed = 3, 919
+    ann = qa.SQAParallelTemperingAnnealer(model, betas, gammas, P)
+    res = ann.run_optimal_reads(steps, spb, wls, eps, alpha, je, cls, swap, cts, probes, csweeps, reads=reads,
+                                seed=seed)
+    Pr = cts if cts > P else P
+    swaps = 0.0
+    for r in range(reads):
+        o = oracle.sqapt_opt_run(om, betas, gammas, Pr, spb, wls, cls, steps, swap, eps, alpha, je, probes, csweeps,
+                                 seed, r)
+        np.testing.assert_array_equal(res[r].best_state.as_array(), o["best"])
+        if kind in REAL_KINDS:
+            assert res[r].best_energy == pytest.approx(oracle.energy64(om, o["best"]), rel=1e-12, abs=1e-12)
+        else:
+            assert res[r].best_energy == o["best_energy"]
+        np.testing.assert_array_equal(np.asarray(res[r].final_energies), o["final_E"])
+        for k in range(R):
+            np.testing.assert_array_equal(res[r].final_states[k].as_array(), o["final_spins"][k])
+        np.testing.assert_array_equal(np.asarray(res[r].average_energy_trace), o["avg"])
+        np.testing.assert_array_equal(np.asarray(res[r].swap_acceptance_trace), o["swap"])
+        np.testing.assert_array_equal(np.asarray(res[r].j_perp_trace), o["j_perp"])
+        np.testing.assert_array_equal(np.asarray(res[r].chi_B_trace), o["chi"])
+        sc = o["scalars"]
+        assert (res[r].calibrated_eps_tilde, res[r].j_perp_start, res[r].resolved_j_perp_end,
+                res[r].final_j_perp) == (sc[0], sc[1], sc[2], sc[3])
+        swaps += float(np.sum(o["swap"]))
+    if kind == "dense":
+        assert swaps > 0.0  # the SK ladders exchange rungs; the other instances need not
+
+
+def test_sqapt_run_optimal_errors_and_solve():
+    h, J = sk_dense(30, 2)
+    d = qa.DenseIsing(h, J)
+    ann = qa.SQAParallelTemperingAnnealer(d, [0.5, 2.0], [2.0, 0.5], 4)
+    with pytest.raises(ValueError):
+        ann.run_optimal(0, 1)
+    with pytest.raises(ValueError):
+        ann.run_optimal(5, 1, swap_interval=0)
+    with pytest.raises(ValueError):
+        ann.run_optimal(5, 0, 0, cluster_sweeps=0)
+    with pytest.raises(NotImplementedError):
+        qa.SQAParallelTemperingAnnealer(d, [0.5, 2.0], [2.0, 0.5], 65).run_optimal(4, 1, cluster_sweeps=1)
+    kw = dict(trotter_slices=8, sweeps_per_beta=1, worldline_sweeps=1, replicas=3, optimal_num_steps=20,
+              optimal_calib_probes=4, optimal_calib_sweeps=2)
+    r = qa.solve(d, method="sqapt", schedule_type="optimal", reads=3, seed=5, **kw)
+    assert r.best_energy == min(r.energies) and len(r.trace) == 20
+    assert r.best_energy == pytest.approx(d.energy(r.best_sample), abs=1e-9)
+    one = qa.solve(d, method="sqapt", schedule_type="optimal", reads=1, seed=7, **kw)
+    assert one.energies[0] == r.energies[2]

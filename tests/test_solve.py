@@ -41,8 +41,6 @@ def test_normalize_problem_forms():
         qa.solve(qa.DenseIsing(np.zeros(2), np.zeros((2, 2))), return_bits=True)
     with pytest.raises(NotImplementedError):
         qa.solve(Q, method="ctpimc")
-    with pytest.raises(NotImplementedError):
-        qa.solve(Q, method="sqapt", schedule_type="optimal")
 
 
 @pytest.mark.gpu
