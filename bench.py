@@ -546,7 +546,9 @@ def main():
         m2.release()
         e2e_times.append(time.perf_counter() - t0)
         st = a2.last_stats
-        h2d = n * 12 + n * n * 12 + st.h2d_bytes
+        # model: h (float32 + float64) and J (float64); the float32 mirror of J
+        # and the +-1 bit rows are derived on the device
+        h2d = n * 12 + n * n * 8 + st.h2d_bytes
         d2h = st.d2h_bytes
     barrier()
     t = torch.tensor([sum(e2e_times)], dtype=torch.float64, device=dev)

@@ -66,6 +66,14 @@ QA_API int qa_destroy(qa_ctx *ctx);
  * DenseIsing::energy (dense_ising.cpp:29-44). */
 QA_API int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, double c, qa_problem **out);
 
+/* QUBO(Q, n).to_ising() (qubo.cpp:33-69) built on the device: Q is the n*n
+ * row-major float64 matrix on the host; W = (Q + Q^T)/2, J = W/2, h = W.1/2
+ * are formed by device kernels straight into the problem's device block, the
+ * constant c = tr(W)/4 + 1^T W 1/4 (one running sum, the reference's order) on
+ * the host meanwhile.  The result is the DenseIsing the reference converts to,
+ * bit for bit.  h_out [n] and c_out (either may be NULL) receive h and c. */
+QA_API int qa_problem_qubo(qa_ctx *ctx, int n, const double *Q, double *h_out, double *c_out, qa_problem **out);
+
 /* SparseIsing(h, edges, n, c) (sparse_ising.hpp:22-25); edge e couples ei[e], ej[e]
  * with weight w[e]; self-edges are rejected (sparse_ising.cpp:29-31). */
 QA_API int qa_problem_sparse(qa_ctx *ctx, int n, const double *h, int m, const int64_t *ei, const int64_t *ej,

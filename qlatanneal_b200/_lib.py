@@ -19,7 +19,7 @@ QA_OK, QA_ERR_ARG, QA_ERR_CUDA, QA_ERR_OOM, QA_ERR_TIMEOUT, QA_ERR_DRIFT, QA_ERR
 # Every symbol include/qa_gpu.h declares (checked by the CPU test suite).
 EXPORTED = [
     "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy",
-    "qa_problem_dense", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
+    "qa_problem_dense", "qa_problem_qubo", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
     "qa_sa_run", "qa_replica_run", "qa_sqa_run", "qa_sqa_opt_run", "qa_sqapt_run", "qa_sqapt_opt_run", "qa_pt_run",
     "qa_chi_run", "qa_chi_pilot",
     "qa_mlp_create", "qa_mlp_free", "qa_mlp_num_params", "qa_mlp_get_params", "qa_mlp_set_params",
@@ -136,6 +136,7 @@ def load():
         L.qa_create.argtypes = [C.POINTER(vp), i]
         L.qa_destroy.argtypes = [vp]
         L.qa_problem_dense.argtypes = [vp, i, vp, vp, d, C.POINTER(vp)]
+        L.qa_problem_qubo.argtypes = [vp, i, vp, vp, vp, C.POINTER(vp)]
         L.qa_problem_sparse.argtypes = [vp, i, vp, i, vp, vp, vp, d, C.POINTER(vp)]
         L.qa_problem_hubo.argtypes = [vp, i, vp, i, vp, vp, vp, d, C.POINTER(vp)]
         L.qa_problem_free.argtypes = [vp]

@@ -19,6 +19,7 @@
 #include "qa_sparse.cuh"
 #include "qa_pm1.cuh"
 #include "qa_pt.cuh"
+#include "qa_ingest.cuh"
 
 using namespace qa;
 
@@ -106,7 +107,8 @@ struct qa_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int smem_optin = 0;
-    DevBuf ws[32];
+    static constexpr int kWsSlots = 48;
+    DevBuf ws[kWsSlots];
 };
 
 struct qa_mlp {
@@ -133,6 +135,8 @@ struct qa_problem {
     // built, then sent with one copy into one device block; fix = (offset,
     // device pointer to patch)
     std::vector<std::pair<size_t, const void **>> fix;
+    // arrays the device fills after the block exists: (bytes, pointer to patch)
+    std::vector<std::pair<size_t, const void **>> resv;
     std::shared_ptr<BlockPool> pool;  // where the block goes back
     void *block = nullptr;
     size_t block_bytes = 0;
@@ -142,7 +146,8 @@ namespace {
 
 enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
               W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP, W_JP,
-              W_BSAMP, W_SSAVE, W_FSAVE, W_CBESTE, W_CBSTEP, W_CBITS, W_CBOND };
+              W_BSAMP, W_SSAVE, W_FSAVE, W_CBESTE, W_CBSTEP, W_CBITS, W_CBOND, W_FLAG, W_QSTAGE, W_COUNT };
+static_assert(W_COUNT <= qa_ctx::kWsSlots, "qa_ctx::ws has a slot per WsSlot");
 
 int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
     DevBuf &b = ctx->ws[slot];
@@ -171,6 +176,12 @@ T *stage_array(qa_problem *P, size_t count, const T **dev) {
     return reinterpret_cast<T *>(st.data() + off);
 }
 
+// Space in the problem's device block for an array the device writes itself.
+template <class T>
+void reserve_array(qa_problem *P, size_t count, const T **dev) {
+    P->resv.push_back({std::max<size_t>(count * sizeof(T), 16), reinterpret_cast<const void **>(dev)});
+}
+
 template <class T>
 int upload(qa_problem *P, const T *host, size_t count, const T **dev) {
     T *dst = stage_array(P, count, dev);
@@ -184,7 +195,8 @@ int begin(qa_ctx *ctx) {
     return QA_OK;
 }
 
-// Sends the staged arrays (one allocation, one copy) and sets the scalars.
+// Sends the staged arrays (one allocation, one copy; the reserved arrays follow
+// them in the block, uncopied) and sets the scalars.
 int finish_problem(qa_problem *P) {
     P->dev.kind = P->kind;
     P->dev.n = P->n;
@@ -193,7 +205,15 @@ int finish_problem(qa_problem *P) {
     P->dev.m = P->m;
     P->dev.c = P->c;
     std::vector<unsigned char> &st = P->ctx->stage;
-    const size_t bytes = std::max<size_t>(st.size(), 16);
+    if (P->fix.empty()) st.clear();  // nothing staged for this problem
+    std::vector<size_t> roff;
+    size_t end = st.size();
+    for (auto &r : P->resv) {
+        end = (end + 255) & ~(size_t)255;
+        roff.push_back(end);
+        end += r.first;
+    }
+    const size_t bytes = std::max<size_t>(end, 16);
     P->pool = P->ctx->pool;
     size_t got = 0;
     void *d = P->pool->take(bytes, &got);
@@ -208,16 +228,20 @@ int finish_problem(qa_problem *P) {
     }
     P->block = d;
     P->block_bytes = got;
-    const cudaError_t e = cudaMemcpy(d, st.data(), st.size(), cudaMemcpyHostToDevice);
+    const cudaError_t e = st.empty() ? cudaSuccess : cudaMemcpy(d, st.data(), st.size(), cudaMemcpyHostToDevice);
     st.clear();
     if (e != cudaSuccess) {
         P->fix.clear();
+        P->resv.clear();
         return fail(QA_ERR_CUDA, cudaGetErrorString(e));
     }
     for (auto &f : P->fix) *f.second = static_cast<unsigned char *>(d) + f.first;
+    for (size_t k = 0; k < P->resv.size(); ++k) *P->resv[k].second = static_cast<unsigned char *>(d) + roff[k];
     P->fix.clear();
+    P->resv.clear();
     return QA_OK;
 }
+
 
 int common_h(qa_problem *P, const double *h) {
     std::vector<float> h32(P->n);
@@ -650,6 +674,25 @@ int qa_problem_size(const qa_problem *p, int *n) {
     return QA_OK;
 }
 
+// The device-derived dense arrays (J32, and Jw when every upper coupling is
+// +-1) from the J64 already in the block; one flag read back decides Jw.
+static int derive_dense(qa_problem *P) {
+    qa_ctx *ctx = P->ctx;
+    const int n = P->n, nw = (n + 31) / 32, np = pm1_npad(n);
+    int *d_flag;
+    QA_TRY(ws_array(ctx, W_FLAG, 1, &d_flag));
+    QA_CK(cudaMemsetAsync(d_flag, 0, sizeof(int), ctx->stream));
+    QA_CK(cudaMemsetAsync(const_cast<uint32_t *>(P->dev.Jw), 0, sizeof(uint32_t) * (size_t)nw * np, ctx->stream));
+    dense_derive_kernel<<<dim3(nw, nw), dim3(kIngestTile, 8), 0, ctx->stream>>>(
+        P->dev.J64, n, const_cast<float *>(P->dev.J32), const_cast<uint32_t *>(P->dev.Jw), np, d_flag);
+    QA_CK(cudaGetLastError());
+    int not_pm1 = 0;
+    QA_CK(cudaMemcpyAsync(&not_pm1, d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    if (not_pm1) P->dev.Jw = nullptr;
+    return QA_OK;
+}
+
 int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, double c, qa_problem **out) {
     QA_TRY(begin(ctx));
     if (!out) return fail(QA_ERR_ARG, "null output pointer");
@@ -662,41 +705,76 @@ int qa_problem_dense(qa_ctx *ctx, int n, const double *h, const double *J, doubl
     P->n = n;
     P->nw = (n + 31) / 32;
     P->c = c;
-    // the upper triangle defines J (DenseIsing::energy reads i < j), mirrored
+    // J64 as given; the float32 mirror of its upper triangle (DenseIsing::energy
+    // reads i < j) and the +-1 bit rows are derived on the device
     int rc = common_h(P, h);
     if (rc == QA_OK) rc = upload(P, J, (size_t)n * n, &P->dev.J64);
-    // J32 is written straight into the staging buffer: the upper triangle
-    // defines J (DenseIsing::energy reads i < j), mirrored, zero diagonal
-    float *J32 = stage_array(P, (size_t)n * n, &P->dev.J32);
-    bool pm1 = true;  // couplings all in {-1,+1}: bit-packed rows for ring_pm1_kernel
-    for (int i = 0; i < n; ++i) {
-        J32[(size_t)i * n + i] = 0.0f;
-        for (int j = i + 1; j < n; ++j) {
-            const double v = J[(size_t)i * n + j];
-            pm1 = pm1 && (v == 1.0 || v == -1.0);
-            J32[(size_t)i * n + j] = J32[(size_t)j * n + i] = (float)v;
-        }
+    if (rc == QA_OK) {
+        reserve_array(P, (size_t)n * n, &P->dev.J32);
+        reserve_array(P, (size_t)P->nw * pm1_npad(n), &P->dev.Jw);
+        rc = finish_problem(P);
     }
-    if (pm1) {
-        const int nw = (n + 31) / 32, np = pm1_npad(n);
-        std::vector<uint32_t> Jw((size_t)nw * np, 0u);
-        for (int m = 0; m < n; ++m) {
-            const float *row = J32 + (size_t)m * n;  // read before the next staging call moves the buffer
-            for (int q = 0; q < nw; ++q) {
-                uint32_t word = 0;
-                const int j1 = std::min(n, 32 * q + 32);
-                for (int j = 32 * q; j < j1; ++j)
-                    if (j != m && row[j] > 0.0f) word |= 1u << (j & 31);
-                Jw[(size_t)q * np + m] = word;
-            }
-        }
-        if (rc == QA_OK) rc = upload(P, Jw.data(), Jw.size(), &P->dev.Jw);
-    }
+    if (rc == QA_OK) rc = derive_dense(P);
     if (rc != QA_OK) {
         qa_problem_free(P);
         return rc;
     }
-    rc = finish_problem(P);
+    *out = P;
+    return QA_OK;
+}
+
+int qa_problem_qubo(qa_ctx *ctx, int n, const double *Q, double *h_out, double *c_out, qa_problem **out) {
+    QA_TRY(begin(ctx));
+    if (!out) return fail(QA_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    if (n <= 0) return fail(QA_ERR_ARG, "QUBO size must be > 0.");
+    if (!Q) return fail(QA_ERR_ARG, "QUBO matrix must not be null.");
+    qa_problem *P = new qa_problem();
+    P->ctx = ctx;
+    P->kind = K_DENSE;
+    P->n = n;
+    P->nw = (n + 31) / 32;
+    reserve_array(P, (size_t)n, &P->dev.h32);
+    reserve_array(P, (size_t)n, &P->dev.h64);
+    reserve_array(P, (size_t)n * n, &P->dev.J64);
+    reserve_array(P, (size_t)n * n, &P->dev.J32);
+    reserve_array(P, (size_t)P->nw * pm1_npad(n), &P->dev.Jw);
+    int rc = finish_problem(P);
+    double *d_Q = nullptr;
+    if (rc == QA_OK) rc = ws_array(ctx, W_QSTAGE, (size_t)n * n, &d_Q);
+    if (rc == QA_OK) {
+        const cudaError_t e = cudaMemcpyAsync(d_Q, Q, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice,
+                                              ctx->stream);
+        if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (rc == QA_OK) {
+        qubo_rows_kernel<<<(n + kIngestTile - 1) / kIngestTile, dim3(kIngestTile, 8), 0, ctx->stream>>>(
+            d_Q, n, const_cast<double *>(P->dev.J64), const_cast<double *>(P->dev.h64),
+            const_cast<float *>(P->dev.h32));
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (rc == QA_OK) {
+        // c = sum_i (W[i][i]/4 + sum_j W[i][j]/4), the single running sum of
+        // qubo.cpp:57-66, on the host while the device builds the arrays
+        double c = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double *qi = Q + (size_t)i * n;
+            const double wii = 0.5 * (qi[i] + qi[i]);
+            c += 0.25 * wii;
+            for (int j = 0; j < n; ++j) {
+                const double w = 0.5 * (qi[j] + Q[(size_t)j * n + i]);
+                c += 0.25 * w;
+            }
+        }
+        P->c = P->dev.c = c;
+        if (c_out) *c_out = c;
+        rc = derive_dense(P);
+    }
+    if (rc == QA_OK && h_out) {
+        const cudaError_t e = cudaMemcpy(h_out, P->dev.h64, sizeof(double) * n, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, cudaGetErrorString(e));
+    }
     if (rc != QA_OK) {
         qa_problem_free(P);
         return rc;

@@ -122,7 +122,7 @@ struct ProbDev {
     const int *incptr, *incterm, *tptr, *tvars;
     const float *coef32;
     const double *coef64;
-    // dense with every coupling in {-1,+1}: bit-packed rows, Jw[q*n + m] =
+    // dense with every coupling in {-1,+1}: bit-packed rows, Jw[q*np + m] =
     // bits J[m][32q .. 32q+31] (1 = +1; diagonal and padding bits 0); else null
     const uint32_t *Jw;
     // hubo with every term of degree <= 4: the field updates of a flip of

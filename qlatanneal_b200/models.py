@@ -93,8 +93,24 @@ class DenseIsing(_DeviceModel):
             raise ValueError("h vector length mismatch.")
         if n == 0:
             raise ValueError("DenseIsing size must be > 0.")
-        self._h, self._J, self._c, self._n = h, J, float(c), n
+        self._h, self._Jm, self._c, self._n = h, J, float(c), n
         self._upper_cache = None
+
+    @classmethod
+    def _device_built(cls, n: int, h: np.ndarray, c: float, J_fn, device: int, handle) -> "DenseIsing":
+        """A model whose device copy was built on the GPU (``handle``); the host
+        coupling matrix is formed by ``J_fn`` only when something asks for it."""
+        self = cls.__new__(cls)
+        self._h, self._Jm, self._J_fn, self._c, self._n = h, None, J_fn, float(c), int(n)
+        self._upper_cache = None
+        self.__dict__["_dev"] = {device: handle}
+        return self
+
+    @property
+    def _J(self) -> np.ndarray:
+        if self._Jm is None:
+            self._Jm = np.ascontiguousarray(self._J_fn(), dtype=np.float64)
+        return self._Jm
 
     @property
     def _upper(self) -> np.ndarray:
@@ -257,6 +273,21 @@ class QUBO:
         seq = np.concatenate([0.25 * np.diag(W)[:, None], 0.25 * W], axis=1).reshape(-1)
         c = float(np.cumsum(seq)[-1])
         return DenseIsing(h, J, c)
+
+    def to_ising_device(self, device: int = None) -> DenseIsing:
+        """``to_ising()`` with the conversion on the GPU (``qa_problem_qubo``): Q
+        goes to the device once, W, J and h are formed there straight into the
+        model's device copy, c on the host meanwhile.  The model equals
+        ``to_ising()`` bit for bit; its host coupling matrix is built only if
+        asked for (``couplings()``, ``energy()``)."""
+        eng = _lib.Engine.get(device)
+        Q = self._Q
+        n = Q.shape[0]
+        h = np.zeros(n, dtype=np.float64)
+        c = C.c_double()
+        out = C.c_void_p()
+        _lib.check(eng.L.qa_problem_qubo(eng.h, n, _lib.ptr(Q), _lib.ptr(h), C.byref(c), C.byref(out)))
+        return DenseIsing._device_built(n, h, c.value, lambda: 0.5 * (0.5 * (Q + Q.T)), eng.device, out)
 
 
 def _consolidate(n: int, raw: Iterable[Tuple[Sequence[int], float]], c: float):

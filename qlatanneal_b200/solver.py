@@ -106,12 +106,16 @@ def _is_higher_order_keys(keys: Iterable[Any]) -> bool:
     return False
 
 
-def _normalize_problem(problem: Any, n: Optional[int] = None) -> Tuple[Any, List[Any], bool]:
-    """(ising, var_order, returns_bits) for the input forms of solver.py:284-335."""
+def _normalize_problem(problem: Any, n: Optional[int] = None, convert=None) -> Tuple[Any, List[Any], bool]:
+    """(ising, var_order, returns_bits) for the input forms of solver.py:284-335.
+    ``convert`` turns a QUBO into its Ising model (default ``QUBO.to_ising``;
+    ``solve`` passes ``QUBO.to_ising_device``)."""
+    if convert is None:
+        convert = QUBO.to_ising
     if isinstance(problem, (DenseIsing, SparseIsing, HigherOrderIsing)):
         return problem, list(range(problem.size())), False
     if isinstance(problem, QUBO):
-        return problem.to_ising(), list(range(problem.size())), True
+        return convert(problem), list(range(problem.size())), True
     if nx is not None and isinstance(problem, nx.Graph):
         nodes = list(problem.nodes())
         idx = {v: i for i, v in enumerate(nodes)}
@@ -122,9 +126,9 @@ def _normalize_problem(problem: Any, n: Optional[int] = None) -> Tuple[Any, List
             w = float(d.get("weight", 0.0))
             Q[idx[u], idx[v]] += w
             Q[idx[v], idx[u]] += w
-        return QUBO(Q).to_ising(), nodes, True
+        return convert(QUBO(Q)), nodes, True
     if isinstance(problem, np.ndarray):
-        return QUBO(problem).to_ising(), list(range(problem.shape[0])), True
+        return convert(QUBO(problem)), list(range(problem.shape[0])), True
     if isinstance(problem, dict):
         if _is_higher_order_keys(problem.keys()):
             size = n
@@ -133,12 +137,12 @@ def _normalize_problem(problem: Any, n: Optional[int] = None) -> Tuple[Any, List
             return HigherOrderIsing(problem, size), list(range(size)), False
         if n is None:
             n = _guess_n([(i, j, float(v)) for (i, j), v in problem.items()])
-        return QUBO(problem, n).to_ising(), list(range(n)), True
+        return convert(QUBO(problem, n)), list(range(n)), True
     if isinstance(problem, (list, tuple)) and problem and isinstance(problem[0], (list, tuple)):
         entries = [(int(e[0]), int(e[1]), float(e[2])) for e in problem]
         if n is None:
             n = _guess_n(entries)
-        return QUBO(entries, n).to_ising(), list(range(n)), True
+        return convert(QUBO(entries, n)), list(range(n)), True
     raise ValueError("Unsupported problem type. Provide QUBO, DenseIsing, SparseIsing, HigherOrderIsing, "
                      "networkx graph, ndarray, dict, or entries list.")
 
@@ -272,7 +276,8 @@ def solve(problem: Any, method: str = "sqa", reads: int = 1, sweeps_per_beta: in
     if reads <= 0:
         raise ValueError("reads must be > 0.")
 
-    ising, var_order, is_qubo = _normalize_problem(problem, n=n)
+    # QUBO inputs are converted on the GPU, straight into the model's device copy
+    ising, var_order, is_qubo = _normalize_problem(problem, n=n, convert=lambda q: q.to_ising_device())
     if return_bits and not is_qubo:
         raise ValueError("return_bits=True requires a QUBO-type input (QUBO, ndarray, dict, entries list, or "
                          "networkx graph). DenseIsing and SparseIsing use Ising spins {-1, +1}; set "
