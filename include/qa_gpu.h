@@ -199,6 +199,38 @@ typedef struct {
 QA_API int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
                           const qa_sqaopt_params *params, qa_sqaopt_out *outs, qa_stats *stats);
 
+/* ---- observers: Annealer::run / SQAAnnealer::run with an observer
+ *      (annealer.cpp:48-71, sqa_annealer.cpp:318-473) --------------------------
+ * The run is the same as qa_sa_run / qa_sqa_run (identical results); the sweep
+ * kernels also write a strided trace into a device buffer, read back once at
+ * the end.  A sweep is recorded when its index within its phase of the step is
+ * a multiple of stride.  Every output pointer may be NULL (not recorded). */
+typedef struct {
+    int stride;              /* >= 1 */
+    int8_t *states;          /* [reads][steps][rps][n] the state after each recorded sweep, rps = ceil(sweeps_per_beta/stride) */
+    double *energies;        /* [reads][steps][rps] the running energy after each recorded sweep */
+    int8_t *step_states;     /* [reads][steps][n] the state at each step end */
+    double *magnetization;   /* [reads][steps] mean spin at each step end */
+} qa_sa_trace;
+
+QA_API int qa_sa_trace_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *params,
+                           const qa_sa_trace *traces, qa_run_out *outs, qa_stats *stats);
+
+/* rps = ceil(sweeps_per_beta/stride) + ceil(cluster_sweeps/stride) + ceil(worldline_sweeps/stride); the
+ * records of a step are the slice, then the cluster, then the worldline sweeps. */
+typedef struct {
+    int stride;              /* >= 1 */
+    int8_t *ring_states;     /* [reads][replicas][steps][rps][P][n] each replica after each recorded sweep */
+    double *ring_energies;   /* [reads][replicas][steps][rps][P] its slice energies */
+    int8_t *step_states;     /* [reads][replicas][steps + 1][P][n] each replica at the start (0) and each step end */
+    double *step_energies;   /* [reads][replicas][steps + 1][P] */
+    double *magnetization;   /* [reads][steps] mean spin over replicas, slices and spins at each step end */
+} qa_sqa_trace;
+
+QA_API int qa_sqa_trace_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
+                            const qa_sqa_params *params, const qa_sqa_trace *traces, qa_run_out *outs,
+                            qa_stats *stats);
+
 /* ---- SQA parallel tempering: SQAParallelTemperingAnnealer::run
  *      (sqa_parallel_tempering.cpp:81-346) ----------------------------------
  * rungs (beta_r, Gamma_r) pairs, one Trotter ring per rung, swaps of

@@ -537,6 +537,34 @@ static double trotter_coupling(double beta, double gamma, int P) {
 /* mag_trace (nullable): magnetisation after each step (ReplicaAnnealer,
    replica_annealer.cpp:119-131); best_step (nullable): the step whose sweeps
    last lowered the best energy, -1 for the starting state. */
+/* Sweep traces for the observer tests (annealer.cpp:48-71,
+   sqa_annealer.cpp:318-473): set before one run, cleared with stride 0.
+   SA: the state and running energy after every recorded sweep
+   ([steps][rps][n], [steps][rps]), the state at each step end (end_states,
+   [steps][n]) and the magnetisation per step.  SQA: per
+   ring the bits and slice energies after every recorded sweep
+   ([K][steps][rps][P][n], [K][steps][rps][P]; records of a step: slice,
+   cluster, worldline sweeps), at the start and each step end
+   ([K][steps+1][P][n], [K][steps+1][P]), and the magnetisation over all rings
+   per step.  A sweep is recorded when its index in its phase is a multiple
+   of stride. */
+static struct {
+    int stride;
+    int8_t *states, *ring_states, *end_states;
+    double *energies, *ring_E, *end_E, *mag;
+} g_tr;
+
+OR_EXPORT void or_trace_set(int stride, int8_t *states, double *energies, int8_t *ring_states, double *ring_E,
+                            int8_t *end_states, double *end_E, double *mag) {
+    g_tr.stride = stride;
+    g_tr.states = states; g_tr.energies = energies;
+    g_tr.ring_states = ring_states; g_tr.ring_E = ring_E;
+    g_tr.end_states = end_states; g_tr.end_E = end_E;
+    g_tr.mag = mag;
+}
+
+static int tr_count(int sweeps) { return g_tr.stride > 0 ? (sweeps + g_tr.stride - 1) / g_tr.stride : 0; }
+
 OR_EXPORT int or_sa_run(const or_model *M, const double *betas, int steps, int spb, uint64_t seed, int read,
                         int8_t *best_spins, double *best_E, double *trace, int64_t *counters, double *mag_trace,
                         int *best_step) {
@@ -571,12 +599,19 @@ OR_EXPORT int or_sa_run(const or_model *M, const double *betas, int steps, int s
                     if (E < best) { best = E; bstep = step; memcpy(best_spins, s, (size_t)n); }
                 }
             }
+            if (g_tr.stride > 0 && sw % g_tr.stride == 0) {
+                const size_t rec = (size_t)step * tr_count(spb) + (size_t)(sw / g_tr.stride);
+                if (g_tr.states) memcpy(g_tr.states + rec * n, s, (size_t)n);
+                if (g_tr.energies) g_tr.energies[rec] = E;
+            }
         }
         trace[step] = E;
-        if (mag_trace) {
+        if (g_tr.stride > 0 && g_tr.end_states) memcpy(g_tr.end_states + (size_t)step * n, s, (size_t)n);
+        if (mag_trace || (g_tr.stride > 0 && g_tr.mag)) {
             long long m = 0;
             for (int i = 0; i < n; ++i) m += s[i];
-            mag_trace[step] = (double)m / (double)n;
+            if (mag_trace) mag_trace[step] = (double)m / (double)n;
+            if (g_tr.stride > 0 && g_tr.mag) g_tr.mag[step] = (double)m / (double)n;
         }
     }
     *best_E = best;
@@ -781,17 +816,51 @@ OR_EXPORT int or_sqa_run(const or_model *M, const double *betas, const double *g
     int8_t *rstate = (int8_t *)malloc((size_t)K * n);
     double *rsum = (double *)malloc(sizeof(double) * (size_t)K);
     for (int k = 0; k < K; ++k) { rbest[k] = INFINITY; rstep[k] = -1; }
+    const int tr_s = tr_count(spb), tr_c = tr_count(cls), rps = tr_s + tr_c + tr_count(wls);
+    /* ring k's bits and slice energies into trace record rec (of records of P*n and P) */
+    #define TR_RING(STATES, ENERGIES, K_, REC)                                                       \
+        do {                                                                                         \
+            const size_t rec_ = (REC);                                                               \
+            if (STATES) memcpy((STATES) + rec_ * P * n, R.s + (size_t)(K_) * P * n, (size_t)P * n);  \
+            if (ENERGIES)                                                                            \
+                for (int t_ = 0; t_ < P; ++t_) (ENERGIES)[rec_ * P + t_] = cell_energy(&R, (K_) * P + t_); \
+        } while (0)
+    if (g_tr.stride > 0)
+        for (int k = 0; k < K; ++k) TR_RING(g_tr.end_states, g_tr.end_E, k, (size_t)k * (steps + 1));
     for (int step = 0; step < steps; ++step) {
         float B, T4;
         step_consts(betas[step], gammas[step], P, &B, &T4);
-        for (int sw = 0; sw < spb; ++sw) slice_sweep(&R, (uint32_t)(step * spb + sw), DOM_SLICE, B, T4, NULL);
+        for (int sw = 0; sw < spb; ++sw) {
+            slice_sweep(&R, (uint32_t)(step * spb + sw), DOM_SLICE, B, T4, NULL);
+            if (g_tr.stride > 0 && sw % g_tr.stride == 0)
+                for (int k = 0; k < K; ++k)
+                    TR_RING(g_tr.ring_states, g_tr.ring_E, k,
+                            ((size_t)k * steps + step) * rps + (size_t)(sw / g_tr.stride));
+        }
         if (cls > 0) {
             const float JP = join_prob(betas[step], gammas[step], P);
             for (int sw = 0; sw < cls; ++sw)
-                for (int k = 0; k < K; ++k) cluster_sweep(&R, k, (uint32_t)k, (uint32_t)(step * cls + sw), B, T4, JP);
+                for (int k = 0; k < K; ++k) {
+                    cluster_sweep(&R, k, (uint32_t)k, (uint32_t)(step * cls + sw), B, T4, JP);
+                    if (g_tr.stride > 0 && sw % g_tr.stride == 0)
+                        TR_RING(g_tr.ring_states, g_tr.ring_E, k,
+                                ((size_t)k * steps + step) * rps + (size_t)(tr_s + sw / g_tr.stride));
+                }
         }
         for (int sw = 0; sw < wls; ++sw)
-            for (int k = 0; k < K; ++k) worldline_sweep(&R, k, (uint32_t)k, (uint32_t)(step * wls + sw), B);
+            for (int k = 0; k < K; ++k) {
+                worldline_sweep(&R, k, (uint32_t)k, (uint32_t)(step * wls + sw), B);
+                if (g_tr.stride > 0 && sw % g_tr.stride == 0)
+                    TR_RING(g_tr.ring_states, g_tr.ring_E, k,
+                            ((size_t)k * steps + step) * rps + (size_t)(tr_s + tr_c + sw / g_tr.stride));
+            }
+        if (g_tr.stride > 0) {
+            long long m = 0;
+            for (size_t c = 0; c < (size_t)K * P * n; ++c) m += R.s[c];
+            if (g_tr.mag) g_tr.mag[step] = (double)m / (double)((size_t)K * P * n);
+            for (int k = 0; k < K; ++k)
+                TR_RING(g_tr.end_states, g_tr.end_E, k, (size_t)k * (steps + 1) + step + 1);
+        }
         for (int k = 0; k < K; ++k) {
             double sum = 0.0, emin = INFINITY;
             int tmin = 0;
@@ -823,6 +892,8 @@ OR_EXPORT int or_sqa_run(const or_model *M, const double *betas, const double *g
     ring_free(&R);
     return 0;
 }
+
+#undef TR_RING
 
 /* Step-end scan of one ring: sum and minimum of the slice energies, the
    slice of the minimum, and the imaginary-time bond sum

@@ -32,6 +32,16 @@ from .annealers import (  # noqa: F401
     SQAParallelTemperingAnnealer,
     SQAChiAnnealer,
 )
+from .observers import (  # noqa: F401
+    Observer,
+    SweepObserver,
+    MetricsObserver,
+    StateTraceObserver,
+    SQAObserver,
+    SQASweepObserver,
+    SQAMetricsObserver,
+    SQAStateTraceObserver,
+)
 
 from .solver import (  # noqa: F401
     SolveResult,

@@ -20,7 +20,7 @@ QA_OK, QA_ERR_ARG, QA_ERR_CUDA, QA_ERR_OOM, QA_ERR_TIMEOUT, QA_ERR_DRIFT, QA_ERR
 EXPORTED = [
     "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy",
     "qa_problem_dense", "qa_problem_qubo", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
-    "qa_sa_run", "qa_replica_run", "qa_sqa_run", "qa_sqa_opt_run", "qa_sqapt_run", "qa_sqapt_opt_run", "qa_pt_run",
+    "qa_sa_run", "qa_sa_trace_run", "qa_replica_run", "qa_sqa_run", "qa_sqa_trace_run", "qa_sqa_opt_run", "qa_sqapt_run", "qa_sqapt_opt_run", "qa_pt_run",
     "qa_chi_run", "qa_chi_pilot",
     "qa_mlp_create", "qa_mlp_free", "qa_mlp_num_params", "qa_mlp_get_params", "qa_mlp_set_params",
     "qa_mlp_forward", "qa_mlp_loss_grad", "qa_mlp_train_step",
@@ -41,6 +41,16 @@ class qa_stats(C.Structure):
 class qa_sa_params(C.Structure):
     _fields_ = [("betas", C.c_void_p), ("steps", C.c_int), ("sweeps_per_beta", C.c_int), ("reads", C.c_int),
                 ("seed", C.c_uint64)]
+
+
+class qa_sa_trace(C.Structure):
+    _fields_ = [("stride", C.c_int), ("states", C.c_void_p), ("energies", C.c_void_p),
+                ("step_states", C.c_void_p), ("magnetization", C.c_void_p)]
+
+
+class qa_sqa_trace(C.Structure):
+    _fields_ = [("stride", C.c_int), ("ring_states", C.c_void_p), ("ring_energies", C.c_void_p),
+                ("step_states", C.c_void_p), ("step_energies", C.c_void_p), ("magnetization", C.c_void_p)]
 
 
 class qa_replica_out(C.Structure):
@@ -143,6 +153,10 @@ def load():
         L.qa_problem_size.argtypes = [vp, C.POINTER(i)]
         L.qa_sa_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sa_params), C.POINTER(qa_run_out),
                                 C.POINTER(qa_stats)]
+        L.qa_sa_trace_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sa_params), C.POINTER(qa_sa_trace),
+                                      C.POINTER(qa_run_out), C.POINTER(qa_stats)]
+        L.qa_sqa_trace_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sqa_params), C.POINTER(qa_sqa_trace),
+                                       C.POINTER(qa_run_out), C.POINTER(qa_stats)]
         L.qa_replica_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_sa_params), C.POINTER(qa_replica_out),
                                      C.POINTER(qa_stats)]
         L.qa_pt_run.argtypes = [vp, C.POINTER(vp), i, C.POINTER(qa_pt_params), C.POINTER(qa_sqapt_out),

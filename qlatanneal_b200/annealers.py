@@ -211,8 +211,35 @@ class Annealer(_Seeded):
 
     def run(self, sweeps_per_beta: int, observer=None) -> AnnealResult:
         if observer is not None:
-            raise NotImplementedError("observers are not supported by the CUDA sweep engine.")
+            return self._run_observed(sweeps_per_beta, observer)
         return self.run_reads(sweeps_per_beta, reads=1)[0]
+
+    def _run_observed(self, sweeps_per_beta: int, observer) -> AnnealResult:
+        """annealer.cpp:48-71: the kernel records the sweeps; the observer is
+        then called in the reference's order.  Same result as ``run``."""
+        from .observers import observer_stride, replay_sa
+        if sweeps_per_beta <= 0:
+            raise ValueError("sweeps_per_beta must be > 0.")
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        betas = np.ascontiguousarray(self.schedule.betas, dtype=np.float64)
+        S, n, spb = len(betas), self.hamiltonian.size(), int(sweeps_per_beta)
+        stride = observer_stride(observer)
+        rps = -(-spb // stride)
+        sweeps = hasattr(observer, "record_sweep")
+        states = np.zeros((S, rps, n), np.int8) if sweeps else None
+        energies = np.zeros((S, rps)) if sweeps else None
+        step_states = np.zeros((S, n), np.int8)
+        tr = _lib.qa_sa_trace(stride, _lib.ptr(states), _lib.ptr(energies), _lib.ptr(step_states), None)
+        seed = self._next_seed(1)
+        prm = _lib.qa_sa_params(betas.ctypes.data, S, spb, 1, seed)
+        o, spins, energy, trace = _outs(n, 1, S)
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_sa_trace_run(eng.h, probs, 1, C.byref(prm), C.byref(tr), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        replay_sa(observer, betas, spb, stride, trace[0], energies, states, step_states, State)
+        return AnnealResult(State(spins[0]), float(energy[0]), trace[0])
 
     def run_reads(self, sweeps_per_beta: int, reads: int, seed: Optional[int] = None) -> List[AnnealResult]:
         if sweeps_per_beta <= 0:
@@ -358,8 +385,41 @@ class SQAAnnealer(_Seeded):
     def run(self, sweeps_per_beta: int, worldline_sweeps: int, cluster_sweeps: int = 0,
             continuous_time_slices: int = 0, observer=None) -> SQAResult:
         if observer is not None:
-            raise NotImplementedError("observers are not supported by the CUDA sweep engine.")
+            return self._run_observed(sweeps_per_beta, worldline_sweeps, cluster_sweeps, continuous_time_slices,
+                                      observer)
         return self.run_reads(sweeps_per_beta, worldline_sweeps, cluster_sweeps, continuous_time_slices, reads=1)[0]
+
+    def _run_observed(self, spb: int, wls: int, cls: int, cts: int, observer) -> SQAResult:
+        """sqa_annealer.cpp:318-473: the ring kernel records every replica's
+        sweeps and step ends; the observer is then called in the reference's
+        order.  Same result as ``run``."""
+        from .observers import observer_stride, replay_sqa
+        eng = _lib.Engine.get(self.device)
+        prob = self.hamiltonian._device_problem(eng)
+        betas = np.ascontiguousarray(self.schedule.betas, dtype=np.float64)
+        gammas = np.ascontiguousarray(self.schedule.gammas, dtype=np.float64)
+        S, n, K = len(betas), self.hamiltonian.size(), self.replicas
+        P = cts if (cts > 0 and cts > self.trotter_slices) else self.trotter_slices
+        stride = observer_stride(observer)
+        rps = -(-int(spb) // stride) + -(-int(cls) // stride) + -(-int(wls) // stride)
+        sweeps = hasattr(observer, "record_sweep")
+        ring_states = np.zeros((K, S, rps, P, n), np.int8) if sweeps else None
+        ring_E = np.zeros((K, S, rps, P)) if sweeps else None
+        step_states = np.zeros((K, S + 1, P, n), np.int8)
+        step_E = np.zeros((K, S + 1, P)) if sweeps else None
+        tr = _lib.qa_sqa_trace(stride, _lib.ptr(ring_states), _lib.ptr(ring_E), _lib.ptr(step_states),
+                               _lib.ptr(step_E), None)
+        seed = self._next_seed(1)
+        prm = _lib.qa_sqa_params(betas.ctypes.data, gammas.ctypes.data, S, self.trotter_slices, K, int(spb),
+                                 int(wls), int(cls), int(cts), 1, seed)
+        o, spins, energy, trace = _outs(n, 1, S)
+        st = _lib.qa_stats()
+        probs = (C.c_void_p * 1)(prob)
+        _lib.check(eng.L.qa_sqa_trace_run(eng.h, probs, 1, C.byref(prm), C.byref(tr), C.byref(o), C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        replay_sqa(observer, betas, gammas, P, K, int(spb), int(cls), int(wls), stride, trace[0], ring_states,
+                   ring_E, step_states, step_E)
+        return SQAResult(State(spins[0]), float(energy[0]), trace[0])
 
     def run_reads(self, sweeps_per_beta: int, worldline_sweeps: int, cluster_sweeps: int = 0,
                   continuous_time_slices: int = 0, reads: int = 1, seed: Optional[int] = None) -> List[SQAResult]:

@@ -146,7 +146,8 @@ namespace {
 
 enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
               W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP, W_JP,
-              W_BSAMP, W_SSAVE, W_FSAVE, W_CBESTE, W_CBSTEP, W_CBITS, W_CBOND, W_FLAG, W_QSTAGE, W_COUNT };
+              W_BSAMP, W_SSAVE, W_FSAVE, W_CBESTE, W_CBSTEP, W_CBITS, W_CBOND, W_FLAG, W_QSTAGE,
+              W_TRB, W_TRE, W_TREB, W_TREE, W_RSPIN, W_COUNT };
 static_assert(W_COUNT <= qa_ctx::kWsSlots, "qa_ctx::ws has a slot per WsSlot");
 
 int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
@@ -228,7 +229,11 @@ int finish_problem(qa_problem *P) {
     }
     P->block = d;
     P->block_bytes = got;
-    const cudaError_t e = st.empty() ? cudaSuccess : cudaMemcpy(d, st.data(), st.size(), cudaMemcpyHostToDevice);
+    // on the context's stream (non-blocking): every later use of the block,
+    // the device-side derivations first, is ordered after the copy; a
+    // pageable source is staged before the call returns, so the buffer is free
+    const cudaError_t e =
+        st.empty() ? cudaSuccess : cudaMemcpyAsync(d, st.data(), st.size(), cudaMemcpyHostToDevice, P->ctx->stream);
     st.clear();
     if (e != cudaSuccess) {
         P->fix.clear();
@@ -772,7 +777,8 @@ int qa_problem_qubo(qa_ctx *ctx, int n, const double *Q, double *h_out, double *
         rc = derive_dense(P);
     }
     if (rc == QA_OK && h_out) {
-        const cudaError_t e = cudaMemcpy(h_out, P->dev.h64, sizeof(double) * n, cudaMemcpyDeviceToHost);
+        cudaError_t e = cudaMemcpyAsync(h_out, P->dev.h64, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, cudaGetErrorString(e));
     }
     if (rc != QA_OK) {
@@ -965,9 +971,15 @@ int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int6
 // SA reads (qa_sa_run) and SA replicas (qa_replica_run, which adds the
 // magnetisation trace and the step of each replica's best).
 static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *prm,
-                   qa_run_out *outs, qa_stats *stats, double *const *mag_out, int32_t *const *bstep_out) {
+                   qa_run_out *outs, qa_stats *stats, double *const *mag_out, int32_t *const *bstep_out,
+                   const qa_sa_trace *traces = nullptr) {
     QA_TRY(begin(ctx));
     if (!prm) return fail(QA_ERR_ARG, "null params");
+    const int stride = traces && n_problems > 0 ? traces[0].stride : 1;
+    if (traces)
+        for (int p = 0; p < n_problems; ++p)
+            if (traces[p].stride != stride || stride < 1)
+                return fail(QA_ERR_ARG, "trace stride must be >= 1 and the same for every problem.");
     if (prm->steps <= 0 || !prm->betas) return fail(QA_ERR_ARG, "Schedule must contain at least one beta.");
     if (prm->sweeps_per_beta <= 0) return fail(QA_ERR_ARG, "sweeps_per_beta must be > 0.");
     if (prm->reads <= 0) return fail(QA_ERR_ARG, "reads must be > 0.");
@@ -1002,15 +1014,37 @@ static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
     double *d_mag = nullptr;
     int *d_bstep = nullptr;
-    if (mag_out) {
+    bool want_mag = mag_out != nullptr, want_states = false, want_end = false;
+    for (int p = 0; traces && p < n_problems; ++p) {
+        want_mag = want_mag || traces[p].magnetization;
+        want_states = want_states || traces[p].states || traces[p].energies;
+        want_end = want_end || traces[p].step_states;
+    }
+    if (want_mag) {
         QA_TRY(ws_get(ctx, W_MAG, sizeof(double) * (size_t)nr * prm->steps, &v));
         d_mag = static_cast<double *>(v);
+    }
+    if (mag_out) {
         QA_TRY(ws_get(ctx, W_BESTSTEP, sizeof(int) * nr, &v));
         d_bstep = static_cast<int *>(v);
     }
+    const int rps = (prm->sweeps_per_beta + stride - 1) / stride;
+    const size_t n_rec = (size_t)nr * prm->steps * rps;
+    const size_t n_end = want_end ? (size_t)nr * prm->steps : 0;
+    uint32_t *d_trb = nullptr, *d_treb = nullptr;
+    double *d_tre = nullptr;
+    if ((want_states ? n_rec * ((size_t)L.nw_max * 4 + 8) : 0) + n_end * L.nw_max * 4 > ((size_t)4 << 30))
+        return fail(QA_ERR_ARG, "sweep trace over 4 GiB: raise the stride or trace fewer reads.");
+    if (want_states) {
+        QA_TRY(ws_array(ctx, W_TRB, n_rec * L.nw_max, &d_trb));
+        QA_TRY(ws_array(ctx, W_TRE, n_rec, &d_tre));
+    }
+    if (want_end) QA_TRY(ws_array(ctx, W_TREB, n_end * L.nw_max, &d_treb));
 
-    // dense +-1 couplings: bits and int32 fields in shared memory (fields built in-kernel)
-    bool pm1 = kind == K_DENSE && sa_pm1_smem_bytes(n_max) <= (size_t)ctx->smem_optin && !std::getenv("QA_DISABLE_PM1");
+    // dense +-1 couplings: bits and int32 fields in shared memory (fields built in-kernel);
+    // traced runs take the generic kernel, which gives the same results
+    bool pm1 = kind == K_DENSE && !traces && sa_pm1_smem_bytes(n_max) <= (size_t)ctx->smem_optin &&
+               !std::getenv("QA_DISABLE_PM1");
     for (int p = 0; p < n_problems && pm1; ++p) pm1 = problems[p]->dev.Jw != nullptr;
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, 1, n_max, L.nw_max, DOM_INIT, !pm1));
@@ -1023,6 +1057,7 @@ static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     sp.steps = prm->steps; sp.spb = prm->sweeps_per_beta; sp.smem_fields = smem_fields;
     sp.trace = d_trace; sp.best_E = d_best; sp.best_bits = d_bits; sp.nw_max = L.nw_max; sp.counters = d_cnt;
     sp.mag_trace = d_mag; sp.best_step = d_bstep;
+    sp.tr_bits = d_trb; sp.tr_E = d_tre; sp.tr_end_bits = d_treb; sp.tr_stride = stride; sp.tr_rps = rps;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     int rc = QA_OK;
     if (pm1) {
@@ -1052,12 +1087,22 @@ static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
-    std::vector<double> mag(mag_out ? (size_t)nr * prm->steps : 0);
+    std::vector<double> mag(want_mag ? (size_t)nr * prm->steps : 0);
     std::vector<int> bst(mag_out ? nr : 0);
-    if (mag_out) {
+    if (want_mag)
         QA_CK(cudaMemcpyAsync(mag.data(), d_mag, sizeof(double) * mag.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    if (mag_out)
         QA_CK(cudaMemcpyAsync(bst.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<uint32_t> trb(want_states ? n_rec * L.nw_max : 0);
+    std::vector<double> tre(want_states ? n_rec : 0);
+    if (want_states) {
+        QA_CK(cudaMemcpyAsync(trb.data(), d_trb, sizeof(uint32_t) * trb.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaMemcpyAsync(tre.data(), d_tre, sizeof(double) * tre.size(), cudaMemcpyDeviceToHost, ctx->stream));
     }
+    std::vector<uint32_t> treb(n_end * L.nw_max);
+    if (want_end)
+        QA_CK(cudaMemcpyAsync(treb.data(), d_treb, sizeof(uint32_t) * treb.size(), cudaMemcpyDeviceToHost,
+                              ctx->stream));
     QA_CK(cudaStreamSynchronize(ctx->stream));
     for (int i = 0; i < nr; ++i) {
         const RingDev &R = L.rings[i];
@@ -1072,6 +1117,21 @@ static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
             std::memcpy(mag_out[p] + (size_t)r * prm->steps, mag.data() + (size_t)i * prm->steps,
                         sizeof(double) * prm->steps);
         if (bstep_out && bstep_out[p]) bstep_out[p][r] = bst[i];
+        if (traces) {
+            const qa_sa_trace &t = traces[p];
+            const size_t per = (size_t)prm->steps * rps;
+            if (t.magnetization)
+                std::memcpy(t.magnetization + (size_t)r * prm->steps, mag.data() + (size_t)i * prm->steps,
+                            sizeof(double) * prm->steps);
+            if (t.energies) std::memcpy(t.energies + (size_t)r * per, tre.data() + (size_t)i * per, sizeof(double) * per);
+            if (t.states)
+                for (size_t k = 0; k < per; ++k)
+                    unpack_bits(trb.data() + ((size_t)i * per + k) * L.nw_max, n, t.states + ((size_t)r * per + k) * n);
+            if (t.step_states)
+                for (int st = 0; st < prm->steps; ++st)
+                    unpack_bits(treb.data() + ((size_t)i * prm->steps + st) * L.nw_max, n,
+                                t.step_states + ((size_t)r * prm->steps + st) * n);
+        }
     }
     if (stats) {
         float a = 0, b = 0;
@@ -1097,6 +1157,12 @@ int qa_sa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, co
     return sa_impl(ctx, problems, n_problems, prm, outs, stats, nullptr, nullptr);
 }
 
+int qa_sa_trace_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *prm,
+                    const qa_sa_trace *traces, qa_run_out *outs, qa_stats *stats) {
+    if (!traces) return fail(QA_ERR_ARG, "null traces");
+    return sa_impl(ctx, problems, n_problems, prm, outs, stats, nullptr, nullptr, traces);
+}
+
 int qa_replica_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sa_params *prm,
                    qa_replica_out *outs, qa_stats *stats) {
     if (!outs || n_problems <= 0) return fail(QA_ERR_ARG, "null outputs or empty batch");
@@ -1113,10 +1179,17 @@ int qa_replica_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
 }
 
 // ---------------------------------------------------------------------- SQA
-int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *prm,
-               qa_run_out *outs, qa_stats *stats) {
+// SQA reads (qa_sqa_run); with traces, the observer form (qa_sqa_trace_run):
+// the generic ring kernel also writes the sweep trace.
+static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *prm,
+                    qa_run_out *outs, qa_stats *stats, const qa_sqa_trace *traces) {
     QA_TRY(begin(ctx));
     if (!prm) return fail(QA_ERR_ARG, "null params");
+    const int stride = traces && n_problems > 0 ? traces[0].stride : 1;
+    if (traces)
+        for (int p = 0; p < n_problems; ++p)
+            if (traces[p].stride != stride || stride < 1)
+                return fail(QA_ERR_ARG, "trace stride must be >= 1 and the same for every problem.");
     if (prm->steps <= 0 || !prm->betas || !prm->gammas) return fail(QA_ERR_ARG, "SQA schedule must contain betas.");
     if (prm->trotter_slices <= 0) return fail(QA_ERR_ARG, "trotter_slices must be > 0.");
     if (prm->replicas <= 0) return fail(QA_ERR_ARG, "replicas must be > 0.");
@@ -1182,9 +1255,34 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
         QA_CK(cudaStreamSynchronize(ctx->stream));
     }
 
+    // sweep traces (observers): the generic ring kernel writes them
+    bool tr_rec = false, tr_end = false, tr_mag = false;
+    for (int p = 0; traces && p < n_problems; ++p) {
+        tr_rec = tr_rec || traces[p].ring_states || traces[p].ring_energies;
+        tr_end = tr_end || traces[p].step_states || traces[p].step_energies;
+        tr_mag = tr_mag || traces[p].magnetization;
+    }
+    const int rps = (prm->sweeps_per_beta + stride - 1) / stride + (prm->cluster_sweeps + stride - 1) / stride +
+                    (prm->worldline_sweeps + stride - 1) / stride;
+    const size_t n_rec = tr_rec ? (size_t)nr * steps * rps : 0, n_end = tr_end ? (size_t)nr * (steps + 1) : 0;
+    if ((n_rec + n_end) * (size_t)P * ((size_t)L.nw_max * 4 + 8) > ((size_t)4 << 30))
+        return fail(QA_ERR_ARG, "sweep trace over 4 GiB: raise the stride or trace fewer reads.");
+    uint32_t *d_trb = nullptr, *d_treb = nullptr;
+    double *d_tre = nullptr, *d_tree = nullptr;
+    long long *d_rspin = nullptr;
+    if (tr_rec) {
+        QA_TRY(ws_array(ctx, W_TRB, n_rec * P * L.nw_max, &d_trb));
+        QA_TRY(ws_array(ctx, W_TRE, n_rec * P, &d_tre));
+    }
+    if (tr_end) {
+        QA_TRY(ws_array(ctx, W_TREB, n_end * P * L.nw_max, &d_treb));
+        QA_TRY(ws_array(ctx, W_TREE, n_end * P, &d_tree));
+    }
+    if (tr_mag) QA_TRY(ws_array(ctx, W_RSPIN, (size_t)nr * steps, &d_rspin));
+
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     RingPlan pl;
-    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0));
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0 || traces));
     // dense +-1 couplings: the bit-packed kernel builds its fields in-kernel
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
@@ -1197,6 +1295,8 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     rp.counters = d_cnt;
     rp.rec_base = 0;
     rp.rec_stride = steps;
+    rp.tr_bits = d_trb; rp.tr_E = d_tre; rp.tr_end_bits = d_treb; rp.tr_end_E = d_tree; rp.ring_spin = d_rspin;
+    rp.tr_stride = stride; rp.tr_rps = rps;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     const int seg = 256;
     const int n_seg = (steps + seg - 1) / seg;
@@ -1220,7 +1320,55 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<uint32_t> trb(n_rec * P * L.nw_max), treb(n_end * P * L.nw_max);
+    std::vector<double> tre(n_rec * P), tree(n_end * P);
+    std::vector<long long> rspin(tr_mag ? (size_t)nr * steps : 0);
+    if (tr_rec) {
+        QA_CK(cudaMemcpyAsync(trb.data(), d_trb, sizeof(uint32_t) * trb.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        QA_CK(cudaMemcpyAsync(tre.data(), d_tre, sizeof(double) * tre.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (tr_end) {
+        QA_CK(cudaMemcpyAsync(treb.data(), d_treb, sizeof(uint32_t) * treb.size(), cudaMemcpyDeviceToHost,
+                              ctx->stream));
+        QA_CK(cudaMemcpyAsync(tree.data(), d_tree, sizeof(double) * tree.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (tr_mag)
+        QA_CK(cudaMemcpyAsync(rspin.data(), d_rspin, sizeof(long long) * rspin.size(), cudaMemcpyDeviceToHost,
+                              ctx->stream));
     QA_CK(cudaStreamSynchronize(ctx->stream));
+    for (int p = 0; traces && p < n_problems; ++p) {
+        const qa_sqa_trace &t = traces[p];
+        const int n = problems[p]->n;
+        for (int r = 0; r < prm->reads; ++r) {
+            const int base = (p * prm->reads + r) * K;  // ring of (read, replica 0)
+            const size_t per_rec = (size_t)steps * rps, per_end = (size_t)steps + 1;
+            for (int k = 0; k < K; ++k) {
+                const size_t ring = (size_t)base + k, orow = (size_t)r * K + k;
+                for (size_t e = 0; e < per_rec && (t.ring_states || t.ring_energies); ++e) {
+                    const size_t src = ring * per_rec + e, dst = orow * per_rec + e;
+                    for (int sl = 0; sl < P; ++sl) {
+                        if (t.ring_states)
+                            unpack_bits(trb.data() + (src * P + sl) * L.nw_max, n, t.ring_states + (dst * P + sl) * n);
+                        if (t.ring_energies) t.ring_energies[dst * P + sl] = tre[src * P + sl];
+                    }
+                }
+                for (size_t e = 0; e < per_end && (t.step_states || t.step_energies); ++e) {
+                    const size_t src = ring * per_end + e, dst = orow * per_end + e;
+                    for (int sl = 0; sl < P; ++sl) {
+                        if (t.step_states)
+                            unpack_bits(treb.data() + (src * P + sl) * L.nw_max, n, t.step_states + (dst * P + sl) * n);
+                        if (t.step_energies) t.step_energies[dst * P + sl] = tree[src * P + sl];
+                    }
+                }
+            }
+            if (t.magnetization)
+                for (int st = 0; st < steps; ++st) {
+                    long long m = 0;
+                    for (int k = 0; k < K; ++k) m += rspin[(size_t)(base + k) * steps + st];
+                    t.magnetization[(size_t)r * steps + st] = (double)m / ((double)K * P * n);
+                }
+        }
+    }
 
     // per read: trace = (sum_k sum_t E) / (K*P); best ring = min energy, then
     // earliest step, then lowest replica (the (step, replica, slice) scan
@@ -1264,6 +1412,17 @@ int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
                                      sizeof(uint32_t) * bits.size() + sizeof(cnt));
     }
     return QA_OK;
+}
+
+int qa_sqa_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *prm,
+               qa_run_out *outs, qa_stats *stats) {
+    return sqa_impl(ctx, problems, n_problems, prm, outs, stats, nullptr);
+}
+
+int qa_sqa_trace_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, const qa_sqa_params *prm,
+                     const qa_sqa_trace *traces, qa_run_out *outs, qa_stats *stats) {
+    if (!traces) return fail(QA_ERR_ARG, "null traces");
+    return sqa_impl(ctx, problems, n_problems, prm, outs, stats, traces);
 }
 
 // ---------------------------------------------------------------------- SQA run_optimal
@@ -2264,10 +2423,11 @@ int qa_mlp_create(qa_ctx *ctx, const int *dims, int n_dims, uint64_t seed, qa_ml
         qa_mlp_free(m);
         return fail(e == cudaErrorMemoryAllocation ? QA_ERR_OOM : QA_ERR_CUDA, cudaGetErrorString(e));
     }
-    QA_CK(cudaMemcpy(m->W, W.data(), sizeof(float) * m->nparams, cudaMemcpyHostToDevice));
-    QA_CK(cudaMemcpy(m->wmap, wmap.data(), sizeof(long long) * m->nparams, cudaMemcpyHostToDevice));
-    QA_CK(cudaMemset(m->mo, 0, sizeof(float) * m->nparams));
-    QA_CK(cudaMemset(m->vo, 0, sizeof(float) * m->nparams));
+    // all on the context's stream, ordered before the kernels that read them
+    QA_CK(cudaMemcpyAsync(m->W, W.data(), sizeof(float) * m->nparams, cudaMemcpyHostToDevice, ctx->stream));
+    QA_CK(cudaMemcpyAsync(m->wmap, wmap.data(), sizeof(long long) * m->nparams, cudaMemcpyHostToDevice, ctx->stream));
+    QA_CK(cudaMemsetAsync(m->mo, 0, sizeof(float) * m->nparams, ctx->stream));
+    QA_CK(cudaMemsetAsync(m->vo, 0, sizeof(float) * m->nparams, ctx->stream));
     mlp_to_bf16_kernel<<<(unsigned)((m->nparams + 255) / 256), 256, 0, ctx->stream>>>(m->W, m->nparams, m->wmap, m->W16);
     QA_CK(cudaGetLastError());
     QA_CK(cudaStreamSynchronize(ctx->stream));
@@ -2294,16 +2454,17 @@ int qa_mlp_num_params(const qa_mlp *m, int64_t *count) {
 int qa_mlp_get_params(qa_mlp *m, float *host, int64_t count) {
     if (!m || !host || count != m->nparams) return fail(QA_ERR_ARG, "parameter buffer size mismatch");
     QA_TRY(begin(m->ctx));
-    QA_CK(cudaMemcpy(host, m->W, sizeof(float) * count, cudaMemcpyDeviceToHost));
+    QA_CK(cudaMemcpyAsync(host, m->W, sizeof(float) * count, cudaMemcpyDeviceToHost, m->ctx->stream));
+    QA_CK(cudaStreamSynchronize(m->ctx->stream));
     return QA_OK;
 }
 
 int qa_mlp_set_params(qa_mlp *m, const float *host, int64_t count) {
     if (!m || !host || count != m->nparams) return fail(QA_ERR_ARG, "parameter buffer size mismatch");
     QA_TRY(begin(m->ctx));
-    QA_CK(cudaMemcpy(m->W, host, sizeof(float) * count, cudaMemcpyHostToDevice));
-    QA_CK(cudaMemset(m->mo, 0, sizeof(float) * count));
-    QA_CK(cudaMemset(m->vo, 0, sizeof(float) * count));
+    QA_CK(cudaMemcpyAsync(m->W, host, sizeof(float) * count, cudaMemcpyHostToDevice, m->ctx->stream));
+    QA_CK(cudaMemsetAsync(m->mo, 0, sizeof(float) * count, m->ctx->stream));
+    QA_CK(cudaMemsetAsync(m->vo, 0, sizeof(float) * count, m->ctx->stream));
     m->step = 0;
     mlp_to_bf16_kernel<<<(unsigned)((m->nparams + 255) / 256), 256, 0, m->ctx->stream>>>(m->W, m->nparams, m->wmap,
                                                                                        m->W16);
@@ -2330,7 +2491,10 @@ int qa_mlp_loss_grad(qa_mlp *m, const float *X, const float *T, int batch, float
     QA_TRY(mlp_prepare(m, batch, X, T));
     QA_TRY(mlp_forward_dev(m, batch));
     QA_TRY(mlp_backward_dev(m, batch, loss));
-    if (grads) QA_CK(cudaMemcpy(grads, m->g, sizeof(float) * m->nparams, cudaMemcpyDeviceToHost));
+    if (grads) {
+        QA_CK(cudaMemcpyAsync(grads, m->g, sizeof(float) * m->nparams, cudaMemcpyDeviceToHost, m->ctx->stream));
+        QA_CK(cudaStreamSynchronize(m->ctx->stream));
+    }
     return QA_OK;
 }
 

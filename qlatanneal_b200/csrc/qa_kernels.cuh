@@ -70,6 +70,17 @@ struct RingParams {
     int nw_max;
     int *mag;             // [ring][sweeps] spin sums after each sweep (chi pilot), may be null
     unsigned long long *counters;  // [4]
+    // sweep traces (observers; ring_kernel only), or null.  After every sweep
+    // whose index in its phase is a multiple of tr_stride: the ring's bits and
+    // slice energies at record [ring][step][tr_rps] (records of a step: slice,
+    // cluster, worldline sweeps in that order).  At the start and at each step
+    // end the same at [ring][step + 1] (0: the starting state).
+    uint32_t *tr_bits;     // [ring][steps][tr_rps][P][nw_max]
+    double *tr_E;          // [ring][steps][tr_rps][P]
+    uint32_t *tr_end_bits; // [ring][steps + 1][P][nw_max]
+    double *tr_end_E;      // [ring][steps + 1][P]
+    long long *ring_spin;  // [ring][steps] sum of the ring's spins at each step end
+    int tr_stride, tr_rps;
 };
 
 __device__ __forceinline__ int phase_count(int P, int ph) {
@@ -175,6 +186,13 @@ struct SAParams {
     unsigned long long *counters;
     double *mag_trace;      // [ring][steps] magnetisation after each step, or null
     int *best_step;         // [ring] step of the last best improvement (-1: start), or null
+    // sweep trace (observers), or null: after every sweep whose index in its
+    // step is a multiple of tr_stride, the state and the running energy at
+    // record [ring][step][tr_rps]
+    uint32_t *tr_bits;      // [ring][steps][tr_rps][nw_max]
+    double *tr_E;           // [ring][steps][tr_rps]
+    uint32_t *tr_end_bits;  // [ring][steps][nw_max] the state at each step end, or null
+    int tr_stride, tr_rps;
 };
 
 // Magnetisation sum(s) / n of the current state (metrics.hpp:11-20), exact.
@@ -249,8 +267,16 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
                     pending = j == 31 ? 0u : (FULL << (j + 1));
                 }
             }
+            if (p.tr_bits && sw % p.tr_stride == 0) {
+                const long long rec = ((long long)blockIdx.x * p.steps + step) * p.tr_rps + sw / p.tr_stride;
+                for (int q = lane; q < nw; q += 32) p.tr_bits[rec * p.nw_max + q] = S[q];
+                if (lane == 0) p.tr_E[rec] = E;
+                __syncwarp();
+            }
         }
         if (lane == 0) p.trace[(long long)blockIdx.x * p.steps + step] = E;
+        if (p.tr_end_bits)
+            for (int q = lane; q < nw; q += 32) p.tr_end_bits[((long long)blockIdx.x * p.steps + step) * p.nw_max + q] = S[q];
         if (p.mag_trace) sa_record_mag(p, S, n, nw, step, lane);
     }
     for (int q = lane; q < nw; q += 32) p.spins[R.spin_off + q] = S[q];
@@ -399,6 +425,23 @@ __device__ __forceinline__ void cluster_move(const ProbDev &Pd, uint32_t *S, flo
     __syncwarp();
 }
 
+// One trace record of a ring: the slice energies (as the step-end scan
+// computes them) and the bits of every slice.  Whole CTA; ends with a barrier.
+template <int KIND>
+__device__ __forceinline__ void ring_trace(const RingParams &p, const ProbDev &Pd, const RingSmem &sm,
+                                           const float *gbase, int NP, int nw, int n, int W, int warp, int lane,
+                                           uint32_t *bits, double *E) {
+    for (int t = warp; t < NP; t += W) {
+        const double e = cell_energy<KIND>(Pd, sm.S + t * nw, gbase + (long long)t * n, sm.h, lane);
+        if (lane == 0) E[t] = e;
+    }
+    for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) {
+        const int t = idx / nw, q = idx - t * nw;
+        bits[(long long)t * p.nw_max + q] = sm.S[idx];
+    }
+    __syncthreads();
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -427,6 +470,20 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     unsigned long long att_s = 0, acc_s = 0, att_w = 0, acc_w = 0;
     double bestE = p.best_E[blockIdx.x];
     int bestStep = p.best_step[blockIdx.x];
+    // trace records: slice sweeps first, then cluster, then worldline sweeps
+    const int tr_s = p.tr_bits ? (p.spb + p.tr_stride - 1) / p.tr_stride : 0;
+    const int tr_c = p.tr_bits ? (p.cls + p.tr_stride - 1) / p.tr_stride : 0;
+    auto trace_rec = [&](int step, int idx) {
+        const long long rec = ((long long)blockIdx.x * p.steps_total + step) * p.tr_rps + idx;
+        ring_trace<KIND>(p, Pd, sm, gbase, NP, nw, n, W, warp, lane, p.tr_bits + rec * NP * p.nw_max,
+                         p.tr_E + rec * NP);
+    };
+    auto trace_end = [&](int step) {  // the state after `step` (step -1: the start)
+        const long long rec = (long long)blockIdx.x * (p.steps_total + 1) + step + 1;
+        ring_trace<KIND>(p, Pd, sm, gbase, NP, nw, n, W, warp, lane, p.tr_end_bits + rec * NP * p.nw_max,
+                         p.tr_end_E + rec * NP);
+    };
+    if (p.tr_end_bits && p.step0 == 0) trace_end(-1);
 
     for (int step = p.step0 - (p.init_scan ? 1 : 0); step < p.step1; ++step) {
         // step -1 (init_scan) only scores the starting state
@@ -459,6 +516,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                 __syncthreads();
             }
             if (p.bsamp) record_bond_sample(p, sm.S, NP, nw, n, sm.wl_sh, W, step, sw);
+            if (p.tr_bits && sw % p.tr_stride == 0) trace_rec(step, sw / p.tr_stride);
         }
         // cluster sweeps: one warp, spins in order
         const int cls = step >= 0 ? p.cls : 0;
@@ -471,6 +529,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
             }
             __syncthreads();
             if (p.bsamp) record_bond_sample(p, sm.S, NP, nw, n, sm.wl_sh, W, step, p.spb + sw);
+            if (p.tr_bits && sw % p.tr_stride == 0) trace_rec(step, tr_s + sw / p.tr_stride);
         }
         for (int sw = 0; sw < wls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
@@ -523,6 +582,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                     pending = j == 31 ? 0u : (FULL << (j + 1));
                 }
             }
+            if (p.tr_bits && sw % p.tr_stride == 0) trace_rec(step, tr_s + tr_c + sw / p.tr_stride);
         }
         // ---- step end: energy of every slice, ring sum, best (sqa_annealer.cpp:455-469)
         for (int t = warp; t < NP; t += W) {
@@ -581,6 +641,25 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
             for (int q = threadIdx.x; q < nw; q += blockDim.x)
                 p.final_bits[(long long)blockIdx.x * p.nw_max + q] = sm.S[sm.flag[1] * nw + q];
         __syncthreads();
+        if (p.tr_end_bits && step >= 0) trace_end(step);
+        if (p.ring_spin && step >= 0) {
+            long long c = 0;
+            for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) {
+                const int q = idx % nw, rem = n - 32 * q;
+                uint32_t x = sm.S[idx];
+                if (rem < 32) x &= (1u << rem) - 1u;
+                c += 2 * __popc(x) - min(32, rem);
+            }
+            c = warp_sum_ll(c);
+            if (lane == 0) sm.wl_sh[warp] = (int)c;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                long long tot = 0;
+                for (int w = 0; w < W; ++w) tot += sm.wl_sh[w];
+                p.ring_spin[(long long)blockIdx.x * p.steps_total + step] = tot;
+            }
+            __syncthreads();
+        }
     }
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) p.spins[R.spin_off + idx] = sm.S[idx];
     if (p.smem_fields)

@@ -88,6 +88,7 @@ class Oracle:
         L.or_sqapt_opt_run.argtypes = ([C.c_void_p, _f8p, _f8p] + [C.c_int] * 7 + [C.c_double] * 3 +
                                        [C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double), _f8p,
                                         _i8p] + [_f8p] * 5)
+        L.or_trace_set.argtypes = [C.c_int] + [C.c_void_p] * 7
         L.or_chi_schedule.argtypes = ([C.c_int, _f8p, _f8p, _f8p] + [C.c_double] * 4 + [C.c_int, C.c_int] +
                                       [C.c_double] * 3 + [_f8p] * 4)
         L.or_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 3 + [C.c_int] * 5 +
@@ -211,6 +212,37 @@ class Oracle:
         self.L.or_pt_run(m.h, betas, R, spb, steps, swap_interval, seed, read, best, C.byref(E), fE, fs, avg, swp,
                          cnt)
         return best, E.value, fE, fs.reshape(R, m.n), avg, swp
+
+    def sa_trace_run(self, m, betas, spb, stride, seed, read=0):
+        """SA read with the sweep trace: (best, best_E, trace, states[steps][rps][n],
+        energies[steps][rps], step_states[steps][n], magnetization[steps])."""
+        S, rps = len(betas), -(-spb // stride)
+        states, energies = np.zeros((S, rps, m.n), np.int8), np.zeros((S, rps))
+        ends, mag = np.zeros((S, m.n), np.int8), np.zeros(S)
+        p = lambda a: a.ctypes.data  # noqa: E731
+        self.L.or_trace_set(stride, p(states), p(energies), None, None, p(ends), None, p(mag))
+        try:
+            best, E, trace, _ = self.sa_run(m, betas, spb, seed, read)
+        finally:
+            self.L.or_trace_set(0, None, None, None, None, None, None, None)
+        return best, E, trace, states, energies, ends, mag
+
+    def sqa_trace_run(self, m, betas, gammas, P, K, spb, wls, cls, stride, seed, read=0):
+        """SQA read with the sweep trace: dict of ring_states[K][S][rps][P][n],
+        ring_E[K][S][rps][P], step_states[K][S+1][P][n], step_E[K][S+1][P],
+        magnetization[S] and the run's (best, best_E, trace)."""
+        S = len(betas)
+        rps = -(-spb // stride) + -(-cls // stride) + -(-wls // stride)
+        rs, rE = np.zeros((K, S, rps, P, m.n), np.int8), np.zeros((K, S, rps, P))
+        es, eE = np.zeros((K, S + 1, P, m.n), np.int8), np.zeros((K, S + 1, P))
+        mag = np.zeros(S)
+        p = lambda a: a.ctypes.data  # noqa: E731
+        self.L.or_trace_set(stride, None, None, p(rs), p(rE), p(es), p(eE), p(mag))
+        try:
+            best, E, trace, _ = self.sqa_run(m, betas, gammas, P, K, spb, wls, seed, read, cls=cls)
+        finally:
+            self.L.or_trace_set(0, None, None, None, None, None, None, None)
+        return dict(best=best, best_E=E, trace=trace, ring_states=rs, ring_E=rE, step_states=es, step_E=eE, mag=mag)
 
     def sqa_run(self, m, betas, gammas, P, K, spb, wls, seed, read=0, cls=0):
         betas, gammas = _c64(betas), _c64(gammas)
