@@ -187,9 +187,10 @@ class _Seeded:
 
 
 def _outs(n: int, reads: int, steps: int):
-    spins = np.zeros((reads, n), dtype=np.int8)
-    energies = np.zeros(reads, dtype=np.float64)
-    trace = np.zeros((reads, steps), dtype=np.float64)
+    # every entry is written by the run (unpacked best states, energies, traces)
+    spins = np.empty((reads, n), dtype=np.int8)
+    energies = np.empty(reads, dtype=np.float64)
+    trace = np.empty((reads, steps), dtype=np.float64)
     o = _lib.qa_run_out(spins.ctypes.data, energies.ctypes.data, trace.ctypes.data)
     return o, spins, energies, trace
 
@@ -239,7 +240,7 @@ class Annealer(_Seeded):
         _lib.check(eng.L.qa_sa_trace_run(eng.h, probs, 1, C.byref(prm), C.byref(tr), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         replay_sa(observer, betas, spb, stride, trace[0], energies, states, step_states, State)
-        return AnnealResult(State(spins[0]), float(energy[0]), trace[0])
+        return AnnealResult(State._view(spins[0]), float(energy[0]), trace[0])
 
     def run_reads(self, sweeps_per_beta: int, reads: int, seed: Optional[int] = None) -> List[AnnealResult]:
         if sweeps_per_beta <= 0:
@@ -255,7 +256,7 @@ class Annealer(_Seeded):
         probs = (C.c_void_p * 1)(prob)
         _lib.check(eng.L.qa_sa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
-        return [AnnealResult(State(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
+        return [AnnealResult(State._view(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
 
 
 class ReplicaAnnealer(_Seeded):
@@ -300,10 +301,10 @@ class ReplicaAnnealer(_Seeded):
         probs = (C.c_void_p * 1)(prob)
         _lib.check(eng.L.qa_replica_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
-        reps = [ReplicaResult(State(spins[r]), float(best[r]), trace[r], mag[r]) for r in range(R)]
+        reps = [ReplicaResult(State._view(spins[r]), float(best[r]), trace[r], mag[r]) for r in range(R)]
         # replica_annealer.cpp:75-81, 112-117: the lowest energy, first reached (earliest step, then replica)
         g = min(range(R), key=lambda r: (best[r], int(bstep[r]), r))
-        return MultiAnnealResult(reps, State(spins[g]), float(best[g]), trace.mean(axis=0), mag.mean(axis=0))
+        return MultiAnnealResult(reps, State._view(spins[g]), float(best[g]), trace.mean(axis=0), mag.mean(axis=0))
 
 
 class ParallelTemperingAnnealer(_Seeded):
@@ -353,7 +354,7 @@ class ParallelTemperingAnnealer(_Seeded):
         probs = (C.c_void_p * 1)(prob)
         _lib.check(eng.L.qa_pt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
-        return [ParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
+        return [ParallelTemperingResult([State._view(fin[r, k]) for k in range(R)], finE[r].tolist(), State._view(best[r]),
                                         float(bestE[r]), avg[r], swp[r]) for r in range(reads)]
 
 
@@ -419,7 +420,7 @@ class SQAAnnealer(_Seeded):
         self.last_stats = RunStats.from_c(st)
         replay_sqa(observer, betas, gammas, P, K, int(spb), int(cls), int(wls), stride, trace[0], ring_states,
                    ring_E, step_states, step_E)
-        return SQAResult(State(spins[0]), float(energy[0]), trace[0])
+        return SQAResult(State._view(spins[0]), float(energy[0]), trace[0])
 
     def run_reads(self, sweeps_per_beta: int, worldline_sweeps: int, cluster_sweeps: int = 0,
                   continuous_time_slices: int = 0, reads: int = 1, seed: Optional[int] = None) -> List[SQAResult]:
@@ -437,7 +438,7 @@ class SQAAnnealer(_Seeded):
         probs = (C.c_void_p * 1)(prob)
         _lib.check(eng.L.qa_sqa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
-        return [SQAResult(State(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
+        return [SQAResult(State._view(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
 
 
 def _write_opt_debug_csv(path: str, res: "SQAResult", beta_ramp_steps: int, alpha: float) -> None:
@@ -485,7 +486,7 @@ def _sqa_run_optimal_reads(self, beta: float, j_perp_start: float, j_perp_end: f
     probs = (C.c_void_p * 1)(prob)
     _lib.check(eng.L.qa_sqa_opt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
     self.last_stats = RunStats.from_c(st)
-    return [SQAResult(State(spins[r]), float(best[r]), tr[r], jt[r].tolist(), ct[r].tolist(), float(sc[r, 0]),
+    return [SQAResult(State._view(spins[r]), float(best[r]), tr[r], jt[r].tolist(), ct[r].tolist(), float(sc[r, 0]),
                       float(sc[r, 1]), float(sc[r, 2]), float(sc[r, 3])) for r in range(reads)]
 
 
@@ -559,7 +560,7 @@ class SQAParallelTemperingAnnealer(_Seeded):
         probs = (C.c_void_p * 1)(prob)
         _lib.check(eng.L.qa_sqapt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
-        return [SQAParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
+        return [SQAParallelTemperingResult([State._view(fin[r, k]) for k in range(R)], finE[r].tolist(), State._view(best[r]),
                                            float(bestE[r]), avg[r], swp[r])
                 for r in range(reads)]
 
@@ -608,7 +609,7 @@ class SQAParallelTemperingAnnealer(_Seeded):
         probs = (C.c_void_p * 1)(prob)
         _lib.check(eng.L.qa_sqapt_opt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
-        return [SQAParallelTemperingResult([State(fin[r, k]) for k in range(R)], finE[r].tolist(), State(best[r]),
+        return [SQAParallelTemperingResult([State._view(fin[r, k]) for k in range(R)], finE[r].tolist(), State._view(best[r]),
                                            float(bestE[r]), avg[r], swp[r], jt[r].tolist(), ct[r].tolist(),
                                            float(sc[r, 0]), float(sc[r, 1]), float(sc[r, 2]), float(sc[r, 3]))
                 for r in range(reads)]

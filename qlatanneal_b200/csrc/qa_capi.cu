@@ -5,7 +5,9 @@
 #include <cmath>
 #include <cstdio>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
+#include <new>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -100,10 +102,60 @@ int set_last_error(int code, const char *msg) {
 }
 }  // namespace qa
 
+// Host staging of problem arrays, reused across problems (grown, never
+// shrunk): pinned, so the one copy of a problem block is a direct DMA that
+// overlaps the host.  `sent` marks the end of the last copy out of it; the
+// buffer is rewritten only after that copy has completed.  If pinned memory
+// cannot be had it falls back to pageable memory (copies then stage
+// synchronously).
+struct HostStage {
+    unsigned char *p = nullptr;
+    size_t n = 0, cap = 0;
+    bool pinned = false, pending = false;
+    cudaEvent_t sent = nullptr;
+    size_t size() const { return n; }
+    bool empty() const { return n == 0; }
+    unsigned char *data() { return p; }
+    void clear() { n = 0; }
+    void wait() {
+        if (pending) cudaEventSynchronize(sent);
+        pending = false;
+    }
+    void resize(size_t m) {
+        if (m > cap) {
+            wait();
+            const size_t want = std::max(m, cap * 3 / 2);
+            unsigned char *q = nullptr;
+            const bool pin = cudaHostAlloc(reinterpret_cast<void **>(&q), want, cudaHostAllocDefault) == cudaSuccess;
+            if (!pin) {
+                cudaGetLastError();  // clear the allocation error; pageable memory still works
+                q = static_cast<unsigned char *>(std::malloc(want));
+                if (!q) throw std::bad_alloc();
+            }
+            if (n) std::memcpy(q, p, n);
+            release();
+            p = q;
+            cap = want;
+            pinned = pin;
+        }
+        n = m;
+    }
+    void release() {
+        wait();
+        if (p) {
+            if (pinned) cudaFreeHost(p);
+            else std::free(p);
+        }
+        p = nullptr;
+        cap = 0;
+    }
+};
+
 struct qa_ctx {
     int device = 0;
     std::shared_ptr<BlockPool> pool;
-    std::vector<unsigned char> stage;  // host staging of problem arrays, reused across problems
+    HostStage stage;  // host staging of problem arrays, reused across problems
+    HostStage down;   // pinned landing buffer for a run's large results (used within one call)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int smem_optin = 0;
@@ -169,8 +221,11 @@ int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
 // staging call (which may move the buffer); *dev is set by finish_problem.
 template <class T>
 T *stage_array(qa_problem *P, size_t count, const T **dev) {
-    std::vector<unsigned char> &st = P->ctx->stage;
-    if (P->fix.empty()) st.clear();  // first array of this problem
+    HostStage &st = P->ctx->stage;
+    if (P->fix.empty()) {  // first array of this problem: the previous block's copy must be done
+        st.wait();
+        st.clear();
+    }
     const size_t off = (st.size() + 255) & ~(size_t)255;
     st.resize(off + std::max<size_t>(count * sizeof(T), 16));
     P->fix.push_back({off, reinterpret_cast<const void **>(dev)});
@@ -205,7 +260,7 @@ int finish_problem(qa_problem *P) {
     P->dev.T = P->T;
     P->dev.m = P->m;
     P->dev.c = P->c;
-    std::vector<unsigned char> &st = P->ctx->stage;
+    HostStage &st = P->ctx->stage;
     if (P->fix.empty()) st.clear();  // nothing staged for this problem
     std::vector<size_t> roff;
     size_t end = st.size();
@@ -232,8 +287,12 @@ int finish_problem(qa_problem *P) {
     // on the context's stream (non-blocking): every later use of the block,
     // the device-side derivations first, is ordered after the copy; a
     // pageable source is staged before the call returns, so the buffer is free
-    const cudaError_t e =
+    cudaError_t e =
         st.empty() ? cudaSuccess : cudaMemcpyAsync(d, st.data(), st.size(), cudaMemcpyHostToDevice, P->ctx->stream);
+    if (e == cudaSuccess && !st.empty()) {
+        e = cudaEventRecord(st.sent, P->ctx->stream);
+        st.pending = e == cudaSuccess;
+    }
     st.clear();
     if (e != cudaSuccess) {
         P->fix.clear();
@@ -642,6 +701,7 @@ int qa_create(qa_ctx **out, int device) {
     ctx->pool->device = device;
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->stage.sent, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) {
         qa_destroy(ctx);
@@ -659,6 +719,9 @@ int qa_destroy(qa_ctx *ctx) {
         if (b.p) cudaFree(b.p);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    ctx->stage.release();
+    ctx->down.release();
+    if (ctx->stage.sent) cudaEventDestroy(ctx->stage.sent);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return QA_OK;
@@ -1310,11 +1373,15 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
     QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
 
-    std::vector<double> sums((size_t)nr * steps), bestE(nr), exact(nr);
+    // the per-step ring sums (the largest result) land in the pinned buffer
+    ctx->down.resize(sizeof(double) * (size_t)nr * steps);
+    const double *sums = reinterpret_cast<const double *>(ctx->down.data());
+    std::vector<double> bestE(nr), exact(nr);
     std::vector<int> bstep(nr);
     std::vector<uint32_t> bits((size_t)nr * L.nw_max);
     unsigned long long cnt[4];
-    QA_CK(cudaMemcpyAsync(sums.data(), d_sum, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaMemcpyAsync(ctx->down.data(), d_sum, sizeof(double) * (size_t)nr * steps, cudaMemcpyDeviceToHost,
+                          ctx->stream));
     QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bstep.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1408,7 +1475,7 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
         stats->launches = (pl.own_fields() ? 2 : 3) + n_seg;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * steps +
                                      (sizeof(double) + sizeof(int)) * nr + sizeof(int) * nr);
-        stats->d2h_bytes = (int64_t)(sizeof(double) * sums.size() + (2 * sizeof(double) + sizeof(int)) * nr +
+        stats->d2h_bytes = (int64_t)(sizeof(double) * (size_t)nr * steps + (2 * sizeof(double) + sizeof(int)) * nr +
                                      sizeof(uint32_t) * bits.size() + sizeof(cnt));
     }
     return QA_OK;
@@ -2003,7 +2070,6 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     sp.ring_in = d_rin; sp.slot_of = d_slot; sp.avg_trace = d_avg; sp.swap_trace = d_swp; sp.steps_total = steps;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     int n_seg = 0;
-    float ring_ms = 0.0f;
     for (int s0 = 0; s0 < steps;) {
         const int s1 = std::min({steps, (s0 / prm->swap_interval + 1) * prm->swap_interval, s0 + 256});
         rp.step0 = s0;
@@ -2023,7 +2089,6 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
     QA_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-    (void)ring_ms;
     std::vector<qa_sqapt_out *> po(n_problems);
     for (int p = 0; p < n_problems; ++p) po[p] = outs + p;
     const PTDev dv{d_best, d_exact, d_min, d_avg, d_swp, d_bstep, d_bslot, d_rin, d_bits, d_fbits, d_cnt};

@@ -27,11 +27,20 @@ def _spins(spins: Sequence[int], n: int) -> np.ndarray:
 class State:
     """``qanneal.State``: spins in {-1, +1} (state.hpp:10-31)."""
 
+    __slots__ = ("_spins",)
+
     def __init__(self, n_or_spins: Any = 0):
         if isinstance(n_or_spins, (int, np.integer)):
             self._spins = np.ones(int(n_or_spins), dtype=np.int8)
         else:
             self._spins = np.asarray(n_or_spins, dtype=np.int8).copy()
+
+    @classmethod
+    def _view(cls, spins: np.ndarray) -> "State":
+        """A State over an int8 row the caller owns exclusively (no copy)."""
+        st = cls.__new__(cls)
+        st._spins = spins
+        return st
 
     @property
     def spins(self) -> List[int]:
