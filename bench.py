@@ -217,12 +217,35 @@ SIDE = {
     "sqa-hubo": dict(desc="SQA, HUBO n=1024 (3n 3-body J=+-1, 2n 2-body J~U(-1,1), h~N(0,0.2^2)), P=16, beta "
                           "linear 0.1->4, Gamma 2->0.02 over 500 steps, 1 slice + 1 worldline sweep, 128 reads",
                      method="sqa", kind="hubo", n=1024, reads=128, steps=500, spb=1, wls=1, P=16, seed=13),
+    # instance sets in one launch (BatchRunner): the configurations' instance counts
+    "sqa-hubo-set": dict(desc="SQA, 32 HUBO instances n~U{1024..2048} (3n 3-body J=+-1, 2n 2-body J~U(-1,1), "
+                              "h~N(0,0.2^2)) in one launch, P=16, beta linear 0.1->4, Gamma 2->0.02 over 500 steps, "
+                              "1 slice + 1 worldline sweep, 128 reads each",
+                         method="sqa", kind="hubo", instances=32, n_range=(1024, 2048), reads=128, steps=500, spb=1,
+                         wls=1, P=16, seed=13),
+    "sqapt-sparse-set": dict(desc="SQA-PT, 8 random 3-regular instances n~U{512..4096} even, J=+-1, h in "
+                                  "{-0.5,0,0.5}, in one launch, P=16, 32 rungs (beta geometric 0.2->4, Gamma linear "
+                                  "2.5->0.05), first 20 pt steps x (20 slice + 5 worldline) sweeps, swap interval "
+                                  "10, 32 reads each",
+                             method="sqapt", kind="regular3", instances=8, n_range=(512, 4096), reads=32, steps=20,
+                             spb=20, wls=5, P=16, rungs=32, swap=10, seed=12),
 }
 
 
+def _set_sizes(w):
+    rng = np.random.default_rng(w["seed"])
+    lo, hi = w["n_range"]
+    ns = rng.integers(lo, hi + 1, size=w["instances"])
+    return [int(n) - (int(n) & 1) if w["kind"] == "regular3" else int(n) for n in ns]
+
+
 def _side_spec(w):
-    """The seeded instance data (generated once, outside every timed region)."""
+    """The seeded instance data (generated once, outside every timed region);
+    a list of (spec, n) for an instance set."""
     from qlatanneal_b200.instances import hubo_random, regular3, sk_dense
+    if w.get("instances"):
+        return [(_side_spec(dict(w, instances=0, n=n, seed=w["seed"] + 1000 * k)), n)
+                for k, n in enumerate(_set_sizes(w))]
     if w["kind"] == "sk":
         return ("dense",) + tuple(sk_dense(w["n"], w["seed"]))
     if w["kind"] == "regular3":
@@ -231,8 +254,10 @@ def _side_spec(w):
 
 
 def _side_build(w, spec):
-    """The model through the public API, from host data."""
+    """The model (or the set's models) through the public API, from host data."""
     import qlatanneal_b200 as qa
+    if w.get("instances"):
+        return [_side_build(dict(w, instances=0, n=n), sp) for sp, n in spec]
     kind, a, b = spec
     if kind == "dense":
         return qa.DenseIsing(a, b)
@@ -243,6 +268,19 @@ def _side_build(w, spec):
 
 def _side_annealer(w, model):
     import qlatanneal_b200 as qa
+    if w.get("instances"):
+        runner = qa.BatchRunner()
+        if w["method"] == "sqapt":
+            R = w["rungs"]
+            betas = 0.2 * (4.0 / 0.2) ** (np.arange(R) / (R - 1))
+            gammas = np.linspace(2.5, 0.05, R)
+            return runner, (lambda seed: runner.sqapt(model, betas, gammas, w["P"], w["spb"], w["wls"], w["steps"],
+                                                      w["swap"], reads=w["reads"], seed=seed)), betas, gammas
+        betas = np.linspace(0.1, 4.0, w["steps"])
+        gammas = np.linspace(2.0, 0.02, w["steps"])
+        sched = qa.SQASchedule.from_vectors(betas, gammas)
+        return runner, (lambda seed: runner.sqa(model, sched, w["P"], 1, w["spb"], w["wls"], reads=w["reads"],
+                                                seed=seed)), betas, gammas
     if w["method"] == "sa":
         betas = w["b0"] * (w["b1"] / w["b0"]) ** (np.arange(w["steps"]) / (w["steps"] - 1))
         ann = qa.Annealer(model, qa.AnnealSchedule.from_betas(betas))
@@ -346,9 +384,13 @@ def run_side(args, w):
         m2 = _side_build(w, spec)
         a2, c2, _, _ = _side_annealer(w, m2)
         c2(w["seed"])
-        m2.release()
+        for m in (m2 if isinstance(m2, list) else [m2]):
+            m.release()
         e2e.append(time.perf_counter() - t0)
-    cpu = None if args.no_cpu_baseline else _side_cpu(w, spec)
+    if w.get("instances"):  # the CPU sample: the set's first instance
+        cpu = None if args.no_cpu_baseline else _side_cpu(dict(w, instances=0, n=spec[0][1]), spec[0][0])
+    else:
+        cpu = None if args.no_cpu_baseline else _side_cpu(w, spec)
     st = stats[0]
     line = {"metric": "spin-flip attempts/s (site-attempts)", "workload": args.workload,
             "value": sites * args.steps / (dev_ms / 1e3), "unit": "site-attempts/s", "n_gpus": 1,

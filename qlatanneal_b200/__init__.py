@@ -31,6 +31,7 @@ from .annealers import (  # noqa: F401
     SQAAnnealer,
     SQAParallelTemperingAnnealer,
     SQAChiAnnealer,
+    BatchRunner,
 )
 from .observers import (  # noqa: F401
     Observer,

@@ -714,3 +714,82 @@ def _write_chi_debug_csv(path: str, res: SQAChiResult, beta: float, slices: int,
 
 SQAAnnealer.run_optimal = _sqa_run_optimal
 SQAAnnealer.run_optimal_reads = _sqa_run_optimal_reads
+
+
+class BatchRunner:
+    """Several models of one kind in one launch: the batched form of
+    ``Annealer.run_reads``, ``SQAAnnealer.run_reads`` and
+    ``SQAParallelTemperingAnnealer.run_reads``.  Read r of every model is keyed
+    seed + r, so model p's results equal its own single-model run with the same
+    seed; models may differ in size.  The reference runs such instance sets one
+    after another (its benchmark scripts loop over instances)."""
+
+    def __init__(self, device: Optional[int] = None):
+        self.device = device
+        self.last_stats: Optional[RunStats] = None
+
+    def _prep(self, models):
+        if len(models) == 0:
+            raise ValueError("at least one model is required.")
+        eng = _lib.Engine.get(self.device)
+        hdl = [m._device_problem(eng) for m in models]
+        return eng, (C.c_void_p * len(hdl))(*hdl)
+
+    def anneal(self, models, schedule: AnnealSchedule, sweeps_per_beta: int, reads: int = 1,
+               seed: int = 0) -> List[List[AnnealResult]]:
+        if sweeps_per_beta <= 0:
+            raise ValueError("sweeps_per_beta must be > 0.")
+        eng, probs = self._prep(models)
+        betas = np.ascontiguousarray(schedule.betas, dtype=np.float64)
+        prm = _lib.qa_sa_params(betas.ctypes.data, len(betas), int(sweeps_per_beta), int(reads), int(seed))
+        outs = [_outs(m.size(), reads, len(betas)) for m in models]
+        arr = (_lib.qa_run_out * len(models))(*[o[0] for o in outs])
+        st = _lib.qa_stats()
+        _lib.check(eng.L.qa_sa_run(eng.h, probs, len(models), C.byref(prm), arr, C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        return [[AnnealResult(State._view(sp[r]), float(en[r]), tr[r]) for r in range(reads)]
+                for _, sp, en, tr in outs]
+
+    def sqa(self, models, schedule: SQASchedule, trotter_slices: int, replicas: int = 1, sweeps_per_beta: int = 1,
+            worldline_sweeps: int = 0, cluster_sweeps: int = 0, continuous_time_slices: int = 0, reads: int = 1,
+            seed: int = 0) -> List[List[SQAResult]]:
+        eng, probs = self._prep(models)
+        betas = np.ascontiguousarray(schedule.betas, dtype=np.float64)
+        gammas = np.ascontiguousarray(schedule.gammas, dtype=np.float64)
+        prm = _lib.qa_sqa_params(betas.ctypes.data, gammas.ctypes.data, len(betas), int(trotter_slices),
+                                 int(replicas), int(sweeps_per_beta), int(worldline_sweeps), int(cluster_sweeps),
+                                 int(continuous_time_slices), int(reads), int(seed))
+        outs = [_outs(m.size(), reads, len(betas)) for m in models]
+        arr = (_lib.qa_run_out * len(models))(*[o[0] for o in outs])
+        st = _lib.qa_stats()
+        _lib.check(eng.L.qa_sqa_run(eng.h, probs, len(models), C.byref(prm), arr, C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        return [[SQAResult(State._view(sp[r]), float(en[r]), tr[r]) for r in range(reads)]
+                for _, sp, en, tr in outs]
+
+    def sqapt(self, models, betas: Sequence[float], gammas: Sequence[float], trotter_slices: int,
+              sweeps_per_step: int, worldline_sweeps: int, steps: int, swap_interval: int = 1,
+              cluster_sweeps: int = 0, continuous_time_slices: int = 0, reads: int = 1,
+              seed: int = 0) -> List[List[SQAParallelTemperingResult]]:
+        if len(betas) < 2 or len(betas) != len(gammas):
+            raise ValueError("SQA parallel tempering requires >=2 beta/gamma pairs.")
+        eng, probs = self._prep(models)
+        b = np.ascontiguousarray(betas, dtype=np.float64)
+        g = np.ascontiguousarray(gammas, dtype=np.float64)
+        R, S = len(b), max(int(steps), 1)
+        prm = _lib.qa_sqapt_params(b.ctypes.data, g.ctypes.data, R, int(trotter_slices), int(sweeps_per_step),
+                                   int(worldline_sweeps), int(steps), int(swap_interval), int(cluster_sweeps),
+                                   int(continuous_time_slices), int(reads), int(seed))
+        bufs = []
+        for m in models:
+            n = m.size()
+            bufs.append((np.empty((reads, n), np.int8), np.empty(reads), np.empty((reads, R, n), np.int8),
+                         np.empty((reads, R)), np.empty((reads, S)), np.empty((reads, S))))
+        arr = (_lib.qa_sqapt_out * len(models))(*[
+            _lib.qa_sqapt_out(*(x.ctypes.data for x in bf)) for bf in bufs])
+        st = _lib.qa_stats()
+        _lib.check(eng.L.qa_sqapt_run(eng.h, probs, len(models), C.byref(prm), arr, C.byref(st)))
+        self.last_stats = RunStats.from_c(st)
+        return [[SQAParallelTemperingResult([State._view(fin[r, k]) for k in range(R)], finE[r].tolist(),
+                                            State._view(best[r]), float(bestE[r]), avg[r], swp[r])
+                 for r in range(reads)] for best, bestE, fin, finE, avg, swp in bufs]

@@ -1016,6 +1016,14 @@ int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int6
         rc = upload(P, upd_ptr.data(), upd_ptr.size(), &P->dev.upd_ptr);
         if (rc == QA_OK) rc = upload(P, upd_run.data(), upd_run.size(), &P->dev.upd_run);
         if (rc == QA_OK) rc = upload(P, upd_rec.data(), upd_rec.size(), &P->dev.upd_rec);
+        // one 16-byte record per term for the per-step energy scan
+        std::vector<int4> trec(std::max(n_terms, 1), make_int4(-1, -1, -1, -1));
+        for (int t = 0; t < n_terms; ++t) {
+            int v[4] = {-1, -1, -1, -1};
+            for (int k = tptr[t]; k < tptr[t + 1]; ++k) v[k - tptr[t]] = tvars[k];
+            trec[t] = make_int4(v[0], v[1], v[2], v[3]);
+        }
+        if (rc == QA_OK) rc = upload(P, trec.data(), trec.size(), &P->dev.trec);
     }
     if (rc != QA_OK) {
         qa_problem_free(P);

@@ -55,12 +55,19 @@ __device__ __forceinline__ uint32_t spin_slot(int i) { return (uint32_t)(((i >> 
 
 __device__ __forceinline__ float u01(uint32_t x) { return __uint2float_rn(x >> 8) * (1.0f / 16777216.0f); }
 
+// The same uniform scaled by 2^24: the integer x >> 8 as a float (exact), so
+// that u24(x) = u01(x) * 2^24 without the multiply.
+__device__ __forceinline__ float u24(uint32_t x) { return __uint2float_rn(x >> 8); }
+
 // Deterministic float32 e^y for y in (-17, 0]: y*log2(e) split into its
 // nearest integer k and a remainder f in [-1/2, 1/2]; 2^f by its Taylor series
 // (coefficients ln2^n/n!, n <= 6, Horner); 2^k added to the exponent field.
 // Each step is one IEEE round-to-nearest op, reproduced bit for bit by the
 // CPU restatement.
-__device__ __forceinline__ float det_expf(float y) {
+// det_expf(y) * 2^scale_log2: the scaling is folded into the exponent add,
+// exact while the result stays a normal float.
+template <int SCALE_LOG2 = 0>
+__device__ __forceinline__ float det_expf_scaled(float y) {
     const float t = __fmul_rn(y, 1.44269504f);
     const int k = __float2int_rn(t);
     const float f = __fsub_rn(t, __int2float_rn(k));
@@ -70,8 +77,9 @@ __device__ __forceinline__ float det_expf(float y) {
     p = __fmaf_rn(p, f, 2.4022651e-1f);
     p = __fmaf_rn(p, f, 6.9314718e-1f);
     p = __fmaf_rn(p, f, 1.0f);
-    return __int_as_float(__float_as_int(p) + (k << 23));
+    return __int_as_float(__float_as_int(p) + ((k + SCALE_LOG2) << 23));
 }
+__device__ __forceinline__ float det_expf(float y) { return det_expf_scaled<0>(y); }
 
 // Metropolis decision on y = -dE: qanneal accepts iff dE <= 0 || u < exp(-dE)
 // (annealer.cpp:55, sqa_annealer.cpp:198).  Moves with y <= -17 are rejected
@@ -80,12 +88,13 @@ __device__ __forceinline__ bool metropolis(float y, float u) {
     return y >= 0.0f || (y > -17.0f && u < det_expf(y));
 }
 
-// The same decision without divergent branches: e^y is evaluated on y
-// clamped to [-17, 0] and only used where -17 < y < 0, so the result is
-// identical to metropolis().
-__device__ __forceinline__ bool metropolis_nb(float y, float u) {
-    const float p = det_expf(fminf(fmaxf(y, -17.0f), 0.0f));
-    return (y >= 0.0f) | ((y > -17.0f) & (u < p));
+// The same decision without divergent branches, on the scaled uniform
+// u24 = u * 2^24: e^y * 2^24 is evaluated on y clamped to [-17, 0]; at y >= 0
+// it is exactly 2^24, above every u24 (at most 2^24 - 1), and the power-of-two
+// scaling is exact on both sides, so the result is identical to
+// metropolis(y, u).
+__device__ __forceinline__ bool metropolis_nb24(float y, float u24v) {
+    return (y > -17.0f) & (u24v < det_expf_scaled<24>(fminf(fmaxf(y, -17.0f), 0.0f)));
 }
 
 __device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
@@ -132,6 +141,9 @@ struct ProbDev {
     // with w1, w2 the term's other spins (-1: none).  Else null.
     const int *upd_ptr, *upd_run;
     const int4 *upd_rec;
+    // hubo with every term of degree <= 4: term t's spins {v0, v1, v2, v3}
+    // (-1: none) in one 16-byte record, for the per-step energy scan; else null
+    const int4 *trec;
     // sparse with integer couplings: CSR (column, value) pairs; else null
     const int2 *spcv;
 };
@@ -259,6 +271,41 @@ __device__ __forceinline__ double cell_energy(const ProbDev &P, const uint32_t *
     }
     pj = warp_sum_d(pj);
     return __dadd_rn(P.c, __dadd_rn(ph, pj));
+}
+
+// 1 when spin v of the bits S is down (-1).
+__device__ __forceinline__ uint32_t down_bit(const uint32_t *S, int v) { return ~(S[v >> 5] >> (v & 31)) & 1u; }
+
+// cell_energy<K_HUBO> of two slices Sa, Sb in one pass over the term records:
+// every term's sign is the parity of its down spins.  Each slice's sums take
+// the spins and terms in cell_energy's order, so both results equal it bit
+// for bit; the records are read once for the two slices.
+__device__ __forceinline__ void hubo_energy2(const ProbDev &P, const uint32_t *Sa, const uint32_t *Sb,
+                                             const float *h32, int lane, double *Ea, double *Eb) {
+    double ha = 0.0, hb = 0.0;
+    for (int i = lane; i < P.n; i += 32) {
+        const double hv = (double)h32[i];
+        ha = __dadd_rn(ha, spin_of(Sa, i) > 0 ? hv : -hv);
+        hb = __dadd_rn(hb, spin_of(Sb, i) > 0 ? hv : -hv);
+    }
+    double ja = 0.0, jb = 0.0;
+    for (int t = lane; t < P.T; t += 32) {
+        const int4 r = __ldg(P.trec + t);
+        const double w = (double)__ldg(P.coef32 + t);
+        uint32_t da = down_bit(Sa, r.x) ^ down_bit(Sa, r.y), db = down_bit(Sb, r.x) ^ down_bit(Sb, r.y);
+        if (r.z >= 0) {
+            da ^= down_bit(Sa, r.z);
+            db ^= down_bit(Sb, r.z);
+        }
+        if (r.w >= 0) {
+            da ^= down_bit(Sa, r.w);
+            db ^= down_bit(Sb, r.w);
+        }
+        ja = __dadd_rn(ja, da ? -w : w);
+        jb = __dadd_rn(jb, db ? -w : w);
+    }
+    *Ea = __dadd_rn(P.c, __dadd_rn(warp_sum_d(ha), warp_sum_d(ja)));
+    *Eb = __dadd_rn(P.c, __dadd_rn(warp_sum_d(hb), warp_sum_d(jb)));
 }
 
 // Float64 energy from the ORIGINAL float64 coefficients (reported energies).

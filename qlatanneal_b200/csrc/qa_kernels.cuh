@@ -148,7 +148,7 @@ __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int 
         const int nsum = (((pw >> lane) & 1u) ? 1 : -1) + (((nx >> lane) & 1u) ? 1 : -1);
         const int qv = si * nsum;
         const float tro = qv == 0 ? 0.0f : (qv > 0 ? T4 : -T4);
-        const float u = u01(pick(rnd, q & 3));
+        const float u = u24(pick(rnd, q & 3));
         const float hi = valid ? h[i] : 0.0f;
         att += (unsigned long long)min(32, n - (q << 5));
         uint32_t pending = FULL;
@@ -156,7 +156,7 @@ __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int 
             const float gi = valid ? gt[i] : 0.0f;
             const float loc = __fadd_rn(hi, gi);
             const float x = si > 0 ? loc : -loc;
-            const bool ok = valid & metropolis_nb(__fsub_rn(__fmul_rn(x, B), tro), u);
+            const bool ok = valid & metropolis_nb24(__fsub_rn(__fmul_rn(x, B), tro), u);
             const uint32_t m = __ballot_sync(FULL, ok) & pending;
             if (!m) break;
             const int j = __ffs(m) - 1;
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
                 const bool valid = i < n;
                 const uint32_t sword = S[q];
                 const int si = ((sword >> lane) & 1u) ? 1 : -1;
-                const float u = u01(pick(rnd, q & 3));
+                const float u = u24(pick(rnd, q & 3));
                 const float hi = valid ? h[i] : 0.0f;
                 att += (unsigned long long)min(32, n - (q << 5));
                 uint32_t pending = FULL;
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(32) sa_kernel(SAParams p) {
                     const float gi = valid ? g[i] : 0.0f;
                     const float loc = __fadd_rn(hi, gi);
                     const float x = si > 0 ? loc : -loc;
-                    const bool ok = valid & metropolis_nb(__fmul_rn(x, B), u);
+                    const bool ok = valid & metropolis_nb24(__fmul_rn(x, B), u);
                     const uint32_t m = __ballot_sync(FULL, ok) & pending;
                     if (!m) break;
                     const int j = __ffs(m) - 1;
@@ -362,7 +362,7 @@ __device__ __forceinline__ void cluster_move(const ProbDev &Pd, uint32_t *S, flo
     const uint32_t c3s = DOM_CSPIN | ((uint32_t)i << 8), c3b = DOM_CBOND | ((uint32_t)i << 8);
     const U4 w = philox(0u, ring, sigma, c3s, key);
     const int t0 = (int)(((unsigned long long)(w.x >> 8) * (unsigned long long)NP) >> 24);
-    const float u = u01(w.y);
+    const float u = u24(w.y);
     const int q = i >> 5;
     const uint32_t bit = 1u << (i & 31);
     const int ta = lane, tb = lane + 32;
@@ -414,7 +414,7 @@ __device__ __forceinline__ void cluster_move(const ProbDev &Pd, uint32_t *S, flo
     const double G = warp_sum_d(acc);
     const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)h[i], (double)(s0 * size)), G));
     const float y = __fsub_rn(__fmul_rn(x, B), __fmul_rn(__int2float_rn(kb), __fmul_rn(0.5f, T4)));
-    if (!metropolis_nb(y, u)) return;
+    if (!metropolis_nb24(y, u)) return;
     if (ta < NP && ((Cm >> ta) & 1ull)) S[ta * nw + q] ^= bit;
     if (tb < NP && ((Cm >> tb) & 1ull)) S[tb * nw + q] ^= bit;
     __syncwarp();
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                     rnd = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
                 const int i = (q << 5) | lane;
                 const bool valid = i < n;
-                const float u = u01(pick(rnd, q & 3));
+                const float u = u24(pick(rnd, q & 3));
                 const float hi = valid ? sm.h[i] : 0.0f;
                 if (threadIdx.x == 0) att_w += (unsigned long long)min(32, n - (q << 5));
                 uint32_t pending = FULL;
@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                     }
                     __syncthreads();
                     const float x = valid ? __double2float_rn(__dadd_rn(__dmul_rn((double)hi, (double)Sh), Gt)) : 0.0f;
-                    const bool ok = valid & metropolis_nb(__fmul_rn(x, B), u);
+                    const bool ok = valid & metropolis_nb24(__fmul_rn(x, B), u);
                     const uint32_t m = __ballot_sync(FULL, ok) & pending;
                     if (!m) break;
                     const int j = __ffs(m) - 1;
@@ -585,9 +585,22 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
             if (p.tr_bits && sw % p.tr_stride == 0) trace_rec(step, tr_s + tr_c + sw / p.tr_stride);
         }
         // ---- step end: energy of every slice, ring sum, best (sqa_annealer.cpp:455-469)
-        for (int t = warp; t < NP; t += W) {
-            const double E = cell_energy<KIND>(Pd, sm.S + t * nw, gbase + (long long)t * n, sm.h, lane);
-            if (lane == 0) sm.cellE[t] = E;
+        if (KIND == K_HUBO && Pd.trec) {
+            // slices t and t + W of this warp in one pass over the term records
+            for (int t = warp; t < NP; t += 2 * W) {
+                const int t2 = t + W < NP ? t + W : t;
+                double Ea, Eb;
+                hubo_energy2(Pd, sm.S + t * nw, sm.S + t2 * nw, sm.h, lane, &Ea, &Eb);
+                if (lane == 0) {
+                    sm.cellE[t] = Ea;
+                    if (t2 != t) sm.cellE[t2] = Eb;
+                }
+            }
+        } else {
+            for (int t = warp; t < NP; t += W) {
+                const double E = cell_energy<KIND>(Pd, sm.S + t * nw, gbase + (long long)t * n, sm.h, lane);
+                if (lane == 0) sm.cellE[t] = E;
+            }
         }
         if (p.ring_bond) {
             long long b = 0;

@@ -108,10 +108,10 @@ __device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, cons
     // s*(s_prev + s_next)/2 = 1 - (number of Trotter neighbours that differ)
     const int d = (int)(((sw ^ Sp[q]) >> lane) & 1u) + (int)(((sw ^ Sn[q]) >> lane) & 1u);
     const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
-    const float u = u01(rw);
+    const float u = u24(rw);
     const float hi = h[i];
     const int gi = (int)Gt[i];
-    bool ok = valid & metropolis_nb(
+    bool ok = valid & metropolis_nb24(
         __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gi)), sbit), B), tro), u);
     uint32_t m = __ballot_sync(FULL, ok);
     if (m == 0) return;
@@ -125,7 +125,7 @@ __device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, cons
         F |= 1u << j;
         if (lane != j) gk += (((sw ^ jd) >> j) & 1u) ? 2 : -2;
         const uint32_t pending = j == 31 ? 0u : (FULL << (j + 1));
-        ok = valid & metropolis_nb(
+        ok = valid & metropolis_nb24(
             __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gk)), sbit), B), tro), u);
         m = __ballot_sync(FULL, ok) & pending;
         ++acc;
@@ -161,7 +161,7 @@ __device__ __forceinline__ bool pm1_world_ok(const float *h, const int *Gs, cons
                                              const float *uw, int i, int n, int NP, float B) {
     const int sh = 2 * __popcll(Wc[i]) - NP;
     const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)h[i], (double)sh), (double)Gs[i]));
-    return (i < n) & metropolis_nb(__fmul_rn(x, B), uw[i]);
+    return (i < n) & metropolis_nb24(__fmul_rn(x, B), uw[i]);
 }
 
 // GT: field type (int: fields as int32; short: int16, for rings whose int32
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                     }
                 Gs[i] = gs;
                 const U4 r = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
-                uw[i] = u01(pick(r, q & 3));
+                uw[i] = u24(pick(r, q & 3));
             }
             if (threadIdx.x == 0) att_w += (unsigned long long)n;
             __syncthreads();
@@ -476,14 +476,14 @@ __global__ void __launch_bounds__(32) sa_pm1_kernel(SAParams p) {
                 const bool valid = i < n;
                 const uint32_t sword = S[q];
                 const uint32_t sbit = (sword >> lane) & 1u;
-                const float u = u01(pick(rnd, q & 3));
+                const float u = u24(pick(rnd, q & 3));
                 const float hi = h[i];
                 att += (unsigned long long)min(32, n - (q << 5));
                 uint32_t pending = FULL;
                 for (;;) {
                     const float gi = __int2float_rn(G[i]);
                     const float loc = __fadd_rn(hi, gi);
-                    const bool ok = valid & metropolis_nb(__fmul_rn(signed_by_bit(loc, sbit), B), u);
+                    const bool ok = valid & metropolis_nb24(__fmul_rn(signed_by_bit(loc, sbit), B), u);
                     const uint32_t m = __ballot_sync(FULL, ok) & pending;
                     if (!m) break;
                     const int j = __ffs(m) - 1;

@@ -68,13 +68,13 @@ __device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, u
         const uint32_t sbit = (sw >> lane) & 1u;
         const int d = (int)(((sw ^ Sp[q]) >> lane) & 1u) + (int)(((sw ^ Sn[q]) >> lane) & 1u);
         const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
-        const float u = u01(pick(rnd, q & 3));
+        const float u = u24(pick(rnd, q & 3));
         const float hi = h[i];
         uint32_t pending = FULL;
         for (;;) {
             const int g = valid ? sp_field(Pd.spcv, Pd.rowptr, St, i) : 0;
             const float loc = __fadd_rn(hi, __int2float_rn(g));
-            const bool ok = valid & metropolis_nb(__fsub_rn(__fmul_rn(signed_by_bit(loc, sbit), B), tro), u);
+            const bool ok = valid & metropolis_nb24(__fsub_rn(__fmul_rn(signed_by_bit(loc, sbit), B), tro), u);
             const uint32_t m = __ballot_sync(FULL, ok) & pending;
             if (!m) break;
             const int j = __ffs(m) - 1;
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
                         rnd = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
                     const int i = (q << 5) | lane;
                     const bool valid = i < n;
-                    const float u = u01(pick(rnd, q & 3));
+                    const float u = u24(pick(rnd, q & 3));
                     const double hi = (double)h[i];
                     att_w += (unsigned long long)min(32, n - (q << 5));
                     uint32_t pending = FULL;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
                             const int sh = 2 * __popcll(Wc[i] & pmask) - NP;
                             const int gs = sp_world_sum(Pd.spcv, Pd.rowptr, Wc, pmask, NP, i);
                             const float x = __double2float_rn(__dadd_rn(__dmul_rn(hi, (double)sh), (double)gs));
-                            ok = metropolis_nb(__fmul_rn(x, B), u);
+                            ok = metropolis_nb24(__fmul_rn(x, B), u);
                         }
                         const uint32_t m = __ballot_sync(FULL, ok) & pending;
                         if (!m) break;
