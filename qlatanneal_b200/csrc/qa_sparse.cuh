@@ -22,6 +22,8 @@ __host__ __device__ inline size_t sparse_smem_bytes(int P, int n) {
     b += (size_t)n32 * 8;                          // W (worldline bits)
     b += (size_t)n32 * 4;                          // h
     b += align_up((size_t)P * 8, 16);              // cellE
+    b += (size_t)n32 * 4;                          // worldline uniforms
+    b += align_up((size_t)nw * 8, 16);             // worldline decisions and marks per block
     b += 32 * 4 + 64;                              // partials, flags
     return b + 64;
 }
@@ -48,6 +50,16 @@ __device__ __forceinline__ int sp_world_sum(const int2 *cv, const int *rowptr, c
         g += c.y * (NP - 2 * __popcll((wi ^ Wc[c.x]) & pmask));
     }
     return g;
+}
+
+// The worldline move of spin i (sqa_annealer.cpp:294-315) on the current
+// worldlines: a function of W_i and its neighbours' worldlines only.
+__device__ __forceinline__ bool sp_world_ok(const ProbDev &Pd, const unsigned long long *Wc, const float *h,
+                                            unsigned long long pmask, int NP, int i, float B, float u) {
+    const int sh = 2 * __popcll(Wc[i] & pmask) - NP;
+    const int gs = sp_world_sum(Pd.spcv, Pd.rowptr, Wc, pmask, NP, i);
+    const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)h[i], (double)sh), (double)gs));
+    return metropolis_nb24(__fmul_rn(x, B), u);
 }
 
 __device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, unsigned long long *Wc,
@@ -98,6 +110,10 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
     unsigned long long *Wc = reinterpret_cast<unsigned long long *>(ptr); ptr += (size_t)n32 * 8;
     float *h = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * 4;
     double *cellE = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)NP * 8, 16);
+    float *uw = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * 4;
+    uint32_t *wmask = reinterpret_cast<uint32_t *>(ptr);  // [nw] decisions on the sweep's starting state
+    uint32_t *wdirty = wmask + nw;                        // [nw] spins whose neighbours have flipped since
+    ptr += align_up((size_t)nw * 8, 16);
     int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
     int *flag = reinterpret_cast<int *>(ptr);  // [0]: best slice, [3]: lowest slice (final state)
 
@@ -149,36 +165,64 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
             }
             if (p.bsamp) record_bond_sample(p, S, NP, nw, n, wpart, W, step, sw);
         }
-        // worldline sweeps: one warp, spins in order, sums from the worldline bits
+        // worldline sweeps, spins in order, sums from the worldline bits.  Every
+        // warp first evaluates all spins' moves on the sweep's starting
+        // worldlines; warp 0 then takes the spins in order.  A move depends only
+        // on the spin's own worldline and its neighbours', so a decision stands
+        // unless a neighbour flipped earlier in the sweep: such spins are marked
+        // and evaluated again when their turn comes.  Every decision is thus
+        // taken on the state the one-spin-at-a-time sweep sees.
         for (int sw = 0; sw < wls; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * p.wls + sw);
+            for (int i = threadIdx.x; i < n32; i += blockDim.x) {  // a warp covers one 32-spin block
+                const int q = i >> 5, l = i & 31;
+                const U4 r = philox((uint32_t)(((q >> 2) << 5) | l), (uint32_t)slot, sigma, DOM_WORLD, R.key);
+                const float u = u24(pick(r, q & 3));
+                uw[i] = u;
+                const bool ok = i < n && sp_world_ok(Pd, Wc, h, pmask, NP, i, B, u);
+                const uint32_t m = __ballot_sync(FULL, ok);
+                if (l == 0) {
+                    wmask[q] = m;
+                    wdirty[q] = 0u;
+                }
+            }
+            if (threadIdx.x == 0) att_w += (unsigned long long)n;
+            __syncthreads();
             if (warp == 0) {
-                const uint32_t sigma = (uint32_t)(step * p.wls + sw);
-                U4 rnd = {0, 0, 0, 0};
                 for (int q = 0; q < nw; ++q) {
-                    if ((q & 3) == 0)
-                        rnd = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
                     const int i = (q << 5) | lane;
                     const bool valid = i < n;
-                    const float u = u24(pick(rnd, q & 3));
-                    const double hi = (double)h[i];
-                    att_w += (unsigned long long)min(32, n - (q << 5));
+                    const float u = uw[i];
+                    uint32_t m = wmask[q];
+                    const uint32_t dq = wdirty[q];  // neighbours flipped in earlier blocks
+                    if (dq) {
+                        const bool ok = valid && ((dq >> lane) & 1u) && sp_world_ok(Pd, Wc, h, pmask, NP, i, B, u);
+                        m = (m & ~dq) | (__ballot_sync(FULL, ok) & dq);
+                    }
                     uint32_t pending = FULL;
-                    for (;;) {
-                        bool ok = false;
-                        if (valid) {
-                            const int sh = 2 * __popcll(Wc[i] & pmask) - NP;
-                            const int gs = sp_world_sum(Pd.spcv, Pd.rowptr, Wc, pmask, NP, i);
-                            const float x = __double2float_rn(__dadd_rn(__dmul_rn(hi, (double)sh), (double)gs));
-                            ok = metropolis_nb24(__fmul_rn(x, B), u);
-                        }
-                        const uint32_t m = __ballot_sync(FULL, ok) & pending;
-                        if (!m) break;
-                        const int j = __ffs(m) - 1;
+                    while (m & pending) {
+                        const int j = __ffs(m & pending) - 1;
+                        const int jj = (q << 5) | j;
                         for (int t = lane; t < NP; t += 32) S[t * nw + q] ^= 1u << j;
-                        if (lane == j) Wc[i] ^= pmask;
-                        __syncwarp();
+                        if (lane == j) Wc[jj] ^= pmask;
                         ++acc_w;
                         pending = j == 31 ? 0u : (FULL << (j + 1));
+                        // jj's neighbours: later spins of this block now, later blocks marked
+                        uint32_t here = 0;
+                        const int e0 = __ldg(Pd.rowptr + jj), e1 = __ldg(Pd.rowptr + jj + 1);
+                        for (int e = e0 + lane; e < e1; e += 32) {
+                            const int v = __ldg(Pd.spcv + e).x;
+                            if ((v >> 5) == q) here |= 1u << (v & 31);
+                            else if ((v >> 5) > q) atomicOr(wdirty + (v >> 5), 1u << (v & 31));
+                        }
+                        here = __reduce_or_sync(FULL, here) & pending;
+                        __syncwarp();
+                        if (here) {
+                            const bool ok =
+                                valid && ((here >> lane) & 1u) && sp_world_ok(Pd, Wc, h, pmask, NP, i, B, u);
+                            m = (m & ~here) | (__ballot_sync(FULL, ok) & here);
+                        }
+                        __syncwarp();
                     }
                 }
             }
