@@ -82,19 +82,37 @@ __device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, u
         const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
         const float u = u24(pick(rnd, q & 3));
         const float hi = h[i];
-        uint32_t pending = FULL;
-        for (;;) {
+        // a lane's move depends on its own and its neighbours' bits: after a
+        // flip only the flipped spin's neighbours later in this block are
+        // evaluated again (later blocks read their fields from the current
+        // bits anyway), so every decision is the spin-at-a-time sweep's
+        auto decide = [&]() {
             const int g = valid ? sp_field(Pd.spcv, Pd.rowptr, St, i) : 0;
             const float loc = __fadd_rn(hi, __int2float_rn(g));
-            const bool ok = valid & metropolis_nb24(__fsub_rn(__fmul_rn(signed_by_bit(loc, sbit), B), tro), u);
-            const uint32_t m = __ballot_sync(FULL, ok) & pending;
-            if (!m) break;
-            const int j = __ffs(m) - 1;
+            return valid & metropolis_nb24(__fsub_rn(__fmul_rn(signed_by_bit(loc, sbit), B), tro), u);
+        };
+        uint32_t m = __ballot_sync(FULL, decide());
+        uint32_t pending = FULL;
+        while (m & pending) {
+            const int j = __ffs(m & pending) - 1;
+            const int jj = (q << 5) | j;
             if (lane == 0) St[q] = St[q] ^ (1u << j);
             if (lane == j) atomicXor(Wc + i, 1ull << t);
-            __syncwarp();
             ++acc;
             pending = j == 31 ? 0u : (FULL << (j + 1));
+            uint32_t here = 0;
+            const int e0 = __ldg(Pd.rowptr + jj), e1 = __ldg(Pd.rowptr + jj + 1);
+            for (int e = e0 + lane; e < e1; e += 32) {
+                const int v = __ldg(Pd.spcv + e).x;
+                if ((v >> 5) == q) here |= 1u << (v & 31);
+            }
+            here = __reduce_or_sync(FULL, here) & pending;
+            __syncwarp();
+            if (here) {
+                const bool ok = ((here >> lane) & 1u) && decide();
+                m = (m & ~here) | (__ballot_sync(FULL, ok) & here);
+            }
+            __syncwarp();
         }
     }
 }
