@@ -102,10 +102,17 @@ class Clocks:
     def __enter__(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-i", str(self.device), "-lms", "200"], stdout=self.f,
+                                       "-i", str(self.device), "-lms", "50"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.p = None
+        # the sampler is running once its first row is out (that row predates
+        # the timed region and is dropped when later rows exist)
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 5.0:
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
@@ -128,6 +135,8 @@ class Clocks:
             os.unlink(self.f.name)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        if len(rows) > 1:
+            rows = rows[1:]
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -500,7 +509,7 @@ def flush_l2(torch, dev):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
