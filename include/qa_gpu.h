@@ -59,6 +59,16 @@ QA_API int qa_device_count(int *count);
 QA_API int qa_create(qa_ctx **out, int device);
 QA_API int qa_destroy(qa_ctx *ctx);
 
+/* Field-drift check of the incremental local-field updates (the property
+ * tests/test_higher_order_ising.cpp:149-167 checks for the reference's float64
+ * cache).  tolerance > 0: every later SA, SQA and SQA-PT call on this context
+ * recomputes the float32 field caches in float64 after the run, reports the
+ * largest deviation in qa_stats.max_field_drift and returns QA_ERR_DRIFT when
+ * it exceeds the tolerance (outputs are written either way).  Kernels with
+ * exact integer fields (+-1 dense, integer sparse) report 0.  tolerance <= 0
+ * (the default): off. */
+QA_API int qa_set_drift_check(qa_ctx *ctx, double tolerance);
+
 /* ---- problems (device copies of one model instance) ------------------- */
 
 /* DenseIsing(h, J, n, c) (dense_ising.hpp:17-21): E = c + sum h s + sum_{i<j} J_ij s_i s_j.
@@ -108,6 +118,10 @@ typedef struct {
     int64_t launches;                               /* kernels launched by the call */
     int64_t sweep_launches;                         /* of which sweep-kernel launches */
     int64_t h2d_bytes, d2h_bytes;                   /* host<->device bytes moved by the call */
+    double max_field_drift;                         /* with a drift check on (qa_set_drift_check): the
+                                                       largest |cached float32 local field - float64
+                                                       recompute from the same couplings| over every
+                                                       replica, slice and spin after the run; else 0 */
 } qa_stats;
 
 /* ---- SA: Annealer::run (annealer.cpp:33-75) ------------------------------ */

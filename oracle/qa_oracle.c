@@ -472,6 +472,15 @@ static void apply_flip(const or_model *M, const int8_t *s, float *g, int j, int 
     }
 }
 
+/* Flip spin i of s (in place) and update the float32 field cache g the way
+   the sweeps do (for the field-drift restatement of
+   test_higher_order_ising.cpp:149-167). */
+OR_EXPORT void or_flip_update(const or_model *M, int8_t *s, float *g, int i) {
+    const int so = s[i];
+    s[i] = (int8_t)-so;
+    apply_flip(M, s, g, i, so);
+}
+
 /* float64 sum in warp order: 32 lane-strided partials, then xor butterfly */
 static double wsum(const double *v, int n) {
     double p[32];

@@ -32,7 +32,9 @@ from .annealers import (  # noqa: F401
     SQAParallelTemperingAnnealer,
     SQAChiAnnealer,
     BatchRunner,
+    set_drift_check,
 )
+from ._lib import FieldDriftError  # noqa: F401
 from .observers import (  # noqa: F401
     Observer,
     SweepObserver,

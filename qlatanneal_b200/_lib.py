@@ -18,7 +18,7 @@ QA_OK, QA_ERR_ARG, QA_ERR_CUDA, QA_ERR_OOM, QA_ERR_TIMEOUT, QA_ERR_DRIFT, QA_ERR
 
 # Every symbol include/qa_gpu.h declares (checked by the CPU test suite).
 EXPORTED = [
-    "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy",
+    "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy", "qa_set_drift_check",
     "qa_problem_dense", "qa_problem_qubo", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
     "qa_sa_run", "qa_sa_trace_run", "qa_replica_run", "qa_sqa_run", "qa_sqa_trace_run", "qa_sqa_opt_run", "qa_sqapt_run", "qa_sqapt_opt_run", "qa_pt_run",
     "qa_chi_run", "qa_chi_pilot",
@@ -35,7 +35,8 @@ class qa_stats(C.Structure):
     _fields_ = [("slice_attempts", C.c_int64), ("slice_accepts", C.c_int64),
                 ("worldline_attempts", C.c_int64), ("worldline_accepts", C.c_int64),
                 ("sweep_ms", C.c_double), ("total_ms", C.c_double), ("launches", C.c_int64),
-                ("sweep_launches", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
+                ("sweep_launches", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+                ("max_field_drift", C.c_double)]
 
 
 class qa_sa_params(C.Structure):
@@ -145,6 +146,7 @@ def load():
         L.qa_device_count.argtypes = [C.POINTER(C.c_int)]
         L.qa_create.argtypes = [C.POINTER(vp), i]
         L.qa_destroy.argtypes = [vp]
+        L.qa_set_drift_check.argtypes = [vp, d]
         L.qa_problem_dense.argtypes = [vp, i, vp, vp, d, C.POINTER(vp)]
         L.qa_problem_qubo.argtypes = [vp, i, vp, vp, vp, C.POINTER(vp)]
         L.qa_problem_sparse.argtypes = [vp, i, vp, i, vp, vp, vp, d, C.POINTER(vp)]
@@ -192,11 +194,18 @@ def last_error() -> str:
     return buf.value.decode(errors="replace")
 
 
+class FieldDriftError(RuntimeError):
+    """The drift check found the incremental float32 local fields farther
+    from a float64 recompute than the tolerance (QA_ERR_DRIFT)."""
+
+
 def check(rc: int) -> None:
     """Map a status code onto the exception qanneal raises for the same failure."""
     if rc == QA_OK:
         return
     msg = last_error()
+    if rc == QA_ERR_DRIFT:
+        raise FieldDriftError(msg)
     if rc == QA_ERR_ARG:
         raise ValueError(msg)
     if rc == QA_ERR_UNSUPPORTED:

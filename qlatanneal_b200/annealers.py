@@ -164,11 +164,23 @@ class RunStats:
     sweep_launches: int = 0
     h2d_bytes: int = 0
     d2h_bytes: int = 0
+    max_field_drift: float = 0.0
 
     @classmethod
     def from_c(cls, s: "_lib.qa_stats") -> "RunStats":
         return cls(s.slice_attempts, s.slice_accepts, s.worldline_attempts, s.worldline_accepts, s.sweep_ms,
-                   s.total_ms, s.launches, s.sweep_launches, s.h2d_bytes, s.d2h_bytes)
+                   s.total_ms, s.launches, s.sweep_launches, s.h2d_bytes, s.d2h_bytes, s.max_field_drift)
+
+
+def set_drift_check(tolerance: float, device: Optional[int] = None) -> None:
+    """Field-drift check of the incremental local-field caches (the property
+    test_higher_order_ising.cpp:149-167 checks for the reference's float64
+    cache): with tolerance > 0, later SA / SQA / SQA-PT runs on the device
+    recompute the float32 fields in float64 after the run, report the largest
+    deviation as ``last_stats.max_field_drift`` and raise
+    ``FieldDriftError`` above the tolerance.  0 turns it off."""
+    eng = _lib.Engine.get(device)
+    _lib.check(eng.L.qa_set_drift_check(eng.h, float(tolerance)))
 
 
 class _Seeded:

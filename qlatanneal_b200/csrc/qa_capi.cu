@@ -159,6 +159,7 @@ struct qa_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int smem_optin = 0;
+    double drift_tol = 0.0;  // > 0: field-drift check after SA / SQA / SQA-PT runs
     static constexpr int kWsSlots = 48;
     DevBuf ws[kWsSlots];
 };
@@ -199,7 +200,7 @@ namespace {
 enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
               W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP, W_JP,
               W_BSAMP, W_SSAVE, W_FSAVE, W_CBESTE, W_CBSTEP, W_CBITS, W_CBOND, W_FLAG, W_QSTAGE,
-              W_TRB, W_TRE, W_TREB, W_TREE, W_RSPIN, W_COUNT };
+              W_TRB, W_TRE, W_TREB, W_TREE, W_RSPIN, W_DRIFT, W_COUNT };
 static_assert(W_COUNT <= qa_ctx::kWsSlots, "qa_ctx::ws has a slot per WsSlot");
 
 int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
@@ -1038,6 +1039,47 @@ int qa_problem_hubo(qa_ctx *ctx, int n, const double *h, int n_terms, const int6
     return QA_OK;
 }
 
+// ---------------------------------------------------------------------- drift check
+int qa_set_drift_check(qa_ctx *ctx, double tolerance) {
+    if (!ctx) return fail(QA_ERR_ARG, "null context");
+    ctx->drift_tol = tolerance > 0.0 ? tolerance : 0.0;
+    return QA_OK;
+}
+
+// After a run on float32 field caches (field rows of ring r at
+// fields + field_off, stride n): the drift check when the context has one.
+// Sets stats->max_field_drift; QA_ERR_DRIFT above the tolerance.
+static int check_drift(qa_ctx *ctx, bool float_fields, int kind, const ProbDev *d_probs, const RingDev *d_rings,
+                       int nr, const uint32_t *d_spins, const float *d_fields, int P, int n_max, int nw_max,
+                       qa_stats *stats) {
+    if (stats) stats->max_field_drift = 0.0;
+    if (!(ctx->drift_tol > 0.0) || !float_fields) return QA_OK;
+    unsigned long long *d_max;
+    QA_TRY(ws_array(ctx, W_DRIFT, 1, &d_max));
+    QA_CK(cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), ctx->stream));
+    const int zb = std::max(1, std::min(64, (n_max + 127) / 128));
+    int rc = QA_OK;
+    dispatch_kind(kind, [&](auto K) {
+        field_drift_kernel<decltype(K)::value><<<dim3(nr, P, zb), 128, nw_max * 4, ctx->stream>>>(
+            d_probs, d_rings, d_spins, d_fields, P, d_max);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(QA_ERR_CUDA, "field_drift_kernel launch failed");
+    });
+    QA_TRY(rc);
+    unsigned long long bits = 0;
+    QA_CK(cudaMemcpyAsync(&bits, d_max, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    double d;
+    std::memcpy(&d, &bits, sizeof(d));
+    if (stats) stats->max_field_drift = d;
+    if (d > ctx->drift_tol) {
+        char msg[160];
+        std::snprintf(msg, sizeof(msg), "incremental local fields drifted by %.3g from a float64 recompute (tolerance %.3g)",
+                      d, ctx->drift_tol);
+        return fail(QA_ERR_DRIFT, msg);
+    }
+    return QA_OK;
+}
+
 // ---------------------------------------------------------------------- SA
 // SA reads (qa_sa_run) and SA replicas (qa_replica_run, which adds the
 // magnetisation trace and the step of each replica's best).
@@ -1213,6 +1255,7 @@ static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
         stats->worldline_attempts = stats->worldline_accepts = 0;
         stats->sweep_ms = a;
         stats->total_ms = b;
+        stats->max_field_drift = 0.0;
         stats->launches = pm1 ? 3 : 4;
         stats->sweep_launches = 1;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + sizeof(float) * A.size() +
@@ -1220,6 +1263,7 @@ static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
         stats->d2h_bytes = (int64_t)(sizeof(double) * trace.size() + sizeof(double) * nr +
                                      sizeof(uint32_t) * bits.size() + sizeof(cnt));
     }
+    QA_TRY(check_drift(ctx, !pm1, kind, d_probs, d_rings, nr, d_spins, d_fields, 1, n_max, L.nw_max, stats));
     return QA_OK;
 }
 
@@ -1479,6 +1523,7 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
         stats->worldline_accepts = (int64_t)cnt[3];
         stats->sweep_ms = a;
         stats->total_ms = b;
+        stats->max_field_drift = 0.0;
         stats->sweep_launches = n_seg;
         stats->launches = (pl.own_fields() ? 2 : 3) + n_seg;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * steps +
@@ -1486,6 +1531,8 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
         stats->d2h_bytes = (int64_t)(sizeof(double) * (size_t)nr * steps + (2 * sizeof(double) + sizeof(int)) * nr +
                                      sizeof(uint32_t) * bits.size() + sizeof(cnt));
     }
+    QA_TRY(check_drift(ctx, !pl.own_fields(), kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max,
+                       stats));
     return QA_OK;
 }
 
@@ -1883,6 +1930,7 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
         stats->worldline_accepts = (int64_t)cnt[3];
         stats->sweep_ms = a;
         stats->total_ms = b;
+        stats->max_field_drift = 0.0;
         stats->sweep_launches = n_launch;
         stats->launches = (pl.own_fields() ? 2 : 3) + n_launch;
         stats->h2d_bytes = 0;
@@ -1965,6 +2013,7 @@ static int pt_collect(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
         stats->worldline_accepts = (int64_t)cnt[3];
         stats->sweep_ms = a;
         stats->total_ms = b;
+        stats->max_field_drift = 0.0;
     }
     *d2h = (int64_t)(sizeof(double) * (3 * (size_t)nr + avg.size() + swp.size()) + 3 * sizeof(int) * (size_t)nr +
                      sizeof(int) * rin.size() + sizeof(uint32_t) * 2 * bits.size() + sizeof(cnt));
@@ -2110,6 +2159,8 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
                                      sizeof(int) * (size_t)reads_total * Rn);
         stats->d2h_bytes = d2h;
     }
+    QA_TRY(check_drift(ctx, !pl.own_fields(), kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max,
+                       stats));
     return QA_OK;
 }
 
@@ -2698,6 +2749,7 @@ int qa_chi_pilot(qa_ctx *ctx, const qa_problem *const *problems, int n_problems,
         stats->slice_accepts = (int64_t)cnt[1];
         stats->sweep_ms = ms;
         stats->total_ms = ms;
+        stats->max_field_drift = 0.0;
         stats->sweep_launches = 1;
         stats->launches = launches;
         stats->h2d_bytes = h2d;
@@ -2902,6 +2954,7 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
         stats->worldline_accepts = (int64_t)cnt_total[3];
         stats->sweep_ms = a + pilot_ms;
         stats->total_ms = b + pilot_ms;
+        stats->max_field_drift = 0.0;
         stats->sweep_launches = n_seg + (prm->scan_chi_in ? 0 : 1);
         stats->launches = launches;
         stats->h2d_bytes = h2d;

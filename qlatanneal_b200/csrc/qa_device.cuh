@@ -218,7 +218,7 @@ __device__ __forceinline__ void apply_flip(const ProbDev &P, float *g, const uin
 // Local field of spin i (J.s part, no h), accumulated in float64 in the
 // model's natural order, then rounded: the field-cache initialisation.
 template <int KIND>
-__device__ __forceinline__ float field_init_one(const ProbDev &P, const uint32_t *S, int i) {
+__device__ __forceinline__ double field_exact64(const ProbDev &P, const uint32_t *S, int i) {
     double acc = 0.0;
     if (KIND == K_DENSE) {
         // J32 is symmetric: read column i (coalesced across the lanes' rows)
@@ -243,7 +243,12 @@ __device__ __forceinline__ float field_init_one(const ProbDev &P, const uint32_t
             acc = __dadd_rn(acc, sg > 0 ? w : -w);
         }
     }
-    return __double2float_rn(acc);
+    return acc;
+}
+
+template <int KIND>
+__device__ __forceinline__ float field_init_one(const ProbDev &P, const uint32_t *S, int i) {
+    return __double2float_rn(field_exact64<KIND>(P, S, i));
 }
 
 // Tracking energy of one slice from its field cache (whole warp, all lanes

@@ -124,6 +124,29 @@ __global__ void init_fields_kernel(const ProbDev *probs, const RingDev *rings, c
         g[i] = field_init_one<KIND>(Pd, sS, i);
 }
 
+// Drift of the float32 field caches: the largest |g - float64 recompute from
+// the same float32 couplings| over every (ring, slice, spin) of the grid
+// (blockIdx.x ring, blockIdx.y slice).  Non-negative doubles order as their
+// bit patterns, so the maximum is an integer atomicMax.
+template <int KIND>
+__global__ void field_drift_kernel(const ProbDev *probs, const RingDev *rings, const uint32_t *spins,
+                                   const float *fields, int P, unsigned long long *max_bits) {
+    extern __shared__ uint32_t sS[];
+    const RingDev R = rings[blockIdx.x];
+    const ProbDev Pd = probs[R.prob];
+    const int t = blockIdx.y;
+    for (int q = threadIdx.x; q < Pd.nw; q += blockDim.x) sS[q] = spins[R.spin_off + (long long)t * Pd.nw + q];
+    __syncthreads();
+    const float *g = fields + R.field_off + (long long)t * Pd.n;
+    double mx = 0.0;
+    for (int i = blockIdx.z * blockDim.x + threadIdx.x; i < Pd.n; i += gridDim.z * blockDim.x)
+        mx = fmax(mx, fabs((double)g[i] - field_exact64<KIND>(Pd, sS, i)));
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(max_bits, (unsigned long long)__double_as_longlong(mx));
+    (void)P;
+}
+
 // ------------------------------------------------------------------ slice sweep
 // One warp sweeps slice t of a ring (sqa_annealer.cpp:180-209 with the parity
 // schedule of sqa_chi_annealer.cpp:90-122).

@@ -202,6 +202,7 @@ extern "C" int qa_sa_dense_run_noalloc(int device, void *stream, int n, const do
         stats->slice_attempts = (int64_t)cnt[0];
         stats->slice_accepts = (int64_t)cnt[1];
         stats->launches = 6;
+        stats->max_field_drift = 0.0;
         stats->sweep_launches = 1;
     }
     NA_CK(cudaStreamSynchronize(st));

@@ -89,6 +89,7 @@ class Oracle:
                                        [C.c_int, C.c_int, C.c_uint64, C.c_int, _i8p, C.POINTER(C.c_double), _f8p,
                                         _i8p] + [_f8p] * 5)
         L.or_trace_set.argtypes = [C.c_int] + [C.c_void_p] * 7
+        L.or_flip_update.argtypes = [C.c_void_p, _i8p, _f4p, C.c_int]
         L.or_chi_schedule.argtypes = ([C.c_int, _f8p, _f8p, _f8p] + [C.c_double] * 4 + [C.c_int, C.c_int] +
                                       [C.c_double] * 3 + [_f8p] * 4)
         L.or_chi_run.argtypes = ([C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 3 + [C.c_int] * 5 +
@@ -159,6 +160,10 @@ class Oracle:
 
     def delta_energy64(self, m, s, flip):
         return float(self.L.or_delta_energy64(m.h, np.ascontiguousarray(s, np.int8), flip))
+
+    def flip_update(self, m, s, g, i):
+        """Flip spin i of s in place and update the float32 fields g in place."""
+        self.L.or_flip_update(m.h, s, g, i)
 
     def fields(self, m, s):
         g = np.zeros(m.n, np.float32)
