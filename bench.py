@@ -15,6 +15,9 @@ Metric: site-attempts/s (a slice proposal counts 1 site, a worldline proposal P)
   roofline : the sweep kernel's algorithmic bytes (per-attempt field/spin reads
           plus one coupling row per accepted flip, 1 byte per +/-1 coupling)
           over its event-timed duration, against the measured HBM copy bandwidth.
+          The unit is the sweep region of one anneal: with more reads than SMs
+          the rings run as many short concurrent launches (groups of rings on
+          side streams), so a single launch has no meaningful duration of its own.
   cpu_baseline : qanneal's own SQAAnnealer (compiled from its sources under
           oracle/_ref) on a bounded sample of the same workload, all host threads.
 
@@ -72,7 +75,8 @@ def load_peaks():
 
 
 def load_traffic():
-    """dram bytes per sweep-kernel launch from the committed ncu summary, or None."""
+    """dram bytes of the sweep kernel per anneal (all its launches in one bench
+    step) from the committed ncu summary, or None."""
     p = os.path.join(ROOT, "profiles", "ring_kernel_traffic.txt")
     if not os.path.exists(p):
         return None
@@ -82,7 +86,7 @@ def load_traffic():
             k, v = line.split(":", 1)
             vals[k.strip()] = v.strip()
     try:
-        return float(vals["dram_bytes_per_launch"])
+        return float(vals["dram_bytes_per_anneal"])
     except (KeyError, ValueError):
         return None
 
@@ -513,6 +517,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reads", type=int, default=WL["reads"],
+                    help="sqa: reads per GPU (at most the SM count: one whole-grid launch per segment)")
     ap.add_argument("--workload", default="sqa", choices=["sqa", "chi-ttt"] + sorted(SIDE),
                     help="sqa: the sweep-throughput line (default); chi-ttt: time-to-target of SQA-Chi with the "
                          "learned vs the pilot-scan schedule, training set included; " + "; ".join(
@@ -546,7 +552,9 @@ def main():
     from qlatanneal_b200.distributed import minloc_best, read_block
     _lib.Engine.get(local)
 
-    n, P, reads = WL["n"], WL["P"], WL["reads"]
+    n, P, reads = WL["n"], WL["P"], args.reads
+    if reads < 1:
+        raise SystemExit("--reads must be >= 1")
     h, J = instance()
     betas, gammas = schedule()
     sched = qa.SQASchedule.from_vectors(betas, gammas)
@@ -611,9 +619,9 @@ def main():
     peak, peak_kind = load_peaks()
     bytes_step = algorithmic_bytes(stats[0], n, P)
     launches = stats[0].sweep_launches
-    avg_launch_ms = sweep_ms / (args.steps * launches)
-    achieved = (bytes_step / launches) / (avg_launch_ms / 1e3) / 1e9
-    traffic = load_traffic()
+    sweep_ms_step = sweep_ms / args.steps
+    achieved = bytes_step / (sweep_ms_step / 1e3) / 1e9
+    traffic = load_traffic() if reads == WL["reads"] else None
 
     # best energy over all ranks (the MINLOC + broadcast of qanneal's MPI reads helper)
     i_best = int(np.argmin([r.best_energy for r in res]))
@@ -640,7 +648,8 @@ def main():
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "n": n, "trotter_slices": P, "reads_per_gpu": reads,
+            "config": {"workload": WORKLOAD_NAME.replace("%d reads" % WL["reads"], "%d reads" % reads), "n": n,
+                       "trotter_slices": P, "reads_per_gpu": reads,
                        "steps": WL["steps"], "sweeps_per_step": [WL["spb"], WL["wls"]],
                        "site_attempts_per_step": sites_step, "l2": "flushed (256 MiB write) between steps",
                        "parallelism": f"replicas x{world}", "best_energy": best_E,
@@ -648,9 +657,10 @@ def main():
                        "worldline_accept_rate": st.worldline_accepts / max(1, st.worldline_attempts)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "ring_kernel (slice + worldline sweeps)",
-                         "avg_launch_ms": avg_launch_ms, "launches_per_step": launches,
-                         "algorithmic_bytes_per_launch": bytes_step / launches},
+                         "kernel": "ring_pm1_kernel (slice + worldline sweeps)",
+                         "per": "sweep region of one anneal (all ring launches of one step)",
+                         "sweep_ms_per_step": sweep_ms_step, "launches_per_step": launches,
+                         "algorithmic_bytes_per_step": bytes_step},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "site-attempts/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * float(np.mean(e2e_times))},

@@ -159,7 +159,11 @@ struct qa_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int smem_optin = 0;
+    int sms = 0;             // streaming multiprocessors of the device
     double drift_tol = 0.0;  // > 0: field-drift check after SA / SQA / SQA-PT runs
+    // side streams for the rotated ring launches (run_rings_rotated) and their events
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> side_ev;
     static constexpr int kWsSlots = 48;
     DevBuf ws[kWsSlots];
 };
@@ -569,7 +573,9 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
 }
 
 // One launch of the planned ring kernel over steps [rp.step0, rp.step1).
-int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n_rings) {
+int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n_rings,
+                 cudaStream_t stream = nullptr) {
+    cudaStream_t strm = stream ? stream : ctx->stream;
     rp.W = pl.W;
     rp.smem_fields = pl.smem_fields;
     if (pl.pm1) {
@@ -577,14 +583,14 @@ int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n
                                    : (pl.jw_smem ? ring_pm1_kernel<short, true> : ring_pm1_kernel<short, false>);
         if (pl.smem > 48 * 1024)
             QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
-        kern<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
+        kern<<<n_rings, 32 * pl.W, pl.smem, strm>>>(rp);
         QA_CK(cudaGetLastError());
         return QA_OK;
     }
     if (pl.sparse) {
         if (pl.smem > 48 * 1024)
             QA_CK(cudaFuncSetAttribute(ring_sparse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
-        ring_sparse_kernel<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
+        ring_sparse_kernel<<<n_rings, 32 * pl.W, pl.smem, strm>>>(rp);
         QA_CK(cudaGetLastError());
         return QA_OK;
     }
@@ -592,7 +598,7 @@ int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n
     dispatch_kind(kind, [&](auto Kd) {
         auto kern = ring_kernel<decltype(Kd)::value>;
         if (pl.smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
-        kern<<<n_rings, 32 * pl.W, pl.smem, ctx->stream>>>(rp);
+        kern<<<n_rings, 32 * pl.W, pl.smem, strm>>>(rp);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, std::string("ring_kernel launch: ") + cudaGetErrorString(e));
     });
@@ -604,6 +610,64 @@ int ws_array(qa_ctx *ctx, int slot, size_t count, T **out) {
     void *v;
     QA_TRY(ws_get(ctx, slot, sizeof(T) * count, &v));
     *out = static_cast<T *>(v);
+    return QA_OK;
+}
+
+// Ring groups and segment length of a rotated run (run_rings_rotated).
+struct RotPlan {
+    int G, streams, seg, launches;
+};
+static RotPlan rot_plan(int nr, int steps) {
+    RotPlan r;
+    r.G = std::max(2, (nr + 127) / 128);  // at most 128 streams, one group each
+    r.streams = (nr + r.G - 1) / r.G;
+    r.seg = std::max(25, std::min(100, steps / 8));
+    r.launches = r.streams * ((steps + r.seg - 1) / r.seg);
+    return r;
+}
+
+// Steps [0, steps) of every ring as independent chains of short launches:
+// groups of G rings, each group on its own stream, one launch per segment.
+// When the rings outnumber the SMs but do not fill whole waves, some SMs hold
+// two rings and some one; a group that ran alone finishes its segment early
+// and its next launch takes whatever slot is free, so rings move between
+// shared and lone SMs at segment boundaries and all finish together, instead
+// of the lone SMs idling while the shared ones finish.  Each ring keeps its
+// key, counters and records (the per-ring pointers are offset per group), so
+// the results are those of whole-grid launches.  Joins into the context
+// stream.
+static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const RingParams &rp, int nr, int steps) {
+    const RotPlan rt = rot_plan(nr, steps);
+    while ((int)ctx->side.size() < rt.streams) {
+        cudaStream_t x;
+        cudaEvent_t e;
+        QA_CK(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        ctx->side.push_back(x);
+        QA_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->side_ev.push_back(e);
+    }
+    // fork: every side stream starts after the context stream's work so far
+    QA_CK(cudaEventRecord(ctx->side_ev[0], ctx->stream));
+    for (int k = 0; k < rt.streams; ++k) QA_CK(cudaStreamWaitEvent(ctx->side[k], ctx->side_ev[0], 0));
+    for (int s0 = 0; s0 < steps; s0 += rt.seg) {  // segment-major issue keeps the streams in step
+        for (int k = 0; k < rt.streams; ++k) {
+            const int g0 = k * rt.G;
+            RingParams r2 = rp;
+            r2.rings = rp.rings + g0;
+            r2.best_E = rp.best_E + g0;
+            r2.best_step = rp.best_step + g0;
+            r2.best_bits = rp.best_bits + (size_t)g0 * rp.nw_max;
+            if (rp.ring_sum) r2.ring_sum = rp.ring_sum + (size_t)g0 * rp.rec_stride;
+            r2.step0 = s0;
+            r2.step1 = std::min(steps, s0 + rt.seg);
+            r2.init_fields = s0 == 0;
+            QA_TRY(launch_rings(ctx, kind, pl, r2, std::min(rt.G, nr - g0), ctx->side[k]));
+        }
+    }
+    for (int k = 0; k < rt.streams; ++k) {  // join
+        QA_CK(cudaEventRecord(ctx->side_ev[k], ctx->side[k]));
+        QA_CK(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[k], 0));
+    }
     return QA_OK;
 }
 
@@ -704,6 +768,7 @@ int qa_create(qa_ctx **out, int device) {
     for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->stage.sent, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
         qa_destroy(ctx);
         return fail(QA_ERR_CUDA, std::string("context setup: ") + cudaGetErrorString(e));
@@ -720,6 +785,8 @@ int qa_destroy(qa_ctx *ctx) {
         if (b.p) cudaFree(b.p);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    for (auto &x : ctx->side) cudaStreamDestroy(x);
+    for (auto &x : ctx->side_ev) cudaEventDestroy(x);
     ctx->stage.release();
     ctx->down.release();
     if (ctx->stage.sent) cudaEventDestroy(ctx->stage.sent);
@@ -1414,12 +1481,19 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     rp.tr_stride = stride; rp.tr_rps = rps;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     const int seg = 256;
-    const int n_seg = (steps + seg - 1) / seg;
-    for (int s0 = 0; s0 < steps; s0 += seg) {
-        rp.step0 = s0;
-        rp.step1 = std::min(steps, s0 + seg);
-        rp.init_fields = s0 == 0;
-        QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+    int n_seg = (steps + seg - 1) / seg;
+    // more rings than SMs: rotated launches (a traced run's records are
+    // indexed by the position in a whole-grid launch, so those stay whole)
+    if (!traces && nr > ctx->sms && steps >= 200) {
+        QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, steps));
+        n_seg = rot_plan(nr, steps).launches;
+    } else {
+        for (int s0 = 0; s0 < steps; s0 += seg) {
+            rp.step0 = s0;
+            rp.step1 = std::min(steps, s0 + seg);
+            rp.init_fields = s0 == 0;
+            QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+        }
     }
     QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));
