@@ -97,6 +97,20 @@ __device__ __forceinline__ bool metropolis_nb24(float y, float u24v) {
     return (y > -17.0f) & (u24v < det_expf_scaled<24>(fminf(fmaxf(y, -17.0f), 0.0f)));
 }
 
+// False only when metropolis_nb24(y, u24v) is false, without the exponential.
+// With t = y log2(e): det_expf_scaled<24>(y) = p 2^(k + 24), p within 1e-6 of
+// 2^(t - k) (degree-6 Taylor remainder on [-1/2, 1/2] plus the roundings), so
+// log2 of it is below t + 24 + 1e-5; at y >= 0 it is 2^24.  The float bits of
+// u24v give bits / 2^23 - 127 = e + m <= e + log2(1 + m) = log2(u24v).  Hence
+// bits(u24v) >= (t + 151.001) 2^23 implies u24v > e^y 2^24: rejected.  The
+// 0.001 margin covers this test's own roundings (the fused multiply-add of a
+// value near 2^30: below 1e-5 in log2 units) a hundred times over.  y <= -17
+// and non-finite y land on either side; metropolis_nb24 rejects them anyway.
+__device__ __forceinline__ bool metropolis_maybe24(float y, float u24v) {
+    const int K = __float2int_ru(__fmaf_rn(y, 1.44269504f * 8388608.0f, 151.001f * 8388608.0f));
+    return __float_as_int(u24v) < K;
+}
+
 __device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
 
 // float64 warp sum in the canonical order: lane-strided partials (already in

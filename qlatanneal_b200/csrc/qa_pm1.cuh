@@ -111,8 +111,10 @@ __device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, cons
     const float u = u24(rw);
     const float hi = h[i];
     const int gi = (int)Gt[i];
-    bool ok = valid & metropolis_nb24(
-        __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gi)), sbit), B), tro), u);
+    const float y = __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gi)), sbit), B), tro);
+    // most blocks reject every proposal: a sufficient test first, the exact one if any lane may accept
+    if (!__any_sync(FULL, valid & metropolis_maybe24(y, u))) return;
+    bool ok = valid & metropolis_nb24(y, u);
     uint32_t m = __ballot_sync(FULL, ok);
     if (m == 0) return;
     // resolve the block in spin order; gk is this lane's field with the

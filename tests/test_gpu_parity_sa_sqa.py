@@ -199,6 +199,32 @@ def _sqa_case(oracle, kind, n, P, K, spb, wls, bscale, cls=0):
     assert st.slice_accepts == acc_s and st.worldline_accepts == acc_w
 
 
+@pytest.mark.parametrize("kind,n,P,K,reads", [("dense", 40, 4, 1, 160), ("dense_h", 33, 6, 2, 80),
+                                               ("sparse", 64, 4, 1, 150), ("hubo", 24, 4, 1, 152)])
+def test_sqa_rotated_launches_bit_exact(oracle, kind, n, P, K, reads):
+    """More rings than SMs and >= 200 steps: the rings run as groups on side
+    streams in short launches; every read equals the oracle's."""
+    model = make(kind, n, 23)
+    om = oracle_model(oracle, model)
+    steps = 210
+    betas = np.full(steps, 0.6 * P)
+    gammas = np.linspace(2.5, 0.05, steps)
+    ann = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors(betas, gammas), P, K)
+    res = ann.run_reads(1, 1, reads=reads, seed=4242)
+    assert ann.last_stats.sweep_launches > (steps + 255) // 256  # not one whole-grid launch per segment
+    acc_s = acc_w = 0
+    for r in range(reads):
+        best, E, trace, cnt = oracle.sqa_run(om, betas, gammas, P, K, 1, 1, 4242, r)
+        acc_s += cnt[1]
+        acc_w += cnt[3]
+        np.testing.assert_array_equal(res[r].best_state.as_array(), best)
+        _check_best_energy(oracle, om, kind, res[r], E, best)
+        np.testing.assert_array_equal(np.asarray(res[r].energy_trace), trace)
+    st = ann.last_stats
+    assert st.slice_attempts == reads * K * P * steps * n
+    assert st.slice_accepts == acc_s and st.worldline_accepts == acc_w
+
+
 def test_single_run_matches_batch(oracle):
     """run() after set_seed(s + r) reproduces read r of a batch seeded s (solve()'s seeding)."""
     model = make("dense", 64, 3)
