@@ -166,6 +166,17 @@ __device__ __forceinline__ bool pm1_world_ok(const float *h, const int *Gs, cons
     return (i < n) & metropolis_nb24(__fmul_rn(x, B), uw[i]);
 }
 
+// The warp's ballot of pm1_world_ok over spins i (one per lane, i < npad),
+// the exponential skipped when the pre-test rejects every lane.
+__device__ __forceinline__ uint32_t pm1_world_ballot(const float *h, const int *Gs, const unsigned long long *Wc,
+                                                     const float *uw, int i, int n, int NP, float B) {
+    const int sh = 2 * __popcll(Wc[i]) - NP;
+    const float y =
+        __fmul_rn(__double2float_rn(__dadd_rn(__dmul_rn((double)h[i], (double)sh), (double)Gs[i])), B);
+    if (!__any_sync(FULL, (i < n) & metropolis_maybe24(y, uw[i]))) return 0u;
+    return __ballot_sync(FULL, (i < n) & metropolis_nb24(y, uw[i]));
+}
+
 // GT: field type (int: fields as int32; short: int16, for rings whose int32
 // fields would not fit).  JW_SMEM: J bits staged in shared memory, else read
 // from global memory (L2-resident: every ring of an instance reads the same
@@ -274,15 +285,20 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                         gs += ((S[t * nw + q] >> lane) & 1u) ? g : -g;
                     }
                 Gs[i] = gs;
-                const U4 r = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
-                uw[i] = u24(pick(r, q & 3));
+                if ((q & 3) == 0) {  // one Philox call per lane serves blocks q .. q+3 (npad: a multiple of 128)
+                    const U4 r = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
+                    uw[i] = u24(r.x);
+                    uw[i + 32] = u24(r.y);
+                    uw[i + 64] = u24(r.z);
+                    uw[i + 96] = u24(r.w);
+                }
             }
             if (threadIdx.x == 0) att_w += (unsigned long long)n;
             __syncthreads();
             int q0 = 0;
             for (;;) {
                 for (int i = threadIdx.x + q0 * 32; i < npad; i += blockDim.x) {
-                    const uint32_t m = __ballot_sync(FULL, pm1_world_ok(h, Gs, Wc, uw, i, n, NP, B));
+                    const uint32_t m = pm1_world_ballot(h, Gs, Wc, uw, i, n, NP, B);
                     if (lane == 0) mask[i >> 5] = m;
                 }
                 __syncthreads();
