@@ -613,31 +613,84 @@ int ws_array(qa_ctx *ctx, int slot, size_t count, T **out) {
     return QA_OK;
 }
 
-// Ring groups and segment length of a rotated run (run_rings_rotated).
+// Ring groups of a rotated run (run_rings_rotated): groups of G rings, one
+// stream each, at most 128 streams.
 struct RotPlan {
-    int G, streams, seg, launches;
+    int G, streams;
 };
-static RotPlan rot_plan(int nr, int steps) {
+static RotPlan rot_plan(int nr) {
     RotPlan r;
-    r.G = std::max(2, (nr + 127) / 128);  // at most 128 streams, one group each
+    r.G = std::max(2, (nr + 127) / 128);
     r.streams = (nr + r.G - 1) / r.G;
-    r.seg = std::max(25, std::min(100, steps / 8));
-    r.launches = r.streams * ((steps + r.seg - 1) / r.seg);
+    return r;
+}
+// SQA: launches of 25..100 steps (an eighth of the run)
+static int sqa_rot_seg(int steps) { return std::max(25, std::min(100, steps / 8)); }
+
+// Whether nr rings are worth rotating: more rings than SMs, and whole-grid
+// launches would leave more than 3% of the resident slots idle.  With w the
+// number of waves (rings over resident CTAs per SM times SMs), the last of
+// ceil(w) waves is part-empty: the idle fraction is (ceil(w) - w) / ceil(w).
+// For many full waves that is small and the extra launches cost more than the
+// balance gains (an 8-instance sparse set of 8192 rings ran 1.7% slower).
+static bool rotation_pays(qa_ctx *ctx, int kind, const RingPlan &pl, int nr) {
+    if (nr <= ctx->sms) return false;
+    const int threads = 32 * pl.W;
+    const void *kern = nullptr;
+    if (pl.pm1)
+        kern = pl.gbytes == 4 ? (const void *)ring_pm1_kernel<int, true>
+                              : (pl.jw_smem ? (const void *)ring_pm1_kernel<short, true>
+                                            : (const void *)ring_pm1_kernel<short, false>);
+    else if (pl.sparse)
+        kern = (const void *)ring_sparse_kernel;
+    else
+        dispatch_kind(kind, [&](auto Kd) { kern = (const void *)ring_kernel<decltype(Kd)::value>; });
+    if (pl.smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem) != cudaSuccess)
+        return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, pl.smem) != cudaSuccess || per_sm < 1)
+        return false;
+    const double w = (double)nr / ((double)per_sm * ctx->sms), full = std::ceil(w);
+    return (full - w) / full > 0.03;
+}
+
+// The parameters of a launch over rings g0, g0 + 1, ...: every per-ring array
+// the ring kernels index by block (ring records, best and final states, slot,
+// samples) advanced to ring g0.  Sweep traces are indexed by grid position
+// and are not offset: rotated runs carry none.
+static RingParams ring_offset(RingParams r, int g0) {
+    r.rings += g0;
+    if (r.slot) r.slot += g0;
+    r.best_E += g0;
+    r.best_step += g0;
+    if (r.best_slot) r.best_slot += g0;
+    r.best_bits += (size_t)g0 * r.nw_max;
+    if (r.final_bits) r.final_bits += (size_t)g0 * r.nw_max;
+    if (r.ring_sum) r.ring_sum += (size_t)g0 * r.rec_stride;
+    if (r.ring_min) r.ring_min += (size_t)g0 * r.rec_stride;
+    if (r.ring_bond) r.ring_bond += (size_t)g0 * r.rec_stride;
+    if (r.mag) r.mag += (size_t)g0 * r.steps_total * r.spb;
+    if (r.bsamp) r.bsamp += (size_t)g0 * r.bstride;
     return r;
 }
 
-// Steps [0, steps) of every ring as independent chains of short launches:
-// groups of G rings, each group on its own stream, one launch per segment.
-// When the rings outnumber the SMs but do not fill whole waves, some SMs hold
-// two rings and some one; a group that ran alone finishes its segment early
-// and its next launch takes whatever slot is free, so rings move between
-// shared and lone SMs at segment boundaries and all finish together, instead
-// of the lone SMs idling while the shared ones finish.  Each ring keeps its
-// key, counters and records (the per-ring pointers are offset per group), so
-// the results are those of whole-grid launches.  Joins into the context
-// stream.
-static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const RingParams &rp, int nr, int steps) {
-    const RotPlan rt = rot_plan(nr, steps);
+// Steps [s_begin, s_end) of every ring as independent chains of short
+// launches: groups of G rings, each group on its own stream, one launch per
+// seg steps.  When the rings outnumber the SMs but do not fill whole waves,
+// some SMs hold more rings than others (or a second wave runs part-empty); a
+// group that ran on a lightly loaded SM finishes its launch early and its next
+// launch takes whatever slot is free, so rings move between SMs at launch
+// boundaries and all finish together, instead of SMs idling while the loaded
+// ones finish.  Each ring keeps its key, counters and records, so the results
+// are those of whole-grid launches.  rp's init_scan / init_fields apply to
+// the first launch.  Forks from and joins into the context stream; returns
+// the number of launches in *launches.
+static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const RingParams &rp, int nr, int s_begin,
+                             int s_end, int seg, int *launches) {
+    if (rp.tr_bits || rp.tr_E || rp.tr_end_bits || rp.tr_end_E || rp.ring_spin)
+        return fail(QA_ERR_ARG, "rotated ring launches carry no sweep traces");
+    const RotPlan rt = rot_plan(nr);
     while ((int)ctx->side.size() < rt.streams) {
         cudaStream_t x;
         cudaEvent_t e;
@@ -649,25 +702,23 @@ static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const Ri
     // fork: every side stream starts after the context stream's work so far
     QA_CK(cudaEventRecord(ctx->side_ev[0], ctx->stream));
     for (int k = 0; k < rt.streams; ++k) QA_CK(cudaStreamWaitEvent(ctx->side[k], ctx->side_ev[0], 0));
-    for (int s0 = 0; s0 < steps; s0 += rt.seg) {  // segment-major issue keeps the streams in step
+    int n = 0;
+    for (int s0 = s_begin; s0 < s_end; s0 += seg) {  // segment-major issue keeps the streams in step
         for (int k = 0; k < rt.streams; ++k) {
-            const int g0 = k * rt.G;
-            RingParams r2 = rp;
-            r2.rings = rp.rings + g0;
-            r2.best_E = rp.best_E + g0;
-            r2.best_step = rp.best_step + g0;
-            r2.best_bits = rp.best_bits + (size_t)g0 * rp.nw_max;
-            if (rp.ring_sum) r2.ring_sum = rp.ring_sum + (size_t)g0 * rp.rec_stride;
+            RingParams r2 = ring_offset(rp, k * rt.G);
             r2.step0 = s0;
-            r2.step1 = std::min(steps, s0 + rt.seg);
-            r2.init_fields = s0 == 0;
-            QA_TRY(launch_rings(ctx, kind, pl, r2, std::min(rt.G, nr - g0), ctx->side[k]));
+            r2.step1 = std::min(s_end, s0 + seg);
+            r2.init_fields = rp.init_fields && s0 == s_begin;
+            r2.init_scan = rp.init_scan && s0 == s_begin;
+            QA_TRY(launch_rings(ctx, kind, pl, r2, std::min(rt.G, nr - k * rt.G), ctx->side[k]));
+            ++n;
         }
     }
     for (int k = 0; k < rt.streams; ++k) {  // join
         QA_CK(cudaEventRecord(ctx->side_ev[k], ctx->side[k]));
         QA_CK(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[k], 0));
     }
+    *launches = n;
     return QA_OK;
 }
 
@@ -1484,9 +1535,9 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     int n_seg = (steps + seg - 1) / seg;
     // more rings than SMs: rotated launches (a traced run's records are
     // indexed by the position in a whole-grid launch, so those stay whole)
-    if (!traces && nr > ctx->sms && steps >= 200) {
-        QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, steps));
-        n_seg = rot_plan(nr, steps).launches;
+    if (!traces && steps >= 200 && rotation_pays(ctx, kind, pl, nr)) {
+        rp.init_fields = 1;
+        QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, 0, steps, sqa_rot_seg(steps), &n_seg));
     } else {
         for (int s0 = 0; s0 < steps; s0 += seg) {
             rp.step0 = s0;
@@ -2200,14 +2251,24 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     sp.ring_sum = d_sum; sp.ring_min = d_min; sp.ring_bond = d_bond; sp.rec_base = 1; sp.rec_stride = steps + 1;
     sp.ring_in = d_rin; sp.slot_of = d_slot; sp.avg_trace = d_avg; sp.swap_trace = d_swp; sp.steps_total = steps;
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    int n_seg = 0;
+    int n_seg = 0, n_launch = 0;
+    const bool rotate = rotation_pays(ctx, kind, pl, nr);
     for (int s0 = 0; s0 < steps;) {
         const int s1 = std::min({steps, (s0 / prm->swap_interval + 1) * prm->swap_interval, s0 + 256});
         rp.step0 = s0;
         rp.step1 = s1;
         rp.init_scan = s0 == 0;
         rp.init_fields = s0 == 0;
-        QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+        // at least 8 sweeps in the segment and rings worth rotating: launches
+        // of an eighth of it (at least one step), joined before the swaps
+        if ((long long)(s1 - s0) * (rp.spb + rp.wls + rp.cls) >= 8 && rotate) {
+            int nl = 0;
+            QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, std::max(1, (s1 - s0) / 8), &nl));
+            n_launch += nl;
+        } else {
+            QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+            ++n_launch;
+        }
         sp.s0 = s0;
         sp.s1 = s1;
         sp.swap = s1 % prm->swap_interval == 0;
@@ -2226,8 +2287,8 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     int64_t d2h = 0;
     QA_TRY(pt_collect(ctx, problems, n_problems, prm->reads, Rn, steps, L, dv, po.data(), stats, &d2h));
     if (stats) {
-        stats->sweep_launches = n_seg;
-        stats->launches = (pl.own_fields() ? 2 : 3) + 2 * n_seg;
+        stats->sweep_launches = n_launch;
+        stats->launches = (pl.own_fields() ? 2 : 3) + n_launch + n_seg;
         stats->h2d_bytes = (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * Rn +
                                      2 * sizeof(double) * Rn + (sizeof(double) + 3 * sizeof(int)) * nr +
                                      sizeof(int) * (size_t)reads_total * Rn);

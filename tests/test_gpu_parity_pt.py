@@ -46,6 +46,33 @@ def test_sqapt_bit_exact(oracle, kind, n, P, R, spb, wls, steps, swap):
     assert swaps_seen > 0.0  # the ladder actually exchanged states
 
 
+@pytest.mark.parametrize("kind,n,P,R,reads", [("dense", 40, 4, 4, 40), ("sparse", 64, 4, 5, 32), ("hubo", 24, 4, 4, 38)])
+def test_sqapt_rotated_launches_bit_exact(oracle, kind, n, P, R, reads):
+    """More rings than SMs and >= 8 sweeps per swap interval: each interval
+    runs as short launches of ring groups on side streams, joined before the
+    swaps; every read equals the oracle's."""
+    model = make(kind, n, 37)
+    om = oracle_model(oracle, model)
+    betas = np.geomspace(0.3, 3.0, R) * P / 8.0
+    gammas = np.linspace(2.5, 0.05, R)
+    spb, wls, steps, swap, seed = 2, 1, 24, 6, 1357
+    ann = qa.SQAParallelTemperingAnnealer(model, betas, gammas, P)
+    res = ann.run_reads(spb, wls, steps, swap, reads=reads, seed=seed)
+    assert ann.last_stats.sweep_launches > steps // swap  # not one whole-grid launch per interval
+    acc = 0
+    for r in range(reads):
+        best, E, fE, fs, avg, swp, cnt = oracle.sqapt_run(om, betas, gammas, P, spb, wls, steps, swap, seed, r)
+        acc += cnt[1]
+        np.testing.assert_array_equal(res[r].best_state.as_array(), best)
+        assert res[r].best_energy == E
+        np.testing.assert_array_equal(np.asarray(res[r].final_energies), fE)
+        for k in range(R):
+            np.testing.assert_array_equal(res[r].final_states[k].as_array(), fs[k])
+        np.testing.assert_array_equal(np.asarray(res[r].average_energy_trace), avg)
+        np.testing.assert_array_equal(np.asarray(res[r].swap_acceptance_trace), swp)
+    assert ann.last_stats.slice_accepts == acc
+
+
 def test_reference_sqapt_shapes():
     """tests/test_sqa_parallel_tempering.cpp: n=3, 3 rungs, P=8, 5 steps."""
     h = np.zeros(3)
