@@ -706,6 +706,7 @@ static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const Ri
     for (int s0 = s_begin; s0 < s_end; s0 += seg) {  // segment-major issue keeps the streams in step
         for (int k = 0; k < rt.streams; ++k) {
             RingParams r2 = ring_offset(rp, k * rt.G);
+            if (r2.bsamp) r2.bsamp += (size_t)(s0 - s_begin) * (rp.spb + rp.cls);  // indexed from step0
             r2.step0 = s0;
             r2.step1 = std::min(s_end, s0 + seg);
             r2.init_fields = rp.init_fields && s0 == s_begin;
