@@ -633,8 +633,9 @@ static int sqa_rot_seg(int steps) { return std::max(25, std::min(100, steps / 8)
 // ceil(w) waves is part-empty: the idle fraction is (ceil(w) - w) / ceil(w).
 // For many full waves that is small and the extra launches cost more than the
 // balance gains (an 8-instance sparse set of 8192 rings ran 1.7% slower).
+// QA_WHOLE_GRID set: never (one launch over all rings per segment).
 static bool rotation_pays(qa_ctx *ctx, int kind, const RingPlan &pl, int nr) {
-    if (nr <= ctx->sms) return false;
+    if (nr <= ctx->sms || std::getenv("QA_WHOLE_GRID")) return false;
     const int threads = 32 * pl.W;
     const void *kern = nullptr;
     if (pl.pm1)

@@ -73,6 +73,33 @@ def test_sqapt_rotated_launches_bit_exact(oracle, kind, n, P, R, reads):
     assert ann.last_stats.slice_accepts == acc
 
 
+def test_rotated_equals_whole_grid(monkeypatch):
+    """The same SQA-PT and SQA runs with rotated launches and with one launch
+    over all rings per segment (QA_WHOLE_GRID) agree bit for bit."""
+    model = make("sparse", 96, 41)
+    betas, gammas = np.geomspace(0.3, 3.0, 4) * 0.5, np.linspace(2.5, 0.05, 4)
+
+    def runs():
+        pt = qa.SQAParallelTemperingAnnealer(model, betas, gammas, 4)
+        a = pt.run_reads(2, 1, 12, 4, reads=40, seed=77)
+        sq = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors(np.full(210, 2.0), np.linspace(2.0, 0.1, 210)), 4, 1)
+        b = sq.run_reads(1, 1, reads=160, seed=78)
+        return a, b, pt.last_stats.sweep_launches, sq.last_stats.sweep_launches
+
+    a1, b1, l1, m1 = runs()
+    monkeypatch.setenv("QA_WHOLE_GRID", "1")
+    a2, b2, l2, m2 = runs()
+    assert l1 > l2 and m1 > m2
+    for x, y in zip(a1, a2):
+        assert x.best_energy == y.best_energy
+        np.testing.assert_array_equal(x.best_state.as_array(), y.best_state.as_array())
+        np.testing.assert_array_equal(np.asarray(x.average_energy_trace), np.asarray(y.average_energy_trace))
+        np.testing.assert_array_equal(np.asarray(x.swap_acceptance_trace), np.asarray(y.swap_acceptance_trace))
+    for x, y in zip(b1, b2):
+        assert x.best_energy == y.best_energy
+        np.testing.assert_array_equal(np.asarray(x.energy_trace), np.asarray(y.energy_trace))
+
+
 def test_reference_sqapt_shapes():
     """tests/test_sqa_parallel_tempering.cpp: n=3, 3 rungs, P=8, 5 steps."""
     h = np.zeros(3)
