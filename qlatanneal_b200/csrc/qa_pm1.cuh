@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     uint32_t *mask = reinterpret_cast<uint32_t *>(ptr); ptr += (size_t)(npad / 32) * 4;
     unsigned long long *Wold = reinterpret_cast<unsigned long long *>(ptr); ptr += 32 * 8;
     int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
-    int *flag = reinterpret_cast<int *>(ptr);  // [0]: best slice, [1]: block flips F, [2]: block index
+    int *flag = reinterpret_cast<int *>(ptr);  // [1]: worldline block flips F, [2]: their block index
 
     if (JW_SMEM)
         for (int idx = threadIdx.x; idx < nw * npad; idx += blockDim.x) Jw_s[idx] = Pd.Jw[idx];
@@ -305,10 +305,9 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 int qs = -1;
                 for (int q = q0; q < nw; ++q)
                     if (mask[q]) { qs = q; break; }
-                if (qs < 0) {
-                    __syncthreads();  // every thread has read mask[] before it is rewritten
-                    break;
-                }
+                // no block with a move: done.  mask[] is written next by the next
+                // sweep's decision pass, behind that sweep's barrier after its sums
+                if (qs < 0) break;
                 if (warp == 0) {
                     // resolve block qs in spin order
                     const int i = (qs << 5) | lane;
@@ -386,38 +385,39 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
             if (lane == 0) wpart[warp] = b;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            double sum = 0.0, emin = __longlong_as_double(0x7ff0000000000000LL);
-            int tmin = 0;
-            for (int t = 0; t < NP; ++t) {
-                const double E = cellE[t];
-                sum = __dadd_rn(sum, E);
-                if (E < emin) { emin = E; tmin = t; }
+        // warp 0 alone: ring sum, minimum, records, best and final states (only
+        // its lanes keep bestE / bestStep; thread 0 writes them at the end)
+        if (warp == 0) {
+            int tb = -1, tmin = 0;
+            if (lane == 0) {
+                double sum = 0.0, emin = __longlong_as_double(0x7ff0000000000000LL);
+                for (int t = 0; t < NP; ++t) {
+                    const double E = cellE[t];
+                    sum = __dadd_rn(sum, E);
+                    if (E < emin) { emin = E; tmin = t; }
+                }
+                const long long ro = (long long)blockIdx.x * p.rec_stride + p.rec_base + step;
+                if (p.ring_sum) p.ring_sum[ro] = sum;
+                if (p.ring_min) p.ring_min[ro] = emin;
+                if (p.ring_bond) {
+                    long long bsum = 0;
+                    for (int w = 0; w < W; ++w) bsum += wpart[w];
+                    p.ring_bond[ro] = bsum;
+                }
+                tb = emin < bestE ? tmin : -1;
             }
-            const long long ro = (long long)blockIdx.x * p.rec_stride + p.rec_base + step;
-            if (p.ring_sum) p.ring_sum[ro] = sum;
-            if (p.ring_min) p.ring_min[ro] = emin;
-            if (p.ring_bond) {
-                long long tb = 0;
-                for (int w = 0; w < W; ++w) tb += wpart[w];
-                p.ring_bond[ro] = tb;
+            tb = __shfl_sync(FULL, tb, 0);
+            tmin = __shfl_sync(FULL, tmin, 0);
+            if (tb >= 0) {
+                bestE = cellE[tb];
+                bestStep = step;
+                if (lane == 0 && p.best_slot) p.best_slot[blockIdx.x] = slot;
+                for (int q = lane; q < nw; q += 32) p.best_bits[(long long)blockIdx.x * p.nw_max + q] = S[tb * nw + q];
             }
-            flag[0] = emin < bestE ? tmin : -1;
-            flag[3] = tmin;
+            if (p.final_bits && step == p.steps_total - 1)
+                for (int q = lane; q < nw; q += 32) p.final_bits[(long long)blockIdx.x * p.nw_max + q] = S[tmin * nw + q];
         }
-        __syncthreads();
-        const int tb = flag[0];
-        if (tb >= 0) {
-            bestE = cellE[tb];
-            bestStep = step;
-            if (threadIdx.x == 0 && p.best_slot) p.best_slot[blockIdx.x] = slot;
-            for (int q = threadIdx.x; q < nw; q += blockDim.x)
-                p.best_bits[(long long)blockIdx.x * p.nw_max + q] = S[tb * nw + q];
-        }
-        if (p.final_bits && step == p.steps_total - 1)
-            for (int q = threadIdx.x; q < nw; q += blockDim.x)
-                p.final_bits[(long long)blockIdx.x * p.nw_max + q] = S[flag[3] * nw + q];
-        __syncthreads();
+        __syncthreads();  // S is swept again next step
     }
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) p.spins[R.spin_off + idx] = S[idx];
     for (int idx = threadIdx.x; idx < NP * npad; idx += blockDim.x) Gg[idx] = G[idx];
