@@ -9,7 +9,8 @@
 //  * A block of 32 spins is resolved in spin order by ballots; the fields of
 //    the whole slice are then updated once for all flips F of the block:
 //        g[m] += 2|F| - 4 popc(~(Jw[q*npad+m] ^ s_old) & F)
-//    four fields per lane per 128-bit shared-memory access.
+//    four fields per lane per 128-bit shared-memory access; a flipped spin's
+//    own field then takes -2 s_m(old) (its zero diagonal bit reads as -1).
 //  * Worldline moves (sqa_annealer.cpp:294-315): the slice sums
 //    G_i = sum_t s_t,i g_t,i are built once per sweep; decisions for all
 //    remaining spins are taken in parallel; the first block holding an
@@ -58,20 +59,31 @@ __device__ __forceinline__ int flip_delta(uint32_t jw, uint32_t sold, uint32_t F
 }
 
 // Fields of one slice after the spins F of block q (old word sold) flipped.
-// Whole warp; the field of a flipped spin excludes its own (zero) diagonal.
+// Whole warp.  Every field takes the flips of all of F: the diagonal bit of
+// a row is 0, which the sum reads as J_mm = -1, so a flipped spin m's own
+// field comes out 2 s_m too high and is corrected by its lane afterwards.
+__device__ __forceinline__ void pm1_self_fix(int *Gt, int q, uint32_t F, uint32_t sold, int lane) {
+    __syncwarp();
+    if ((F >> lane) & 1u) Gt[(q << 5) | lane] += ((sold >> lane) & 1u) ? -2 : 2;
+}
+__device__ __forceinline__ void pm1_self_fix(short *Gt, int q, uint32_t F, uint32_t sold, int lane) {
+    __syncwarp();
+    if ((F >> lane) & 1u) Gt[(q << 5) | lane] = (short)(Gt[(q << 5) | lane] + (((sold >> lane) & 1u) ? -2 : 2));
+}
 __device__ __forceinline__ void pm1_block_update(int *Gt, const uint32_t *Jw, int npad, int n, int q, uint32_t F,
                                                  uint32_t sold, int lane) {
     const uint32_t *Jq = Jw + q * npad;
+    const int f2 = 2 * __popc(F);
     for (int base = lane * 4; base < n; base += 128) {
         const uint4 jw = *reinterpret_cast<const uint4 *>(Jq + base);
         int4 g = *reinterpret_cast<int4 *>(Gt + base);
-        const uint32_t d = (base >> 5) == q ? (1u << (base & 31)) : 0u;
-        g.x += flip_delta(jw.x, sold, F & ~d);
-        g.y += flip_delta(jw.y, sold, F & ~(d << 1));
-        g.z += flip_delta(jw.z, sold, F & ~(d << 2));
-        g.w += flip_delta(jw.w, sold, F & ~(d << 3));
+        g.x += f2 - 4 * __popc(~(jw.x ^ sold) & F);
+        g.y += f2 - 4 * __popc(~(jw.y ^ sold) & F);
+        g.z += f2 - 4 * __popc(~(jw.z ^ sold) & F);
+        g.w += f2 - 4 * __popc(~(jw.w ^ sold) & F);
         *reinterpret_cast<int4 *>(Gt + base) = g;
     }
+    pm1_self_fix(Gt, q, F, sold, lane);
 }
 
 // int16 fields (|g| <= n - 1 < 2^15): eight per lane per 128-bit access,
@@ -87,13 +99,13 @@ __device__ __forceinline__ void pm1_block_update(short *Gt, const uint32_t *Jw, 
         const uint4 ja = *reinterpret_cast<const uint4 *>(Jq + base);
         const uint4 jb = *reinterpret_cast<const uint4 *>(Jq + base + 4);
         uint4 g = *reinterpret_cast<uint4 *>(Gt + base);
-        const uint32_t d = (base >> 5) == q ? (1u << (base & 31)) : 0u;
-        g.x = __vadd2(g.x, pack_delta2(flip_delta(ja.x, sold, F & ~d), flip_delta(ja.y, sold, F & ~(d << 1))));
-        g.y = __vadd2(g.y, pack_delta2(flip_delta(ja.z, sold, F & ~(d << 2)), flip_delta(ja.w, sold, F & ~(d << 3))));
-        g.z = __vadd2(g.z, pack_delta2(flip_delta(jb.x, sold, F & ~(d << 4)), flip_delta(jb.y, sold, F & ~(d << 5))));
-        g.w = __vadd2(g.w, pack_delta2(flip_delta(jb.z, sold, F & ~(d << 6)), flip_delta(jb.w, sold, F & ~(d << 7))));
+        g.x = __vadd2(g.x, pack_delta2(flip_delta(ja.x, sold, F), flip_delta(ja.y, sold, F)));
+        g.y = __vadd2(g.y, pack_delta2(flip_delta(ja.z, sold, F), flip_delta(ja.w, sold, F)));
+        g.z = __vadd2(g.z, pack_delta2(flip_delta(jb.x, sold, F), flip_delta(jb.y, sold, F)));
+        g.w = __vadd2(g.w, pack_delta2(flip_delta(jb.z, sold, F), flip_delta(jb.w, sold, F)));
         *reinterpret_cast<uint4 *>(Gt + base) = g;
     }
+    pm1_self_fix(Gt, q, F, sold, lane);
 }
 
 // One block of 32 spins (lane = spin) of slice t; rw is this lane's Philox word.
