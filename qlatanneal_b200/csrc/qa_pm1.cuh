@@ -145,7 +145,8 @@ __device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, cons
         ++acc;
     } while (m);
     if (lane == 0) St[q] = sw ^ F;
-    if ((F >> lane) & 1u) atomicXor(Wc + i, 1ull << t);
+    // bit t of the worldline, as a 32-bit atomic on the half that holds it (little-endian)
+    if ((F >> lane) & 1u) atomicXor(reinterpret_cast<uint32_t *>(Wc + i) + (t >> 5), 1u << (t & 31));
     pm1_block_update(Gt, Jw, npad, n, q, F, sw, lane);
     __syncwarp();
 }

@@ -97,7 +97,8 @@ __device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, u
             const int j = __ffs(m & pending) - 1;
             const int jj = (q << 5) | j;
             if (lane == 0) St[q] = St[q] ^ (1u << j);
-            if (lane == j) atomicXor(Wc + i, 1ull << t);
+            // bit t of the worldline, as a 32-bit atomic on the half that holds it (little-endian)
+            if (lane == j) atomicXor(reinterpret_cast<uint32_t *>(Wc + i) + (t >> 5), 1u << (t & 31));
             ++acc;
             pending = j == 31 ? 0u : (FULL << (j + 1));
             uint32_t here = 0;
