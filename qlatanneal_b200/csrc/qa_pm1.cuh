@@ -523,16 +523,20 @@ __global__ void __launch_bounds__(32) sa_pm1_kernel(SAParams p) {
                     const uint32_t sj = (sword >> j) & 1u;  // old spin bit of j
                     if (lane == 0) S[q] = S[q] ^ (1u << j);
                     const int jj = (q << 5) | j;
+                    // g_m += -2 J_mj s_j = 4 (bit_j(row m) ^ s_j) - 2 for every m; the zero
+                    // diagonal bit gives spin j's own field 4 s_j - 2, taken back after
                     const uint32_t *Jq = Jw + q * npad;
                     for (int base = lane * 4; base < n; base += 128) {
                         const uint4 jw = *reinterpret_cast<const uint4 *>(Jq + base);
                         int4 g = *reinterpret_cast<int4 *>(G + base);
-                        g.x += base + 0 == jj ? 0 : ((((jw.x >> j) & 1u) == sj) ? -2 : 2);
-                        g.y += base + 1 == jj ? 0 : ((((jw.y >> j) & 1u) == sj) ? -2 : 2);
-                        g.z += base + 2 == jj ? 0 : ((((jw.z >> j) & 1u) == sj) ? -2 : 2);
-                        g.w += base + 3 == jj ? 0 : ((((jw.w >> j) & 1u) == sj) ? -2 : 2);
+                        g.x += 4 * (int)(((jw.x >> j) ^ sj) & 1u) - 2;
+                        g.y += 4 * (int)(((jw.y >> j) ^ sj) & 1u) - 2;
+                        g.z += 4 * (int)(((jw.z >> j) ^ sj) & 1u) - 2;
+                        g.w += 4 * (int)(((jw.w >> j) ^ sj) & 1u) - 2;
                         *reinterpret_cast<int4 *>(G + base) = g;
                     }
+                    __syncwarp();
+                    if (lane == 0) G[jj] -= 4 * (int)sj - 2;
                     __syncwarp();
                     ++acc;
                     E = __dadd_rn(E, __dmul_rn(-2.0, xj));
