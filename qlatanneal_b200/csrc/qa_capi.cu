@@ -164,6 +164,8 @@ struct qa_ctx {
     // side streams for the rotated ring launches (run_rings_rotated) and their events
     std::vector<cudaStream_t> side;
     std::vector<cudaEvent_t> side_ev;
+    // the dynamic shared memory each ring kernel is opted in to (a function attribute)
+    std::vector<std::pair<const void *, size_t>> smem_attr;
     static constexpr int kWsSlots = 48;
     DevBuf ws[kWsSlots];
 };
@@ -573,6 +575,22 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
 }
 
 // One launch of the planned ring kernel over steps [rp.step0, rp.step1).
+// Opt kernel kern in to smem bytes of dynamic shared memory (above the
+// default 48 KB), once per size increase rather than before every launch.
+static int opt_in_smem(qa_ctx *ctx, const void *kern, size_t smem) {
+    if (smem <= 48 * 1024) return QA_OK;
+    for (auto &e : ctx->smem_attr)
+        if (e.first == kern) {
+            if (e.second >= smem) return QA_OK;
+            QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            e.second = smem;
+            return QA_OK;
+        }
+    QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ctx->smem_attr.emplace_back(kern, smem);
+    return QA_OK;
+}
+
 int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n_rings,
                  cudaStream_t stream = nullptr) {
     cudaStream_t strm = stream ? stream : ctx->stream;
@@ -581,15 +599,13 @@ int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n
     if (pl.pm1) {
         auto kern = pl.gbytes == 4 ? ring_pm1_kernel<int, true>
                                    : (pl.jw_smem ? ring_pm1_kernel<short, true> : ring_pm1_kernel<short, false>);
-        if (pl.smem > 48 * 1024)
-            QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        QA_TRY(opt_in_smem(ctx, (const void *)kern, pl.smem));
         kern<<<n_rings, 32 * pl.W, pl.smem, strm>>>(rp);
         QA_CK(cudaGetLastError());
         return QA_OK;
     }
     if (pl.sparse) {
-        if (pl.smem > 48 * 1024)
-            QA_CK(cudaFuncSetAttribute(ring_sparse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        QA_TRY(opt_in_smem(ctx, (const void *)ring_sparse_kernel, pl.smem));
         ring_sparse_kernel<<<n_rings, 32 * pl.W, pl.smem, strm>>>(rp);
         QA_CK(cudaGetLastError());
         return QA_OK;
@@ -597,7 +613,10 @@ int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n
     int rc = QA_OK;
     dispatch_kind(kind, [&](auto Kd) {
         auto kern = ring_kernel<decltype(Kd)::value>;
-        if (pl.smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+        if (opt_in_smem(ctx, (const void *)kern, pl.smem) != QA_OK) {
+            rc = QA_ERR_CUDA;
+            return;
+        }
         kern<<<n_rings, 32 * pl.W, pl.smem, strm>>>(rp);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) rc = fail(QA_ERR_CUDA, std::string("ring_kernel launch: ") + cudaGetErrorString(e));
@@ -646,9 +665,7 @@ static bool rotation_pays(qa_ctx *ctx, int kind, const RingPlan &pl, int nr) {
         kern = (const void *)ring_sparse_kernel;
     else
         dispatch_kind(kind, [&](auto Kd) { kern = (const void *)ring_kernel<decltype(Kd)::value>; });
-    if (pl.smem > 48 * 1024 &&
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem) != cudaSuccess)
-        return false;
+    if (opt_in_smem(ctx, kern, pl.smem) != QA_OK) return false;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, pl.smem) != cudaSuccess || per_sm < 1)
         return false;
@@ -1622,13 +1639,18 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     for (int p = 0; p < n_problems; ++p) {
         const int n = problems[p]->n;
         qa_run_out &o = outs[p];
+        // a power-of-two K*P: the product with its exact reciprocal is the
+        // correctly rounded quotient, without a division per entry
+        const int kp = K * P;
+        const bool kp_pow2 = (kp & (kp - 1)) == 0;
+        const double kp_inv = 1.0 / (double)kp;
         for (int r = 0; r < prm->reads; ++r) {
             const int base = (p * prm->reads + r) * K;
             if (o.energy_trace)
                 for (int s = 0; s < steps; ++s) {
                     double tot = 0.0;
                     for (int k = 0; k < K; ++k) tot += sums[(size_t)(base + k) * steps + s];
-                    o.energy_trace[(size_t)r * steps + s] = tot / (double)(K * P);
+                    o.energy_trace[(size_t)r * steps + s] = kp_pow2 ? tot * kp_inv : tot / (double)kp;
                 }
             int kb = 0;
             for (int k = 1; k < K; ++k) {
