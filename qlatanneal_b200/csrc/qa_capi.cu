@@ -577,17 +577,26 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
 // One launch of the planned ring kernel over steps [rp.step0, rp.step1).
 // Opt kernel kern in to smem bytes of dynamic shared memory (above the
 // default 48 KB), once per size increase rather than before every launch.
+// The attribute belongs to the function on the device, which other contexts
+// share: it is only ever raised (to the larger of the request and its current
+// value), so what a context has recorded stays a lower bound.
 static int opt_in_smem(qa_ctx *ctx, const void *kern, size_t smem) {
     if (smem <= 48 * 1024) return QA_OK;
+    std::pair<const void *, size_t> *rec = nullptr;
     for (auto &e : ctx->smem_attr)
-        if (e.first == kern) {
-            if (e.second >= smem) return QA_OK;
-            QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            e.second = smem;
-            return QA_OK;
-        }
-    QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ctx->smem_attr.emplace_back(kern, smem);
+        if (e.first == kern) rec = &e;
+    if (rec && rec->second >= smem) return QA_OK;
+    cudaFuncAttributes fa{};
+    QA_CK(cudaFuncGetAttributes(&fa, kern));
+    size_t now = (size_t)std::max(fa.maxDynamicSharedSizeBytes, 0);
+    if (now < smem) {
+        QA_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        now = smem;
+    }
+    if (rec)
+        rec->second = now;
+    else
+        ctx->smem_attr.emplace_back(kern, now);
     return QA_OK;
 }
 
