@@ -1561,8 +1561,9 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     const int seg = 256;
     int n_seg = (steps + seg - 1) / seg;
-    // more rings than SMs: rotated launches (a traced run's records are
-    // indexed by the position in a whole-grid launch, so those stay whole)
+    // rotated launches where whole-grid ones would leave slots idle (a traced
+    // run's records are indexed by the position in a whole-grid launch, so
+    // those stay whole)
     if (!traces && steps >= 200 && rotation_pays(ctx, kind, pl, nr)) {
         rp.init_fields = 1;
         QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, 0, steps, sqa_rot_seg(steps), &n_seg));
