@@ -147,6 +147,13 @@ def test_sqa_generic_kernel_on_pm1_models(oracle, monkeypatch, kind, n, P, K, sp
     _sqa_case(oracle, kind, n, P, K, spb, wls, bscale)
 
 
+def test_sqa_pm1_int32_only_falls_back(oracle, monkeypatch):
+    """A +-1 ring too large for int32 fields in shared memory (n=1024, P=32)
+    runs on the generic kernel under QA_PM1_INT32_ONLY, with the same bits."""
+    monkeypatch.setenv("QA_PM1_INT32_ONLY", "1")
+    _sqa_case(oracle, "dense", 1024, 32, 1, 1, 1, 1.0)
+
+
 @pytest.mark.parametrize("kind,n,P,K,spb,wls,bscale", [("sparse", 128, 8, 1, 1, 1, 1.0), ("sparse", 64, 7, 2, 2, 1, 1.0)])
 def test_sqa_cached_field_kernel_on_integer_sparse(oracle, monkeypatch, kind, n, P, K, spb, wls, bscale):
     """The field-cache kernel gives the same bits as the on-demand one."""
