@@ -207,7 +207,9 @@ def _sqa_case(oracle, kind, n, P, K, spb, wls, bscale, cls=0):
 
 
 @pytest.mark.parametrize("kind,n,P,K,reads", [("dense", 40, 4, 1, 160), ("dense_h", 33, 6, 2, 80),
-                                               ("sparse", 64, 4, 1, 150), ("hubo", 24, 4, 1, 152)])
+                                               ("sparse", 64, 4, 1, 150), ("hubo", 24, 4, 1, 152),
+                                               ("dense", 36, 4, 1, 151),    # a last group of one ring
+                                               ("sparse", 48, 4, 1, 300)])  # groups of 3 rings
 def test_sqa_rotated_launches_bit_exact(oracle, kind, n, P, K, reads):
     """More rings than SMs and >= 200 steps: the rings run as groups on side
     streams in short launches; every read equals the oracle's."""
