@@ -3057,12 +3057,19 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     rp.B = d_B; rp.T4 = d_T4; rp.ring_sum = d_sum; rp.rec_base = 0; rp.rec_stride = steps;
     rp.best_E = d_best; rp.best_step = d_bstep; rp.best_bits = d_bits; rp.nw_max = L.nw_max; rp.counters = d_cnt;
     int n_seg = 0;
-    for (int s0 = 0; s0 < steps; s0 += 256) {
-        rp.step0 = s0;
-        rp.step1 = std::min(steps, s0 + 256);
-        rp.init_fields = s0 == 0;
-        QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
-        ++n_seg;
+    // rotated launches of an eighth of the anneal where whole-grid ones would
+    // leave slots idle and the anneal has at least 200 sweeps
+    if ((long long)steps * rp.spb >= 200 && rotation_pays(ctx, kind, pl, nr)) {
+        rp.init_fields = 1;
+        QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, 0, steps, std::max(1, steps / 8), &n_seg));
+    } else {
+        for (int s0 = 0; s0 < steps; s0 += 256) {
+            rp.step0 = s0;
+            rp.step1 = std::min(steps, s0 + 256);
+            rp.init_fields = s0 == 0;
+            QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+            ++n_seg;
+        }
     }
     QA_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     QA_TRY(exact_energies(ctx, kind, d_probs, L, d_bits, d_exact));

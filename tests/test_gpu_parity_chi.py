@@ -51,6 +51,20 @@ def test_chi_bit_exact(oracle, kind, n, P, K, steps, spb, points, sweeps, burn):
                                          scan_chi_in=curve))
 
 
+def test_chi_rotated_production_bit_exact(oracle):
+    """More rings than SMs and >= 200 production sweeps: the production anneal
+    runs as rotated launches of ring groups; every read equals the oracle's."""
+    model = make("dense", 40, 43)
+    om = oracle_model(oracle, model)
+    P, K, steps, spb, points, sweeps, burn = 4, 2, 30, 8, 5, 6, 2
+    beta, g0, g1, reads, seed = 0.4 * P, 3.0, 0.05, 80, 2468
+    ann = qa.SQAChiAnnealer(model, P, K)
+    res = ann.run_chi_reads(beta, g0, g1, steps, spb, points, sweeps, burn, reads=reads, seed=seed)
+    assert ann.last_stats.sweep_launches > 10  # ring groups, not one whole-grid launch (plus the pilot)
+    for r in range(reads):
+        _compare(res[r], oracle.chi_run(om, P, K, beta, g0, g1, steps, spb, points, sweeps, burn, seed, r))
+
+
 def test_reference_chi_checks_on_gpu():
     # (A) schedule structure on the xorshift SK instance
     h, J = xorshift_sk(10)
