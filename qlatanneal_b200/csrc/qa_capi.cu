@@ -1887,7 +1887,21 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     bool fresh = true;  // the next launch builds its fields from the spins (own-field kernels)
     int n_launch = 0;
+    const bool rotate = rotation_pays(ctx, kind, pl, nr);
     auto run_steps = [&](int s0, int s1, long long *bsamp, int bstride) -> int {
+        // rotated launches of an eighth of the range where whole-grid ones
+        // would leave slots idle and the range has at least 200 sweeps
+        if (rotate && (long long)(s1 - s0) * (rp.spb + rp.wls + rp.cls) >= 200) {
+            rp.step0 = s0;
+            rp.init_fields = fresh;
+            rp.bsamp = bsamp;
+            rp.bstride = bstride;
+            int nl = 0;
+            QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, std::max(1, (s1 - s0) / 8), &nl));
+            fresh = false;
+            n_launch += nl;
+            return QA_OK;
+        }
         for (int a = s0; a < s1; a += 256) {
             rp.step0 = a;
             rp.step1 = std::min(s1, a + 256);

@@ -56,6 +56,28 @@ def test_run_optimal_bit_exact(oracle, kind, n, P, K, eps, spb, wls, cls, probes
     assert jt[-1] > js and jt[-1] <= je + 1e-12
 
 
+def test_run_optimal_rotated_bit_exact(oracle):
+    """More rings than SMs: the phases with >= 200 sweeps run as rotated
+    launches of ring groups; every read equals the oracle's."""
+    model = make("dense", 40, 61)
+    om = oracle_model(oracle, model)
+    P, K, eps, spb, wls, cls, probes, csweeps, steps = 4, 2, 0.0, 2, 1, 0, 6, 3, 120
+    beta, js, je, alpha, rf, rs = 2.0, 0.05, 2.0, 15.0 / 14.0, 0.3, 0.1
+    reads, seed = 80, 717
+    ann = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors([1.0], [1.0]), P, K)
+    res = ann.run_optimal_reads(beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps, rf, rs,
+                                reads=reads, seed=seed)
+    assert ann.last_stats.sweep_launches > 20  # ring groups, not whole-grid launches
+    for r in range(reads):
+        o = oracle.sqa_opt_run(om, P, K, beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps, rf, rs,
+                               seed, r)
+        np.testing.assert_array_equal(res[r].best_state.as_array(), o["best"])
+        assert res[r].best_energy == o["best_energy"]
+        np.testing.assert_array_equal(np.asarray(res[r].energy_trace), o["trace"])
+        np.testing.assert_array_equal(np.asarray(res[r].j_perp_trace), o["j_perp"])
+        np.testing.assert_array_equal(np.asarray(res[r].chi_B_trace), o["chi"])
+
+
 def test_run_optimal_single_read_and_csv(oracle, tmp_path):
     """run_optimal() after set_seed(s + r) reproduces read r of a batch; the
     diagnostic CSV holds one row per step."""
