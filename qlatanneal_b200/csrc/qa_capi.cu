@@ -2585,15 +2585,24 @@ int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_probl
             Jcur[rd] = jtraj[rd][S - 1];
         }
         QA_TRY(upload_tables());
+        const bool rotate = rotation_pays(ctx, kind, pl, nr);
         for (int s0 = 0; s0 < S;) {
             const int s1 = std::min({S, (s0 / prm->swap_interval + 1) * prm->swap_interval, s0 + 256});
             rp.step0 = s0;
             rp.step1 = s1;
             rp.init_scan = s0 == 0;
             rp.init_fields = fresh;
-            QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+            // as in SQA-PT runs: rotated launches of an eighth of a segment with
+            // at least 8 sweeps, joined before the swaps
+            if (rotate && (long long)(s1 - s0) * (rp.spb + rp.wls + rp.cls) >= 8) {
+                int nl = 0;
+                QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, std::max(1, (s1 - s0) / 8), &nl));
+                n_launch += nl;
+            } else {
+                QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
+                ++n_launch;
+            }
             fresh = false;
-            ++n_launch;
             sp.s0 = s0;
             sp.s1 = s1;
             sp.swap = s1 % prm->swap_interval == 0;

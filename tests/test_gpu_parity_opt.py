@@ -178,6 +178,29 @@ def test_sqapt_run_optimal_bit_exact(oracle, kind, n, R, P, spb, wls, cls, steps
         assert swaps > 0.0  # the SK ladders exchange rungs; the other instances need not
 
 
+def test_sqapt_run_optimal_rotated_bit_exact(oracle):
+    """More rings than SMs: segments with >= 8 sweeps run as rotated launches
+    joined before the swaps; every read equals the oracle's."""
+    model = make("dense", 48, 67)
+    om = oracle_model(oracle, model)
+    R, P, spb, wls, cls, steps, swap, eps, je, cts = 4, 4, 2, 1, 0, 24, 6, 0.0, 2.0, 0
+    betas, gammas = np.geomspace(0.5, 3.0, R), np.geomspace(2.0, 0.3, R)
+    alpha, probes, csweeps, reads, seed = 15.0 / 14.0, 5, 3, 40, 929
+    ann = qa.SQAParallelTemperingAnnealer(model, betas, gammas, P)
+    res = ann.run_optimal_reads(steps, spb, wls, eps, alpha, je, cls, swap, cts, probes, csweeps, reads=reads,
+                                seed=seed)
+    assert ann.last_stats.sweep_launches > 2 * (steps // swap)  # ring groups, not whole-grid launches
+    for r in range(reads):
+        o = oracle.sqapt_opt_run(om, betas, gammas, P, spb, wls, cls, steps, swap, eps, alpha, je, probes, csweeps,
+                                 seed, r)
+        np.testing.assert_array_equal(res[r].best_state.as_array(), o["best"])
+        assert res[r].best_energy == o["best_energy"]
+        np.testing.assert_array_equal(np.asarray(res[r].final_energies), o["final_E"])
+        np.testing.assert_array_equal(np.asarray(res[r].average_energy_trace), o["avg"])
+        np.testing.assert_array_equal(np.asarray(res[r].swap_acceptance_trace), o["swap"])
+        np.testing.assert_array_equal(np.asarray(res[r].j_perp_trace), o["j_perp"])
+
+
 def test_sqapt_run_optimal_errors_and_solve():
     h, J = sk_dense(30, 2)
     d = qa.DenseIsing(h, J)
