@@ -412,6 +412,11 @@ QA_API int qa_mlp_train_step(qa_mlp *m, const float *X, const float *T, int batc
  * library until exit); runs needing more (about 4 n^2 + 8 reads n +
  * 4 steps bytes) are rejected with QA_ERR_ARG.  The first call on a device
  * looks up that array's device address: make it before any stream capture.
+ * With CUDA's default lazy module loading that first call is also when the
+ * 16 MiB are reserved on the device: make it (a small warm-up run) before a
+ * framework claims most of the memory, or set CUDA_MODULE_LOADING=EAGER.
+ * The call runs on `device` and restores the caller's current device before
+ * it returns.
  * Calls share the array, so calls that overlap on the GPU race; serialise
  * them.  stream may be NULL (the legacy default stream); the call returns
  * after the run has finished on it.  stats may be NULL (counters only). */

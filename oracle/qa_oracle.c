@@ -1096,8 +1096,8 @@ OR_EXPORT void or_chi_schedule(int Pts, const double *scan_s, const double *scan
     const int n2 = num_steps - n1;
     enum { GRID = 4096 };
     const double hs = (s_hi - s_lo) / (double)GRID;
-    double *Wcum = (double *)calloc(GRID + 2, sizeof(double));
-#define WEIGHT_AT(S, OUT)                                                   \
+    double *cdf = (double *)calloc(GRID + 2, sizeof(double));
+#define CHI_WEIGHT(S, OUT)                                                   \
     do {                                                                    \
         const double s_ = (S);                                              \
         double c_;                                                          \
@@ -1112,36 +1112,36 @@ OR_EXPORT void or_chi_schedule(int Pts, const double *scan_s, const double *scan
         }                                                                   \
         (OUT) = c_ > floor_ ? c_ : floor_;                                  \
     } while (0)
-    double prev_w;
-    WEIGHT_AT(s_lo, prev_w);
+    double w_left;
+    CHI_WEIGHT(s_lo, w_left);
     for (int k = 1; k <= GRID; ++k) {
         const double sk = s_lo + (double)k * hs;
-        double cur_w;
-        WEIGHT_AT(sk, cur_w);
-        Wcum[k] = Wcum[k - 1] + 0.5 * (prev_w + cur_w) * hs;
-        prev_w = cur_w;
+        double w_right;
+        CHI_WEIGHT(sk, w_right);
+        cdf[k] = cdf[k - 1] + 0.5 * (w_left + w_right) * hs;
+        w_left = w_right;
     }
-#undef WEIGHT_AT
-    const double W_total = Wcum[GRID];
+#undef CHI_WEIGHT
+    const double cdf_end = cdf[GRID];
     for (int s = 0; s < num_steps; ++s) { betas[s] = beta; gammas[s] = gamma_start; s_sched[s] = s_lo; }
     for (int step = 0; step < n1; ++step) {
         const double frac = n1 > 1 ? (double)step / (double)(n1 - 1) : 1.0;
         betas[step] = beta_ramp_start + (beta - beta_ramp_start) * frac;
     }
-    int k_idx = 0;
+    int cell = 0;
     for (int t = 0; t < n2; ++t) {
-        const double target = W_total > 0.0 ? ((double)t / (double)(n2 - 1)) * W_total : 0.0;
-        while (k_idx < GRID && Wcum[k_idx + 1] < target) ++k_idx;
-        const double w0 = Wcum[k_idx], w1 = Wcum[k_idx + 1];
-        const double frac = w1 > w0 ? (target - w0) / (w1 - w0) : 0.0;
-        const double s_t = s_lo + ((double)k_idx + frac) * hs;
+        const double target = cdf_end > 0.0 ? ((double)t / (double)(n2 - 1)) * cdf_end : 0.0;
+        while (cell < GRID && cdf[cell + 1] < target) ++cell;
+        const double c0 = cdf[cell], c1 = cdf[cell + 1];
+        const double frac = c1 > c0 ? (target - c0) / (c1 - c0) : 0.0;
+        const double s_t = s_lo + ((double)cell + frac) * hs;
         double g_t = chi_s_to_gamma(A0, s_t);
         if (g_t < gamma_end) g_t = gamma_end;
         if (g_t > gamma_start) g_t = gamma_start;
         s_sched[n1 + t] = s_t;
         gammas[n1 + t] = g_t;
     }
-    free(Wcum);
+    free(cdf);
 }
 
 /* The pilot probe of one s point (sqa_chi_annealer.cpp:232-266): a fresh

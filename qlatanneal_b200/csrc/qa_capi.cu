@@ -413,7 +413,7 @@ void chi_schedule(int Pts, const double *xs, const double *gs, const double *ys,
     const double floor_ = degenerate ? 1.0 : std::max(floor_fraction * max_chi, 1e-12);
     scalars[3] = floor_;
     const double s_lo = A0 / (A0 + gamma_start), s_hi = A0 / (A0 + gamma_end);
-    auto weight_at = [&](double s) {
+    auto chi_weight = [&](double s) {
         double chi;
         if (s <= xs[0]) chi = ys[0];
         else if (s >= xs[Pts - 1]) chi = ys[Pts - 1];
@@ -434,15 +434,15 @@ void chi_schedule(int Pts, const double *xs, const double *gs, const double *ys,
     const int n2 = num_steps - n1;
     const int GRID = 4096;
     const double hs = (s_hi - s_lo) / (double)GRID;
-    std::vector<double> Wcum(GRID + 2, 0.0);
-    double prev_w = weight_at(s_lo);
+    std::vector<double> cdf(GRID + 2, 0.0);
+    double w_left = chi_weight(s_lo);
     for (int k = 1; k <= GRID; ++k) {
         const double sk = s_lo + (double)k * hs;
-        const double cur_w = weight_at(sk);
-        Wcum[k] = Wcum[k - 1] + 0.5 * (prev_w + cur_w) * hs;
-        prev_w = cur_w;
+        const double w_right = chi_weight(sk);
+        cdf[k] = cdf[k - 1] + 0.5 * (w_left + w_right) * hs;
+        w_left = w_right;
     }
-    const double W_total = Wcum[GRID];
+    const double cdf_end = cdf[GRID];
     for (int s = 0; s < num_steps; ++s) {
         betas[s] = beta;
         gammas[s] = gamma_start;
@@ -452,13 +452,13 @@ void chi_schedule(int Pts, const double *xs, const double *gs, const double *ys,
         const double frac = n1 > 1 ? (double)step / (double)(n1 - 1) : 1.0;
         betas[step] = ramp_start + (beta - ramp_start) * frac;
     }
-    int k_idx = 0;
+    int cell = 0;
     for (int t = 0; t < n2; ++t) {
-        const double target = W_total > 0.0 ? ((double)t / (double)(n2 - 1)) * W_total : 0.0;
-        while (k_idx < GRID && Wcum[k_idx + 1] < target) ++k_idx;
-        const double w0 = Wcum[k_idx], w1 = Wcum[k_idx + 1];
-        const double frac = w1 > w0 ? (target - w0) / (w1 - w0) : 0.0;
-        const double s_t = s_lo + ((double)k_idx + frac) * hs;
+        const double target = cdf_end > 0.0 ? ((double)t / (double)(n2 - 1)) * cdf_end : 0.0;
+        while (cell < GRID && cdf[cell + 1] < target) ++cell;
+        const double c0 = cdf[cell], c1 = cdf[cell + 1];
+        const double frac = c1 > c0 ? (target - c0) / (c1 - c0) : 0.0;
+        const double s_t = s_lo + ((double)cell + frac) * hs;
         s_sched[n1 + t] = s_t;
         gammas[n1 + t] = std::min(std::max(chi_s_to_gamma(A0, s_t), gamma_end), gamma_start);
     }
@@ -729,8 +729,8 @@ static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const Ri
     // fork: every side stream starts after the context stream's work so far
     QA_CK(cudaEventRecord(ctx->side_ev[0], ctx->stream));
     for (int k = 0; k < rt.streams; ++k) QA_CK(cudaStreamWaitEvent(ctx->side[k], ctx->side_ev[0], 0));
-    int n = 0;
-    for (int s0 = s_begin; s0 < s_end; s0 += seg) {  // segment-major issue keeps the streams in step
+    int n = 0, rc = QA_OK;
+    for (int s0 = s_begin; s0 < s_end && rc == QA_OK; s0 += seg) {  // segment-major issue keeps the streams in step
         for (int k = 0; k < rt.streams; ++k) {
             RingParams r2 = ring_offset(rp, k * rt.G);
             if (r2.bsamp) r2.bsamp += (size_t)(s0 - s_begin) * (rp.spb + rp.cls);  // indexed from step0
@@ -738,16 +738,21 @@ static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const Ri
             r2.step1 = std::min(s_end, s0 + seg);
             r2.init_fields = rp.init_fields && s0 == s_begin;
             r2.init_scan = rp.init_scan && s0 == s_begin;
-            QA_TRY(launch_rings(ctx, kind, pl, r2, std::min(rt.G, nr - k * rt.G), ctx->side[k]));
+            rc = launch_rings(ctx, kind, pl, r2, std::min(rt.G, nr - k * rt.G), ctx->side[k]);
+            if (rc != QA_OK) break;
             ++n;
         }
     }
-    for (int k = 0; k < rt.streams; ++k) {  // join
-        QA_CK(cudaEventRecord(ctx->side_ev[k], ctx->side[k]));
-        QA_CK(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[k], 0));
+    // join, also after a failed launch: the context stream must wait for
+    // whatever the side streams already hold before its next workspace write
+    for (int k = 0; k < rt.streams; ++k) {
+        cudaError_t e1 = cudaEventRecord(ctx->side_ev[k], ctx->side[k]);
+        cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(ctx->stream, ctx->side_ev[k], 0) : e1;
+        if (e2 != cudaSuccess && rc == QA_OK)
+            rc = fail(QA_ERR_CUDA, std::string("rotated launches, join: ") + cudaGetErrorString(e2));
     }
     *launches = n;
-    return QA_OK;
+    return rc;
 }
 
 // Batch buffers of an MLP (grown on demand) and the inputs/targets copied in.
@@ -1751,7 +1756,7 @@ double opt_profile(const std::vector<double> &pj, const std::vector<double> &pc,
 
 // The calibrated J_perp trajectory: step t of nt sits where
 // G(J) = int_js^J max(chi(J'), min_chi)^alpha dJ' (trapezoids on a 4096 grid)
-// reaches t/(nt-1) of G(je) (sqa_annealer.cpp:848-872,
+// reaches t/(nt-1) of G(je) (sqa_annealer.cpp:895-920,
 // sqa_parallel_tempering.cpp:768-794).
 std::vector<double> opt_trajectory(const std::vector<double> &pj, const std::vector<double> &pc, double js, double je,
                                    double min_chi, double alpha, int nt) {

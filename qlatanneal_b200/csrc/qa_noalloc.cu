@@ -10,10 +10,16 @@
 // pointers; everything else this run needs lives in g_scratch below.
 //
 // g_scratch is a file-scope __device__ array of QA_NOALLOC_SCRATCH_BYTES
-// (16 MiB).  Every GPU that loads the library holds it until the process
-// exits.  Host code never dereferences the symbol: its device address is
-// looked up once per device with cudaGetSymbolAddress, on the first call
-// made with that device (make that first call before any stream capture).
+// (16 MiB).  Every GPU that loads the library's device code holds it until
+// the process exits.  Under CUDA's default lazy module loading that happens
+// inside the first call on a device, which is when the 16 MiB are reserved:
+// make that first call (a small warm-up run will do) before the framework
+// reserves most of the device memory, or set CUDA_MODULE_LOADING=EAGER so the
+// array is reserved when the context is created.  Host code never
+// dereferences the symbol: its device address is looked up once per device
+// with cudaGetSymbolAddress, on the first call made with that device (make
+// that first call before any stream capture).  The call switches to `device`
+// for its work and puts the caller's current device back before it returns.
 // Every call reuses the same array and leaves its contents behind; what must
 // start at zero (the counters) is cleared on each call.  Two calls whose work
 // overlaps on the GPU (different streams, or different host threads) race on
@@ -44,6 +50,19 @@ std::mutex g_scratch_mu;
 unsigned char *g_scratch_addr[QA_NOALLOC_MAX_DEVICES] = {};
 
 int noalloc_fail(int code, const std::string &msg) { return qa::set_last_error(code, msg.c_str()); }
+
+// Puts the calling thread's current device back when the call returns, on
+// every path: a framework caller working on another device must not find
+// itself switched to this call's device.
+struct DeviceRestore {
+    int prev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~DeviceRestore() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
 
 size_t carve(size_t &off, size_t bytes) {
     const size_t at = (off + 255) / 256 * 256;
@@ -114,6 +133,7 @@ extern "C" int qa_sa_dense_run_noalloc(int device, void *stream, int n, const do
                                             " bytes of scratch (about 4*n*n + 8*reads*n + 4*steps); the static "
                                             "scratch holds " + std::to_string(QA_NOALLOC_SCRATCH_BYTES) + " bytes.");
 
+    DeviceRestore restore_device;
     NA_CK(cudaSetDevice(device));
     unsigned char *base = nullptr;
     {

@@ -56,7 +56,7 @@ def test_run_optimal_bit_exact(oracle, kind, n, P, K, eps, spb, wls, cls, probes
     assert jt[-1] > js and jt[-1] <= je + 1e-12
 
 
-def test_run_optimal_rotated_bit_exact(oracle):
+def test_run_optimal_rotated_bit_exact(oracle, monkeypatch):
     """More rings than SMs: the phases with >= 200 sweeps run as rotated
     launches of ring groups; every read equals the oracle's."""
     model = make("dense", 40, 61)
@@ -65,9 +65,18 @@ def test_run_optimal_rotated_bit_exact(oracle):
     beta, js, je, alpha, rf, rs = 2.0, 0.05, 2.0, 15.0 / 14.0, 0.3, 0.1
     reads, seed = 80, 717
     ann = qa.SQAAnnealer(model, qa.SQASchedule.from_vectors([1.0], [1.0]), P, K)
-    res = ann.run_optimal_reads(beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps, rf, rs,
-                                reads=reads, seed=seed)
-    assert ann.last_stats.sweep_launches > 20  # ring groups, not whole-grid launches
+    args = (beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps, rf, rs)
+    res = ann.run_optimal_reads(*args, reads=reads, seed=seed)
+    rotated = ann.last_stats.sweep_launches
+    with monkeypatch.context() as mp:
+        mp.setenv("QA_WHOLE_GRID", "1")
+        whole = ann.run_optimal_reads(*args, reads=reads, seed=seed)
+        whole_launches = ann.last_stats.sweep_launches
+    # the rotated run issued ring-group launches that the whole-grid run did not
+    assert rotated > whole_launches, (rotated, whole_launches)
+    for r in range(reads):
+        np.testing.assert_array_equal(res[r].best_state.as_array(), whole[r].best_state.as_array())
+        assert res[r].best_energy == whole[r].best_energy
     for r in range(reads):
         o = oracle.sqa_opt_run(om, P, K, beta, js, je, eps, alpha, steps, spb, wls, cls, probes, csweeps, rf, rs,
                                seed, r)
@@ -178,7 +187,7 @@ def test_sqapt_run_optimal_bit_exact(oracle, kind, n, R, P, spb, wls, cls, steps
         assert swaps > 0.0  # the SK ladders exchange rungs; the other instances need not
 
 
-def test_sqapt_run_optimal_rotated_bit_exact(oracle):
+def test_sqapt_run_optimal_rotated_bit_exact(oracle, monkeypatch):
     """More rings than SMs: segments with >= 8 sweeps run as rotated launches
     joined before the swaps; every read equals the oracle's."""
     model = make("dense", 48, 67)
@@ -187,9 +196,14 @@ def test_sqapt_run_optimal_rotated_bit_exact(oracle):
     betas, gammas = np.geomspace(0.5, 3.0, R), np.geomspace(2.0, 0.3, R)
     alpha, probes, csweeps, reads, seed = 15.0 / 14.0, 5, 3, 40, 929
     ann = qa.SQAParallelTemperingAnnealer(model, betas, gammas, P)
-    res = ann.run_optimal_reads(steps, spb, wls, eps, alpha, je, cls, swap, cts, probes, csweeps, reads=reads,
-                                seed=seed)
-    assert ann.last_stats.sweep_launches > 2 * (steps // swap)  # ring groups, not whole-grid launches
+    args = (steps, spb, wls, eps, alpha, je, cls, swap, cts, probes, csweeps)
+    res = ann.run_optimal_reads(*args, reads=reads, seed=seed)
+    rotated = ann.last_stats.sweep_launches
+    with monkeypatch.context() as mp:
+        mp.setenv("QA_WHOLE_GRID", "1")
+        ann.run_optimal_reads(*args, reads=reads, seed=seed)
+        whole_launches = ann.last_stats.sweep_launches
+    assert rotated > whole_launches, (rotated, whole_launches)  # ring groups, not whole-grid launches
     for r in range(reads):
         o = oracle.sqapt_opt_run(om, betas, gammas, P, spb, wls, cls, steps, swap, eps, alpha, je, probes, csweeps,
                                  seed, r)
