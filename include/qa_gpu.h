@@ -69,6 +69,26 @@ QA_API int qa_destroy(qa_ctx *ctx);
  * (the default): off. */
 QA_API int qa_set_drift_check(qa_ctx *ctx, double tolerance);
 
+/* Update order of the SQA and SQA-PT sweeps (qa_sqa_run, qa_sqa_opt_run,
+ * qa_sqapt_run, qa_sqapt_opt_run and the traced SQA run).
+ * QA_ORDER_REFERENCE (the default) is qanneal's order: before every slice,
+ * cluster and worldline sweep of a replica a fresh uniformly random spin
+ * order (the std::shuffle of sqa_annealer.cpp:181,216,295 and
+ * sqa_parallel_tempering.cpp:209,224,281), the Trotter slices swept one after
+ * another, t = 0 .. P-1, each in that order; the engine then samples the
+ * reference's Markov chain, so finite-time statistics (best-energy
+ * distributions, ground-state probabilities) match the reference's.
+ * QA_ORDER_CHECKERBOARD sweeps the slices in parity phases (even, odd) with
+ * the spins ascending, the order qanneal's SQAChiAnnealer uses
+ * (sqa_chi_annealer.cpp:68-140): the same stationary distribution, faster on
+ * the GPU, different finite-time dynamics.  SQA-Chi always keeps its
+ * checkerboard, SA and classical parallel tempering their ascending order.
+ * A pipeline wait that runs out (it cannot in a correct run) makes the call
+ * return QA_ERR_TIMEOUT. */
+enum { QA_ORDER_CHECKERBOARD = 0, QA_ORDER_REFERENCE = 1 };
+QA_API int qa_set_update_order(qa_ctx *ctx, int order);
+QA_API int qa_get_update_order(const qa_ctx *ctx, int *order);
+
 /* ---- problems (device copies of one model instance) ------------------- */
 
 /* DenseIsing(h, J, n, c) (dense_ising.hpp:17-21): E = c + sum h s + sum_{i<j} J_ij s_i s_j.

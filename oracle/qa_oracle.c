@@ -82,7 +82,7 @@ OR_EXPORT void or_philox(const uint32_t ctr_in[4], const uint32_t key_in[2], uin
 enum {
     DOM_INIT = 1, DOM_SA = 2, DOM_SLICE = 3, DOM_WORLD = 4, DOM_SWAP = 5,
     DOM_PILOT_INIT = 6, DOM_PILOT = 7, DOM_PROD_INIT = 8, DOM_PROD = 9, DOM_CSPIN = 10, DOM_CBOND = 11,
-    DOM_OPTCAL = 12
+    DOM_OPTCAL = 12, DOM_PERM = 13
 };
 
 static inline uint32_t spin_slot(int i) { return (uint32_t)(((i >> 7) << 5) | (i & 31)); }
@@ -648,6 +648,51 @@ static int phase_of(int t, int P) {
     return t & 1;
 }
 
+/* Update order of the SQA and SQA-PT sweeps (the SQA-Chi kernel keeps its own
+   parity checkerboard, sqa_chi_annealer.cpp:68-140, in every mode):
+   1 (default): qanneal's order in law -- before every slice, cluster and
+     worldline sweep a fresh uniformly random spin order (std::shuffle at
+     sqa_annealer.cpp:181,216,295,599,631,703 and
+     sqa_parallel_tempering.cpp:209,224,281,489), the slices of a ring swept
+     one after another, t = 0 .. P-1, each in that order;
+   0: parity checkerboard over the slices (even, odd, the last odd one alone),
+     spins ascending. */
+static int g_order = 1;
+OR_EXPORT void or_set_update_order(int order) { g_order = order ? 1 : 0; }
+OR_EXPORT int or_get_update_order(void) { return g_order; }
+
+static int u64_cmp(const void *a, const void *b) {
+    const uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* The random spin order of one sweep: spins sorted by the 64-bit keys
+   K_i = (r_i with its low 20 bits cleared) | i, r_i = (x_a << 32) | x_b from
+   philox(i >> 1, ring, sweep, (tag << 8) | DOM_PERM) -- words 0, 1 for even
+   i, words 2, 3 for odd i.  44 random bits a key make ties (broken by the
+   spin index) negligible, so the order is uniform over all n! orders, as
+   std::shuffle's.  order[p] is the spin visited p-th. */
+static void sweep_order(uint64_t key, uint32_t ring, uint32_t sigma, uint32_t tag, int n, int *order) {
+    uint64_t *K = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)n);
+    uint32_t out[4] = {0, 0, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        if ((i & 1) == 0) {
+            uint32_t ctr[4] = {(uint32_t)(i >> 1), ring, sigma, (tag << 8) | DOM_PERM};
+            uint32_t kk[2] = {(uint32_t)key, (uint32_t)(key >> 32)};
+            or_philox(ctr, kk, out);
+        }
+        const uint64_t r = ((uint64_t)out[2 * (i & 1)] << 32) | out[2 * (i & 1) + 1];
+        K[i] = (r & ~(uint64_t)0xFFFFF) | (uint64_t)i;
+    }
+    qsort(K, (size_t)n, sizeof(uint64_t), u64_cmp);
+    for (int p = 0; p < n; ++p) order[p] = (int)(K[p] & 0xFFFFF);
+    free(K);
+}
+
+OR_EXPORT void or_sweep_order(uint64_t key, uint32_t ring, uint32_t sigma, uint32_t tag, int n, int *order) {
+    sweep_order(key, ring, sigma, tag, n, order);
+}
+
 static void ring_alloc(ring_t *R, const or_model *M, int P, int K, uint64_t key) {
     memset(R, 0, sizeof(*R));
     R->M = M; R->n = M->n; R->P = P; R->K = K; R->key = key;
@@ -667,7 +712,8 @@ static void ring_init(ring_t *R, uint32_t tag) {
 /* One slice of one ring: sqa_annealer.cpp:180-209 / sqa_chi_annealer.cpp:96-121.
    rng_cell is the cell index used in the counter (ring-relative k*P+t unless
    a slot remap applies). */
-static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigma, uint32_t tag, float B, float T4) {
+static void sweep_cell_ord(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigma, uint32_t tag, float B,
+                           float T4, const int *order) {
     const or_model *M = R->M;
     const int n = R->n, P = R->P;
     const int prev = t == 0 ? P - 1 : t - 1, next = (t + 1) % P;
@@ -675,11 +721,13 @@ static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigm
     const int8_t *sp = R->s + ((size_t)k * P + prev) * n;
     const int8_t *sn = R->s + ((size_t)k * P + next) * n;
     float *g = R->g + ((size_t)k * P + t) * n;
-    for (int i = 0; i < n; ++i) {
+    for (int pos = 0; pos < n; ++pos) {
+        /* the uniform belongs to the visiting position, the spin to the order */
+        const int i = order ? order[pos] : pos;
         const int si = s[i];
         const int q = si * (sp[i] + sn[i]) / 2;
         const float tro = q == 0 ? 0.0f : (q > 0 ? T4 : -T4);
-        float u = u01(draw(R->key, spin_slot(i), rng_cell, sigma, tag, spin_word(i)));
+        float u = u01(draw(R->key, spin_slot(pos), rng_cell, sigma, tag, spin_word(pos)));
         float loc = M->h32[i] + g[i];
         float x = si > 0 ? loc : -loc;
         R->att_slice++;
@@ -691,7 +739,22 @@ static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigm
     }
 }
 
-static void slice_sweep(ring_t *R, uint32_t sigma, uint32_t tag, float B, float T4, const int *slot_of_ring) {
+static void sweep_cell(ring_t *R, int k, int t, uint32_t rng_cell, uint32_t sigma, uint32_t tag, float B, float T4) {
+    sweep_cell_ord(R, k, t, rng_cell, sigma, tag, B, T4, NULL);
+}
+
+/* One slice sweep of ring k in qanneal's order: one random spin order for the
+   sweep, slices t = 0 .. P-1 in turn (sqa_annealer.cpp:180-209,
+   sqa_parallel_tempering.cpp:208-221).  B and T4 may differ per ring (PT). */
+static void ring_slice_sweep_ref(ring_t *R, int k, uint32_t slot, uint32_t sigma, uint32_t tag, float B, float T4) {
+    int *order = (int *)malloc(sizeof(int) * (size_t)R->n);
+    sweep_order(R->key, slot, sigma, tag, R->n, order);
+    for (int t = 0; t < R->P; ++t) sweep_cell_ord(R, k, t, slot * (uint32_t)R->P + (uint32_t)t, sigma, tag, B, T4, order);
+    free(order);
+}
+
+/* The parity checkerboard (SQA-Chi's order, and the opt-in order of SQA / SQA-PT). */
+static void slice_sweep_cb(ring_t *R, uint32_t sigma, uint32_t tag, float B, float T4, const int *slot_of_ring) {
     for (int ph = 0; ph < 3; ++ph)
         for (int k = 0; k < R->K; ++k)
             for (int t = 0; t < R->P; ++t) {
@@ -701,11 +764,26 @@ static void slice_sweep(ring_t *R, uint32_t sigma, uint32_t tag, float B, float 
             }
 }
 
+static void slice_sweep(ring_t *R, uint32_t sigma, uint32_t tag, float B, float T4, const int *slot_of_ring) {
+    if (!g_order) {
+        slice_sweep_cb(R, sigma, tag, B, T4, slot_of_ring);
+        return;
+    }
+    for (int k = 0; k < R->K; ++k)
+        ring_slice_sweep_ref(R, k, (uint32_t)(slot_of_ring ? slot_of_ring[k] : k), sigma, tag, B, T4);
+}
+
 /* sqa_annealer.cpp:294-315 */
 static void worldline_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma, float B) {
     const or_model *M = R->M;
     const int n = R->n, P = R->P;
-    for (int i = 0; i < n; ++i) {
+    int *order = NULL;
+    if (g_order) {
+        order = (int *)malloc(sizeof(int) * (size_t)n);
+        sweep_order(R->key, rng_ring, sigma, DOM_WORLD, n, order);
+    }
+    for (int pos = 0; pos < n; ++pos) {
+        const int i = order ? order[pos] : pos;
         int sh = 0;
         double G = 0.0;
         for (int t = 0; t < P; ++t) {
@@ -714,7 +792,7 @@ static void worldline_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma,
             G += (double)st * (double)R->g[((size_t)k * P + t) * n + i];
         }
         float x = (float)((double)M->h32[i] * (double)sh + G);
-        float u = u01(draw(R->key, spin_slot(i), rng_ring, sigma, DOM_WORLD, spin_word(i)));
+        float u = u01(draw(R->key, spin_slot(pos), rng_ring, sigma, DOM_WORLD, spin_word(pos)));
         R->att_world++;
         if (metropolis(x * B, u)) {
             R->acc_world++;
@@ -726,6 +804,7 @@ static void worldline_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma,
             }
         }
     }
+    free(order);
 }
 
 /* Cluster move of spin i of replica k along imaginary time, the
@@ -792,7 +871,14 @@ static int cluster_move(ring_t *R, int k, int i, uint32_t rng_ring, uint32_t sig
 }
 
 static void cluster_sweep(ring_t *R, int k, uint32_t rng_ring, uint32_t sigma, float B, float T4, float JP) {
-    for (int i = 0; i < R->n; ++i) cluster_move(R, k, i, rng_ring, sigma, B, T4, JP);
+    if (!g_order) {
+        for (int i = 0; i < R->n; ++i) cluster_move(R, k, i, rng_ring, sigma, B, T4, JP);
+        return;
+    }
+    int *order = (int *)malloc(sizeof(int) * (size_t)R->n);
+    sweep_order(R->key, rng_ring, sigma, DOM_CSPIN, R->n, order);
+    for (int p = 0; p < R->n; ++p) cluster_move(R, k, order[p], rng_ring, sigma, B, T4, JP);
+    free(order);
 }
 
 static float join_prob(double beta, double gamma, int P) {
@@ -989,13 +1075,17 @@ static int sqapt_core(const or_model *M, const double *betas, const double *gamm
     for (int step = 0; step < steps; ++step) {
         for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * spb + sw);
-            for (int ph = 0; ph < 3; ++ph)
+            if (g_order && !classical)  /* classical PT: ascending (parallel_tempering.cpp:36-122) */
                 for (int k = 0; k < Rn; ++k)
-                    for (int t = 0; t < P; ++t) {
-                        if (phase_of(t, P) != ph) continue;
-                        const int sl = slot_of[k];
-                        sweep_cell(&R, k, t, (uint32_t)(sl * P + t), sigma, DOM_SLICE, B[sl], T4[sl]);
-                    }
+                    ring_slice_sweep_ref(&R, k, (uint32_t)slot_of[k], sigma, DOM_SLICE, B[slot_of[k]], T4[slot_of[k]]);
+            else
+                for (int ph = 0; ph < 3; ++ph)
+                    for (int k = 0; k < Rn; ++k)
+                        for (int t = 0; t < P; ++t) {
+                            if (phase_of(t, P) != ph) continue;
+                            const int sl = slot_of[k];
+                            sweep_cell(&R, k, t, (uint32_t)(sl * P + t), sigma, DOM_SLICE, B[sl], T4[sl]);
+                        }
         }
         for (int sw = 0; sw < cls; ++sw)
             for (int k = 0; k < Rn; ++k) {
@@ -1157,7 +1247,7 @@ static double chi_pilot_point(const or_model *M, int P, int K, uint64_t key, int
     double m2_sum = 0.0, mabs_sum = 0.0;
     long long count = 0;
     for (int sw = 0; sw < burn + sweeps; ++sw) {
-        slice_sweep(&R, (uint32_t)sw, DOM_PILOT | ((uint32_t)m << 8), B, T4, NULL);
+        slice_sweep_cb(&R, (uint32_t)sw, DOM_PILOT | ((uint32_t)m << 8), B, T4, NULL);
         if (sw >= burn)
             for (int k = 0; k < K; ++k) {
                 long long sum = 0;
@@ -1214,7 +1304,7 @@ OR_EXPORT int or_chi_run(const or_model *M, int P, int K, double beta, double ga
     for (int step = 0; step < num_steps; ++step) {
         float B, T4;
         step_consts(beta_sched[step], gamma_sched[step], P, &B, &T4);
-        for (int sw = 0; sw < spb; ++sw) slice_sweep(&R, (uint32_t)(step * spb + sw), DOM_PROD, B, T4, NULL);
+        for (int sw = 0; sw < spb; ++sw) slice_sweep_cb(&R, (uint32_t)(step * spb + sw), DOM_PROD, B, T4, NULL);
         for (int k = 0; k < K; ++k) {
             double sum = 0.0, emin = INFINITY;
             int tmin = 0;
@@ -1504,13 +1594,17 @@ static void ptopt_sweep(ring_t *R, const int *slot_of, const float *B, int step,
     const int Rn = R->K, P = R->P, ns = spb + cls;
     for (int sw = 0; sw < spb; ++sw) {
         const uint32_t sigma = (uint32_t)(step * spb + sw);
-        for (int ph = 0; ph < 3; ++ph)
+        if (g_order)
             for (int k = 0; k < Rn; ++k)
-                for (int t = 0; t < P; ++t) {
-                    if (phase_of(t, P) != ph) continue;
-                    const int sl = slot_of[k];
-                    sweep_cell(R, k, t, (uint32_t)(sl * P + t), sigma, slice_tag, B[sl], T4);
-                }
+                ring_slice_sweep_ref(R, k, (uint32_t)slot_of[k], sigma, slice_tag, B[slot_of[k]], T4);
+        else
+            for (int ph = 0; ph < 3; ++ph)
+                for (int k = 0; k < Rn; ++k)
+                    for (int t = 0; t < P; ++t) {
+                        if (phase_of(t, P) != ph) continue;
+                        const int sl = slot_of[k];
+                        sweep_cell(R, k, t, (uint32_t)(sl * P + t), sigma, slice_tag, B[sl], T4);
+                    }
         for (int k = 0; k < Rn; ++k) samp[(size_t)k * ns + sw] = bond_sum(R, k);
     }
     for (int sw = 0; sw < cls; ++sw)

@@ -33,6 +33,8 @@ from .annealers import (  # noqa: F401
     SQAChiAnnealer,
     BatchRunner,
     set_drift_check,
+    set_update_order,
+    get_update_order,
 )
 from ._lib import FieldDriftError  # noqa: F401
 from .observers import (  # noqa: F401

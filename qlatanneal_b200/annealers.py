@@ -183,6 +183,33 @@ def set_drift_check(tolerance: float, device: Optional[int] = None) -> None:
     _lib.check(eng.L.qa_set_drift_check(eng.h, float(tolerance)))
 
 
+_ORDERS = {"reference": _lib.QA_ORDER_REFERENCE, "checkerboard": _lib.QA_ORDER_CHECKERBOARD}
+
+
+def set_update_order(order: str, device: Optional[int] = None) -> None:
+    """Sweep order of the SQA and SQA-PT runs on the device.
+
+    ``"reference"`` (the default) is qanneal's: a fresh random spin order
+    before every slice, cluster and worldline sweep, the Trotter slices swept
+    one after another -- the engine then samples qanneal's own Markov chain,
+    so its finite-time statistics match qanneal's.  ``"checkerboard"`` sweeps
+    the slices in parity phases with the spins ascending (the order of
+    qanneal's SQAChiAnnealer): the same stationary distribution, faster,
+    different finite-time dynamics.  SQA-Chi, SA and classical parallel
+    tempering keep their own orders either way."""
+    if order not in _ORDERS:
+        raise ValueError("update order must be 'reference' or 'checkerboard'.")
+    eng = _lib.Engine.get(device)
+    _lib.check(eng.L.qa_set_update_order(eng.h, _ORDERS[order]))
+
+
+def get_update_order(device: Optional[int] = None) -> str:
+    eng = _lib.Engine.get(device)
+    v = _lib.C.c_int(0)
+    _lib.check(eng.L.qa_get_update_order(eng.h, _lib.C.byref(v)))
+    return "reference" if v.value == _lib.QA_ORDER_REFERENCE else "checkerboard"
+
+
 class _Seeded:
     def __init__(self):
         self._seed = _random_seed()

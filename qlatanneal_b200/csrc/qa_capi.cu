@@ -34,6 +34,15 @@ int fail(int code, const std::string &msg) {
     return code;
 }
 
+// The error word the sweep kernels leave in counters[4]: a bounded wait of
+// the slice pipeline that ran out (the outputs of that call are void).
+int check_device_error(const unsigned long long *cnt) {
+    if (cnt[4] & QA_DEV_ERR_TIMEOUT)
+        return fail(QA_ERR_TIMEOUT, "a sweep kernel's bounded wait for its slice pipeline ran out; the run's "
+                                    "outputs are void");
+    return QA_OK;
+}
+
 #define QA_CK(call)                                                                                   \
     do {                                                                                              \
         cudaError_t e_ = (call);                                                                      \
@@ -161,6 +170,7 @@ struct qa_ctx {
     int smem_optin = 0;
     int sms = 0;             // streaming multiprocessors of the device
     double drift_tol = 0.0;  // > 0: field-drift check after SA / SQA / SQA-PT runs
+    int update_order = QA_ORDER_REFERENCE;  // SQA / SQA-PT sweep order (qa_set_update_order)
     // side streams for the rotated ring launches (run_rings_rotated) and their events
     std::vector<cudaStream_t> side;
     std::vector<cudaEvent_t> side_ev;
@@ -522,6 +532,7 @@ struct RingPlan {
     bool own_fields() const { return pm1 || sparse; }  // no field cache to initialise
     int gbytes = 4;       // pm1: bytes per field (4 int32, 2 int16)
     bool jw_smem = true;  // pm1: J bits in shared memory
+    bool ref_order = false;  // qanneal's update order (else the parity checkerboard)
     int W = 1;
     size_t smem = 0;
     int smem_fields = 1;
@@ -532,43 +543,47 @@ struct RingPlan {
 // fields, int16 fields with J read from L2.  P <= 64 (worldlines are 64-bit
 // columns) and n <= 2048.  Anything else runs ring_kernel.
 int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, int P, int n_max, RingPlan *pl,
-               bool clusters = false) {
+               bool clusters = false, bool ref_order = false) {
     pl->W = std::max(1, std::min(32, (P + 1) / 2));
+    pl->ref_order = ref_order;
+    if (ref_order && n_max > (1 << 20))
+        return fail(QA_ERR_ARG, "the shuffled update order supports at most 2^20 spins per model.");
     // cluster moves are in ring_kernel only
     pl->pm1 = !clusters && kind == K_DENSE && P <= 64 && n_max <= 2048 && !std::getenv("QA_DISABLE_PM1");
     for (int p = 0; p < np && pl->pm1; ++p) pl->pm1 = probs[p]->dev.Jw != nullptr;
     if (pl->pm1) {
         const size_t cap = (size_t)ctx->smem_optin;
         const bool int32_only = std::getenv("QA_PM1_INT32_ONLY") != nullptr;
-        if (pm1_smem_bytes(P, n_max, 4, true) <= cap) {
+        if (pm1_smem_bytes(P, n_max, 4, true, ref_order) <= cap) {
             pl->gbytes = 4; pl->jw_smem = true;
-        } else if (!int32_only && pm1_smem_bytes(P, n_max, 2, true) <= cap) {
+        } else if (!int32_only && pm1_smem_bytes(P, n_max, 2, true, ref_order) <= cap) {
             pl->gbytes = 2; pl->jw_smem = true;
-        } else if (!int32_only && pm1_smem_bytes(P, n_max, 2, false) <= cap) {
+        } else if (!int32_only && pm1_smem_bytes(P, n_max, 2, false, ref_order) <= cap) {
             pl->gbytes = 2; pl->jw_smem = false;
         } else {
             pl->pm1 = false;
         }
     }
     if (pl->pm1) {
-        pl->smem = pm1_smem_bytes(P, n_max, pl->gbytes, pl->jw_smem);
+        pl->smem = pm1_smem_bytes(P, n_max, pl->gbytes, pl->jw_smem, ref_order);
         pl->smem_fields = 0;
         return QA_OK;
     }
     // sparse integer couplings: fields on demand, worldline sums from bits
-    pl->sparse = !clusters && kind == K_SPARSE && P <= 64 && sparse_smem_bytes(P, n_max) <= (size_t)ctx->smem_optin &&
+    pl->sparse = !clusters && kind == K_SPARSE && P <= 64 &&
+                 sparse_smem_bytes(P, n_max, ref_order) <= (size_t)ctx->smem_optin &&
                  !std::getenv("QA_DISABLE_SPARSE_INT");
     for (int p = 0; p < np && pl->sparse; ++p) pl->sparse = probs[p]->dev.spcv != nullptr;
     if (pl->sparse) {
-        pl->smem = sparse_smem_bytes(P, n_max);
+        pl->smem = sparse_smem_bytes(P, n_max, ref_order);
         pl->smem_fields = 0;
         return QA_OK;
     }
-    pl->smem = ring_smem_bytes(P, n_max, pl->W, true);
+    pl->smem = ring_smem_bytes(P, n_max, pl->W, true, ref_order);
     pl->smem_fields = 1;
     if (pl->smem > (size_t)std::min(ctx->smem_optin, 200 * 1024)) {
         pl->smem_fields = 0;
-        pl->smem = ring_smem_bytes(P, n_max, pl->W, false);
+        pl->smem = ring_smem_bytes(P, n_max, pl->W, false, ref_order);
     }
     if (pl->smem > (size_t)ctx->smem_optin) return fail(QA_ERR_ARG, "ring state does not fit in shared memory.");
     return QA_OK;
@@ -605,6 +620,7 @@ int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n
     cudaStream_t strm = stream ? stream : ctx->stream;
     rp.W = pl.W;
     rp.smem_fields = pl.smem_fields;
+    rp.ref_order = pl.ref_order ? 1 : 0;
     if (pl.pm1) {
         auto kern = pl.gbytes == 4 ? ring_pm1_kernel<int, true>
                                    : (pl.jw_smem ? ring_pm1_kernel<short, true> : ring_pm1_kernel<short, false>);
@@ -1197,6 +1213,20 @@ int qa_set_drift_check(qa_ctx *ctx, double tolerance) {
     return QA_OK;
 }
 
+int qa_set_update_order(qa_ctx *ctx, int order) {
+    if (!ctx) return fail(QA_ERR_ARG, "null context");
+    if (order != QA_ORDER_REFERENCE && order != QA_ORDER_CHECKERBOARD)
+        return fail(QA_ERR_ARG, "update order must be QA_ORDER_REFERENCE or QA_ORDER_CHECKERBOARD.");
+    ctx->update_order = order;
+    return QA_OK;
+}
+
+int qa_get_update_order(const qa_ctx *ctx, int *order) {
+    if (!ctx || !order) return fail(QA_ERR_ARG, "null argument");
+    *order = ctx->update_order;
+    return QA_OK;
+}
+
 // After a run on float32 field caches (field rows of ring r at
 // fields + field_off, stride n): the drift check when the context has one.
 // Sets stats->max_field_drift; QA_ERR_DRIFT above the tolerance.
@@ -1271,11 +1301,11 @@ static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     double *d_best = static_cast<double *>(v);
     QA_TRY(ws_get(ctx, W_BITS, sizeof(uint32_t) * (size_t)nr * L.nw_max, &v));
     uint32_t *d_bits = static_cast<uint32_t *>(v);
-    QA_TRY(ws_get(ctx, W_CNT, sizeof(unsigned long long) * 4, &v));
+    QA_TRY(ws_get(ctx, W_CNT, sizeof(unsigned long long) * 5, &v));
     unsigned long long *d_cnt = static_cast<unsigned long long *>(v);
     QA_TRY(ws_get(ctx, W_EXACT, sizeof(double) * nr, &v));
     double *d_exact = static_cast<double *>(v);
-    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 5, ctx->stream));
     double *d_mag = nullptr;
     int *d_bstep = nullptr;
     bool want_mag = mag_out != nullptr, want_states = false, want_end = false;
@@ -1346,7 +1376,7 @@ static int sa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
 
     std::vector<double> trace((size_t)nr * prm->steps), exact(nr);
     std::vector<uint32_t> bits((size_t)nr * L.nw_max);
-    unsigned long long cnt[4];
+    unsigned long long cnt[5];
     QA_CK(cudaMemcpyAsync(trace.data(), d_trace, sizeof(double) * trace.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(exact.data(), d_exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1508,11 +1538,11 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     int *d_bstep = static_cast<int *>(v);
     QA_TRY(ws_get(ctx, W_BITS, sizeof(uint32_t) * (size_t)nr * L.nw_max, &v));
     uint32_t *d_bits = static_cast<uint32_t *>(v);
-    QA_TRY(ws_get(ctx, W_CNT, sizeof(unsigned long long) * 4, &v));
+    QA_TRY(ws_get(ctx, W_CNT, sizeof(unsigned long long) * 5, &v));
     unsigned long long *d_cnt = static_cast<unsigned long long *>(v);
     QA_TRY(ws_get(ctx, W_EXACT, sizeof(double) * nr, &v));
     double *d_exact = static_cast<double *>(v);
-    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 5, ctx->stream));
     {
         std::vector<double> inf(nr, INFINITY);
         std::vector<int> neg(nr, -1);
@@ -1548,7 +1578,8 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
 
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     RingPlan pl;
-    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0 || traces));
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0 || traces,
+                      ctx->update_order == QA_ORDER_REFERENCE));
     // dense +-1 couplings: the bit-packed kernel builds its fields in-kernel
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
@@ -1590,7 +1621,7 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     std::vector<double> bestE(nr), exact(nr);
     std::vector<int> bstep(nr);
     std::vector<uint32_t> bits((size_t)nr * L.nw_max);
-    unsigned long long cnt[4];
+    unsigned long long cnt[5];
     QA_CK(cudaMemcpyAsync(ctx->down.data(), d_sum, sizeof(double) * (size_t)nr * steps, cudaMemcpyDeviceToHost,
                           ctx->stream));
     QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1614,6 +1645,7 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
         QA_CK(cudaMemcpyAsync(rspin.data(), d_rspin, sizeof(long long) * rspin.size(), cudaMemcpyDeviceToHost,
                               ctx->stream));
     QA_CK(cudaStreamSynchronize(ctx->stream));
+    QA_TRY(check_device_error(cnt));
     for (int p = 0; traces && p < n_problems; ++p) {
         const qa_sqa_trace &t = traces[p];
         const int n = problems[p]->n;
@@ -1860,9 +1892,9 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     QA_TRY(ws_array(ctx, W_CBSTEP, nr, &d_cbstep));
     QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
     QA_TRY(ws_array(ctx, W_CBITS, (size_t)nr * L.nw_max, &d_cbits));
-    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    QA_TRY(ws_array(ctx, W_CNT, 5, &d_cnt));
     QA_TRY(ws_array(ctx, W_EXACT, nr, &d_exact));
-    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 5, ctx->stream));
     auto upload_tables = [&]() -> int {
         QA_CK(cudaMemcpyAsync(d_A, A.data(), sizeof(float) * A.size(), cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * A.size(), cudaMemcpyHostToDevice, ctx->stream));
@@ -1879,7 +1911,7 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
 
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     RingPlan pl;
-    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, cls > 0));
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, cls > 0, ctx->update_order == QA_ORDER_REFERENCE));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
                       !pl.own_fields()));
     RingParams rp{};
@@ -2061,7 +2093,7 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     std::vector<double> sums((size_t)nr * S), bestE(nr), exact(nr);
     std::vector<int> bstep(nr);
     std::vector<uint32_t> bits((size_t)nr * L.nw_max);
-    unsigned long long cnt[4];
+    unsigned long long cnt[5];
     QA_CK(cudaMemcpyAsync(sums.data(), d_sum, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bstep.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
@@ -2069,6 +2101,7 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaStreamSynchronize(ctx->stream));
+    QA_TRY(check_device_error(cnt));
     for (int p = 0; p < n_problems; ++p) {
         const int n = problems[p]->n;
         qa_sqaopt_out &o = outs[p];
@@ -2138,7 +2171,7 @@ static int pt_collect(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
         swp((size_t)reads_total * steps);
     std::vector<int> bstep(nr), bslot(nr), rin((size_t)reads_total * Rn);
     std::vector<uint32_t> bits((size_t)nr * L.nw_max), fbits((size_t)nr * L.nw_max);
-    unsigned long long cnt[4];
+    unsigned long long cnt[5];
     QA_CK(cudaMemcpyAsync(bestE.data(), d.best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(exact.data(), d.exact, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpy2DAsync(lastmin.data(), sizeof(double), d.min + steps, sizeof(double) * (steps + 1),
@@ -2152,6 +2185,7 @@ static int pt_collect(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_CK(cudaMemcpyAsync(fbits.data(), d.fbits, sizeof(uint32_t) * fbits.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(cnt, d.cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaStreamSynchronize(ctx->stream));
+    QA_TRY(check_device_error(cnt));
     for (int p = 0; p < n_problems; ++p) {
         const int n = problems[p]->n;
         qa_sqapt_out &o = *outs[p];
@@ -2269,7 +2303,7 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_TRY(ws_array(ctx, W_EXACT, nr, &d_exact));
     QA_TRY(ws_array(ctx, W_AVG, (size_t)reads_total * steps, &d_avg));
     QA_TRY(ws_array(ctx, W_SWP, (size_t)reads_total * steps, &d_swp));
-    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    QA_TRY(ws_array(ctx, W_CNT, 5, &d_cnt));
     {
         std::vector<double> inf(nr, INFINITY);
         std::vector<int> neg(nr, -2), slot(nr), rin((size_t)reads_total * Rn);
@@ -2284,11 +2318,13 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
         QA_CK(cudaMemcpyAsync(d_bslot, slot.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_slot, slot.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_rin, rin.data(), sizeof(int) * rin.size(), cudaMemcpyHostToDevice, ctx->stream));
-        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 5, ctx->stream));
         QA_CK(cudaStreamSynchronize(ctx->stream));
     }
     RingPlan pl;
-    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0));
+    // classical parallel tempering keeps its ascending order (parallel_tempering.cpp:36-122)
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0,
+                      !classical && ctx->update_order == QA_ORDER_REFERENCE));
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
@@ -2459,7 +2495,7 @@ int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_probl
     QA_TRY(ws_array(ctx, W_EXACT, nr, &d_exact));
     QA_TRY(ws_array(ctx, W_AVG, (size_t)reads_total * S, &d_avg));
     QA_TRY(ws_array(ctx, W_SWP, (size_t)reads_total * S, &d_swp));
-    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    QA_TRY(ws_array(ctx, W_CNT, 5, &d_cnt));
     auto upload_tables = [&]() -> int {
         QA_CK(cudaMemcpyAsync(d_B, Bt.data(), sizeof(float) * tab, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_T4, T4t.data(), sizeof(float) * tab, cudaMemcpyHostToDevice, ctx->stream));
@@ -2490,11 +2526,11 @@ int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_probl
         QA_CK(cudaMemcpyAsync(d_bslot, slot.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_slot, slot.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_rin, rin.data(), sizeof(int) * rin.size(), cudaMemcpyHostToDevice, ctx->stream));
-        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 5, ctx->stream));
         QA_CK(cudaStreamSynchronize(ctx->stream));
     }
     RingPlan pl;
-    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, cls > 0));
+    QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, cls > 0, ctx->update_order == QA_ORDER_REFERENCE));
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
                       !pl.own_fields()));
@@ -2871,7 +2907,7 @@ static int chi_stage1(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
     QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
     QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
-    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    QA_TRY(ws_array(ctx, W_CNT, 5, &d_cnt));
     QA_TRY(ws_array(ctx, W_MAG, (size_t)nr * sweeps_total, &d_mag));
     QA_TRY(ws_array(ctx, W_PROBOF, (size_t)reads_total * Pts, &d_nof));
     QA_TRY(ws_array(ctx, W_EXACT, (size_t)reads_total * Pts, &d_chi));
@@ -2883,7 +2919,7 @@ static int chi_stage1(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * Pts, cudaMemcpyHostToDevice, ctx->stream));
     QA_CK(cudaMemcpyAsync(d_nof, nof.data(), sizeof(int) * nof.size(), cudaMemcpyHostToDevice, ctx->stream));
     QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
-    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+    QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 5, ctx->stream));
     h2d += (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * Pts +
                      sizeof(int) * nof.size() + sizeof(double) * nr);
     RingPlan pl;
@@ -2902,7 +2938,7 @@ static int chi_stage1(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
                                                                      prm->scan_burn, d_nof, P, d_chi);
     QA_CK(cudaGetLastError());
     launches += (pl.own_fields() ? 1 : 2) + 2;
-    unsigned long long c[4];
+    unsigned long long c[5];
     QA_CK(cudaMemcpyAsync(chi.data(), d_chi, sizeof(double) * chi.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
@@ -3061,7 +3097,7 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     QA_TRY(ws_array(ctx, W_BESTE, nr, &d_best));
     QA_TRY(ws_array(ctx, W_BESTSTEP, nr, &d_bstep));
     QA_TRY(ws_array(ctx, W_BITS, (size_t)nr * L.nw_max, &d_bits));
-    QA_TRY(ws_array(ctx, W_CNT, 4, &d_cnt));
+    QA_TRY(ws_array(ctx, W_CNT, 5, &d_cnt));
     QA_TRY(ws_array(ctx, W_EXACT, nr, &d_exact));
     {
         std::vector<double> inf(nr, INFINITY);
@@ -3070,7 +3106,7 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
         QA_CK(cudaMemcpyAsync(d_T4, T4.data(), sizeof(float) * T4.size(), cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_best, inf.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, ctx->stream));
         QA_CK(cudaMemcpyAsync(d_bstep, neg.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, ctx->stream));
-        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, ctx->stream));
+        QA_CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 5, ctx->stream));
         QA_CK(cudaStreamSynchronize(ctx->stream));
         h2d += (int64_t)(sizeof(ProbDev) * n_problems + sizeof(RingDev) * nr + 2 * sizeof(float) * B.size() +
                          (sizeof(double) + sizeof(int)) * nr);
@@ -3106,7 +3142,7 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     std::vector<double> sums((size_t)nr * steps), bestE(nr), exact(nr);
     std::vector<int> bstep(nr);
     std::vector<uint32_t> bits((size_t)nr * L.nw_max);
-    unsigned long long cnt[4];
+    unsigned long long cnt[5];
     QA_CK(cudaMemcpyAsync(sums.data(), d_sum, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bestE.data(), d_best, sizeof(double) * nr, cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(bstep.data(), d_bstep, sizeof(int) * nr, cudaMemcpyDeviceToHost, ctx->stream));
@@ -3114,6 +3150,7 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     QA_CK(cudaMemcpyAsync(bits.data(), d_bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaStreamSynchronize(ctx->stream));
+    QA_TRY(check_device_error(cnt));
     d2h += (int64_t)(sizeof(double) * (sums.size() + 2 * nr) + sizeof(int) * nr + sizeof(uint32_t) * bits.size() +
                      sizeof(cnt));
     for (int i = 0; i < 4; ++i) cnt_total[i] += cnt[i];

@@ -24,7 +24,7 @@ constexpr unsigned FULL = 0xffffffffu;
 enum Dom : uint32_t {
     DOM_INIT = 1, DOM_SA = 2, DOM_SLICE = 3, DOM_WORLD = 4, DOM_SWAP = 5,
     DOM_PILOT_INIT = 6, DOM_PILOT = 7, DOM_PROD_INIT = 8, DOM_PROD = 9, DOM_CSPIN = 10, DOM_CBOND = 11,
-    DOM_OPTCAL = 12
+    DOM_OPTCAL = 12, DOM_PERM = 13
 };
 
 enum Kind : int { K_DENSE = 0, K_SPARSE = 1, K_HUBO = 2 };

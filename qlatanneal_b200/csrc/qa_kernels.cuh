@@ -20,6 +20,7 @@
 // at a cost of (accepted flips + 1) ballots per block.
 #pragma once
 #include "qa_device.cuh"
+#include "qa_order.cuh"
 
 namespace qa {
 
@@ -54,6 +55,8 @@ struct RingParams {
     int per_slot_sched;   // 1: index B/T4/JP by slot (+ step * slot_step) instead of step
     int slot_step;        //   0: one entry per slot; R: a row of R slots per step (one J_perp per step)
     int smem_fields;
+    int ref_order;        // 1: qanneal's order (a random spin order per sweep, slices in turn); 0: parity
+                          //    checkerboard, spins ascending (the SQA-Chi kernel's order)
     int init_fields;      // ring_pm1_kernel: build the int32 fields from the spins first
     int init_scan;        // score the starting state as "step -1" before step0 (PT)
     int rec_base;         // per-step records live at [ring][rec_base + step]
@@ -69,7 +72,7 @@ struct RingParams {
     uint32_t *final_bits; // [ring][nw_max] min-energy slice after the last step, may be null
     int nw_max;
     int *mag;             // [ring][sweeps] spin sums after each sweep (chi pilot), may be null
-    unsigned long long *counters;  // [4]
+    unsigned long long *counters;  // [5]: slice attempts, accepts, worldline attempts, accepts, error word
     // sweep traces (observers; ring_kernel only), or null.  After every sweep
     // whose index in its phase is a multiple of tr_stride: the ring's bits and
     // slice energies at record [ring][step][tr_rps] (records of a step: slice,
@@ -190,6 +193,59 @@ __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int 
             ++acc;
             pending = j == 31 ? 0u : (FULL << (j + 1));
         }
+    }
+}
+
+// Slice t of a ring in qanneal's order: visiting position p holds spin
+// ord[p]; the uniform belongs to the position.  Block q (positions
+// 32q .. 32q+31) waits until slice t - 1 has finished it (pipeline counters
+// prog) and publishes its own progress after.  The Trotter neighbours' bits
+// of the block's spins are final for this sweep in slice t - 1 and untouched
+// in slice t + 1 while slice t holds the block.
+template <int KIND>
+__device__ __forceinline__ void sweep_slice_ord(const ProbDev &Pd, uint32_t *S, int NP, int t, float *gt,
+                                                const float *h, const int *ord, int *prog, int *abortf,
+                                                unsigned long long *err, float B, float T4, uint64_t key,
+                                                uint32_t rng_cell, uint32_t sigma, uint32_t tag, int lane,
+                                                unsigned long long &att, unsigned long long &acc) {
+    const int n = Pd.n, nw = Pd.nw;
+    uint32_t *St = S + t * nw;
+    const int prev = t == 0 ? NP - 1 : t - 1;
+    const int next = t + 1 == NP ? 0 : t + 1;
+    const uint32_t *Sp = S + prev * nw;
+    const uint32_t *Sn = S + next * nw;
+    U4 rnd = {0, 0, 0, 0};
+    att += (unsigned long long)n;
+    for (int q = 0; q < nw; ++q) {
+        if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), rng_cell, sigma, tag, key);
+        if (t > 0) wait_at_least(prog + t - 1, q + 1, abortf, err, lane);
+        const int pos = (q << 5) | lane;
+        const bool valid = pos < n;
+        const int i = valid ? ord[pos] : 0;
+        const int si = spin_of(St, i);
+        const int qv = si * (spin_of(Sp, i) + spin_of(Sn, i));
+        const float tro = qv == 0 ? 0.0f : (qv > 0 ? T4 : -T4);
+        const float u = u24(pick(rnd, q & 3));
+        const float hi = valid ? h[i] : 0.0f;
+        uint32_t pending = FULL;
+        for (;;) {
+            const float gi = valid ? gt[i] : 0.0f;
+            const float loc = __fadd_rn(hi, gi);
+            const float x = si > 0 ? loc : -loc;
+            const bool ok = valid & metropolis_nb24(__fsub_rn(__fmul_rn(x, B), tro), u);
+            const uint32_t m = __ballot_sync(FULL, ok) & pending;
+            if (!m) break;
+            const int j = __ffs(m) - 1;
+            const int jj = __shfl_sync(FULL, i, j);
+            const int so = __shfl_sync(FULL, si, j);
+            if (lane == 0) St[jj >> 5] ^= 1u << (jj & 31);
+            __syncwarp();
+            apply_flip<KIND>(Pd, gt, St, jj, so, lane);
+            __syncwarp();
+            ++acc;
+            pending = j == 31 ? 0u : (FULL << (j + 1));
+        }
+        publish_count(prog + t, q + 1, lane);
     }
 }
 
@@ -323,6 +379,10 @@ struct RingSmem {
     double *wl_G;
     int *flag;
     float *g;
+    // qanneal's order: keys and bucket counters of the order build, the
+    // visiting order, the slices' progress counters, the wait-abort flag
+    unsigned long long *okeys;
+    int *ocnt, *ord, *prog, *abortf;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -356,7 +416,11 @@ __device__ __forceinline__ void record_bond_sample(const RingParams &p, const ui
         p.bsamp[(long long)blockIdx.x * p.bstride + (long long)(step - p.step0) * (p.spb + p.cls) + j] = tb;
 }
 
-__host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fields) {
+__host__ __device__ inline size_t ring_order_bytes(int P, int n) {
+    return order_keys_bytes(n) + order_cnt_bytes(n) + order_idx_bytes(n) + align_up((size_t)P * 4, 16) + 16;
+}
+
+__host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fields, bool ref_order = false) {
     const int nw = (n + 31) / 32;
     size_t b = align_up((size_t)P * nw * 4, 16);
     b += align_up((size_t)n * 4, 16);
@@ -364,6 +428,7 @@ __host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fiel
     b += align_up((size_t)W * 32 * 4, 16);
     b += align_up((size_t)W * 32 * 8, 16);
     b += 16;
+    if (ref_order) b += ring_order_bytes(P, n);
     if (fields) b += (size_t)P * n * 4;
     return b;
 }
@@ -481,6 +546,14 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     sm.wl_sh = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)W * 32 * 4, 16);
     sm.wl_G = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)W * 32 * 8, 16);
     sm.flag = reinterpret_cast<int *>(ptr); ptr += 16;
+    if (p.ref_order) {
+        sm.okeys = reinterpret_cast<unsigned long long *>(ptr); ptr += order_keys_bytes(n);
+        sm.ocnt = reinterpret_cast<int *>(ptr); ptr += order_cnt_bytes(n);
+        sm.ord = reinterpret_cast<int *>(ptr); ptr += order_idx_bytes(n);
+        sm.prog = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)NP * 4, 16);
+        sm.abortf = reinterpret_cast<int *>(ptr); ptr += 16;
+        if (threadIdx.x == 0) *sm.abortf = 0;
+    }
     float *gbase = p.smem_fields ? reinterpret_cast<float *>(ptr) : p.fields + R.field_off;
 
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) sm.S[idx] = p.spins[R.spin_off + idx];
@@ -515,15 +588,26 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
         const float B = p.B[si_tab], T4 = p.T4[si_tab];
         for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
-            for (int ph = 0; ph < 3; ++ph) {
-                const int cnt = phase_count(NP, ph);
-                for (int c = warp; c < cnt; c += W) {
-                    const int t = phase_slice(NP, ph, c);
-                    sweep_slice<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, B, T4, R.key,
-                                      (uint32_t)(slot * NP + t), sigma, p.slice_tag | R.tag_extra, lane, att_s,
-                                      acc_s);
+            if (p.ref_order) {
+                const uint32_t tag = p.slice_tag | R.tag_extra;
+                for (int t = threadIdx.x; t < NP; t += blockDim.x) sm.prog[t] = 0;
+                build_sweep_order(R.key, (uint32_t)slot, sigma, tag, n, sm.okeys, sm.ocnt, sm.ord);
+                for (int t = warp; t < NP; t += W)
+                    sweep_slice_ord<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, sm.ord, sm.prog,
+                                          sm.abortf, p.counters + 4, B, T4, R.key, (uint32_t)(slot * NP + t), sigma,
+                                          tag, lane, att_s, acc_s);
+                __syncthreads();
+            } else {
+                for (int ph = 0; ph < 3; ++ph) {
+                    const int cnt = phase_count(NP, ph);
+                    for (int c = warp; c < cnt; c += W) {
+                        const int t = phase_slice(NP, ph, c);
+                        sweep_slice<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, B, T4, R.key,
+                                          (uint32_t)(slot * NP + t), sigma, p.slice_tag | R.tag_extra, lane, att_s,
+                                          acc_s);
+                    }
+                    if (cnt) __syncthreads();
                 }
-                if (cnt) __syncthreads();
             }
             if (p.mag) {
                 long long ps = 0;
@@ -541,14 +625,17 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
             if (p.bsamp) record_bond_sample(p, sm.S, NP, nw, n, sm.wl_sh, W, step, sw);
             if (p.tr_bits && sw % p.tr_stride == 0) trace_rec(step, sw / p.tr_stride);
         }
-        // cluster sweeps: one warp, spins in order
+        // cluster sweeps: one warp, spins in the sweep's visiting order
+        // (qanneal's order) or ascending
         const int cls = step >= 0 ? p.cls : 0;
         for (int sw = 0; sw < cls; ++sw) {
+            const uint32_t sigma = (uint32_t)(step * p.cls + sw);
+            if (p.ref_order) build_sweep_order(R.key, (uint32_t)slot, sigma, DOM_CSPIN, n, sm.okeys, sm.ocnt, sm.ord);
             if (warp == 0) {
-                const uint32_t sigma = (uint32_t)(step * p.cls + sw);
                 const float JPv = p.JP[si_tab];
-                for (int i = 0; i < n; ++i)
-                    cluster_move<KIND>(Pd, sm.S, gbase, sm.h, NP, i, (uint32_t)slot, sigma, B, T4, JPv, R.key, lane);
+                for (int pos = 0; pos < n; ++pos)
+                    cluster_move<KIND>(Pd, sm.S, gbase, sm.h, NP, p.ref_order ? sm.ord[pos] : pos, (uint32_t)slot,
+                                       sigma, B, T4, JPv, R.key, lane);
             }
             __syncthreads();
             if (p.bsamp) record_bond_sample(p, sm.S, NP, nw, n, sm.wl_sh, W, step, p.spb + sw);
@@ -556,12 +643,16 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
         }
         for (int sw = 0; sw < wls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
+            // visiting position (q << 5) | lane holds spin ord[position]
+            // (qanneal's order) or spin position (ascending)
+            if (p.ref_order) build_sweep_order(R.key, (uint32_t)slot, sigma, DOM_WORLD, n, sm.okeys, sm.ocnt, sm.ord);
             U4 rnd = {0, 0, 0, 0};
             for (int q = 0; q < nw; ++q) {
                 if ((q & 3) == 0)
                     rnd = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
-                const int i = (q << 5) | lane;
-                const bool valid = i < n;
+                const int pos = (q << 5) | lane;
+                const bool valid = pos < n;
+                const int i = !valid ? 0 : (p.ref_order ? sm.ord[pos] : pos);
                 const float u = u24(pick(rnd, q & 3));
                 const float hi = valid ? sm.h[i] : 0.0f;
                 if (threadIdx.x == 0) att_w += (unsigned long long)min(32, n - (q << 5));
@@ -591,12 +682,12 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
                     const uint32_t m = __ballot_sync(FULL, ok) & pending;
                     if (!m) break;
                     const int j = __ffs(m) - 1;
-                    const int jj = (q << 5) | j;
+                    const int jj = __shfl_sync(FULL, i, j);
                     for (int t = warp; t < NP; t += W) {
                         uint32_t *St = sm.S + t * nw;
                         const int so = spin_of(St, jj);
                         __syncwarp();
-                        if (lane == 0) St[q] = St[q] ^ (1u << j);
+                        if (lane == 0) St[jj >> 5] = St[jj >> 5] ^ (1u << (jj & 31));
                         __syncwarp();
                         apply_flip<KIND>(Pd, gbase + (long long)t * n, St, jj, so, lane);
                     }

@@ -27,8 +27,12 @@ namespace qa {
 __host__ __device__ inline int pm1_npad(int n) { return (n + 127) / 128 * 128; }
 
 // Shared memory of one ring: gbytes = bytes per field (4: int32, 2: int16);
-// jw_smem = J bits staged in shared memory (else read through L1/L2).
-__host__ __device__ inline size_t pm1_smem_bytes(int P, int n, int gbytes = 4, bool jw_smem = true) {
+// jw_smem = J bits staged in shared memory (else read through L1/L2);
+// ref_order = qanneal's update order (the visiting order of a sweep, its
+// bucket counters, the slices' progress counters and the flipped spins of a
+// worldline block; the order's keys reuse the worldline sums and uniforms).
+__host__ __device__ inline size_t pm1_smem_bytes(int P, int n, int gbytes = 4, bool jw_smem = true,
+                                                 bool ref_order = false) {
     const int nw = (n + 31) / 32, np = pm1_npad(n);
     size_t b = jw_smem ? (size_t)nw * np * 4 : 0;  // Jw
     b += align_up((size_t)P * nw * 4, 16);         // S
@@ -40,6 +44,8 @@ __host__ __device__ inline size_t pm1_smem_bytes(int P, int n, int gbytes = 4, b
     b += align_up((size_t)P * 8, 16);              // cellE
     b += (size_t)(np / 32) * 4;                    // worldline move masks, one per block (np/32 >= nw)
     b += 32 * 8 + 32 * 4 + 64;                     // old worldlines, partials, flags
+    if (ref_order)
+        b += order_idx_bytes(np) + order_cnt_bytes(n) + ord_align16((size_t)P * 4) + 16 + 32 * 4;
     return b + 64;
 }
 
@@ -151,6 +157,80 @@ __device__ __forceinline__ void pm1_block(const uint32_t *Jw, uint32_t *St, cons
     __syncwarp();
 }
 
+// Flip the spins of mask F (lanes; spin sp of each lane) in slice t's spin
+// words St and update its fields: one block update per 32-spin word holding
+// flipped spins (spins in one word share a popcount pass).  Whole warp.
+template <typename GT>
+__device__ __forceinline__ void pm1_flip_spins(uint32_t *St, GT *Gt, const uint32_t *Jw, int npad, int n, uint32_t F,
+                                               int sp, int lane) {
+    uint32_t rest = F;
+    while (rest) {
+        const int wq = __shfl_sync(FULL, sp, __ffs(rest) - 1) >> 5;
+        const bool in = ((rest >> lane) & 1u) && (sp >> 5) == wq;
+        const uint32_t lanes = __ballot_sync(FULL, in);
+        const uint32_t Fq = __reduce_or_sync(FULL, in ? (1u << (sp & 31)) : 0u);
+        const uint32_t sold = St[wq];
+        __syncwarp();
+        if (lane == 0) St[wq] = sold ^ Fq;
+        pm1_block_update(Gt, Jw, npad, n, wq, Fq, sold, lane);
+        rest &= ~lanes;
+    }
+    __syncwarp();
+}
+
+// One block of 32 visiting positions of slice t in qanneal's order: lane =
+// position (q << 5) | lane, spin ord[position]; rw is the position's Philox
+// word.  The spin's own and Trotter neighbours' bits (slices tp, tn) come
+// from its worldline word: while slice t holds the block no other slice
+// touches these spins (the pipeline), so slice tp shows this sweep's state and
+// slice tn the last sweep's.  Flips are resolved in position order.
+template <typename GT>
+__device__ __forceinline__ void pm1_block_ord(const uint32_t *Jw, uint32_t *St, GT *Gt, unsigned long long *Wc,
+                                              const float *h, const int *ord, int n, int npad, int q, int t, int tp,
+                                              int tn, uint32_t rw, float B, float T4, int lane,
+                                              unsigned long long &acc) {
+    const int pos = (q << 5) | lane;
+    const bool valid = pos < n;
+    const int i = valid ? ord[pos] : 0;
+    const unsigned long long wc = Wc[i];
+    const uint32_t sbit = (uint32_t)(wc >> t) & 1u;
+    const int d = (int)(((uint32_t)(wc >> tp) & 1u) ^ sbit) + (int)(((uint32_t)(wc >> tn) & 1u) ^ sbit);
+    const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
+    const float u = u24(rw);
+    const float hi = h[i];
+    const int gi = (int)Gt[i];
+    const float y = __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gi)), sbit), B), tro);
+    if (!__any_sync(FULL, valid & metropolis_maybe24(y, u))) return;
+    bool ok = valid & metropolis_nb24(y, u);
+    uint32_t m = __ballot_sync(FULL, ok);
+    if (m == 0) return;
+    // gk: this lane's field with the block's earlier flips applied,
+    // g_i += -2 J_i,j s_j(old) for each flipped spin j
+    uint32_t F = 0;
+    int gk = gi;
+    do {
+        const int j = __ffs(m) - 1;
+        F |= 1u << j;
+        const int ij = __shfl_sync(FULL, i, j);
+        const uint32_t sj = __shfl_sync(FULL, sbit, j);
+        if (lane != j) gk += ((((Jw[(ij >> 5) * npad + i] >> (ij & 31)) & 1u) ^ sj) != 0u) ? 2 : -2;
+        const uint32_t pending = j == 31 ? 0u : (FULL << (j + 1));
+        ok = valid & metropolis_nb24(
+            __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gk)), sbit), B), tro), u);
+        m = __ballot_sync(FULL, ok) & pending;
+        ++acc;
+    } while (m);
+    // bit t of each flipped spin's worldline (32-bit atomic on the half that holds it)
+    if ((F >> lane) & 1u) atomicXor(reinterpret_cast<uint32_t *>(Wc + i) + (t >> 5), 1u << (t & 31));
+    pm1_flip_spins(St, Gt, Jw, npad, n, F, i, lane);
+}
+
+// y = -dE of a worldline move of spin i with slice sum gs (B = 2 beta/P).
+__device__ __forceinline__ float pm1_world_y(float hi, unsigned long long wi, int gs, int NP, float B) {
+    const int sh = 2 * __popcll(wi) - NP;
+    return __fmul_rn(__double2float_rn(__dadd_rn(__dmul_rn((double)hi, (double)sh), (double)gs)), B);
+}
+
 // One warp sweeps slice t; one Philox call per lane serves four blocks.
 template <typename GT>
 __device__ __forceinline__ void pm1_sweep_slice(const uint32_t *Jw, uint32_t *S, GT *G, unsigned long long *Wc,
@@ -215,7 +295,21 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     uint32_t *mask = reinterpret_cast<uint32_t *>(ptr); ptr += (size_t)(npad / 32) * 4;
     unsigned long long *Wold = reinterpret_cast<unsigned long long *>(ptr); ptr += 32 * 8;
     int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
-    int *flag = reinterpret_cast<int *>(ptr);  // [1]: worldline block flips F, [2]: their block index
+    int *flag = reinterpret_cast<int *>(ptr); ptr += 64;  // [1]: worldline block flips F, [2]: their block index
+    // qanneal's order: the visiting order of the current sweep, its bucket
+    // counters, the slices' progress counters, the wait-abort flag and the
+    // spins of a resolved worldline block; the order's keys use Gs and uw
+    // (8 npad bytes, free while the order is built)
+    int *ord = nullptr, *ocnt = nullptr, *prog = nullptr, *abortf = nullptr, *Wsp = nullptr;
+    unsigned long long *okeys = reinterpret_cast<unsigned long long *>(Gs);
+    if (p.ref_order) {
+        ord = reinterpret_cast<int *>(ptr); ptr += order_idx_bytes(npad);
+        ocnt = reinterpret_cast<int *>(ptr); ptr += order_cnt_bytes(n);
+        prog = reinterpret_cast<int *>(ptr); ptr += ord_align16((size_t)NP * 4);
+        abortf = reinterpret_cast<int *>(ptr); ptr += 16;
+        Wsp = reinterpret_cast<int *>(ptr);
+        if (threadIdx.x == 0) *abortf = 0;
+    }
 
     if (JW_SMEM)
         for (int idx = threadIdx.x; idx < nw * npad; idx += blockDim.x) Jw_s[idx] = Pd.Jw[idx];
@@ -261,14 +355,44 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
         const float B = p.B[si_tab], T4 = p.T4[si_tab];
         for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
-            for (int ph = 0; ph < 3; ++ph) {
-                const int cnt = phase_count(NP, ph);
-                for (int c = warp; c < cnt; c += W) {
-                    const int t = phase_slice(NP, ph, c);
-                    pm1_sweep_slice(Jw, S, G, Wc, h, n, nw, npad, NP, t, B, T4, R.key, (uint32_t)(slot * NP + t),
-                                    sigma, p.slice_tag | R.tag_extra, lane, att_s, acc_s);
+            if (p.ref_order) {
+                // one visiting order for the sweep; slices in turn, pipelined:
+                // slice t takes block q once slice t - 1 has finished it
+                const uint32_t tag = p.slice_tag | R.tag_extra;
+                for (int t = threadIdx.x; t < NP; t += blockDim.x) prog[t] = 0;
+                build_sweep_order(R.key, (uint32_t)slot, sigma, tag, n, okeys, ocnt, ord);
+                for (int t = warp; t < NP; t += W) {
+                    const int tp = t == 0 ? NP - 1 : t - 1, tn = t + 1 == NP ? 0 : t + 1;
+                    uint32_t *St = S + t * nw;
+                    GT *Gt = G + t * npad;
+                    const uint32_t rng_cell = (uint32_t)(slot * NP + t);
+                    att_s += (unsigned long long)n;
+                    for (int q4 = 0; q4 < nw; q4 += 4) {
+                        const U4 r = philox((uint32_t)(((q4 >> 2) << 5) | lane), rng_cell, sigma, tag, R.key);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int q = q4 + k;
+                            if (q < nw) {
+                                if (t > 0) wait_at_least(prog + t - 1, q + 1, abortf, p.counters + 4, lane);
+                                pm1_block_ord(Jw, St, Gt, Wc, h, ord, n, npad, q, t, tp, tn, pick(r, k), B, T4, lane,
+                                              acc_s);
+                                publish_count(prog + t, q + 1, lane);
+                            }
+                        }
+                    }
                 }
-                if (cnt) __syncthreads();
+                __syncthreads();
+            } else {
+                for (int ph = 0; ph < 3; ++ph) {
+                    const int cnt = phase_count(NP, ph);
+                    for (int c = warp; c < cnt; c += W) {
+                        const int t = phase_slice(NP, ph, c);
+                        pm1_sweep_slice(Jw, S, G, Wc, h, n, nw, npad, NP, t, B, T4, R.key,
+                                        (uint32_t)(slot * NP + t), sigma, p.slice_tag | R.tag_extra, lane, att_s,
+                                        acc_s);
+                    }
+                    if (cnt) __syncthreads();
+                }
             }
             if (p.mag) {
                 int ps = 0;
@@ -285,7 +409,98 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
             }
             if (p.bsamp) record_bond_sample(p, S, NP, nw, n, wpart, W, step, sw);
         }
-        for (int sw = 0; sw < wls; ++sw) {
+        for (int sw = 0; sw < wls && p.ref_order; ++sw) {
+            // qanneal's order: a fresh visiting order; slice sums by spin,
+            // uniforms by visiting position
+            const uint32_t sigma = (uint32_t)(step * p.wls + sw);
+            build_sweep_order(R.key, (uint32_t)slot, sigma, DOM_WORLD, n, okeys, ocnt, ord);
+            for (int i = threadIdx.x; i < npad; i += blockDim.x) {
+                const int q = i >> 5;
+                int gs = 0;
+                if (i < n)
+                    for (int t = 0; t < NP; ++t) {
+                        const int g = (int)G[t * npad + i];
+                        gs += ((S[t * nw + q] >> lane) & 1u) ? g : -g;
+                    }
+                Gs[i] = gs;
+                if ((q & 3) == 0) {  // positions q*32 + lane .. + 96: one Philox call
+                    const U4 r = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
+                    uw[i] = u24(r.x);
+                    uw[i + 32] = u24(r.y);
+                    uw[i + 64] = u24(r.z);
+                    uw[i + 96] = u24(r.w);
+                }
+            }
+            if (threadIdx.x == 0) att_w += (unsigned long long)n;
+            __syncthreads();
+            int q0 = 0;
+            for (;;) {
+                // decisions of every later position on the current worldlines
+                for (int pp = threadIdx.x + q0 * 32; pp < npad; pp += blockDim.x) {
+                    const bool valid = pp < n;
+                    const int i = valid ? ord[pp] : 0;
+                    const float y = pm1_world_y(h[i], Wc[i], Gs[i], NP, B);
+                    const float u = uw[pp];
+                    uint32_t m = 0u;
+                    if (__any_sync(FULL, valid & metropolis_maybe24(y, u)))
+                        m = __ballot_sync(FULL, valid & metropolis_nb24(y, u));
+                    if (lane == 0) mask[pp >> 5] = m;
+                }
+                __syncthreads();
+                int qs = -1;
+                for (int q = q0; q < nw; ++q)
+                    if (mask[q]) { qs = q; break; }
+                if (qs < 0) break;
+                if (warp == 0) {
+                    // resolve block qs in position order; sums of the block's
+                    // later spins corrected by -2 J_ij (P - 2 popc(W_i ^ W_j))
+                    const int pos = (qs << 5) | lane;
+                    const bool valid = pos < n;
+                    const int i = valid ? ord[pos] : 0;
+                    const unsigned long long wi = Wc[i];
+                    const float hi = h[i], u = uw[pos];
+                    int gk = Gs[i];
+                    uint32_t m = mask[qs], F = 0;
+                    do {
+                        const int j = __ffs(m) - 1;
+                        F |= 1u << j;
+                        const int ij = __shfl_sync(FULL, i, j);
+                        const unsigned long long wj = __shfl_sync(FULL, wi, j);
+                        const int overlap = NP - 2 * __popcll(wi ^ wj);  // sum_t s_t,i s_t,j
+                        if (lane != j)
+                            gk += ((Jw[(ij >> 5) * npad + i] >> (ij & 31)) & 1u) ? -2 * overlap : 2 * overlap;
+                        const uint32_t pending = j == 31 ? 0u : (FULL << (j + 1));
+                        m = __ballot_sync(FULL, valid & metropolis_nb24(pm1_world_y(hi, wi, gk, NP, B), u)) & pending;
+                    } while (m);
+                    Wold[lane] = wi;
+                    Wsp[lane] = i;
+                    if (lane == 0) { flag[1] = (int)F; flag[2] = qs; }
+                }
+                __syncthreads();
+                const uint32_t F = (uint32_t)flag[1];
+                // later positions: exact correction of their spins' slice sums
+                for (int pp = threadIdx.x + (qs + 1) * 32; pp < n; pp += blockDim.x) {
+                    const int i = ord[pp];
+                    const unsigned long long wi = Wc[i];
+                    int dg = 0;
+                    for (uint32_t f = F; f; f &= f - 1) {
+                        const int j = __ffs(f) - 1, sj = Wsp[j];
+                        const int overlap = NP - 2 * __popcll(wi ^ Wold[j]);
+                        dg += ((Jw[(sj >> 5) * npad + i] >> (sj & 31)) & 1u) ? -2 * overlap : 2 * overlap;
+                    }
+                    Gs[i] += dg;
+                }
+                // every slice: flip the block's flipped spins and update its fields
+                const int spl = Wsp[lane];
+                for (int t = warp; t < NP; t += W) pm1_flip_spins(S + t * nw, G + t * npad, Jw, npad, n, F, spl, lane);
+                if (warp == 0 && ((F >> lane) & 1u)) Wc[spl] = Wold[lane] ^ pmask;
+                if (threadIdx.x == 0) acc_w += (unsigned long long)__popc(F);
+                __syncthreads();
+                q0 = qs + 1;
+                if (q0 >= nw) break;
+            }
+        }
+        for (int sw = 0; sw < wls && !p.ref_order; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
             // slice sums and uniforms of every spin (thread per spin; a warp
             // holds one 32-spin block, so lane == spin & 31)

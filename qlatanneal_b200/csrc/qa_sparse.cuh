@@ -16,15 +16,17 @@
 
 namespace qa {
 
-__host__ __device__ inline size_t sparse_smem_bytes(int P, int n) {
+__host__ __device__ inline size_t sparse_smem_bytes(int P, int n, bool ref_order = false) {
     const int nw = (n + 31) / 32, n32 = nw * 32;
     size_t b = align_up((size_t)P * nw * 4, 16);  // S
     b += (size_t)n32 * 8;                          // W (worldline bits)
     b += (size_t)n32 * 4;                          // h
     b += align_up((size_t)P * 8, 16);              // cellE
-    b += (size_t)n32 * 4;                          // worldline uniforms
-    b += align_up((size_t)nw * 8, 16);             // worldline decisions and marks per block
+    b += (size_t)n32 * (ref_order ? 8 : 4);        // worldline uniforms (qanneal's order: and the order's keys)
+    b += align_up((size_t)nw * 8, 16);             // worldline decisions per block, marks per spin
     b += 32 * 4 + 64;                              // partials, flags
+    if (ref_order)                                 // the visiting order, bucket and progress counters, abort flag
+        b += order_idx_bytes(n32) + order_cnt_bytes(n) + align_up((size_t)P * 4, 16) + 16;
     return b + 64;
 }
 
@@ -118,6 +120,56 @@ __device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, u
     }
 }
 
+// Slice t in qanneal's order (the pipelined form of sp_sweep_slice; see
+// sweep_slice_ord): visiting position p holds spin ord[p], the Trotter
+// neighbours' bits come from the worldline words.  After a flip every later
+// lane of the block decides again on the current bits.
+__device__ __forceinline__ void sp_sweep_slice_ord(const ProbDev &Pd, uint32_t *S, unsigned long long *Wc,
+                                                   const float *h, const int *ord, int *prog, int *abortf,
+                                                   unsigned long long *err, int NP, int t, float B, float T4,
+                                                   uint64_t key, uint32_t rng_cell, uint32_t sigma, uint32_t tag,
+                                                   int lane, unsigned long long &att, unsigned long long &acc) {
+    const int n = Pd.n, nw = Pd.nw;
+    uint32_t *St = S + t * nw;
+    const int tp = t == 0 ? NP - 1 : t - 1, tn = t + 1 == NP ? 0 : t + 1;
+    U4 rnd = {0, 0, 0, 0};
+    att += (unsigned long long)n;
+    for (int q = 0; q < nw; ++q) {
+        if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), rng_cell, sigma, tag, key);
+        if (t > 0) wait_at_least(prog + t - 1, q + 1, abortf, err, lane);
+        const int pos = (q << 5) | lane;
+        const bool valid = pos < n;
+        const int i = valid ? ord[pos] : 0;
+        const unsigned long long wc = Wc[i];
+        const uint32_t sbit = (uint32_t)(wc >> t) & 1u;
+        const int d = (int)(((uint32_t)(wc >> tp) & 1u) ^ sbit) + (int)(((uint32_t)(wc >> tn) & 1u) ^ sbit);
+        const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
+        const float u = u24(pick(rnd, q & 3));
+        const float hi = h[i];
+        auto decide = [&]() {
+            const int g = valid ? sp_field(Pd.spcv, Pd.rowptr, St, i) : 0;
+            const float loc = __fadd_rn(hi, __int2float_rn(g));
+            return valid & metropolis_nb24(__fsub_rn(__fmul_rn(signed_by_bit(loc, sbit), B), tro), u);
+        };
+        uint32_t m = __ballot_sync(FULL, decide());
+        uint32_t pending = FULL;
+        while (m & pending) {
+            const int j = __ffs(m & pending) - 1;
+            const int jj = __shfl_sync(FULL, i, j);
+            if (lane == 0) St[jj >> 5] ^= 1u << (jj & 31);
+            // bit t of the worldline, as a 32-bit atomic on the half that holds it (little-endian)
+            if (lane == j) atomicXor(reinterpret_cast<uint32_t *>(Wc + i) + (t >> 5), 1u << (t & 31));
+            ++acc;
+            pending = j == 31 ? 0u : (FULL << (j + 1));
+            __syncwarp();
+            const bool again = ((pending >> lane) & 1u) && decide();
+            m = (m & ~pending) | (__ballot_sync(FULL, again) & pending);
+            __syncwarp();
+        }
+        publish_count(prog + t, q + 1, lane);
+    }
+}
+
 __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const RingDev R = p.rings[blockIdx.x];
@@ -129,12 +181,23 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
     unsigned long long *Wc = reinterpret_cast<unsigned long long *>(ptr); ptr += (size_t)n32 * 8;
     float *h = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * 4;
     double *cellE = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)NP * 8, 16);
-    float *uw = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * 4;
+    float *uw = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * (p.ref_order ? 8 : 4);
     uint32_t *wmask = reinterpret_cast<uint32_t *>(ptr);  // [nw] decisions on the sweep's starting state
     uint32_t *wdirty = wmask + nw;                        // [nw] spins whose neighbours have flipped since
     ptr += align_up((size_t)nw * 8, 16);
     int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
-    int *flag = reinterpret_cast<int *>(ptr);  // [0]: best slice, [3]: lowest slice (final state)
+    int *flag = reinterpret_cast<int *>(ptr); ptr += 64;  // [0]: best slice, [3]: lowest slice (final state)
+    // qanneal's order: the visiting order, its bucket counters, the slices'
+    // progress counters, the wait-abort flag; the order's keys use uw (8 n32 bytes)
+    unsigned long long *okeys = reinterpret_cast<unsigned long long *>(uw);
+    int *ord = nullptr, *ocnt = nullptr, *prog = nullptr, *abortf = nullptr;
+    if (p.ref_order) {
+        ord = reinterpret_cast<int *>(ptr); ptr += order_idx_bytes(n32);
+        ocnt = reinterpret_cast<int *>(ptr); ptr += order_cnt_bytes(n);
+        prog = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)NP * 4, 16);
+        abortf = reinterpret_cast<int *>(ptr);
+        if (threadIdx.x == 0) *abortf = 0;
+    }
 
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) S[idx] = p.spins[R.spin_off + idx];
     for (int i = threadIdx.x; i < n32; i += blockDim.x) h[i] = i < n ? Pd.h32[i] : 0.0f;
@@ -160,14 +223,24 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
         const float B = p.B[si_tab], T4 = p.T4[si_tab];
         for (int sw = 0; sw < spb; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
-            for (int ph = 0; ph < 3; ++ph) {
-                const int cnt = phase_count(NP, ph);
-                for (int c = warp; c < cnt; c += W) {
-                    const int t = phase_slice(NP, ph, c);
-                    sp_sweep_slice(Pd, S, Wc, h, NP, t, B, T4, R.key, (uint32_t)(slot * NP + t), sigma,
-                                   p.slice_tag | R.tag_extra, lane, att_s, acc_s);
+            if (p.ref_order) {
+                const uint32_t tag = p.slice_tag | R.tag_extra;
+                for (int t = threadIdx.x; t < NP; t += blockDim.x) prog[t] = 0;
+                build_sweep_order(R.key, (uint32_t)slot, sigma, tag, n, okeys, ocnt, ord);
+                for (int t = warp; t < NP; t += W)
+                    sp_sweep_slice_ord(Pd, S, Wc, h, ord, prog, abortf, p.counters + 4, NP, t, B, T4, R.key,
+                                       (uint32_t)(slot * NP + t), sigma, tag, lane, att_s, acc_s);
+                __syncthreads();
+            } else {
+                for (int ph = 0; ph < 3; ++ph) {
+                    const int cnt = phase_count(NP, ph);
+                    for (int c = warp; c < cnt; c += W) {
+                        const int t = phase_slice(NP, ph, c);
+                        sp_sweep_slice(Pd, S, Wc, h, NP, t, B, T4, R.key, (uint32_t)(slot * NP + t), sigma,
+                                       p.slice_tag | R.tag_extra, lane, att_s, acc_s);
+                    }
+                    if (cnt) __syncthreads();
                 }
-                if (cnt) __syncthreads();
             }
             if (p.mag) {
                 int ps = 0;
@@ -191,7 +264,67 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
         // unless a neighbour flipped earlier in the sweep: such spins are marked
         // and evaluated again when their turn comes.  Every decision is thus
         // taken on the state the one-spin-at-a-time sweep sees.
-        for (int sw = 0; sw < wls; ++sw) {
+        for (int sw = 0; sw < wls && p.ref_order; ++sw) {
+            // qanneal's order: the same scheme over visiting positions; the
+            // marks of flipped neighbours are kept per spin
+            const uint32_t sigma = (uint32_t)(step * p.wls + sw);
+            build_sweep_order(R.key, (uint32_t)slot, sigma, DOM_WORLD, n, okeys, ocnt, ord);
+            for (int pp = threadIdx.x; pp < n32; pp += blockDim.x) {  // a warp covers one block of positions
+                const int q = pp >> 5, l = pp & 31;
+                const U4 r = philox((uint32_t)(((q >> 2) << 5) | l), (uint32_t)slot, sigma, DOM_WORLD, R.key);
+                const float u = u24(pick(r, q & 3));
+                uw[pp] = u;
+                const bool valid = pp < n;
+                const int i = valid ? ord[pp] : 0;
+                const bool ok = valid && sp_world_ok(Pd, Wc, h, pmask, NP, i, B, u);
+                const uint32_t m = __ballot_sync(FULL, ok);
+                if (l == 0) {
+                    wmask[q] = m;
+                    wdirty[q] = 0u;
+                }
+            }
+            if (threadIdx.x == 0) att_w += (unsigned long long)n;
+            __syncthreads();
+            if (warp == 0) {
+                for (int q = 0; q < nw; ++q) {
+                    const int pos = (q << 5) | lane;
+                    const bool valid = pos < n;
+                    const int i = valid ? ord[pos] : 0;
+                    const float u = uw[pos];
+                    uint32_t m = wmask[q];
+                    const bool dirty0 = valid && ((wdirty[i >> 5] >> (i & 31)) & 1u);  // a neighbour flipped earlier
+                    const uint32_t dq = __ballot_sync(FULL, dirty0);
+                    if (dq) {
+                        const bool ok = dirty0 && sp_world_ok(Pd, Wc, h, pmask, NP, i, B, u);
+                        m = (m & ~dq) | (__ballot_sync(FULL, ok) & dq);
+                    }
+                    uint32_t pending = FULL;
+                    while (m & pending) {
+                        const int j = __ffs(m & pending) - 1;
+                        const int jj = __shfl_sync(FULL, i, j);
+                        for (int t = lane; t < NP; t += 32) S[t * nw + (jj >> 5)] ^= 1u << (jj & 31);
+                        if (lane == j) Wc[jj] ^= pmask;
+                        ++acc_w;
+                        pending = j == 31 ? 0u : (FULL << (j + 1));
+                        const int e0 = __ldg(Pd.rowptr + jj), e1 = __ldg(Pd.rowptr + jj + 1);
+                        for (int e = e0 + lane; e < e1; e += 32) {
+                            const int v = __ldg(Pd.spcv + e).x;
+                            atomicOr(wdirty + (v >> 5), 1u << (v & 31));
+                        }
+                        __syncwarp();
+                        const bool mark = ((pending >> lane) & 1u) && valid && ((wdirty[i >> 5] >> (i & 31)) & 1u);
+                        const uint32_t here = __ballot_sync(FULL, mark);
+                        if (here) {
+                            const bool ok = mark && sp_world_ok(Pd, Wc, h, pmask, NP, i, B, u);
+                            m = (m & ~here) | (__ballot_sync(FULL, ok) & here);
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        for (int sw = 0; sw < wls && !p.ref_order; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
             for (int i = threadIdx.x; i < n32; i += blockDim.x) {  // a warp covers one 32-spin block
                 const int q = i >> 5, l = i & 31;

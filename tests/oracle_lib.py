@@ -54,6 +54,9 @@ class Oracle:
         L = C.CDLL(path)
         self.L = L
         L.or_philox.argtypes = [_u32p, _u32p, _u32p]
+        L.or_set_update_order.argtypes = [C.c_int]
+        L.or_get_update_order.restype = C.c_int
+        L.or_sweep_order.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _i32p]
         L.or_expf.argtypes = [C.c_float]
         L.or_expf.restype = C.c_float
         L.or_model_dense.argtypes = [C.c_int, _f8p, _f8p, C.c_double]
@@ -100,6 +103,20 @@ class Oracle:
     def philox(self, ctr, key):
         out = np.zeros(4, np.uint32)
         self.L.or_philox(np.asarray(ctr, np.uint32), np.asarray(key, np.uint32), out)
+        return out
+
+    def set_update_order(self, order: str) -> None:
+        """'reference' (qanneal's shuffled sequential sweeps) or 'checkerboard'."""
+        if order not in ("reference", "checkerboard"):
+            raise ValueError(order)
+        self.L.or_set_update_order(1 if order == "reference" else 0)
+
+    def update_order(self) -> str:
+        return "reference" if self.L.or_get_update_order() else "checkerboard"
+
+    def sweep_order(self, key, ring, sigma, tag, n):
+        out = np.zeros(n, np.int32)
+        self.L.or_sweep_order(key, ring, sigma, tag, n, out)
         return out
 
     def expf(self, y: float) -> float:
