@@ -158,6 +158,89 @@ def _sample_len(local: Any, group=None) -> int:
 
 
 @dataclass
+class ShardedSetResult:
+    """An instance set run over the ranks of a group: the LPT plan, this
+    rank's own per-instance results (``local[j]`` belongs to instance
+    ``plan[rank][j]``) and, on every rank, each instance's best energy over its
+    reads, the read that reached it and its best state."""
+    plan: List[List[int]]
+    local: List[Any]
+    best_energy: np.ndarray
+    best_read: np.ndarray
+    best_state: List[np.ndarray]
+
+
+_SET_METHODS = ("anneal", "sqa", "sqapt")
+
+
+def _set_cost(method: str, n: int, kw: dict, reads: int) -> float:
+    if method == "anneal":
+        return sweep_cost(n, 1, 1, len(kw["schedule"].betas), kw["sweeps_per_beta"], reads)
+    if method == "sqa":
+        sweeps = kw.get("sweeps_per_beta", 1) + kw.get("worldline_sweeps", 0) + kw.get("cluster_sweeps", 0)
+        return sweep_cost(n, kw["trotter_slices"] * kw.get("replicas", 1), 1, len(kw["schedule"].betas), sweeps,
+                          reads)
+    sweeps = kw["sweeps_per_step"] + kw["worldline_sweeps"] + kw.get("cluster_sweeps", 0)
+    return sweep_cost(n, kw["trotter_slices"], len(kw["betas"]), kw["steps"], sweeps, reads)
+
+
+def run_instances_sharded(method: str, models: Sequence[Any], reads: int, seed: int, group=None,
+                          runner: Optional[Callable[..., Any]] = None, **kwargs) -> ShardedSetResult:
+    """An instance set (``BatchRunner.anneal / sqa / sqapt``) spread over the
+    ranks of ``group``: the instances are assigned by LPT on their site-attempt
+    cost (``lpt_partition``; every rank computes the same plan), each rank runs
+    its share as one batched launch with the same ``reads`` and ``seed`` (read
+    r of every instance keeps the key seed + r, so every instance's results are
+    those of the single-process run), and one all-gather brings every
+    instance's best (energy, read, state) to every rank -- the per-instance
+    form of the MINLOC exchange of mpi_replica.cpp:39,49.
+
+    ``runner(method, models, reads=, seed=, **kwargs)`` defaults to a
+    :class:`BatchRunner` on this rank's device and returns, per model, a list
+    of per-read results with ``best_energy`` and ``best_state``."""
+    import torch
+    import torch.distributed as dist
+    if method not in _SET_METHODS:
+        raise ValueError(f"method must be one of {_SET_METHODS}.")
+    if len(models) == 0:
+        raise ValueError("at least one model is required.")
+    if runner is None:
+        def runner(meth, ms, reads, seed, **kw):
+            from .annealers import BatchRunner
+            return getattr(BatchRunner(), meth)(ms, reads=reads, seed=seed, **kw)
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    sizes = [int(m.size()) for m in models]
+    plan = lpt_partition([_set_cost(method, n, kwargs, reads) for n in sizes], world)
+    mine = plan[rank]
+    local = runner(method, [models[i] for i in mine], reads=int(reads), seed=int(seed), **kwargs) if mine else []
+    # one record per assigned instance: index, best energy, best read, best state (padded)
+    n_max, width = max(sizes), max(len(p) for p in plan)
+    rec = np.full((width, 3 + n_max), np.nan)
+    for j, i in enumerate(mine):
+        es = [float(r.best_energy) for r in local[j]]
+        k = min(range(len(es)), key=lambda q: (es[q], q))
+        st = local[j][k].best_state
+        s = np.asarray(st.as_array() if hasattr(st, "as_array") else st, np.float64)
+        rec[j, 0], rec[j, 1], rec[j, 2] = i, es[k], k
+        rec[j, 3:3 + len(s)] = s
+    dev = _device_for(group)
+    t = torch.as_tensor(rec, device=dev)
+    parts = [torch.empty_like(t) for _ in range(world)]
+    dist.all_gather(parts, t, group=group)
+    best_e = np.full(len(models), np.inf)
+    best_r = np.full(len(models), -1, np.int64)
+    best_s: List[np.ndarray] = [np.zeros(0, np.int8)] * len(models)
+    for part in parts:
+        for row in part.cpu().numpy():
+            if np.isnan(row[0]):
+                continue
+            i = int(row[0])
+            best_e[i], best_r[i] = row[1], int(row[2])
+            best_s[i] = row[3:3 + sizes[i]].astype(np.int8)
+    return ShardedSetResult(plan, local, best_e, best_r, best_s)
+
+
+@dataclass
 class MPIReplicaSummary:
     """``qanneal.mpi.MPIReplicaSummary`` (mpi_replica.hpp:13-20)."""
     rank: int

@@ -61,6 +61,14 @@ def _worker(rank, world, port, out_dir, mode):
             with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
                 json.dump({"best": res.best_energy, "spins": res.best_sample.tolist(), "src": res.best_rank,
                            "energies": res.energies.tolist(), "reads": list(res.reads)}, f)
+        elif mode == "set":
+            from qlatanneal_b200.distributed import run_instances_sharded
+            res = run_instances_sharded("anneal", _set_models(), reads=5, seed=71, runner=_oracle_set_runner,
+                                        schedule=_SetSchedule(), sweeps_per_beta=2)
+            with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
+                json.dump({"plan": res.plan, "best": res.best_energy.tolist(), "read": res.best_read.tolist(),
+                           "states": [x.tolist() for x in res.best_state],
+                           "local": [[r.best_energy for r in lst] for lst in res.local]}, f)
         elif mode == "tie":
             e, s, src = minloc_best(-3.0, np.full(5, 1 if rank == 0 else -1, np.int8))
             with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
@@ -133,6 +141,65 @@ def _oracle_replicas(h_, sched_, spb, reps, seed):
     out = R()
     out.global_best_energy, out.global_best_state = runs[g][1], runs[g][0]
     return out
+
+
+class _SetSchedule:
+    betas = np.geomspace(0.1, 3.0, 12)
+
+
+class _SetModel:
+    def __init__(self, n, seed):
+        from qlatanneal_b200.instances import sk_dense
+        self.n, (self.h, self.J) = n, sk_dense(n, seed)
+
+    def size(self):
+        return self.n
+
+
+def _set_models():
+    # uneven sizes, so the LPT plan is not a round robin
+    return [_SetModel(n, 100 + n) for n in (40, 12, 33, 20, 28, 16, 24)]
+
+
+def _oracle_set_runner(method, models, reads, seed, schedule, sweeps_per_beta):
+    """BatchRunner.anneal stand-in on the CPU oracle: read r of every model
+    keyed seed + r."""
+    from oracle_lib import Oracle
+
+    class Res:
+        def __init__(self, E, s):
+            self.best_energy, self.best_state = E, s
+
+    o = Oracle()
+    out = []
+    for m in models:
+        om = o.dense(m.h, m.J)
+        out.append([Res(*o.sa_run(om, schedule.betas, sweeps_per_beta, seed, read=r)[1::-1]) for r in range(reads)])
+    return out
+
+
+def test_sharded_instance_set_equals_single_process():
+    """An instance set over two ranks by LPT (mpi_replica.cpp:39,49 per
+    instance): both ranks end with every instance's best energy, read and
+    state, equal to one process running the whole set."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    with tempfile.TemporaryDirectory() as d:
+        assert _spawn("set", d)
+        r0 = json.load(open(os.path.join(d, "r0.json")))
+        r1 = json.load(open(os.path.join(d, "r1.json")))
+    models = _set_models()
+    full = _oracle_set_runner("anneal", models, 5, 71, _SetSchedule(), 2)
+    assert r0["plan"] == r1["plan"] and sorted(r0["plan"][0] + r0["plan"][1]) == list(range(len(models)))
+    assert r0["plan"][0] and r0["plan"][1]
+    for i, reads in enumerate(full):
+        es = [r.best_energy for r in reads]
+        k = min(range(len(es)), key=lambda q: (es[q], q))
+        for r in (r0, r1):
+            assert r["best"][i] == es[k] and r["read"][i] == k
+            assert r["states"][i] == np.asarray(reads[k].best_state).tolist()
+    for rk, r in enumerate((r0, r1)):  # each rank's own runs are the single-process reads
+        for j, i in enumerate(r["plan"][rk]):
+            assert r["local"][j] == [x.best_energy for x in full[i]]
 
 
 def _spawn(mode, out_dir):

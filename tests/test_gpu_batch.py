@@ -52,3 +52,27 @@ def test_batch_rejects_mixed_kinds():
                                 qa.AnnealSchedule.from_betas([1.0]), 1)
     with pytest.raises(ValueError):
         qa.BatchRunner().anneal([], qa.AnnealSchedule.from_betas([1.0]), 1)
+
+
+def test_sharded_instance_set_single_rank_equals_batch(tmp_path):
+    """run_instances_sharded with its default runner (BatchRunner) on a
+    one-rank group: the same per-instance results as the batched call."""
+    import torch.distributed as dist
+    from qlatanneal_b200.distributed import run_instances_sharded
+    from qlatanneal_b200.instances import sk_dense
+    models = [qa.DenseIsing(*sk_dense(n, 300 + n)) for n in (40, 72, 24)]
+    betas, gammas = np.full(8, 2.0), np.linspace(2.0, 0.1, 8)
+    sched = qa.SQASchedule.from_vectors(betas, gammas)
+    dist.init_process_group("gloo", init_method=f"file://{tmp_path}/pg", rank=0, world_size=1)
+    try:
+        res = run_instances_sharded("sqa", models, reads=4, seed=9, schedule=sched, trotter_slices=8,
+                                    sweeps_per_beta=1, worldline_sweeps=1)
+    finally:
+        dist.destroy_process_group()
+    want = qa.BatchRunner().sqa(models, sched, 8, sweeps_per_beta=1, worldline_sweeps=1, reads=4, seed=9)
+    assert res.plan == [[0, 1, 2]]
+    for i, reads in enumerate(want):
+        es = [r.best_energy for r in reads]
+        k = min(range(len(es)), key=lambda q: (es[q], q))
+        assert res.best_energy[i] == es[k] and res.best_read[i] == k
+        np.testing.assert_array_equal(res.best_state[i], reads[k].best_state.as_array())
