@@ -14,7 +14,9 @@ Metric: site-attempts/s (a slice proposal counts 1 site, a worldline proposal P)
           upload (H2D), the run, and the results back on the host (D2H), wall time.
   roofline : the sweep kernel's algorithmic bytes (per-attempt field/spin reads
           plus one coupling row per accepted flip, 1 byte per +/-1 coupling)
-          over its event-timed duration, against the measured HBM copy bandwidth.
+          over its event-timed duration, against the measured HBM copy bandwidth
+          (frac) and against the L2 read bandwidth measured in the same run
+          (frac_l2, qa_probe_l2_read).
           The unit is the sweep region of one anneal: with more reads than SMs
           the rings run as many short concurrent launches (groups of rings on
           side streams), so a single launch has no meaningful duration of its own.
@@ -504,6 +506,19 @@ def run_chi_ttt(args):
     return 0
 
 
+def measure_l2_peak(lib, device):
+    """L2 read bandwidth (GB/s) of this device: the best of three L2-resident
+    buffer sizes, each read 200 times (qa_probe_l2_read), outside any timed region."""
+    import ctypes as C
+    L = lib.load()
+    best = 0.0
+    for mib in (16, 32, 64):
+        g = C.c_double(0.0)
+        if L.qa_probe_l2_read(int(device), mib << 20, 200, C.byref(g)) == 0:
+            best = max(best, g.value)
+    return best or None
+
+
 def flush_l2(torch, dev):
     buf = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     buf.fill_(1)
@@ -622,6 +637,7 @@ def main():
     sweep_ms_step = sweep_ms / args.steps
     achieved = bytes_step / (sweep_ms_step / 1e3) / 1e9
     traffic = load_traffic() if reads == WL["reads"] else None
+    l2_peak = measure_l2_peak(_lib, local)
 
     # best energy over all ranks (the MINLOC + broadcast of qanneal's MPI reads helper)
     i_best = int(np.argmin([r.best_energy for r in res]))
@@ -660,7 +676,9 @@ def main():
                          "kernel": "ring_pm1_kernel (slice + worldline sweeps)",
                          "per": "sweep region of one anneal (all ring launches of one step)",
                          "sweep_ms_per_step": sweep_ms_step, "launches_per_step": launches,
-                         "algorithmic_bytes_per_step": bytes_step},
+                         "algorithmic_bytes_per_step": bytes_step,
+                         "l2_peak": l2_peak, "frac_l2": achieved / l2_peak if l2_peak else None,
+                         "l2_peak_source": "measured in this run: qa_probe_l2_read, best of 16/32/64 MiB"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "site-attempts/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * float(np.mean(e2e_times))},

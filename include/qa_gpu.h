@@ -444,6 +444,15 @@ QA_API int qa_sa_dense_run_noalloc(int device, void *stream, int n, const double
                                    const qa_sa_params *params, int8_t *d_best_spins, double *d_best_energy,
                                    double *d_energy_trace, qa_stats *stats);
 
+/* ---- measurement ---------------------------------------------------------
+ * No counterpart in the reference: the L2 read bandwidth of `device`, the
+ * denominator of the sweep kernels' L2 roofline.  A buffer of `bytes`
+ * (1 MiB .. 96 MiB, small enough to stay in L2) is read `passes` times with
+ * 16-byte L2-only loads by a grid of eight 256-thread CTAs per SM after one
+ * warm pass; *gbs = bytes * passes / device time (CUDA events).  Allocates
+ * and frees its own buffer; restores the caller's current device. */
+QA_API int qa_probe_l2_read(int device, size_t bytes, int passes, double *gbs);
+
 #ifdef __cplusplus
 }
 #endif
