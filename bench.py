@@ -50,8 +50,8 @@ WORKLOAD_NAME = ("dense SQA, SK n=512 J=+-1, h~N(0,0.1^2) fp32, P=32, beta=0.5P,
 
 # SQA-Chi with a learned schedule: training set, pilot and production runs.
 CHI = dict(train=2000, n_min=256, n_max=2048, P=64, beta=4.0, gamma0=3.0, gamma1=0.01, points=64, sweeps=200,
-           burn=50, train_seed=7, prod_n=1024, reads=512, num_steps=100, sweeps_per_step=20, instances=3,
-           prod_seed=9001)
+           burn=50, train_seed=7, prod_n=1024, reads=512, num_steps=100, sweeps_per_step=20, instances=6,
+           prod_seed=9001, shared_pilot_reads=16)
 
 
 def schedule(steps=None):
@@ -432,10 +432,32 @@ def tts99(t_call, reads, p):
     return t if p >= 0.99 else t * np.log(0.01) / np.log(1.0 - p)
 
 
+def wilson95(k, n):
+    z = 1.96
+    p = k / n
+    d = 1 + z * z / n
+    c = (p + z * z / (2 * n)) / d
+    w = z * np.sqrt(p * (1 - p) / n + z * z / (4 * n * n)) / d
+    return max(0.0, c - w), min(1.0, c + w)
+
+
 def run_chi_ttt(args):
     """Learned vs pilot-scan SQA-Chi: build the training set with the plain
     pilot on the GPU, train the MLP with the library's kernels, then anneal
-    SK instances with both schedules and compare time-to-99%-of-best-known."""
+    SK instances with three schedules and compare time-to-99%-of-best-known:
+
+    * pilot per read: run_chi as the reference runs it, every read scanning
+      its own chi_B curve (sqa_chi_annealer.cpp:217-281);
+    * shared pilot: one pilot per instance (the mean curve of a
+      ``shared_pilot_reads``-read scan), reused by every production read --
+      the natural GPU baseline for the learned model;
+    * learned: the network's predicted curve (features, inference and the
+      uncertainty check included), the pilot only as its fallback.
+
+    The success probability p_s (a read reaching 0.99 of the best-known
+    energy, the best over all arms) carries its 95% Wilson interval, and
+    TTS99 = (t_call / reads) ln(0.01) / ln(1 - p_s) is reported with the
+    interval that p_s's bounds give."""
     import torch
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -458,49 +480,71 @@ def run_chi_ttt(args):
     kw = dict(num_steps=c["num_steps"], sweeps_per_step=c["sweeps_per_step"], scan_points=c["points"],
               scan_sweeps=c["sweeps"], scan_burn=c["burn"], reads=c["reads"])
     rows = []
-    for k in range(args.chi_instances):
-        h, J = sk_dense(c["prod_n"], c["prod_seed"] + k)
-        m = qa.DenseIsing(h, J)
-        ann = qa.SQAChiAnnealer(m, c["P"], 1)
-        ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], num_steps=2, sweeps_per_step=1, scan_points=4,
-                          scan_sweeps=2, scan_burn=1, reads=2, seed=1)  # device copy + warm-up
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        rp = ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], seed=1000 * k, **kw)
-        t_p = time.perf_counter() - t0
-        st_p = ann.last_stats
-        t0 = time.perf_counter()
-        curve = model.curve(m)
-        fallback = curve is None
-        rl = ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], seed=1000 * k + 500, scan_chi=curve, **kw)
-        t_l = time.perf_counter() - t0
-        st_l = ann.last_stats
-        ep = np.array([r.best_energy for r in rp])
-        el = np.array([r.best_energy for r in rl])
-        best = float(min(ep.min(), el.min()))
-        target = 0.99 * best
-        pp, pl = float(np.mean(ep <= target)), float(np.mean(el <= target))
-        rows.append(dict(instance_seed=c["prod_seed"] + k, best_known=best, p_pilot=pp, p_learned=pl,
-                         t_pilot_s=t_p, t_learned_s=t_l, gpu_ms_pilot=st_p.total_ms, gpu_ms_learned=st_l.total_ms,
-                         tts99_pilot_s=tts99(t_p, c["reads"], pp), tts99_learned_s=tts99(t_l, c["reads"], pl),
-                         mean_E_pilot=float(ep.mean()), mean_E_learned=float(el.mean()), fallback=fallback,
-                         predicted_std=model.last_std))
-        m.release()
-    tl = float(np.median([r["tts99_learned_s"] for r in rows]))
-    tp = float(np.median([r["tts99_pilot_s"] for r in rows]))
+    with Clocks(0) as clk:
+        for k in range(args.chi_instances):
+            h, J = sk_dense(c["prod_n"], c["prod_seed"] + k)
+            m = qa.DenseIsing(h, J)
+            ann = qa.SQAChiAnnealer(m, c["P"], 1)
+            ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], num_steps=2, sweeps_per_step=1, scan_points=4,
+                              scan_sweeps=2, scan_burn=1, reads=2, seed=1)  # device copy + warm-up
+            torch.cuda.synchronize()
+            arms = {}
+            # pilot per read
+            t0 = time.perf_counter()
+            res = ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], seed=1000 * k, **kw)
+            arms["pilot_per_read"] = (time.perf_counter() - t0, res, False)
+            # one shared pilot per instance
+            t0 = time.perf_counter()
+            shared = learned.pilot_curves([m], c["beta"], c["gamma0"], c["gamma1"], c["P"], c["points"], c["sweeps"],
+                                          c["burn"], reads=c["shared_pilot_reads"], seed=1000 * k + 250)[0]
+            res = ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], seed=1000 * k + 300, scan_chi=shared, **kw)
+            arms["pilot_shared"] = (time.perf_counter() - t0, res, False)
+            # learned curve (pilot only when the prediction is too uncertain)
+            t0 = time.perf_counter()
+            curve = model.curve(m)
+            res = ann.run_chi_reads(c["beta"], c["gamma0"], c["gamma1"], seed=1000 * k + 500, scan_chi=curve, **kw)
+            arms["learned"] = (time.perf_counter() - t0, res, curve is None)
+            best = float(min(min(r.best_energy for r in a[1]) for a in arms.values()))
+            target = 0.99 * best
+            row = dict(instance_seed=c["prod_seed"] + k, best_known=best, predicted_std=model.last_std)
+            for name, (t_call, res, fb) in arms.items():
+                e = np.array([r.best_energy for r in res])
+                hits = int(np.sum(e <= target))
+                lo, hi = wilson95(hits, len(e))
+                row[name] = dict(t_call_s=t_call, p_s=hits / len(e), p_s_ci95=[lo, hi], hits=hits, reads=len(e),
+                                 tts99_s=tts99(t_call, len(e), hits / len(e)),
+                                 tts99_ci95_s=[tts99(t_call, len(e), hi), tts99(t_call, len(e), lo)],
+                                 mean_E=float(e.mean()), fallback=fb)
+            rows.append(row)
+            m.release()
+    clocks = clk.summary()
+
+    def med(arm):
+        return float(np.median([r[arm]["tts99_s"] for r in rows]))
+
+    tl, tp, ts = med("learned"), med("pilot_per_read"), med("pilot_shared")
+    ratio = [r["pilot_shared"]["tts99_s"] / r["learned"]["tts99_s"] for r in rows
+             if np.isfinite(r["learned"]["tts99_s"]) and np.isfinite(r["pilot_shared"]["tts99_s"])]
     line = {
         "metric": "time-to-target (99% of best-known energy, TTS99), SQA-Chi learned vs pilot-scan schedule",
-        "value": tl, "unit": "s", "higher_is_better": False, "n_gpus": 1, "pilot_value": tp,
-        "speedup_vs_pilot": tp / tl if tl > 0 else None, "dtype": "f32", "data": "synthetic",
+        "value": tl, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+        "pilot_per_read_value": tp, "pilot_shared_value": ts,
+        "speedup_vs_pilot_per_read": tp / tl if tl > 0 else None,
+        "speedup_vs_pilot_shared": ts / tl if tl > 0 else None,
+        "tts99_ratio_shared_over_learned_per_instance": ratio,
+        "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"SQA-Chi, SK n={c['prod_n']} J=+-1 h=0, P={c['P']}, beta={c['beta']}, Gamma "
                                f"{c['gamma0']}->{c['gamma1']}, {c['num_steps']} steps x {c['sweeps_per_step']} "
                                f"sweeps, {c['reads']} reads per call; pilot {c['points']} points x "
-                               f"({c['burn']} burn + {c['sweeps']}) sweeps per read",
+                               f"({c['burn']} burn + {c['sweeps']}) sweeps per read; shared pilot "
+                               f"{c['shared_pilot_reads']} reads per instance",
+                   "instances": args.chi_instances,
                    "training": {"instances": int(len(X)), "n_range": [c["n_min"], c["n_max"]],
                                 "kinds": "half dense SK +-1, half 3-regular +-1, h=0",
                                 "pilot_gpu_s": t_data, "fit_s": t_fit, "epochs_run": len(hist),
                                 "val_loss": model.val_loss, "max_std": model.max_std}},
         "instances": rows,
+        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
     return 0
