@@ -216,7 +216,7 @@ namespace {
 enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
               W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP, W_JP,
               W_BSAMP, W_SSAVE, W_FSAVE, W_CBESTE, W_CBSTEP, W_CBITS, W_CBOND, W_FLAG, W_QSTAGE,
-              W_TRB, W_TRE, W_TREB, W_TREE, W_RSPIN, W_DRIFT, W_COUNT };
+              W_TRB, W_TRE, W_TREB, W_TREE, W_RSPIN, W_DRIFT, W_ORDER, W_COUNT };
 static_assert(W_COUNT <= qa_ctx::kWsSlots, "qa_ctx::ws has a slot per WsSlot");
 
 int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
@@ -533,6 +533,7 @@ struct RingPlan {
     int gbytes = 4;       // pm1: bytes per field (4 int32, 2 int16)
     bool jw_smem = true;  // pm1: J bits in shared memory
     bool ref_order = false;  // qanneal's update order (else the parity checkerboard)
+    bool order_global = false;  // ring_kernel: the order's scratch in global memory (too large for shared)
     int W = 1;
     size_t smem = 0;
     int smem_fields = 1;
@@ -579,12 +580,22 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
         pl->smem_fields = 0;
         return QA_OK;
     }
-    pl->smem = ring_smem_bytes(P, n_max, pl->W, true, ref_order);
-    pl->smem_fields = 1;
-    if (pl->smem > (size_t)std::min(ctx->smem_optin, 200 * 1024)) {
-        pl->smem_fields = 0;
-        pl->smem = ring_smem_bytes(P, n_max, pl->W, false, ref_order);
+    // fields in shared memory where they fit (up to 200 KB), the order's
+    // scratch too, else the order's scratch in global memory first
+    const size_t fcap = (size_t)std::min(ctx->smem_optin, 200 * 1024), cap = (size_t)ctx->smem_optin;
+    bool placed = false;
+    for (int form = 0; form < 4 && !placed; ++form) {
+        const bool fields = form == 0 || form == 1, ord_smem = form == 0 || form == 2;
+        if (!ref_order && !ord_smem) continue;
+        const size_t b = ring_smem_bytes(P, n_max, pl->W, fields, ref_order, ord_smem);
+        if (b <= (fields ? fcap : cap)) {
+            pl->smem = b;
+            pl->smem_fields = fields ? 1 : 0;
+            pl->order_global = ref_order && !ord_smem;
+            placed = true;
+        }
     }
+    if (!placed) pl->smem = ring_smem_bytes(P, n_max, pl->W, false, ref_order, false);
     if (pl->smem > (size_t)ctx->smem_optin) return fail(QA_ERR_ARG, "ring state does not fit in shared memory.");
     return QA_OK;
 }
@@ -657,6 +668,20 @@ int ws_array(qa_ctx *ctx, int slot, size_t count, T **out) {
     return QA_OK;
 }
 
+// The global-memory scratch of the order builds when the plan put it there:
+// one region per ring (rotated launches offset it by their first ring).
+static int order_scratch(qa_ctx *ctx, const RingPlan &pl, int nr, int n_max, RingParams *rp) {
+    rp->oscratch = nullptr;
+    rp->oscratch_bytes = 0;
+    if (!pl.order_global) return QA_OK;
+    const size_t per = ring_order_scratch_bytes(n_max);
+    void *v;
+    QA_TRY(ws_get(ctx, W_ORDER, per * (size_t)nr, &v));
+    rp->oscratch = static_cast<unsigned char *>(v);
+    rp->oscratch_bytes = (long long)per;
+    return QA_OK;
+}
+
 // Ring groups of a rotated run (run_rings_rotated): groups of G rings, one
 // stream each, at most 128 streams.
 struct RotPlan {
@@ -715,6 +740,7 @@ static RingParams ring_offset(RingParams r, int g0) {
     if (r.ring_bond) r.ring_bond += (size_t)g0 * r.rec_stride;
     if (r.mag) r.mag += (size_t)g0 * r.steps_total * r.spb;
     if (r.bsamp) r.bsamp += (size_t)g0 * r.bstride;
+    if (r.oscratch) r.oscratch += (size_t)g0 * r.oscratch_bytes;
     return r;
 }
 
@@ -1583,6 +1609,7 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     // dense +-1 couplings: the bit-packed kernel builds its fields in-kernel
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
+    QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_beta; rp.wls = prm->worldline_sweeps;
     rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.B = d_A; rp.T4 = d_T4; rp.per_slot_sched = 0;
@@ -1915,6 +1942,7 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
                       !pl.own_fields()));
     RingParams rp{};
+    QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = S; rp.spb = spb; rp.wls = wls; rp.cls = cls;
     rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.B = d_A; rp.T4 = d_T4; rp.JP = d_JP; rp.per_slot_sched = 0;
@@ -2328,6 +2356,7 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
     RingParams rp{};
+    QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_step; rp.wls = prm->worldline_sweeps;
     rp.slice_tag = DOM_SLICE; rp.slot = d_slot; rp.B = d_B; rp.T4 = d_T4; rp.per_slot_sched = 1;
@@ -2535,6 +2564,7 @@ int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_probl
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
                       !pl.own_fields()));
     RingParams rp{};
+    QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = S; rp.spb = spb; rp.wls = wls; rp.cls = cls;
     rp.slice_tag = DOM_SLICE; rp.slot = d_slot; rp.B = d_B; rp.T4 = d_T4; rp.JP = d_JP;

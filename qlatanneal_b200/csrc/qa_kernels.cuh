@@ -57,6 +57,8 @@ struct RingParams {
     int smem_fields;
     int ref_order;        // 1: qanneal's order (a random spin order per sweep, slices in turn); 0: parity
                           //    checkerboard, spins ascending (the SQA-Chi kernel's order)
+    unsigned char *oscratch;   // ring_kernel, qanneal's order, when shared memory cannot hold it: the order's
+    long long oscratch_bytes;  //   keys, bucket counters and order, oscratch_bytes per CTA (else null)
     int init_fields;      // ring_pm1_kernel: build the int32 fields from the spins first
     int init_scan;        // score the starting state as "step -1" before step0 (PT)
     int rec_base;         // per-step records live at [ring][rec_base + step]
@@ -416,11 +418,19 @@ __device__ __forceinline__ void record_bond_sample(const RingParams &p, const ui
         p.bsamp[(long long)blockIdx.x * p.bstride + (long long)(step - p.step0) * (p.spb + p.cls) + j] = tb;
 }
 
-__host__ __device__ inline size_t ring_order_bytes(int P, int n) {
-    return order_keys_bytes(n) + order_cnt_bytes(n) + order_idx_bytes(n) + align_up((size_t)P * 4, 16) + 16;
+// The order build's keys, bucket counters and the order itself (shared or global memory).
+__host__ __device__ inline size_t ring_order_scratch_bytes(int n) {
+    return order_keys_bytes(n) + order_cnt_bytes(n) + order_idx_bytes(n);
 }
 
-__host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fields, bool ref_order = false) {
+// qanneal's order in shared memory: the scratch above unless it lives in
+// global memory, plus the slices' progress counters and the abort flag.
+__host__ __device__ inline size_t ring_order_bytes(int P, int n, bool scratch_in_smem = true) {
+    return (scratch_in_smem ? ring_order_scratch_bytes(n) : 0) + align_up((size_t)P * 4, 16) + 16;
+}
+
+__host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fields, bool ref_order = false,
+                                                 bool order_in_smem = true) {
     const int nw = (n + 31) / 32;
     size_t b = align_up((size_t)P * nw * 4, 16);
     b += align_up((size_t)n * 4, 16);
@@ -428,7 +438,7 @@ __host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fiel
     b += align_up((size_t)W * 32 * 4, 16);
     b += align_up((size_t)W * 32 * 8, 16);
     b += 16;
-    if (ref_order) b += ring_order_bytes(P, n);
+    if (ref_order) b += ring_order_bytes(P, n, order_in_smem);
     if (fields) b += (size_t)P * n * 4;
     return b;
 }
@@ -547,9 +557,11 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     sm.wl_G = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)W * 32 * 8, 16);
     sm.flag = reinterpret_cast<int *>(ptr); ptr += 16;
     if (p.ref_order) {
-        sm.okeys = reinterpret_cast<unsigned long long *>(ptr); ptr += order_keys_bytes(n);
-        sm.ocnt = reinterpret_cast<int *>(ptr); ptr += order_cnt_bytes(n);
-        sm.ord = reinterpret_cast<int *>(ptr); ptr += order_idx_bytes(n);
+        unsigned char *q = p.oscratch ? p.oscratch + (long long)blockIdx.x * p.oscratch_bytes : ptr;
+        sm.okeys = reinterpret_cast<unsigned long long *>(q); q += order_keys_bytes(n);
+        sm.ocnt = reinterpret_cast<int *>(q); q += order_cnt_bytes(n);
+        sm.ord = reinterpret_cast<int *>(q); q += order_idx_bytes(n);
+        if (!p.oscratch) ptr = q;
         sm.prog = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)NP * 4, 16);
         sm.abortf = reinterpret_cast<int *>(ptr); ptr += 16;
         if (threadIdx.x == 0) *sm.abortf = 0;
