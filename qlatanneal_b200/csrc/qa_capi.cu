@@ -19,6 +19,7 @@
 #include "qa_chi.cuh"
 #include "qa_mlp.cuh"
 #include "qa_sparse.cuh"
+#include "qa_tc.cuh"
 #include "qa_pm1.cuh"
 #include "qa_pt.cuh"
 #include "qa_ingest.cuh"
@@ -197,6 +198,11 @@ struct qa_mlp {
 struct qa_problem {
     qa_ctx *ctx = nullptr;
     int kind = 0, n = 0, nw = 0, T = 0, m = 0;
+    // dense couplings as int8 rows for the tensor-core field init (built on
+    // first use when every coupling is an integer in [-127, 127])
+    int tc_int8 = -1;  // -1 unknown, 0 no, 1 yes
+    int8_t *J8 = nullptr;
+    int tc_ldj = 0;
     double c = 0.0;
     std::vector<void *> allocs;
     ProbDev dev{};
@@ -493,11 +499,85 @@ int upload_common(qa_ctx *ctx, const qa_problem *const *probs, int np, const Lay
     return QA_OK;
 }
 
+// Whether a dense problem's couplings are integers in [-127, 127]; if so its
+// int8 rows for the tensor-core field init are built (once per problem).
+int tc_prepare(qa_ctx *ctx, qa_problem *P) {
+    if (P->tc_int8 >= 0) return QA_OK;
+    P->tc_int8 = 0;
+    if (P->kind != K_DENSE || !P->dev.J32) return QA_OK;
+    const int n = P->n;
+    int *d_ok = nullptr;
+    QA_CK(cudaMallocAsync(reinterpret_cast<void **>(&d_ok), sizeof(int), ctx->stream));
+    const int one = 1;
+    QA_CK(cudaMemcpyAsync(d_ok, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    tc_int8_check_kernel<<<256, 256, 0, ctx->stream>>>(P->dev.J32, (long long)n * n, d_ok);
+    QA_CK(cudaGetLastError());
+    int ok = 0;
+    QA_CK(cudaMemcpyAsync(&ok, d_ok, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    QA_CK(cudaStreamSynchronize(ctx->stream));
+    QA_CK(cudaFreeAsync(d_ok, ctx->stream));
+    if (!ok) return QA_OK;
+    const int ldj = (n + TC_K - 1) / TC_K * TC_K, rows = (n + TC_N - 1) / TC_N * TC_N;
+    void *d = nullptr;
+    QA_CK(cudaMalloc(&d, (size_t)rows * ldj));
+    P->allocs.push_back(d);
+    P->J8 = static_cast<int8_t *>(d);
+    P->tc_ldj = ldj;
+    tc_pack_couplings_kernel<<<256, 256, 0, ctx->stream>>>(P->dev.J32, n, ldj, rows, P->J8);
+    QA_CK(cudaGetLastError());
+    P->tc_int8 = 1;
+    return QA_OK;
+}
+
+// The initial fields of every cell of dense problems with int8-exact
+// couplings on the tensor cores (tc_fields_kernel), one launch per problem
+// over its rings (rings are ordered by problem).  *done = false when some
+// problem does not qualify (the caller then runs the float64 init).
+int tc_init_fields(qa_ctx *ctx, const qa_problem *const *probs, int np, const Layout &L, const RingDev *d_rings,
+                   uint32_t *d_spins, float *d_fields, int P, unsigned long long *err, bool *done) {
+    *done = false;
+    if (std::getenv("QA_DISABLE_TC_INIT")) return QA_OK;
+    for (int p = 0; p < np; ++p) {
+        QA_TRY(tc_prepare(ctx, const_cast<qa_problem *>(probs[p])));
+        if (probs[p]->tc_int8 != 1) return QA_OK;
+    }
+    int r0 = 0;
+    for (int p = 0; p < np; ++p) {
+        int cnt = 0;
+        while (r0 + cnt < (int)L.rings.size() && L.rings[r0 + cnt].prob == p) ++cnt;
+        if (cnt == 0) continue;
+        TcFieldParams tp{};
+        tp.rings = d_rings + r0;
+        tp.spins = d_spins;
+        tp.fields = d_fields;
+        tp.J8 = probs[p]->J8;
+        tp.ldj = probs[p]->tc_ldj;
+        tp.n = probs[p]->n;
+        tp.nw = probs[p]->nw;
+        tp.P = P;
+        tp.n_cells = cnt * P;
+        tp.err = err;
+        const dim3 grid((tp.n_cells + TC_M - 1) / TC_M, (tp.n + TC_N - 1) / TC_N);
+        tc_fields_kernel<<<grid, 128, 0, ctx->stream>>>(tp);
+        QA_CK(cudaGetLastError());
+        r0 += cnt;
+    }
+    *done = true;
+    return QA_OK;
+}
+
 int init_state(qa_ctx *ctx, int kind, const ProbDev *d_probs, const RingDev *d_rings, int n_rings, uint32_t *d_spins,
-               float *d_fields, int P, int n_max, int nw_max, uint32_t tag, bool with_fields = true) {
+               float *d_fields, int P, int n_max, int nw_max, uint32_t tag, bool with_fields = true,
+               const qa_problem *const *probs = nullptr, int np = 0, const Layout *L = nullptr,
+               unsigned long long *err = nullptr) {
     init_spins_kernel<<<dim3(n_rings, P), 128, 0, ctx->stream>>>(d_probs, d_rings, d_spins, P, tag, nw_max);
     QA_CK(cudaGetLastError());
     if (!with_fields) return QA_OK;
+    if (kind == K_DENSE && probs && L && err) {
+        bool done = false;
+        QA_TRY(tc_init_fields(ctx, probs, np, *L, d_rings, d_spins, d_fields, P, err, &done));
+        if (done) return QA_OK;
+    }
     const int zb = std::max(1, std::min(64, (n_max + 127) / 128));
     int rc = QA_OK;
     dispatch_kind(kind, [&](auto K) {
@@ -1607,7 +1687,8 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0 || traces,
                       ctx->update_order == QA_ORDER_REFERENCE));
     // dense +-1 couplings: the bit-packed kernel builds its fields in-kernel
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields(),
+                      problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
     QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
@@ -1940,7 +2021,7 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     RingPlan pl;
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, cls > 0, ctx->update_order == QA_ORDER_REFERENCE));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
-                      !pl.own_fields()));
+                      !pl.own_fields(), problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
     QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
@@ -2354,7 +2435,8 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, prm->cluster_sweeps > 0,
                       !classical && ctx->update_order == QA_ORDER_REFERENCE));
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields()));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields(),
+                      problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
     QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
@@ -2562,7 +2644,7 @@ int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_probl
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl, cls > 0, ctx->update_order == QA_ORDER_REFERENCE));
     QA_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
-                      !pl.own_fields()));
+                      !pl.own_fields(), problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
     QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
@@ -2955,7 +3037,7 @@ static int chi_stage1(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     RingPlan pl;
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PILOT_INIT,
-                      !pl.own_fields()));
+                      !pl.own_fields(), problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = 1; rp.spb = sweeps_total; rp.wls = 0; rp.slice_tag = DOM_PILOT;
@@ -2973,6 +3055,7 @@ static int chi_stage1(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_CK(cudaMemcpyAsync(c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     QA_CK(cudaStreamSynchronize(ctx->stream));
+    QA_TRY(check_device_error(c));
     QA_CK(cudaEventElapsedTime(&pilot_ms, ctx->ev[0], ctx->ev[1]));
     d2h += (int64_t)(sizeof(double) * chi.size() + sizeof(c));
     for (int i = 0; i < 4; ++i) cnt_total[i] += c[i];
@@ -3144,7 +3227,8 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     RingPlan pl;
     QA_TRY(plan_rings(ctx, problems, n_problems, kind, P, n_max, &pl));
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PROD_INIT, !pl.own_fields()));
+    QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_PROD_INIT, !pl.own_fields(),
+                      problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_step; rp.wls = 0; rp.slice_tag = DOM_PROD;
