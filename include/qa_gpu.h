@@ -89,6 +89,31 @@ enum { QA_ORDER_CHECKERBOARD = 0, QA_ORDER_REFERENCE = 1 };
 QA_API int qa_set_update_order(qa_ctx *ctx, int order);
 QA_API int qa_get_update_order(const qa_ctx *ctx, int *order);
 
+/* Launch-shape overrides of a context, for the autotuner (no counterpart in
+ * the reference: its loops have no launch shape).  Every choice leaves the
+ * results unchanged bit for bit; it moves only time.  0 / -1 is automatic.
+ *   warps_per_ring: warps of a ring's CTA (1..32, at most P; automatic:
+ *                   ceil(P/2));
+ *   field_form:     the dense +-1 kernel's ring state: 0 int32 fields and the
+ *                   coupling bits in shared memory, 1 int16 fields and the
+ *                   bits in shared memory, 2 int16 fields and the bits read
+ *                   through L2 (a form that does not fit falls back to the
+ *                   automatic order of the three);
+ *   rotate:         0 whole-grid launches, 1 rotated ring groups whenever the
+ *                   rings outnumber the SMs, -1 when whole-grid waves would
+ *                   leave slots idle;
+ *   rot_steps:      steps per rotated launch;
+ *   rot_group:      rings per rotated group (at most 128 groups). */
+typedef struct {
+    int warps_per_ring;
+    int field_form;
+    int rotate;
+    int rot_steps;
+    int rot_group;
+} qa_tuning;
+QA_API int qa_set_tuning(qa_ctx *ctx, const qa_tuning *tuning);  /* NULL: all automatic */
+QA_API int qa_get_tuning(const qa_ctx *ctx, qa_tuning *tuning);
+
 /* ---- problems (device copies of one model instance) ------------------- */
 
 /* DenseIsing(h, J, n, c) (dense_ising.hpp:17-21): E = c + sum h s + sum_{i<j} J_ij s_i s_j.

@@ -20,13 +20,18 @@ QA_ORDER_CHECKERBOARD, QA_ORDER_REFERENCE = 0, 1
 # Every symbol include/qa_gpu.h declares (checked by the CPU test suite).
 EXPORTED = [
     "qa_version", "qa_last_error", "qa_device_count", "qa_create", "qa_destroy", "qa_set_drift_check",
-    "qa_set_update_order", "qa_get_update_order", "qa_probe_l2_read",
+    "qa_set_update_order", "qa_get_update_order", "qa_probe_l2_read", "qa_set_tuning", "qa_get_tuning",
     "qa_problem_dense", "qa_problem_qubo", "qa_problem_sparse", "qa_problem_hubo", "qa_problem_free", "qa_problem_size",
     "qa_sa_run", "qa_sa_trace_run", "qa_replica_run", "qa_sqa_run", "qa_sqa_trace_run", "qa_sqa_opt_run", "qa_sqapt_run", "qa_sqapt_opt_run", "qa_pt_run",
     "qa_chi_run", "qa_chi_pilot",
     "qa_mlp_create", "qa_mlp_free", "qa_mlp_num_params", "qa_mlp_get_params", "qa_mlp_set_params",
     "qa_mlp_forward", "qa_mlp_loss_grad", "qa_mlp_train_step",
 ]
+
+
+class qa_tuning(C.Structure):
+    _fields_ = [("warps_per_ring", C.c_int), ("field_form", C.c_int), ("rotate", C.c_int), ("rot_steps", C.c_int),
+                ("rot_group", C.c_int)]
 
 
 class qa_run_out(C.Structure):
@@ -152,6 +157,8 @@ def load():
         L.qa_set_update_order.argtypes = [vp, i]
         L.qa_get_update_order.argtypes = [vp, C.POINTER(i)]
         L.qa_probe_l2_read.argtypes = [i, C.c_size_t, i, C.POINTER(d)]
+        L.qa_set_tuning.argtypes = [vp, C.POINTER(qa_tuning)]
+        L.qa_get_tuning.argtypes = [vp, C.POINTER(qa_tuning)]
         L.qa_problem_dense.argtypes = [vp, i, vp, vp, d, C.POINTER(vp)]
         L.qa_problem_qubo.argtypes = [vp, i, vp, vp, vp, C.POINTER(vp)]
         L.qa_problem_sparse.argtypes = [vp, i, vp, i, vp, vp, vp, d, C.POINTER(vp)]

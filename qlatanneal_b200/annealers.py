@@ -14,7 +14,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from . import _lib
+from . import _lib, autotune
 from .models import AnnealSchedule, SQASchedule, State
 
 BACKENDS = ("cuda", "CUDA")
@@ -475,6 +475,7 @@ class SQAAnnealer(_Seeded):
         o, spins, energies, trace = _outs(n, reads, len(betas))
         st = _lib.qa_stats()
         probs = (C.c_void_p * 1)(prob)
+        autotune.apply(eng, self.hamiltonian.kind, n, self.trotter_slices, int(reads) * self.replicas)
         _lib.check(eng.L.qa_sqa_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         return [SQAResult(State._view(spins[r]), float(energies[r]), trace[r]) for r in range(reads)]
@@ -597,6 +598,7 @@ class SQAParallelTemperingAnnealer(_Seeded):
                               avg.ctypes.data, swp.ctypes.data)
         st = _lib.qa_stats()
         probs = (C.c_void_p * 1)(prob)
+        autotune.apply(eng, self.hamiltonian.kind, n, self.trotter_slices, int(reads) * R)
         _lib.check(eng.L.qa_sqapt_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         return [SQAParallelTemperingResult([State._view(fin[r, k]) for k in range(R)], finE[r].tolist(), State._view(best[r]),
@@ -801,6 +803,8 @@ class BatchRunner:
         outs = [_outs(m.size(), reads, len(betas)) for m in models]
         arr = (_lib.qa_run_out * len(models))(*[o[0] for o in outs])
         st = _lib.qa_stats()
+        autotune.apply(eng, models[0].kind, max(m.size() for m in models), int(trotter_slices),
+                       int(reads) * int(replicas) * len(models))
         _lib.check(eng.L.qa_sqa_run(eng.h, probs, len(models), C.byref(prm), arr, C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         return [[SQAResult(State._view(sp[r]), float(en[r]), tr[r]) for r in range(reads)]
@@ -827,6 +831,8 @@ class BatchRunner:
         arr = (_lib.qa_sqapt_out * len(models))(*[
             _lib.qa_sqapt_out(*(x.ctypes.data for x in bf)) for bf in bufs])
         st = _lib.qa_stats()
+        autotune.apply(eng, models[0].kind, max(m.size() for m in models), int(trotter_slices),
+                       int(reads) * R * len(models))
         _lib.check(eng.L.qa_sqapt_run(eng.h, probs, len(models), C.byref(prm), arr, C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         return [[SQAParallelTemperingResult([State._view(fin[r, k]) for k in range(R)], finE[r].tolist(),

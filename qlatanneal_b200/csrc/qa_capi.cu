@@ -172,6 +172,7 @@ struct qa_ctx {
     int sms = 0;             // streaming multiprocessors of the device
     double drift_tol = 0.0;  // > 0: field-drift check after SA / SQA / SQA-PT runs
     int update_order = QA_ORDER_REFERENCE;  // SQA / SQA-PT sweep order (qa_set_update_order)
+    qa_tuning tune{0, -1, -1, 0, 0};        // launch-shape overrides (qa_set_tuning); all automatic
     // side streams for the rotated ring launches (run_rings_rotated) and their events
     std::vector<cudaStream_t> side;
     std::vector<cudaEvent_t> side_ev;
@@ -626,6 +627,7 @@ struct RingPlan {
 int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, int P, int n_max, RingPlan *pl,
                bool clusters = false, bool ref_order = false) {
     pl->W = std::max(1, std::min(32, (P + 1) / 2));
+    if (ctx->tune.warps_per_ring > 0) pl->W = std::max(1, std::min({32, P, ctx->tune.warps_per_ring}));
     pl->ref_order = ref_order;
     if (ref_order && n_max > (1 << 20))
         return fail(QA_ERR_ARG, "the shuffled update order supports at most 2^20 spins per model.");
@@ -635,7 +637,14 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
     if (pl->pm1) {
         const size_t cap = (size_t)ctx->smem_optin;
         const bool int32_only = std::getenv("QA_PM1_INT32_ONLY") != nullptr;
-        if (pm1_smem_bytes(P, n_max, 4, true, ref_order) <= cap) {
+        const int form = ctx->tune.field_form;
+        if (form == 0 && pm1_smem_bytes(P, n_max, 4, true, ref_order) <= cap) {
+            pl->gbytes = 4; pl->jw_smem = true;
+        } else if (form == 1 && !int32_only && pm1_smem_bytes(P, n_max, 2, true, ref_order) <= cap) {
+            pl->gbytes = 2; pl->jw_smem = true;
+        } else if (form == 2 && !int32_only && pm1_smem_bytes(P, n_max, 2, false, ref_order) <= cap) {
+            pl->gbytes = 2; pl->jw_smem = false;
+        } else if (pm1_smem_bytes(P, n_max, 4, true, ref_order) <= cap) {
             pl->gbytes = 4; pl->jw_smem = true;
         } else if (!int32_only && pm1_smem_bytes(P, n_max, 2, true, ref_order) <= cap) {
             pl->gbytes = 2; pl->jw_smem = true;
@@ -767,14 +776,22 @@ static int order_scratch(qa_ctx *ctx, const RingPlan &pl, int nr, int n_max, Rin
 struct RotPlan {
     int G, streams;
 };
-static RotPlan rot_plan(int nr) {
+static RotPlan rot_plan(qa_ctx *ctx, int nr) {
     RotPlan r;
     r.G = std::max(2, (nr + 127) / 128);
+    if (ctx->tune.rot_group > 0) r.G = std::max(ctx->tune.rot_group, (nr + 127) / 128);  // at most 128 streams
     r.streams = (nr + r.G - 1) / r.G;
     return r;
 }
+// Steps per rotated launch: the tuned length, else `auto_steps`.
+static int rot_seg(qa_ctx *ctx, int auto_steps, int range) {
+    const int s = ctx->tune.rot_steps > 0 ? ctx->tune.rot_steps : auto_steps;
+    return std::max(1, std::min(s, std::max(1, range)));
+}
 // SQA: launches of 25..100 steps (an eighth of the run)
-static int sqa_rot_seg(int steps) { return std::max(25, std::min(100, steps / 8)); }
+static int sqa_rot_seg(qa_ctx *ctx, int steps) {
+    return rot_seg(ctx, std::max(25, std::min(100, steps / 8)), steps);
+}
 
 // Whether nr rings are worth rotating: more rings than SMs, and whole-grid
 // launches would leave more than 3% of the resident slots idle.  With w the
@@ -784,7 +801,8 @@ static int sqa_rot_seg(int steps) { return std::max(25, std::min(100, steps / 8)
 // balance gains (an 8-instance sparse set of 8192 rings ran 1.7% slower).
 // QA_WHOLE_GRID set: never (one launch over all rings per segment).
 static bool rotation_pays(qa_ctx *ctx, int kind, const RingPlan &pl, int nr) {
-    if (nr <= ctx->sms || std::getenv("QA_WHOLE_GRID")) return false;
+    if (nr <= ctx->sms || std::getenv("QA_WHOLE_GRID") || ctx->tune.rotate == 0) return false;
+    if (ctx->tune.rotate == 1) return true;
     const int threads = 32 * pl.W;
     const void *kern = nullptr;
     if (pl.pm1)
@@ -839,7 +857,7 @@ static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const Ri
                              int s_end, int seg, int *launches) {
     if (rp.tr_bits || rp.tr_E || rp.tr_end_bits || rp.tr_end_E || rp.ring_spin)
         return fail(QA_ERR_ARG, "rotated ring launches carry no sweep traces");
-    const RotPlan rt = rot_plan(nr);
+    const RotPlan rt = rot_plan(ctx, nr);
     while ((int)ctx->side.size() < rt.streams) {
         cudaStream_t x;
         cudaEvent_t e;
@@ -1319,6 +1337,25 @@ int qa_set_drift_check(qa_ctx *ctx, double tolerance) {
     return QA_OK;
 }
 
+int qa_set_tuning(qa_ctx *ctx, const qa_tuning *t) {
+    if (!ctx) return fail(QA_ERR_ARG, "null context");
+    if (!t) {
+        ctx->tune = qa_tuning{0, -1, -1, 0, 0};
+        return QA_OK;
+    }
+    if (t->warps_per_ring < 0 || t->warps_per_ring > 32 || t->field_form < -1 || t->field_form > 2 ||
+        t->rotate < -1 || t->rotate > 1 || t->rot_steps < 0 || t->rot_group < 0)
+        return fail(QA_ERR_ARG, "qa_set_tuning: a field out of range.");
+    ctx->tune = *t;
+    return QA_OK;
+}
+
+int qa_get_tuning(const qa_ctx *ctx, qa_tuning *t) {
+    if (!ctx || !t) return fail(QA_ERR_ARG, "null argument");
+    *t = ctx->tune;
+    return QA_OK;
+}
+
 int qa_set_update_order(qa_ctx *ctx, int order) {
     if (!ctx) return fail(QA_ERR_ARG, "null context");
     if (order != QA_ORDER_REFERENCE && order != QA_ORDER_CHECKERBOARD)
@@ -1710,7 +1747,7 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     // those stay whole)
     if (!traces && steps >= 200 && rotation_pays(ctx, kind, pl, nr)) {
         rp.init_fields = 1;
-        QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, 0, steps, sqa_rot_seg(steps), &n_seg));
+        QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, 0, steps, sqa_rot_seg(ctx, steps), &n_seg));
     } else {
         for (int s0 = 0; s0 < steps; s0 += seg) {
             rp.step0 = s0;
@@ -2043,7 +2080,8 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
             rp.bsamp = bsamp;
             rp.bstride = bstride;
             int nl = 0;
-            QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, std::max(1, (s1 - s0) / 8), &nl));
+            QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, rot_seg(ctx, std::max(1, (s1 - s0) / 8), s1 - s0),
+                                         &nl));
             fresh = false;
             n_launch += nl;
             return QA_OK;
@@ -2463,7 +2501,8 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
         // of an eighth of it (at least one step), joined before the swaps
         if ((long long)(s1 - s0) * (rp.spb + rp.wls + rp.cls) >= 8 && rotate) {
             int nl = 0;
-            QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, std::max(1, (s1 - s0) / 8), &nl));
+            QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, rot_seg(ctx, std::max(1, (s1 - s0) / 8), s1 - s0),
+                                         &nl));
             n_launch += nl;
         } else {
             QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
@@ -2749,7 +2788,8 @@ int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_probl
             // at least 8 sweeps, joined before the swaps
             if (rotate && (long long)(s1 - s0) * (rp.spb + rp.wls + rp.cls) >= 8) {
                 int nl = 0;
-                QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, std::max(1, (s1 - s0) / 8), &nl));
+                QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, rot_seg(ctx, std::max(1, (s1 - s0) / 8), s1 - s0),
+                                         &nl));
                 n_launch += nl;
             } else {
                 QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
@@ -3239,7 +3279,8 @@ int qa_chi_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problems, c
     // leave slots idle and the anneal has at least 200 sweeps
     if ((long long)steps * rp.spb >= 200 && rotation_pays(ctx, kind, pl, nr)) {
         rp.init_fields = 1;
-        QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, 0, steps, std::max(1, steps / 8), &n_seg));
+        QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, 0, steps, rot_seg(ctx, std::max(1, steps / 8), steps),
+                                 &n_seg));
     } else {
         for (int s0 = 0; s0 < steps; s0 += 256) {
             rp.step0 = s0;
