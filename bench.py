@@ -385,6 +385,8 @@ def run_side(args, w):
         return 0
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
+    import qlatanneal_b200 as qa
+    qa.set_update_order(args.order, device=0)
     spec = _side_spec(w)
     model = _side_build(w, spec)
     ann, call, _, _ = _side_annealer(w, model)
@@ -425,7 +427,8 @@ def run_side(args, w):
                        "l2": "flushed (256 MiB write) between steps",
                        "slice_accept_rate": st.slice_accepts / max(1, st.slice_attempts),
                        "worldline_accept_rate": st.worldline_accepts / max(1, st.worldline_attempts),
-                       "sweep_ms_per_step": sum(x.sweep_ms for x in stats) / args.steps},
+                       "sweep_ms_per_step": sum(x.sweep_ms for x in stats) / args.steps,
+                       "update_order": args.order},
             "e2e": {"value": sites * len(e2e) / sum(e2e), "unit": "site-attempts/s",
                     "ms_per_step": 1e3 * float(np.mean(e2e))},
             "cpu_baseline": cpu, "gpu_launches": int(sum(x.launches for x in stats)), "clocks": clk.summary()}
@@ -586,6 +589,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--order", default="reference", choices=["reference", "checkerboard"],
+                    help="SQA / SQA-PT update order (reference: qanneal's, the default)")
     ap.add_argument("--reads", type=int, default=WL["reads"],
                     help="sqa: reads per GPU (at most the SM count: one whole-grid launch per segment)")
     ap.add_argument("--workload", default="sqa", choices=["sqa", "chi-ttt"] + sorted(SIDE),
@@ -620,6 +625,7 @@ def main():
     from qlatanneal_b200 import _lib
     from qlatanneal_b200.distributed import minloc_best, read_block
     _lib.Engine.get(local)
+    qa.set_update_order(args.order, device=local)
 
     n, P, reads = WL["n"], WL["P"], args.reads
     if reads < 1:
@@ -722,7 +728,7 @@ def main():
                        "trotter_slices": P, "reads_per_gpu": reads,
                        "steps": WL["steps"], "sweeps_per_step": [WL["spb"], WL["wls"]],
                        "site_attempts_per_step": sites_step, "l2": "flushed (256 MiB write) between steps",
-                       "parallelism": f"replicas x{world}", "best_energy": best_E,
+                       "parallelism": f"replicas x{world}", "best_energy": best_E, "update_order": args.order,
                        "slice_accept_rate": st.slice_accepts / max(1, st.slice_attempts),
                        "worldline_accept_rate": st.worldline_accepts / max(1, st.worldline_attempts)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
