@@ -563,6 +563,76 @@ def run_chi_ttt(args):
     return 0
 
 
+def run_chi_pilot(args):
+    """The SQA-Chi pilot scan at the learned-schedule training size: dense SK
+    n = 2048 (J = +-1), P = 64, 64 scan points of 50 burn + 200 sweeps, one
+    read per instance, ``--chi-instances`` instances in one call.  Every scan
+    point starts a fresh ring, so the initial fields H = J.S of every cell
+    (DenseIsing::compute_local_fields, dense_ising.cpp:64-83) are built
+    64 times per read: timed with the tensor-core init (tcgen05 int8) and with
+    the float64 init (QA_DISABLE_TC_INIT), the rest of the call unchanged."""
+    import ctypes as Cc
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    import qlatanneal_b200 as qa
+    from qlatanneal_b200 import _lib
+    from qlatanneal_b200.instances import sk_dense
+    c = CHI
+    n, P, pts = c["n_max"], c["P"], c["points"]
+    models = [qa.DenseIsing(*sk_dense(n, 500 + k)) for k in range(args.chi_instances)]
+    eng = _lib.Engine.get(0)
+    probs = (Cc.c_void_p * len(models))(*[m._device_problem(eng) for m in models])
+    prm = _lib.qa_chi_params(P, 1, c["beta"], c["gamma0"], c["gamma1"], 2, 1, pts, c["sweeps"], c["burn"], 1e-6, 0.0,
+                             0.3, 0.1, 1, 7, None)
+    out = np.zeros(len(models) * pts)
+
+    def call():
+        st = _lib.qa_stats()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _lib.check(eng.L.qa_chi_pilot(eng.h, probs, len(models), Cc.byref(prm), out.ctypes.data, Cc.byref(st)))
+        return time.perf_counter() - t0, st
+
+    res = {}
+    with Clocks(0) as clk:
+        for mode in ("tensor_core", "float64", "tensor_core"):
+            if mode == "float64":
+                os.environ["QA_DISABLE_TC_INIT"] = "1"
+            else:
+                os.environ.pop("QA_DISABLE_TC_INIT", None)
+            for _ in range(max(1, args.warmup)):
+                call()
+            runs = [call() for _ in range(max(1, args.steps))]
+            curve = out.copy()
+            res.setdefault(mode, []).append(dict(wall_s=float(np.median([r[0] for r in runs])),
+                                                 total_ms=float(np.median([r[1].total_ms for r in runs])),
+                                                 sweep_ms=float(np.median([r[1].sweep_ms for r in runs]))))
+            res.setdefault(mode + "_curve", curve)
+    os.environ.pop("QA_DISABLE_TC_INIT", None)
+    same = bool(np.array_equal(res["tensor_core_curve"], res["float64_curve"]))
+    tc, f64 = res["tensor_core"][-1], res["float64"][0]
+    cells = len(models) * pts * P
+    line = {
+        "metric": "SQA-Chi pilot scan time (ms), tensor-core vs float64 initial fields",
+        "value": tc["total_ms"], "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+        "float64_init_value": f64["total_ms"], "speedup": f64["total_ms"] / tc["total_ms"],
+        "init_share_float64": (f64["total_ms"] - f64["sweep_ms"]) / f64["total_ms"],
+        "init_share_tensor_core": (tc["total_ms"] - tc["sweep_ms"]) / tc["total_ms"],
+        "init_tflop_per_call": 2.0 * n * n * cells / 1e12, "curves_identical": same,
+        "dtype": "int8 x int8 -> int32 (tensor cores)", "data": "synthetic",
+        "config": {"workload": f"SQA-Chi pilot, dense SK n={n} J=+-1, P={P}, {pts} scan points x ({c['burn']} burn "
+                               f"+ {c['sweeps']}) sweeps, 1 read, {len(models)} instances in one call",
+                   "cells_per_call": cells},
+        "runs": {k: v for k, v in res.items() if not k.endswith("_curve")},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def measure_l2_peak(lib, device):
     """L2 read bandwidth (GB/s) of this device: the best of three L2-resident
     buffer sizes, each read 200 times (qa_probe_l2_read), outside any timed region."""
@@ -593,7 +663,7 @@ def main():
                     help="SQA / SQA-PT update order (reference: qanneal's, the default)")
     ap.add_argument("--reads", type=int, default=WL["reads"],
                     help="sqa: reads per GPU (at most the SM count: one whole-grid launch per segment)")
-    ap.add_argument("--workload", default="sqa", choices=["sqa", "chi-ttt"] + sorted(SIDE),
+    ap.add_argument("--workload", default="sqa", choices=["sqa", "chi-ttt", "chi-pilot"] + sorted(SIDE),
                     help="sqa: the sweep-throughput line (default); chi-ttt: time-to-target of SQA-Chi with the "
                          "learned vs the pilot-scan schedule, training set included; " + "; ".join(
                              f"{k}: {v['desc']}" for k, v in sorted(SIDE.items())))
@@ -606,6 +676,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "chi-ttt":
         return run_chi_ttt(args)
+    if args.workload == "chi-pilot":
+        return run_chi_pilot(args)
     if args.workload in SIDE:
         return run_side(args, SIDE[args.workload])
 
