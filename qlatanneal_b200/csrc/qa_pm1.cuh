@@ -180,30 +180,44 @@ __device__ __forceinline__ void pm1_flip_spins(uint32_t *St, GT *Gt, const uint3
 
 // One block of 32 visiting positions of slice t in qanneal's order: lane =
 // position (q << 5) | lane, spin ord[position]; rw is the position's Philox
-// word.  The spin's own and Trotter neighbours' bits (slices tp, tn) come
-// from its worldline word: while slice t holds the block no other slice
-// touches these spins (the pipeline), so slice tp shows this sweep's state and
-// slice tn the last sweep's.  Flips are resolved in position order.
+// word.  What does not depend on slice t - 1 -- the spin, its h, its own
+// field, the uniform -- is loaded before the wait for slice t - 1 to finish
+// the block; the spin's own and Trotter neighbours' bits (slices tp, tn) come
+// from its worldline word, read after it.  While slice t holds the block no
+// other slice touches these spins (the pipeline), so slice tp shows this
+// sweep's state and slice tn the last sweep's.  Flips are resolved in
+// position order; the block is published to slice t + 1 as soon as its bits
+// are final (the worldline atomics), before the slice's own field update,
+// which slice t + 1 never reads.
 template <typename GT>
 __device__ __forceinline__ void pm1_block_ord(const uint32_t *Jw, uint32_t *St, GT *Gt, unsigned long long *Wc,
                                               const float *h, const int *ord, int n, int npad, int q, int t, int tp,
                                               int tn, uint32_t rw, float B, float T4, int lane,
-                                              unsigned long long &acc) {
+                                              unsigned long long &acc, const int *prog_prev, int *prog_mine,
+                                              int *abortf, unsigned long long *err) {
     const int pos = (q << 5) | lane;
     const bool valid = pos < n;
     const int i = valid ? ord[pos] : 0;
+    const float u = u24(rw);
+    const float hi = h[i];
+    const int gi = (int)Gt[i];
+    const float hg = __fadd_rn(hi, __int2float_rn(gi));
+    if (prog_prev) wait_at_least(prog_prev, q + 1, abortf, err, lane);
     const unsigned long long wc = Wc[i];
     const uint32_t sbit = (uint32_t)(wc >> t) & 1u;
     const int d = (int)(((uint32_t)(wc >> tp) & 1u) ^ sbit) + (int)(((uint32_t)(wc >> tn) & 1u) ^ sbit);
     const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
-    const float u = u24(rw);
-    const float hi = h[i];
-    const int gi = (int)Gt[i];
-    const float y = __fsub_rn(__fmul_rn(signed_by_bit(__fadd_rn(hi, __int2float_rn(gi)), sbit), B), tro);
-    if (!__any_sync(FULL, valid & metropolis_maybe24(y, u))) return;
+    const float y = __fsub_rn(__fmul_rn(signed_by_bit(hg, sbit), B), tro);
+    if (!__any_sync(FULL, valid & metropolis_maybe24(y, u))) {
+        if (lane == 0) st_release_cta(prog_mine, q + 1);
+        return;
+    }
     bool ok = valid & metropolis_nb24(y, u);
     uint32_t m = __ballot_sync(FULL, ok);
-    if (m == 0) return;
+    if (m == 0) {
+        if (lane == 0) st_release_cta(prog_mine, q + 1);
+        return;
+    }
     // gk: this lane's field with the block's earlier flips applied,
     // g_i += -2 J_i,j s_j(old) for each flipped spin j
     uint32_t F = 0;
@@ -220,8 +234,10 @@ __device__ __forceinline__ void pm1_block_ord(const uint32_t *Jw, uint32_t *St, 
         m = __ballot_sync(FULL, ok) & pending;
         ++acc;
     } while (m);
-    // bit t of each flipped spin's worldline (32-bit atomic on the half that holds it)
+    // bit t of each flipped spin's worldline (32-bit atomic on the half that
+    // holds it), then the block is final for slice t + 1
     if ((F >> lane) & 1u) atomicXor(reinterpret_cast<uint32_t *>(Wc + i) + (t >> 5), 1u << (t & 31));
+    publish_count(prog_mine, q + 1, lane);
     pm1_flip_spins(St, Gt, Jw, npad, n, F, i, lane);
 }
 
@@ -372,12 +388,10 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
                             const int q = q4 + k;
-                            if (q < nw) {
-                                if (t > 0) wait_at_least(prog + t - 1, q + 1, abortf, p.counters + 4, lane);
+                            if (q < nw)
                                 pm1_block_ord(Jw, St, Gt, Wc, h, ord, n, npad, q, t, tp, tn, pick(r, k), B, T4, lane,
-                                              acc_s);
-                                publish_count(prog + t, q + 1, lane);
-                            }
+                                              acc_s, t > 0 ? prog + t - 1 : nullptr, prog + t, abortf,
+                                              p.counters + 4);
                         }
                     }
                 }
