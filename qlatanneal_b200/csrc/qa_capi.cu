@@ -223,7 +223,7 @@ namespace {
 enum WsSlot { W_PROBS, W_RINGS, W_SPINS, W_FIELDS, W_A, W_T4, W_SUM, W_BESTE, W_BESTSTEP, W_BITS, W_CNT, W_EXACT,
               W_PROBOF, W_MIN, W_BOND, W_MAG, W_SLOT, W_RIN, W_BSLOT, W_FBITS, W_AVG, W_SWP, W_BPJP, W_JP,
               W_BSAMP, W_SSAVE, W_FSAVE, W_CBESTE, W_CBSTEP, W_CBITS, W_CBOND, W_FLAG, W_QSTAGE,
-              W_TRB, W_TRE, W_TREB, W_TREE, W_RSPIN, W_DRIFT, W_ORDER, W_COUNT };
+              W_TRB, W_TRE, W_TREB, W_TREE, W_RSPIN, W_DRIFT, W_ORDER, W_OSCR, W_COUNT };
 static_assert(W_COUNT <= qa_ctx::kWsSlots, "qa_ctx::ws has a slot per WsSlot");
 
 int ws_get(qa_ctx *ctx, int slot, size_t bytes, void **out) {
@@ -614,7 +614,8 @@ struct RingPlan {
     int gbytes = 4;       // pm1: bytes per field (4 int32, 2 int16)
     bool jw_smem = true;  // pm1: J bits in shared memory
     bool ref_order = false;  // qanneal's update order (else the parity checkerboard)
-    bool order_global = false;  // ring_kernel: the order's scratch in global memory (too large for shared)
+    bool order_global = false;  // ring_kernel: order rows read in global memory (too large for shared)
+    int n_max = 0;        // largest model of the batch
     int W = 1;
     size_t smem = 0;
     int smem_fields = 1;
@@ -629,8 +630,9 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
     pl->W = std::max(1, std::min(32, (P + 1) / 2));
     if (ctx->tune.warps_per_ring > 0) pl->W = std::max(1, std::min({32, P, ctx->tune.warps_per_ring}));
     pl->ref_order = ref_order;
-    if (ref_order && n_max > (1 << 20))
-        return fail(QA_ERR_ARG, "the shuffled update order supports at most 2^20 spins per model.");
+    pl->n_max = n_max;
+    if (ref_order && n_max > QA_ORDER_MAX_N)
+        return fail(QA_ERR_ARG, "the shuffled update order supports at most 65536 spins per model.");
     // cluster moves are in ring_kernel only
     pl->pm1 = !clusters && kind == K_DENSE && P <= 64 && n_max <= 2048 && !std::getenv("QA_DISABLE_PM1");
     for (int p = 0; p < np && pl->pm1; ++p) pl->pm1 = probs[p]->dev.Jw != nullptr;
@@ -669,8 +671,8 @@ int plan_rings(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, in
         pl->smem_fields = 0;
         return QA_OK;
     }
-    // fields in shared memory where they fit (up to 200 KB), the order's
-    // scratch too, else the order's scratch in global memory first
+    // fields in shared memory where they fit (up to 200 KB), the order rows
+    // too, else the order rows read in global memory first
     const size_t fcap = (size_t)std::min(ctx->smem_optin, 200 * 1024), cap = (size_t)ctx->smem_optin;
     bool placed = false;
     for (int form = 0; form < 4 && !placed; ++form) {
@@ -715,12 +717,90 @@ static int opt_in_smem(qa_ctx *ctx, const void *kern, size_t smem) {
     return QA_OK;
 }
 
+// qanneal's order: the ring kernels take the visiting orders of their sweeps
+// from rows that order_fill_kernel writes before each launch.  Rows a step:
+// the slice, cluster (ring_kernel only) and worldline sweeps.  All rows of a
+// run's rings for the steps of one launch live in the W_ORDER workspace, at
+// most kOrderBudget bytes: longer whole-grid launches are split into chunks of
+// steps, rotated runs shorten their launches.
+constexpr size_t kOrderBudget = (size_t)256 << 20;
+
+static int ord_rows_per_step(const RingPlan &pl, const RingParams &rp) {
+    return rp.spb + (pl.pm1 || pl.sparse ? 0 : rp.cls) + rp.wls;
+}
+
+// Steps of one launch whose rows for nr rings fit the budget.
+static int ord_chunk_steps(const RingPlan &pl, const RingParams &rp, int nr, int steps) {
+    const size_t per = (size_t)ord_rows_per_step(pl, rp) * ord_row_bytes(pl.n_max) * (size_t)std::max(nr, 1);
+    const size_t fit = per ? kOrderBudget / per : (size_t)steps;
+    return (int)std::max<size_t>(1, std::min<size_t>(fit, (size_t)std::max(steps, 1)));
+}
+
+// The rows buffer of nr rings x `steps` steps into rp (ring b at b * ord_ring).
+static int ord_buffer(qa_ctx *ctx, const RingPlan &pl, RingParams *rp, int nr, int steps) {
+    rp->ord_per_step = ord_rows_per_step(pl, *rp);
+    rp->ord_stride = ord_row_entries(pl.n_max);
+    rp->ord_ring = (long long)std::max(steps, 1) * std::max(rp->ord_per_step, 1) * rp->ord_stride;
+    void *v;
+    QA_TRY(ws_get(ctx, W_ORDER, sizeof(OrdT) * (size_t)rp->ord_ring * (size_t)std::max(nr, 1), &v));
+    rp->ordg = static_cast<OrdT *>(v);
+    return QA_OK;
+}
+
+// The rows of one launch (rp.step0 .. rp.step1 of rings rp.rings[0 .. n_rings)).
+// The keys and counters of a row in shared memory where they fit, else in
+// the W_OSCR workspace (used only by launches on the context stream).
+static int fill_orders(qa_ctx *ctx, const RingPlan &pl, const RingParams &rp, int n_rings, cudaStream_t strm) {
+    const long long total = (long long)(rp.step1 - rp.step0) * rp.ord_per_step * n_rings;
+    if (total <= 0) return QA_OK;
+    const size_t need = order_fill_bytes(pl.n_max);
+    const int with_cls = pl.pm1 || pl.sparse ? 0 : 1;
+    if (need <= (size_t)ctx->smem_optin) {
+        const int grid = (int)std::min<long long>(total, (long long)ctx->sms * 8);
+        QA_TRY(opt_in_smem(ctx, (const void *)order_fill_kernel, need));
+        order_fill_kernel<<<grid, 256, need, strm>>>(rp, n_rings, with_cls, nullptr, 0);
+    } else {
+        if (strm != ctx->stream) return fail(QA_ERR_ARG, "order rows of this size need whole-grid launches");
+        const int grid = (int)std::min<long long>(total, (long long)ctx->sms);
+        void *v;
+        QA_TRY(ws_get(ctx, W_OSCR, need * (size_t)grid, &v));
+        order_fill_kernel<<<grid, 256, 0, strm>>>(rp, n_rings, with_cls, static_cast<unsigned char *>(v),
+                                                  (long long)need);
+    }
+    QA_CK(cudaGetLastError());
+    return QA_OK;
+}
+
 int launch_rings(qa_ctx *ctx, int kind, const RingPlan &pl, RingParams rp, int n_rings,
                  cudaStream_t stream = nullptr) {
     cudaStream_t strm = stream ? stream : ctx->stream;
     rp.W = pl.W;
     rp.smem_fields = pl.smem_fields;
     rp.ref_order = pl.ref_order ? 1 : 0;
+    rp.ord_in_smem = pl.order_global ? 0 : 1;
+    if (pl.ref_order && !rp.ordg) {
+        // a whole-grid launch (context stream): the rows of chunks of steps,
+        // each chunk's launch after its rows
+        const int steps = rp.step1 - rp.step0, chunk = ord_chunk_steps(pl, rp, n_rings, steps);
+        QA_TRY(ord_buffer(ctx, pl, &rp, n_rings, std::min(chunk, std::max(steps, 1))));
+        for (int c0 = rp.step0; c0 < rp.step1 || c0 == rp.step0; c0 += chunk) {
+            RingParams r2 = rp;
+            r2.step0 = c0;
+            r2.step1 = std::min(rp.step1, c0 + chunk);
+            if (c0 > rp.step0) {
+                r2.init_fields = 0;
+                r2.init_scan = 0;
+                if (r2.bsamp) r2.bsamp += (size_t)(c0 - rp.step0) * (rp.spb + rp.cls);
+            }
+            QA_TRY(launch_rings(ctx, kind, pl, r2, n_rings, strm));  // fills r2's rows first
+            if (r2.step1 >= rp.step1) break;
+        }
+        return QA_OK;
+    }
+    if (pl.ref_order) {
+        rp.ord_per_step = ord_rows_per_step(pl, rp);
+        QA_TRY(fill_orders(ctx, pl, rp, n_rings, strm));
+    }
     if (pl.pm1) {
         auto kern = pl.gbytes == 4 ? ring_pm1_kernel<int, true>
                                    : (pl.jw_smem ? ring_pm1_kernel<short, true> : ring_pm1_kernel<short, false>);
@@ -757,20 +837,6 @@ int ws_array(qa_ctx *ctx, int slot, size_t count, T **out) {
     return QA_OK;
 }
 
-// The global-memory scratch of the order builds when the plan put it there:
-// one region per ring (rotated launches offset it by their first ring).
-static int order_scratch(qa_ctx *ctx, const RingPlan &pl, int nr, int n_max, RingParams *rp) {
-    rp->oscratch = nullptr;
-    rp->oscratch_bytes = 0;
-    if (!pl.order_global) return QA_OK;
-    const size_t per = ring_order_scratch_bytes(n_max);
-    void *v;
-    QA_TRY(ws_get(ctx, W_ORDER, per * (size_t)nr, &v));
-    rp->oscratch = static_cast<unsigned char *>(v);
-    rp->oscratch_bytes = (long long)per;
-    return QA_OK;
-}
-
 // Ring groups of a rotated run (run_rings_rotated): groups of G rings, one
 // stream each, at most 128 streams.
 struct RotPlan {
@@ -802,6 +868,8 @@ static int sqa_rot_seg(qa_ctx *ctx, int steps) {
 // QA_WHOLE_GRID set: never (one launch over all rings per segment).
 static bool rotation_pays(qa_ctx *ctx, int kind, const RingPlan &pl, int nr) {
     if (nr <= ctx->sms || std::getenv("QA_WHOLE_GRID") || ctx->tune.rotate == 0) return false;
+    // order rows whose keys do not fit in shared memory are filled on the context stream only
+    if (pl.ref_order && order_fill_bytes(pl.n_max) > (size_t)ctx->smem_optin) return false;
     if (ctx->tune.rotate == 1) return true;
     const int threads = 32 * pl.W;
     const void *kern = nullptr;
@@ -838,7 +906,7 @@ static RingParams ring_offset(RingParams r, int g0) {
     if (r.ring_bond) r.ring_bond += (size_t)g0 * r.rec_stride;
     if (r.mag) r.mag += (size_t)g0 * r.steps_total * r.spb;
     if (r.bsamp) r.bsamp += (size_t)g0 * r.bstride;
-    if (r.oscratch) r.oscratch += (size_t)g0 * r.oscratch_bytes;
+    if (r.ordg) r.ordg += (size_t)g0 * r.ord_ring;
     return r;
 }
 
@@ -858,6 +926,12 @@ static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const Ri
     if (rp.tr_bits || rp.tr_E || rp.tr_end_bits || rp.tr_end_E || rp.ring_spin)
         return fail(QA_ERR_ARG, "rotated ring launches carry no sweep traces");
     const RotPlan rt = rot_plan(ctx, nr);
+    RingParams base = rp;
+    if (pl.ref_order) {
+        // every ring's rows of one launch; shorter launches where they would not fit
+        seg = std::min(seg, ord_chunk_steps(pl, rp, nr, seg));
+        QA_TRY(ord_buffer(ctx, pl, &base, nr, seg));
+    }
     while ((int)ctx->side.size() < rt.streams) {
         cudaStream_t x;
         cudaEvent_t e;
@@ -872,7 +946,7 @@ static int run_rings_rotated(qa_ctx *ctx, int kind, const RingPlan &pl, const Ri
     int n = 0, rc = QA_OK;
     for (int s0 = s_begin; s0 < s_end && rc == QA_OK; s0 += seg) {  // segment-major issue keeps the streams in step
         for (int k = 0; k < rt.streams; ++k) {
-            RingParams r2 = ring_offset(rp, k * rt.G);
+            RingParams r2 = ring_offset(base, k * rt.G);
             if (r2.bsamp) r2.bsamp += (size_t)(s0 - s_begin) * (rp.spb + rp.cls);  // indexed from step0
             r2.step0 = s0;
             r2.step1 = std::min(s_end, s0 + seg);
@@ -1727,7 +1801,6 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields(),
                       problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
-    QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_beta; rp.wls = prm->worldline_sweeps;
     rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.B = d_A; rp.T4 = d_T4; rp.per_slot_sched = 0;
@@ -2060,7 +2133,6 @@ int qa_sqa_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_problem
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
                       !pl.own_fields(), problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
-    QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = S; rp.spb = spb; rp.wls = wls; rp.cls = cls;
     rp.slice_tag = DOM_SLICE; rp.slot = nullptr; rp.B = d_A; rp.T4 = d_T4; rp.JP = d_JP; rp.per_slot_sched = 0;
@@ -2476,7 +2548,6 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT, !pl.own_fields(),
                       problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
-    QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = steps; rp.spb = prm->sweeps_per_step; rp.wls = prm->worldline_sweeps;
     rp.slice_tag = DOM_SLICE; rp.slot = d_slot; rp.B = d_B; rp.T4 = d_T4; rp.per_slot_sched = 1;
@@ -2685,7 +2756,6 @@ int qa_sqapt_opt_run(qa_ctx *ctx, const qa_problem *const *problems, int n_probl
     QA_TRY(init_state(ctx, kind, d_probs, d_rings, nr, d_spins, d_fields, P, n_max, L.nw_max, DOM_INIT,
                       !pl.own_fields(), problems, n_problems, &L, d_cnt + 4));
     RingParams rp{};
-    QA_TRY(order_scratch(ctx, pl, nr, n_max, &rp));
     rp.probs = d_probs; rp.rings = d_rings; rp.spins = d_spins; rp.fields = d_fields;
     rp.P = P; rp.steps_total = S; rp.spb = spb; rp.wls = wls; rp.cls = cls;
     rp.slice_tag = DOM_SLICE; rp.slot = d_slot; rp.B = d_B; rp.T4 = d_T4; rp.JP = d_JP;

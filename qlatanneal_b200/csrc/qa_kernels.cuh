@@ -57,8 +57,11 @@ struct RingParams {
     int smem_fields;
     int ref_order;        // 1: qanneal's order (a random spin order per sweep, slices in turn); 0: parity
                           //    checkerboard, spins ascending (the SQA-Chi kernel's order)
-    unsigned char *oscratch;   // ring_kernel, qanneal's order, when shared memory cannot hold it: the order's
-    long long oscratch_bytes;  //   keys, bucket counters and order, oscratch_bytes per CTA (else null)
+    OrdT *ordg;           // qanneal's order: the visiting orders of this launch's sweeps, written by
+    long long ord_ring;   //   order_fill_kernel before it.  Ring b's rows start at ordg + b * ord_ring;
+    int ord_stride;       //   row (s - step0) * ord_per_step + k holds the k-th ordered sweep of step s
+    int ord_per_step;     //   (slice sweeps, cluster sweeps where the kernel has them, worldline sweeps)
+    int ord_in_smem;      // ring_kernel: rows copied into shared memory (else read from ordg)
     int init_fields;      // ring_pm1_kernel: build the int32 fields from the spins first
     int init_scan;        // score the starting state as "step -1" before step0 (PT)
     int rec_base;         // per-step records live at [ring][rec_base + step]
@@ -206,7 +209,7 @@ __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int 
 // in slice t + 1 while slice t holds the block.
 template <int KIND>
 __device__ __forceinline__ void sweep_slice_ord(const ProbDev &Pd, uint32_t *S, int NP, int t, float *gt,
-                                                const float *h, const int *ord, int *prog, int *abortf,
+                                                const float *h, const OrdT *ord, int *prog, int *abortf,
                                                 unsigned long long *err, float B, float T4, uint64_t key,
                                                 uint32_t rng_cell, uint32_t sigma, uint32_t tag, int lane,
                                                 unsigned long long &att, unsigned long long &acc) {
@@ -381,10 +384,10 @@ struct RingSmem {
     double *wl_G;
     int *flag;
     float *g;
-    // qanneal's order: keys and bucket counters of the order build, the
-    // visiting order, the slices' progress counters, the wait-abort flag
-    unsigned long long *okeys;
-    int *ocnt, *ord, *prog, *abortf;
+    // qanneal's order: the two order rows in shared memory (null: read
+    // from global memory), the slices' progress counters, the wait-abort flag
+    OrdT *obuf[2];
+    int *prog, *abortf;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -418,16 +421,50 @@ __device__ __forceinline__ void record_bond_sample(const RingParams &p, const ui
         p.bsamp[(long long)blockIdx.x * p.bstride + (long long)(step - p.step0) * (p.spb + p.cls) + j] = tb;
 }
 
-// The order build's keys, bucket counters and the order itself (shared or global memory).
-__host__ __device__ inline size_t ring_order_scratch_bytes(int n) {
-    return order_keys_bytes(n) + order_cnt_bytes(n) + order_idx_bytes(n);
+// qanneal's order in shared memory: two order rows unless they are read from
+// global memory, plus the slices' progress counters and the abort flag.
+__host__ __device__ inline size_t ring_order_bytes(int P, int n, bool rows_in_smem = true) {
+    return (rows_in_smem ? 2 * ord_row_bytes(n) : 0) + align_up((size_t)P * 4, 16) + 16;
 }
 
-// qanneal's order in shared memory: the scratch above unless it lives in
-// global memory, plus the slices' progress counters and the abort flag.
-__host__ __device__ inline size_t ring_order_bytes(int P, int n, bool scratch_in_smem = true) {
-    return (scratch_in_smem ? ring_order_scratch_bytes(n) : 0) + align_up((size_t)P * 4, 16) + 16;
+// qanneal's order for a launch, run before it on its stream: row k of step s
+// of ring b is the visiting order of the k-th ordered sweep of that step (its
+// slice sweeps, cluster sweeps when with_cls, worldline sweeps), keyed like
+// the sweep (ring key, slot, sweep index, domain tag).  One CTA per row
+// (grid-stride loop); the keys and bucket counters in shared memory, or in
+// `scratch` (scratch_bytes per CTA) when they do not fit.
+static __global__ void __launch_bounds__(256) order_fill_kernel(RingParams p, int n_rings, int with_cls,
+                                                         unsigned char *scratch, long long scratch_bytes) {
+    extern __shared__ __align__(16) unsigned char osm[];
+    const int per = p.ord_per_step, cl = with_cls ? p.cls : 0;
+    const long long per_ring = (long long)(p.step1 - p.step0) * per, total = per_ring * n_rings;
+    unsigned char *base = scratch ? scratch + (long long)blockIdx.x * scratch_bytes : osm;
+    for (long long o = blockIdx.x; o < total; o += gridDim.x) {
+        const int b = (int)(o / per_ring);
+        const long long rem = o - (long long)b * per_ring;
+        const int step = p.step0 + (int)(rem / per), k = (int)(rem % per);
+        const RingDev R = p.rings[b];
+        const int n = p.probs[R.prob].n;
+        const int slot = p.slot ? p.slot[b] : R.k;
+        uint32_t tag, sigma;
+        if (k < p.spb) {
+            tag = p.slice_tag | R.tag_extra;
+            sigma = (uint32_t)(step * p.spb + k);
+        } else if (k < p.spb + cl) {
+            tag = DOM_CSPIN;
+            sigma = (uint32_t)(step * p.cls + (k - p.spb));
+        } else {
+            tag = DOM_WORLD;
+            sigma = (uint32_t)(step * p.wls + (k - p.spb - cl));
+        }
+        build_sweep_order(R.key, (uint32_t)slot, sigma, tag, n, reinterpret_cast<unsigned long long *>(base),
+                          reinterpret_cast<int *>(base + order_keys_bytes(n)),
+                          p.ordg + (long long)b * p.ord_ring + rem * p.ord_stride);
+    }
 }
+
+// Shared or scratch bytes of one order_fill_kernel CTA.
+__host__ __device__ inline size_t order_fill_bytes(int n) { return order_keys_bytes(n) + order_cnt_bytes(n); }
 
 __host__ __device__ inline size_t ring_smem_bytes(int P, int n, int W, bool fields, bool ref_order = false,
                                                  bool order_in_smem = true) {
@@ -556,12 +593,12 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     sm.wl_sh = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)W * 32 * 4, 16);
     sm.wl_G = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)W * 32 * 8, 16);
     sm.flag = reinterpret_cast<int *>(ptr); ptr += 16;
+    sm.obuf[0] = sm.obuf[1] = nullptr;
     if (p.ref_order) {
-        unsigned char *q = p.oscratch ? p.oscratch + (long long)blockIdx.x * p.oscratch_bytes : ptr;
-        sm.okeys = reinterpret_cast<unsigned long long *>(q); q += order_keys_bytes(n);
-        sm.ocnt = reinterpret_cast<int *>(q); q += order_cnt_bytes(n);
-        sm.ord = reinterpret_cast<int *>(q); q += order_idx_bytes(n);
-        if (!p.oscratch) ptr = q;
+        if (p.ord_in_smem) {
+            sm.obuf[0] = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(n);
+            sm.obuf[1] = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(n);
+        }
         sm.prog = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)NP * 4, 16);
         sm.abortf = reinterpret_cast<int *>(ptr); ptr += 16;
         if (threadIdx.x == 0) *sm.abortf = 0;
@@ -575,6 +612,8 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
     __syncthreads();
 
     const int slot = p.slot ? p.slot[blockIdx.x] : R.k;
+    OrderFeed feed = feed_open(sm.obuf[0], sm.obuf[1], p.ref_order ? p.ordg + blockIdx.x * p.ord_ring : nullptr,
+                               p.ord_stride, n, p.ref_order ? (p.step1 - p.step0) * p.ord_per_step : 0);
     unsigned long long att_s = 0, acc_s = 0, att_w = 0, acc_w = 0;
     double bestE = p.best_E[blockIdx.x];
     int bestStep = p.best_step[blockIdx.x];
@@ -603,9 +642,9 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
             if (p.ref_order) {
                 const uint32_t tag = p.slice_tag | R.tag_extra;
                 for (int t = threadIdx.x; t < NP; t += blockDim.x) sm.prog[t] = 0;
-                build_sweep_order(R.key, (uint32_t)slot, sigma, tag, n, sm.okeys, sm.ocnt, sm.ord);
+                const OrdT *ord = feed_take(feed);
                 for (int t = warp; t < NP; t += W)
-                    sweep_slice_ord<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, sm.ord, sm.prog,
+                    sweep_slice_ord<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, ord, sm.prog,
                                           sm.abortf, p.counters + 4, B, T4, R.key, (uint32_t)(slot * NP + t), sigma,
                                           tag, lane, att_s, acc_s);
                 __syncthreads();
@@ -642,11 +681,11 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
         const int cls = step >= 0 ? p.cls : 0;
         for (int sw = 0; sw < cls; ++sw) {
             const uint32_t sigma = (uint32_t)(step * p.cls + sw);
-            if (p.ref_order) build_sweep_order(R.key, (uint32_t)slot, sigma, DOM_CSPIN, n, sm.okeys, sm.ocnt, sm.ord);
+            const OrdT *cord = p.ref_order ? feed_take(feed) : nullptr;
             if (warp == 0) {
                 const float JPv = p.JP[si_tab];
                 for (int pos = 0; pos < n; ++pos)
-                    cluster_move<KIND>(Pd, sm.S, gbase, sm.h, NP, p.ref_order ? sm.ord[pos] : pos, (uint32_t)slot,
+                    cluster_move<KIND>(Pd, sm.S, gbase, sm.h, NP, p.ref_order ? (int)cord[pos] : pos, (uint32_t)slot,
                                        sigma, B, T4, JPv, R.key, lane);
             }
             __syncthreads();
@@ -657,14 +696,14 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
             // visiting position (q << 5) | lane holds spin ord[position]
             // (qanneal's order) or spin position (ascending)
-            if (p.ref_order) build_sweep_order(R.key, (uint32_t)slot, sigma, DOM_WORLD, n, sm.okeys, sm.ocnt, sm.ord);
+            const OrdT *word = p.ref_order ? feed_take(feed) : nullptr;
             U4 rnd = {0, 0, 0, 0};
             for (int q = 0; q < nw; ++q) {
                 if ((q & 3) == 0)
                     rnd = philox((uint32_t)(((q >> 2) << 5) | lane), (uint32_t)slot, sigma, DOM_WORLD, R.key);
                 const int pos = (q << 5) | lane;
                 const bool valid = pos < n;
-                const int i = !valid ? 0 : (p.ref_order ? sm.ord[pos] : pos);
+                const int i = !valid ? 0 : (p.ref_order ? (int)word[pos] : pos);
                 const float u = u24(pick(rnd, q & 3));
                 const float hi = valid ? sm.h[i] : 0.0f;
                 if (threadIdx.x == 0) att_w += (unsigned long long)min(32, n - (q << 5));

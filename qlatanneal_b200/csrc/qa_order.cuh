@@ -42,35 +42,37 @@ __host__ __device__ inline size_t order_keys_bytes(int n) { return ord_align16((
 __host__ __device__ inline size_t order_cnt_bytes(int n) { return ord_align16((size_t)4 << order_nb_log2(n)); }
 __host__ __device__ inline size_t order_idx_bytes(int n) { return ord_align16((size_t)n * 4); }
 
+// A visiting order's entries: spins < 2^16.
+typedef uint16_t OrdT;
+constexpr int QA_ORDER_MAX_N = 1 << 16;
+
 // A bounded wait gives up after this many polls (about a second with the
 // back-off), records QA_DEV_ERR_TIMEOUT and stops every later wait of the CTA.
 constexpr int QA_WAIT_LIMIT = 1 << 23;
 constexpr unsigned long long QA_DEV_ERR_TIMEOUT = 1ull;
 
 // The visiting order of one sweep: order[p] = the spin visited p-th.  Whole
-// CTA; ends with a barrier.  keys: [even(n)] scratch, cnt: [2^order_nb_log2(n)]
-// scratch, order: [n].
+// CTA; ends with a barrier.  keys: [n] scratch, cnt: [2^order_nb_log2(n)]
+// scratch, order: [n] (shared or global memory).
+//  1. every key is drawn and counted in its bucket (top bits of the key);
+//  2. one warp turns the counts into bucket starts;
+//  3. the keys are drawn again and scattered into their buckets;
+//  4. each key's position is its bucket's start plus the number of smaller
+//     keys in its bucket (about four), written as the spin (the key's low
+//     bits).
 __device__ __forceinline__ void build_sweep_order(uint64_t key, uint32_t ring, uint32_t sigma, uint32_t tag, int n,
-                                                  unsigned long long *keys, int *cnt, int *order) {
+                                                  unsigned long long *keys, int *cnt, OrdT *order) {
     const int nbl = order_nb_log2(n), NB = 1 << nbl;
     const int tid = threadIdx.x, T = blockDim.x;
-    for (int b = tid; b < NB; b += T) cnt[b] = 0;
-    __syncthreads();
     const uint32_t c3 = (tag << 8) | (uint32_t)DOM_PERM;
     const int npairs = (n + 1) >> 1;
+    auto bucket = [&](unsigned long long k) { return nbl ? (int)(k >> (64 - nbl)) : 0; };
+    for (int b = tid; b < NB; b += T) cnt[b] = 0;
+    __syncthreads();
     for (int j = tid; j < npairs; j += T) {
         const U4 r = philox((uint32_t)j, ring, sigma, c3, key);
-        const int i0 = 2 * j, i1 = i0 + 1;
-        const unsigned long long k0 =
-            ((((unsigned long long)r.x << 32) | r.y) & ~0xFFFFFull) | (unsigned long long)i0;
-        keys[i0] = k0;
-        atomicAdd(cnt + (nbl ? (int)(k0 >> (64 - nbl)) : 0), 1);
-        if (i1 < n) {
-            const unsigned long long k1 =
-                ((((unsigned long long)r.z << 32) | r.w) & ~0xFFFFFull) | (unsigned long long)i1;
-            keys[i1] = k1;
-            atomicAdd(cnt + (nbl ? (int)(k1 >> (64 - nbl)) : 0), 1);
-        }
+        atomicAdd(cnt + bucket(((unsigned long long)r.x << 32) | r.y), 1);
+        if (2 * j + 1 < n) atomicAdd(cnt + bucket(((unsigned long long)r.z << 32) | r.w), 1);
     }
     __syncthreads();
     // exclusive prefix sum of the bucket counts, one warp: lane l owns a run of buckets
@@ -93,28 +95,79 @@ __device__ __forceinline__ void build_sweep_order(uint64_t key, uint32_t ring, u
         }
     }
     __syncthreads();
-    // scatter by bucket (within a bucket in arrival order: sorted next)
-    for (int i = tid; i < n; i += T) {
-        const unsigned long long k = keys[i];
-        const int pos = atomicAdd(cnt + (nbl ? (int)(k >> (64 - nbl)) : 0), 1);
-        order[pos] = i;
-    }
-    __syncthreads();
-    // cnt[b] now ends bucket b; put each bucket in key order
-    for (int b = tid; b < NB; b += T) {
-        const int s0 = b == 0 ? 0 : cnt[b - 1], s1 = cnt[b];
-        for (int x = s0 + 1; x < s1; ++x) {
-            const int v = order[x];
-            const unsigned long long kv = keys[v];
-            int y = x - 1;
-            while (y >= s0 && keys[order[y]] > kv) {
-                order[y + 1] = order[y];
-                --y;
-            }
-            order[y + 1] = v;
+    // scatter (cnt[b] ends as the end of bucket b)
+    for (int j = tid; j < npairs; j += T) {
+        const U4 r = philox((uint32_t)j, ring, sigma, c3, key);
+        const int i0 = 2 * j, i1 = i0 + 1;
+        const unsigned long long k0 =
+            ((((unsigned long long)r.x << 32) | r.y) & ~0xFFFFFull) | (unsigned long long)i0;
+        keys[atomicAdd(cnt + bucket(k0), 1)] = k0;
+        if (i1 < n) {
+            const unsigned long long k1 =
+                ((((unsigned long long)r.z << 32) | r.w) & ~0xFFFFFull) | (unsigned long long)i1;
+            keys[atomicAdd(cnt + bucket(k1), 1)] = k1;
         }
     }
     __syncthreads();
+    for (int x = tid; x < n; x += T) {
+        const unsigned long long kx = keys[x];
+        const int b = bucket(kx);
+        const int s0 = b == 0 ? 0 : cnt[b - 1], s1 = cnt[b];
+        int rank = 0;
+        for (int y = s0; y < s1; ++y) rank += keys[y] < kx;
+        order[s0 + rank] = (OrdT)(kx & 0xFFFFFull);
+    }
+    __syncthreads();
+}
+
+// The ring kernels take the orders of their sweeps from a buffer that
+// order_fill_kernel writes before each launch (the orders of every sweep of
+// the launch, one row of ord_row_entries(n) entries each): a sweep copies its
+// row into shared memory with 16-byte cp.async chunks while the previous sweep
+// runs.  Whole CTA; order_wait() and a barrier make the copy visible.
+__host__ __device__ inline int ord_row_entries(int n) { return (n + 7) & ~7; }
+__host__ __device__ inline size_t ord_row_bytes(int n) { return (size_t)ord_row_entries(n) * sizeof(OrdT); }
+
+__device__ __forceinline__ void order_fetch(OrdT *dst, const OrdT *src, int n) {
+    const int chunks = ord_row_entries(n) >> 3;
+    for (int c = threadIdx.x; c < chunks; c += blockDim.x)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst + 8 * c)),
+                     "l"(src + 8 * c)
+                     : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void order_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The order rows of one ring's sweeps, taken in the order the kernel sweeps.
+// With shared-memory buffers, row r is copied while row r - 1 is swept.
+struct OrderFeed {
+    OrdT *buf0, *buf1;  // shared memory (null: the rows are read in global memory)
+    const OrdT *g;      // the ring's first row
+    long long stride;   // entries per row
+    int n, rows, row;   // spins, rows of the launch, the next row
+};
+
+__device__ __forceinline__ OrderFeed feed_open(OrdT *buf0, OrdT *buf1, const OrdT *g, long long stride, int n,
+                                               int rows) {
+    OrderFeed f{buf0, buf1, g, stride, n, rows, 0};
+    if (buf0 && rows > 0) order_fetch(buf0, g, n);
+    return f;
+}
+
+// The next sweep's order.  Whole CTA; ends with a barrier after which every
+// thread sees the row (and whatever the CTA wrote before it); starts the copy
+// of the row after it into the buffer the previous sweep used.
+__device__ __forceinline__ const OrdT *feed_take(OrderFeed &f) {
+    const int r = min(f.row, max(f.rows - 1, 0));  // never past the launch's rows
+    ++f.row;
+    if (!f.buf0) {
+        __syncthreads();
+        return f.g + r * f.stride;
+    }
+    order_wait();
+    __syncthreads();
+    if (r + 1 < f.rows) order_fetch((r & 1) ? f.buf0 : f.buf1, f.g + (r + 1) * f.stride, f.n);
+    return (r & 1) ? f.buf1 : f.buf0;
 }
 
 // Pipeline counters: acquire / release accesses of a shared-memory word.

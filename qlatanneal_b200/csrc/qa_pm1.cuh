@@ -28,9 +28,8 @@ __host__ __device__ inline int pm1_npad(int n) { return (n + 127) / 128 * 128; }
 
 // Shared memory of one ring: gbytes = bytes per field (4: int32, 2: int16);
 // jw_smem = J bits staged in shared memory (else read through L1/L2);
-// ref_order = qanneal's update order (the visiting order of a sweep, its
-// bucket counters, the slices' progress counters and the flipped spins of a
-// worldline block; the order's keys reuse the worldline sums and uniforms).
+// ref_order = qanneal's update order (two rows of visiting orders, the
+// slices' progress counters and the flipped spins of a worldline block).
 __host__ __device__ inline size_t pm1_smem_bytes(int P, int n, int gbytes = 4, bool jw_smem = true,
                                                  bool ref_order = false) {
     const int nw = (n + 31) / 32, np = pm1_npad(n);
@@ -45,7 +44,7 @@ __host__ __device__ inline size_t pm1_smem_bytes(int P, int n, int gbytes = 4, b
     b += (size_t)(np / 32) * 4;                    // worldline move masks, one per block (np/32 >= nw)
     b += 32 * 8 + 32 * 4 + 64;                     // old worldlines, partials, flags
     if (ref_order)
-        b += order_idx_bytes(np) + order_cnt_bytes(n) + ord_align16((size_t)P * 4) + 16 + 32 * 4;
+        b += 2 * ord_row_bytes(np) + ord_align16((size_t)P * 4) + 16 + 32 * 4;
     return b + 64;
 }
 
@@ -191,7 +190,7 @@ __device__ __forceinline__ void pm1_flip_spins(uint32_t *St, GT *Gt, const uint3
 // which slice t + 1 never reads.
 template <typename GT>
 __device__ __forceinline__ void pm1_block_ord(const uint32_t *Jw, uint32_t *St, GT *Gt, unsigned long long *Wc,
-                                              const float *h, const int *ord, int n, int npad, int q, int t, int tp,
+                                              const float *h, const OrdT *ord, int n, int npad, int q, int t, int tp,
                                               int tn, uint32_t rw, float B, float T4, int lane,
                                               unsigned long long &acc, const int *prog_prev, int *prog_mine,
                                               int *abortf, unsigned long long *err) {
@@ -312,15 +311,14 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     unsigned long long *Wold = reinterpret_cast<unsigned long long *>(ptr); ptr += 32 * 8;
     int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
     int *flag = reinterpret_cast<int *>(ptr); ptr += 64;  // [1]: worldline block flips F, [2]: their block index
-    // qanneal's order: the visiting order of the current sweep, its bucket
-    // counters, the slices' progress counters, the wait-abort flag and the
-    // spins of a resolved worldline block; the order's keys use Gs and uw
-    // (8 npad bytes, free while the order is built)
-    int *ord = nullptr, *ocnt = nullptr, *prog = nullptr, *abortf = nullptr, *Wsp = nullptr;
-    unsigned long long *okeys = reinterpret_cast<unsigned long long *>(Gs);
+    // qanneal's order: two rows of visiting orders (the current sweep's and
+    // the next one's, copied in the background), the slices' progress
+    // counters, the wait-abort flag and the spins of a resolved worldline block
+    OrdT *ob0 = nullptr, *ob1 = nullptr;
+    int *prog = nullptr, *abortf = nullptr, *Wsp = nullptr;
     if (p.ref_order) {
-        ord = reinterpret_cast<int *>(ptr); ptr += order_idx_bytes(npad);
-        ocnt = reinterpret_cast<int *>(ptr); ptr += order_cnt_bytes(n);
+        ob0 = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(npad);
+        ob1 = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(npad);
         prog = reinterpret_cast<int *>(ptr); ptr += ord_align16((size_t)NP * 4);
         abortf = reinterpret_cast<int *>(ptr); ptr += 16;
         Wsp = reinterpret_cast<int *>(ptr);
@@ -360,6 +358,8 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
 
     const unsigned long long pmask = NP == 64 ? ~0ull : ((1ull << NP) - 1ull);
     const int slot = p.slot ? p.slot[blockIdx.x] : R.k;
+    OrderFeed feed = feed_open(ob0, ob1, p.ref_order ? p.ordg + blockIdx.x * p.ord_ring : nullptr, p.ord_stride, n,
+                               p.ref_order ? (p.step1 - p.step0) * p.ord_per_step : 0);
     unsigned long long att_s = 0, acc_s = 0, att_w = 0, acc_w = 0;
     double bestE = p.best_E[blockIdx.x];
     int bestStep = p.best_step[blockIdx.x];
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 // slice t takes block q once slice t - 1 has finished it
                 const uint32_t tag = p.slice_tag | R.tag_extra;
                 for (int t = threadIdx.x; t < NP; t += blockDim.x) prog[t] = 0;
-                build_sweep_order(R.key, (uint32_t)slot, sigma, tag, n, okeys, ocnt, ord);
+                const OrdT *ord = feed_take(feed);
                 for (int t = warp; t < NP; t += W) {
                     const int tp = t == 0 ? NP - 1 : t - 1, tn = t + 1 == NP ? 0 : t + 1;
                     uint32_t *St = S + t * nw;
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
             // qanneal's order: a fresh visiting order; slice sums by spin,
             // uniforms by visiting position
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
-            build_sweep_order(R.key, (uint32_t)slot, sigma, DOM_WORLD, n, okeys, ocnt, ord);
+            const OrdT *ord = feed_take(feed);
             for (int i = threadIdx.x; i < npad; i += blockDim.x) {
                 const int q = i >> 5;
                 int gs = 0;

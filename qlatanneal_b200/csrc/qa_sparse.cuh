@@ -22,11 +22,11 @@ __host__ __device__ inline size_t sparse_smem_bytes(int P, int n, bool ref_order
     b += (size_t)n32 * 8;                          // W (worldline bits)
     b += (size_t)n32 * 4;                          // h
     b += align_up((size_t)P * 8, 16);              // cellE
-    b += (size_t)n32 * (ref_order ? 8 : 4);        // worldline uniforms (qanneal's order: and the order's keys)
+    b += (size_t)n32 * 4;                          // worldline uniforms
     b += align_up((size_t)nw * 8, 16);             // worldline decisions per block, marks per spin
     b += 32 * 4 + 64;                              // partials, flags
-    if (ref_order)                                 // the visiting order, bucket and progress counters, abort flag
-        b += order_idx_bytes(n32) + order_cnt_bytes(n) + align_up((size_t)P * 4, 16) + 16;
+    if (ref_order)                                 // two order rows, progress counters, abort flag
+        b += 2 * ord_row_bytes(n32) + align_up((size_t)P * 4, 16) + 16;
     return b + 64;
 }
 
@@ -125,7 +125,7 @@ __device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, u
 // neighbours' bits come from the worldline words.  After a flip every later
 // lane of the block decides again on the current bits.
 __device__ __forceinline__ void sp_sweep_slice_ord(const ProbDev &Pd, uint32_t *S, unsigned long long *Wc,
-                                                   const float *h, const int *ord, int *prog, int *abortf,
+                                                   const float *h, const OrdT *ord, int *prog, int *abortf,
                                                    unsigned long long *err, int NP, int t, float B, float T4,
                                                    uint64_t key, uint32_t rng_cell, uint32_t sigma, uint32_t tag,
                                                    int lane, unsigned long long &att, unsigned long long &acc) {
@@ -181,19 +181,20 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
     unsigned long long *Wc = reinterpret_cast<unsigned long long *>(ptr); ptr += (size_t)n32 * 8;
     float *h = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * 4;
     double *cellE = reinterpret_cast<double *>(ptr); ptr += align_up((size_t)NP * 8, 16);
-    float *uw = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * (p.ref_order ? 8 : 4);
+    float *uw = reinterpret_cast<float *>(ptr); ptr += (size_t)n32 * 4;
     uint32_t *wmask = reinterpret_cast<uint32_t *>(ptr);  // [nw] decisions on the sweep's starting state
     uint32_t *wdirty = wmask + nw;                        // [nw] spins whose neighbours have flipped since
     ptr += align_up((size_t)nw * 8, 16);
     int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
     int *flag = reinterpret_cast<int *>(ptr); ptr += 64;  // [0]: best slice, [3]: lowest slice (final state)
-    // qanneal's order: the visiting order, its bucket counters, the slices'
-    // progress counters, the wait-abort flag; the order's keys use uw (8 n32 bytes)
-    unsigned long long *okeys = reinterpret_cast<unsigned long long *>(uw);
-    int *ord = nullptr, *ocnt = nullptr, *prog = nullptr, *abortf = nullptr;
+    // qanneal's order: two rows of visiting orders (the current sweep's and
+    // the next one's, copied in the background), the slices' progress
+    // counters, the wait-abort flag
+    OrdT *ob0 = nullptr, *ob1 = nullptr;
+    int *prog = nullptr, *abortf = nullptr;
     if (p.ref_order) {
-        ord = reinterpret_cast<int *>(ptr); ptr += order_idx_bytes(n32);
-        ocnt = reinterpret_cast<int *>(ptr); ptr += order_cnt_bytes(n);
+        ob0 = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(n32);
+        ob1 = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(n32);
         prog = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)NP * 4, 16);
         abortf = reinterpret_cast<int *>(ptr);
         if (threadIdx.x == 0) *abortf = 0;
@@ -212,6 +213,8 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
 
     const unsigned long long pmask = NP == 64 ? ~0ull : ((1ull << NP) - 1ull);
     const int slot = p.slot ? p.slot[blockIdx.x] : R.k;
+    OrderFeed feed = feed_open(ob0, ob1, p.ref_order ? p.ordg + blockIdx.x * p.ord_ring : nullptr, p.ord_stride, n,
+                               p.ref_order ? (p.step1 - p.step0) * p.ord_per_step : 0);
     unsigned long long att_s = 0, acc_s = 0, att_w = 0, acc_w = 0;
     double bestE = p.best_E[blockIdx.x];
     int bestStep = p.best_step[blockIdx.x];
@@ -226,7 +229,7 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
             if (p.ref_order) {
                 const uint32_t tag = p.slice_tag | R.tag_extra;
                 for (int t = threadIdx.x; t < NP; t += blockDim.x) prog[t] = 0;
-                build_sweep_order(R.key, (uint32_t)slot, sigma, tag, n, okeys, ocnt, ord);
+                const OrdT *ord = feed_take(feed);
                 for (int t = warp; t < NP; t += W)
                     sp_sweep_slice_ord(Pd, S, Wc, h, ord, prog, abortf, p.counters + 4, NP, t, B, T4, R.key,
                                        (uint32_t)(slot * NP + t), sigma, tag, lane, att_s, acc_s);
@@ -268,7 +271,7 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
             // qanneal's order: the same scheme over visiting positions; the
             // marks of flipped neighbours are kept per spin
             const uint32_t sigma = (uint32_t)(step * p.wls + sw);
-            build_sweep_order(R.key, (uint32_t)slot, sigma, DOM_WORLD, n, okeys, ocnt, ord);
+            const OrdT *ord = feed_take(feed);
             for (int pp = threadIdx.x; pp < n32; pp += blockDim.x) {  // a warp covers one block of positions
                 const int q = pp >> 5, l = pp & 31;
                 const U4 r = philox((uint32_t)(((q >> 2) << 5) | l), (uint32_t)slot, sigma, DOM_WORLD, R.key);
