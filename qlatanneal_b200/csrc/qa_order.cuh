@@ -184,35 +184,36 @@ __device__ __forceinline__ void st_release_cta(int *p, int v) {
                  : "memory");
 }
 
-// Whole warp: wait until *flag >= need.  Lane 0 polls (acquire) with a short
-// back-off and at most QA_WAIT_LIMIT polls; past that it sets *abort (shared,
-// so no later wait of the CTA spins) and the error word *err (global), and
-// the warp carries on: the run's outputs are then void and the host reports
-// QA_ERR_TIMEOUT.  The __syncwarp orders the other lanes' reads after the
-// acquire.
+// Whole warp: wait until *flag >= need.  Every lane polls (one broadcast
+// load a poll, so the warp stays converged and each lane's later reads are
+// ordered after its own acquire), with a short back-off and at most
+// QA_WAIT_LIMIT polls; past that lane 0 sets *abort (shared, so no later wait
+// of the CTA spins) and the error word *err (global), and the warp carries
+// on: the run's outputs are then void and the host reports QA_ERR_TIMEOUT.
 __device__ __forceinline__ void wait_at_least(const int *flag, int need, int *abort, unsigned long long *err,
                                               int lane) {
-    if (lane == 0 && ld_acquire_cta(flag) < need) {
-        int it = 0;
-        while (ld_acquire_cta(flag) < need) {
-            if (*(volatile int *)abort) break;
-            if (++it > QA_WAIT_LIMIT) {
+    if (ld_acquire_cta(flag) >= need) return;
+    for (int it = 0; ld_acquire_cta(flag) < need;) {
+        if (*(volatile int *)abort) break;
+        if (++it > QA_WAIT_LIMIT) {
+            if (lane == 0) {
                 *(volatile int *)abort = 1;
                 atomicExch(err, QA_DEV_ERR_TIMEOUT);
-                break;
             }
-            __nanosleep(40);
+            break;
         }
+        __nanosleep(40);
     }
-    __syncwarp();
 }
 
 // Whole warp, after the warp's writes of a finished block: every lane fences
-// its writes, lane 0 publishes the count (release).
+// its writes, the warp synchronises, and every lane stores the count (release;
+// the same value, one store instruction).
 __device__ __forceinline__ void publish_count(int *flag, int value, int lane) {
+    (void)lane;
     __threadfence_block();
     __syncwarp();
-    if (lane == 0) st_release_cta(flag, value);
+    st_release_cta(flag, value);
 }
 
 }  // namespace qa

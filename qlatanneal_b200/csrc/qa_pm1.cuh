@@ -208,13 +208,13 @@ __device__ __forceinline__ void pm1_block_ord(const uint32_t *Jw, uint32_t *St, 
     const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
     const float y = __fsub_rn(__fmul_rn(signed_by_bit(hg, sbit), B), tro);
     if (!__any_sync(FULL, valid & metropolis_maybe24(y, u))) {
-        if (lane == 0) st_release_cta(prog_mine, q + 1);
+        st_release_cta(prog_mine, q + 1);  // every lane: one store, no branch
         return;
     }
     bool ok = valid & metropolis_nb24(y, u);
     uint32_t m = __ballot_sync(FULL, ok);
     if (m == 0) {
-        if (lane == 0) st_release_cta(prog_mine, q + 1);
+        st_release_cta(prog_mine, q + 1);  // every lane: one store, no branch
         return;
     }
     // gk: this lane's field with the block's earlier flips applied,
