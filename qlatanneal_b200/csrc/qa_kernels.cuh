@@ -203,14 +203,14 @@ __device__ __forceinline__ void sweep_slice(const ProbDev &Pd, uint32_t *S, int 
 
 // Slice t of a ring in qanneal's order: visiting position p holds spin
 // ord[p]; the uniform belongs to the position.  Block q (positions
-// 32q .. 32q+31) waits until slice t - 1 has finished it (pipeline counters
-// prog) and publishes its own progress after.  The Trotter neighbours' bits
+// 32q .. 32q+31) waits until slice t - 1 has finished it (the slice
+// pipeline, pipe_wait) and publishes its own progress after.  The Trotter neighbours' bits
 // of the block's spins are final for this sweep in slice t - 1 and untouched
 // in slice t + 1 while slice t holds the block.
 template <int KIND>
 __device__ __forceinline__ void sweep_slice_ord(const ProbDev &Pd, uint32_t *S, int NP, int t, float *gt,
-                                                const float *h, const OrdT *ord, int *prog, int *abortf,
-                                                unsigned long long *err, float B, float T4, uint64_t key,
+                                                const float *h, const OrdT *ord, const SlicePipe &pp,
+                                                float B, float T4, uint64_t key,
                                                 uint32_t rng_cell, uint32_t sigma, uint32_t tag, int lane,
                                                 unsigned long long &att, unsigned long long &acc) {
     const int n = Pd.n, nw = Pd.nw;
@@ -223,7 +223,7 @@ __device__ __forceinline__ void sweep_slice_ord(const ProbDev &Pd, uint32_t *S, 
     att += (unsigned long long)n;
     for (int q = 0; q < nw; ++q) {
         if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), rng_cell, sigma, tag, key);
-        if (t > 0) wait_at_least(prog + t - 1, q + 1, abortf, err, lane);
+        if (t > 0) pipe_wait(pp, t - 1, q, lane);
         const int pos = (q << 5) | lane;
         const bool valid = pos < n;
         const int i = valid ? ord[pos] : 0;
@@ -250,7 +250,7 @@ __device__ __forceinline__ void sweep_slice_ord(const ProbDev &Pd, uint32_t *S, 
             ++acc;
             pending = j == 31 ? 0u : (FULL << (j + 1));
         }
-        publish_count(prog + t, q + 1, lane);
+        pipe_publish(pp, t, q, lane);
     }
 }
 
@@ -385,9 +385,9 @@ struct RingSmem {
     int *flag;
     float *g;
     // qanneal's order: the two order rows in shared memory (null: read
-    // from global memory), the slices' progress counters, the wait-abort flag
+    // from global memory), the slice pipeline
     OrdT *obuf[2];
-    int *prog, *abortf;
+    SlicePipe pipe;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -424,7 +424,7 @@ __device__ __forceinline__ void record_bond_sample(const RingParams &p, const ui
 // qanneal's order in shared memory: two order rows unless they are read from
 // global memory, plus the slices' progress counters and the abort flag.
 __host__ __device__ inline size_t ring_order_bytes(int P, int n, bool rows_in_smem = true) {
-    return (rows_in_smem ? 2 * ord_row_bytes(n) : 0) + align_up((size_t)P * 4, 16) + 16;
+    return (rows_in_smem ? 2 * ord_row_bytes(n) : 0) + pipe_bytes(P);
 }
 
 // qanneal's order for a launch, run before it on its stream: row k of step s
@@ -599,9 +599,7 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
             sm.obuf[0] = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(n);
             sm.obuf[1] = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(n);
         }
-        sm.prog = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)NP * 4, 16);
-        sm.abortf = reinterpret_cast<int *>(ptr); ptr += 16;
-        if (threadIdx.x == 0) *sm.abortf = 0;
+        sm.pipe = pipe_open(ptr, NP, p.counters + 4); ptr += pipe_bytes(NP);
     }
     float *gbase = p.smem_fields ? reinterpret_cast<float *>(ptr) : p.fields + R.field_off;
 
@@ -641,12 +639,11 @@ __global__ void __launch_bounds__(1024, 1) ring_kernel(RingParams p) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
             if (p.ref_order) {
                 const uint32_t tag = p.slice_tag | R.tag_extra;
-                for (int t = threadIdx.x; t < NP; t += blockDim.x) sm.prog[t] = 0;
+                pipe_reset(sm.pipe, NP);
                 const OrdT *ord = feed_take(feed);
                 for (int t = warp; t < NP; t += W)
-                    sweep_slice_ord<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, ord, sm.prog,
-                                          sm.abortf, p.counters + 4, B, T4, R.key, (uint32_t)(slot * NP + t), sigma,
-                                          tag, lane, att_s, acc_s);
+                    sweep_slice_ord<KIND>(Pd, sm.S, NP, t, gbase + (long long)t * n, sm.h, ord, sm.pipe, B, T4,
+                                          R.key, (uint32_t)(slot * NP + t), sigma, tag, lane, att_s, acc_s);
                 __syncthreads();
             } else {
                 for (int ph = 0; ph < 3; ++ph) {

@@ -17,8 +17,7 @@
 //    which is the full sort by K_i in O(n) work and five barriers;
 //  * the slices of a ring run concurrently in a pipeline: slice t takes a
 //    block of 32 visiting positions once slice t - 1 has finished that block
-//    (bounded waits on per-slice progress counters in shared memory).  A
-//    move of spin i in slice t then sees slice t - 1 after this sweep and
+//    (bounded waits on per-slice progress counters in shared memory).  A move of spin i in slice t then sees slice t - 1 after this sweep and
 //    slice t + 1 before it, exactly as the sequential loop does: the block's
 //    spins are touched by no other slice while slice t holds them.
 #pragma once
@@ -46,9 +45,9 @@ __host__ __device__ inline size_t order_idx_bytes(int n) { return ord_align16((s
 typedef uint16_t OrdT;
 constexpr int QA_ORDER_MAX_N = 1 << 16;
 
-// A bounded wait gives up after this many polls (about a second with the
-// back-off), records QA_DEV_ERR_TIMEOUT and stops every later wait of the CTA.
-constexpr int QA_WAIT_LIMIT = 1 << 23;
+// A bounded wait gives up after a second (device global timer), records
+// QA_DEV_ERR_TIMEOUT and stops every later wait of the CTA.
+constexpr unsigned long long QA_WAIT_NS = 1000000000ull;
 constexpr unsigned long long QA_DEV_ERR_TIMEOUT = 1ull;
 
 // The visiting order of one sweep: order[p] = the spin visited p-th.  Whole
@@ -184,21 +183,54 @@ __device__ __forceinline__ void st_release_cta(int *p, int v) {
                  : "memory");
 }
 
-// Whole warp: wait until *flag >= need.  Every lane polls (one broadcast
-// load a poll, so the warp stays converged and each lane's later reads are
-// ordered after its own acquire), with a short back-off and at most
-// QA_WAIT_LIMIT polls; past that lane 0 sets *abort (shared, so no later wait
-// of the CTA spins) and the error word *err (global), and the warp carries
-// on: the run's outputs are then void and the host reports QA_ERR_TIMEOUT.
-__device__ __forceinline__ void wait_at_least(const int *flag, int need, int *abort, unsigned long long *err,
-                                              int lane) {
-    if (ld_acquire_cta(flag) >= need) return;
-    for (int it = 0; ld_acquire_cta(flag) < need;) {
-        if (*(volatile int *)abort) break;
-        if (++it > QA_WAIT_LIMIT) {
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// The slice pipeline of one ring: prog[t] counts the blocks slice t has
+// finished in the current sweep.
+__host__ __device__ inline size_t pipe_bytes(int P) { return ord_align16((size_t)P * 4) + 16; }
+
+struct SlicePipe {
+    int *prog;                 // [P]
+    int *abortf;               // set when a wait ran out: later waits return at once
+    unsigned long long *err;   // the run's device error word
+};
+
+// Carve the pipeline out of pipe_bytes(P) bytes of shared memory at ptr and
+// initialise it (whole CTA; a barrier must follow before the first sweep).
+__device__ __forceinline__ SlicePipe pipe_open(unsigned char *ptr, int P, unsigned long long *err) {
+    SlicePipe pp;
+    pp.prog = reinterpret_cast<int *>(ptr);
+    pp.abortf = reinterpret_cast<int *>(ptr + ord_align16((size_t)P * 4));
+    pp.err = err;
+    if (threadIdx.x == 0) *pp.abortf = 0;
+    return pp;
+}
+
+// Before a sweep (whole CTA, ahead of the barrier that starts it).
+__device__ __forceinline__ void pipe_reset(const SlicePipe &pp, int P) {
+    for (int t = threadIdx.x; t < P; t += blockDim.x) pp.prog[t] = 0;
+}
+
+// Whole warp: wait until slice tp has finished block q.  Every lane polls
+// (one broadcast load a poll, so the warp stays converged and each lane's
+// later reads are ordered after its own acquire), with a short back-off.
+// Past QA_WAIT_NS lane 0 sets the abort flag (no later wait of the CTA spins)
+// and the error word, and the warp carries on: the run's outputs are then
+// void and the host reports QA_ERR_TIMEOUT.
+__device__ __forceinline__ void pipe_wait(const SlicePipe &pp, int tp, int q, int lane) {
+    const int need = q + 1;
+    if (ld_acquire_cta(pp.prog + tp) >= need) return;
+    const unsigned long long t0 = global_ns();
+    while (ld_acquire_cta(pp.prog + tp) < need) {
+        if (*(volatile int *)pp.abortf) break;
+        if (global_ns() - t0 > QA_WAIT_NS) {
             if (lane == 0) {
-                *(volatile int *)abort = 1;
-                atomicExch(err, QA_DEV_ERR_TIMEOUT);
+                *(volatile int *)pp.abortf = 1;
+                atomicExch(pp.err, QA_DEV_ERR_TIMEOUT);
             }
             break;
         }
@@ -206,14 +238,17 @@ __device__ __forceinline__ void wait_at_least(const int *flag, int need, int *ab
     }
 }
 
-// Whole warp, after the warp's writes of a finished block: every lane fences
-// its writes, the warp synchronises, and every lane stores the count (release;
-// the same value, one store instruction).
-__device__ __forceinline__ void publish_count(int *flag, int value, int lane) {
+// Whole warp, block q of slice t finished.  fenced: the warp wrote state a
+// later slice reads (every lane fences its writes and the warp synchronises
+// first).  Every lane stores the count (release; the same value, one store
+// instruction).
+__device__ __forceinline__ void pipe_publish(const SlicePipe &pp, int t, int q, int lane, bool fenced = true) {
     (void)lane;
-    __threadfence_block();
-    __syncwarp();
-    st_release_cta(flag, value);
+    if (fenced) {
+        __threadfence_block();
+        __syncwarp();
+    }
+    st_release_cta(pp.prog + t, q + 1);
 }
 
 }  // namespace qa

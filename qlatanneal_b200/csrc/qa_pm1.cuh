@@ -44,7 +44,7 @@ __host__ __device__ inline size_t pm1_smem_bytes(int P, int n, int gbytes = 4, b
     b += (size_t)(np / 32) * 4;                    // worldline move masks, one per block (np/32 >= nw)
     b += 32 * 8 + 32 * 4 + 64;                     // old worldlines, partials, flags
     if (ref_order)
-        b += 2 * ord_row_bytes(np) + ord_align16((size_t)P * 4) + 16 + 32 * 4;
+        b += 2 * ord_row_bytes(np) + pipe_bytes(P) + 32 * 4;
     return b + 64;
 }
 
@@ -182,18 +182,23 @@ __device__ __forceinline__ void pm1_flip_spins(uint32_t *St, GT *Gt, const uint3
 // word.  What does not depend on slice t - 1 -- the spin, its h, its own
 // field, the uniform -- is loaded before the wait for slice t - 1 to finish
 // the block; the spin's own and Trotter neighbours' bits (slices tp, tn) come
-// from its worldline word, read after it.  While slice t holds the block no
-// other slice touches these spins (the pipeline), so slice tp shows this
-// sweep's state and slice tn the last sweep's.  Flips are resolved in
-// position order; the block is published to slice t + 1 as soon as its bits
-// are final (the worldline atomics), before the slice's own field update,
-// which slice t + 1 never reads.
+// from its worldline word.  While slice t holds the block no other slice
+// touches these spins (the pipeline), so slice tp shows this sweep's state
+// and slice tn the last sweep's (slice 0's of this sweep for the last slice,
+// which therefore also waits for slice 0 to finish the block).
+// Before waiting for slice tp, the block is tried with both values of the one
+// bit slice tp may still change: if every lane rejects under either value
+// (the pre-test), the block has no flips whatever slice tp does, and it is
+// published at once.  Most blocks end there, so the slices stop waiting on one
+// another except where a Trotter neighbour can change a decision.  Flips are
+// resolved in position order; the block is published to slice t + 1 as soon
+// as its bits are final (the worldline atomics), before the slice's own field
+// update, which slice t + 1 never reads.
 template <typename GT>
 __device__ __forceinline__ void pm1_block_ord(const uint32_t *Jw, uint32_t *St, GT *Gt, unsigned long long *Wc,
                                               const float *h, const OrdT *ord, int n, int npad, int q, int t, int tp,
                                               int tn, uint32_t rw, float B, float T4, int lane,
-                                              unsigned long long &acc, const int *prog_prev, int *prog_mine,
-                                              int *abortf, unsigned long long *err) {
+                                              unsigned long long &acc, const SlicePipe &pp) {
     const int pos = (q << 5) | lane;
     const bool valid = pos < n;
     const int i = valid ? ord[pos] : 0;
@@ -201,20 +206,35 @@ __device__ __forceinline__ void pm1_block_ord(const uint32_t *Jw, uint32_t *St, 
     const float hi = h[i];
     const int gi = (int)Gt[i];
     const float hg = __fadd_rn(hi, __int2float_rn(gi));
-    if (prog_prev) wait_at_least(prog_prev, q + 1, abortf, err, lane);
+    if (t > 0) {
+        if (tn == 0) pipe_wait(pp, 0, q, lane);  // the last slice: slice 0 after this sweep
+        // bits t and tn are final; y with slice tp's bit equal to and
+        // differing from s, computed as the exact test below computes it
+        const unsigned long long w0 = Wc[i];
+        const uint32_t sb = (uint32_t)(w0 >> t) & 1u;
+        const int dn = (int)(((uint32_t)(w0 >> tn) & 1u) ^ sb);
+        const float xs = __fmul_rn(signed_by_bit(hg, sb), B);
+        const float ya = __fsub_rn(xs, __fmul_rn(__int2float_rn(1 - dn), T4));
+        const float yb = __fsub_rn(xs, __fmul_rn(__int2float_rn(-dn), T4));
+        if (!__any_sync(FULL, valid & (metropolis_maybe24(ya, u) | metropolis_maybe24(yb, u)))) {
+            pipe_publish(pp, t, q, lane, false);  // no flips in the block, nothing written
+            return;
+        }
+        pipe_wait(pp, t - 1, q, lane);
+    }
     const unsigned long long wc = Wc[i];
     const uint32_t sbit = (uint32_t)(wc >> t) & 1u;
     const int d = (int)(((uint32_t)(wc >> tp) & 1u) ^ sbit) + (int)(((uint32_t)(wc >> tn) & 1u) ^ sbit);
     const float tro = __fmul_rn(__int2float_rn(1 - d), T4);
     const float y = __fsub_rn(__fmul_rn(signed_by_bit(hg, sbit), B), tro);
     if (!__any_sync(FULL, valid & metropolis_maybe24(y, u))) {
-        st_release_cta(prog_mine, q + 1);  // every lane: one store, no branch
+        pipe_publish(pp, t, q, lane, false);  // nothing written
         return;
     }
     bool ok = valid & metropolis_nb24(y, u);
     uint32_t m = __ballot_sync(FULL, ok);
     if (m == 0) {
-        st_release_cta(prog_mine, q + 1);  // every lane: one store, no branch
+        pipe_publish(pp, t, q, lane, false);  // nothing written
         return;
     }
     // gk: this lane's field with the block's earlier flips applied,
@@ -236,7 +256,7 @@ __device__ __forceinline__ void pm1_block_ord(const uint32_t *Jw, uint32_t *St, 
     // bit t of each flipped spin's worldline (32-bit atomic on the half that
     // holds it), then the block is final for slice t + 1
     if ((F >> lane) & 1u) atomicXor(reinterpret_cast<uint32_t *>(Wc + i) + (t >> 5), 1u << (t & 31));
-    publish_count(prog_mine, q + 1, lane);
+    pipe_publish(pp, t, q, lane);
     pm1_flip_spins(St, Gt, Jw, npad, n, F, i, lane);
 }
 
@@ -315,14 +335,13 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
     // the next one's, copied in the background), the slices' progress
     // counters, the wait-abort flag and the spins of a resolved worldline block
     OrdT *ob0 = nullptr, *ob1 = nullptr;
-    int *prog = nullptr, *abortf = nullptr, *Wsp = nullptr;
+    int *Wsp = nullptr;
+    SlicePipe pp{};
     if (p.ref_order) {
         ob0 = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(npad);
         ob1 = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(npad);
-        prog = reinterpret_cast<int *>(ptr); ptr += ord_align16((size_t)NP * 4);
-        abortf = reinterpret_cast<int *>(ptr); ptr += 16;
+        pp = pipe_open(ptr, NP, p.counters + 4); ptr += pipe_bytes(NP);
         Wsp = reinterpret_cast<int *>(ptr);
-        if (threadIdx.x == 0) *abortf = 0;
     }
 
     if (JW_SMEM)
@@ -375,7 +394,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                 // one visiting order for the sweep; slices in turn, pipelined:
                 // slice t takes block q once slice t - 1 has finished it
                 const uint32_t tag = p.slice_tag | R.tag_extra;
-                for (int t = threadIdx.x; t < NP; t += blockDim.x) prog[t] = 0;
+                pipe_reset(pp, NP);
                 const OrdT *ord = feed_take(feed);
                 for (int t = warp; t < NP; t += W) {
                     const int tp = t == 0 ? NP - 1 : t - 1, tn = t + 1 == NP ? 0 : t + 1;
@@ -390,8 +409,7 @@ __global__ void __launch_bounds__(1024, 1) ring_pm1_kernel(RingParams p) {
                             const int q = q4 + k;
                             if (q < nw)
                                 pm1_block_ord(Jw, St, Gt, Wc, h, ord, n, npad, q, t, tp, tn, pick(r, k), B, T4, lane,
-                                              acc_s, t > 0 ? prog + t - 1 : nullptr, prog + t, abortf,
-                                              p.counters + 4);
+                                              acc_s, pp);
                         }
                     }
                 }

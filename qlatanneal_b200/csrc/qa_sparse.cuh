@@ -25,8 +25,8 @@ __host__ __device__ inline size_t sparse_smem_bytes(int P, int n, bool ref_order
     b += (size_t)n32 * 4;                          // worldline uniforms
     b += align_up((size_t)nw * 8, 16);             // worldline decisions per block, marks per spin
     b += 32 * 4 + 64;                              // partials, flags
-    if (ref_order)                                 // two order rows, progress counters, abort flag
-        b += 2 * ord_row_bytes(n32) + align_up((size_t)P * 4, 16) + 16;
+    if (ref_order)                                 // two order rows, the slice pipeline
+        b += 2 * ord_row_bytes(n32) + pipe_bytes(P);
     return b + 64;
 }
 
@@ -125,8 +125,8 @@ __device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, u
 // neighbours' bits come from the worldline words.  After a flip every later
 // lane of the block decides again on the current bits.
 __device__ __forceinline__ void sp_sweep_slice_ord(const ProbDev &Pd, uint32_t *S, unsigned long long *Wc,
-                                                   const float *h, const OrdT *ord, int *prog, int *abortf,
-                                                   unsigned long long *err, int NP, int t, float B, float T4,
+                                                   const float *h, const OrdT *ord, const SlicePipe &pp,
+                                                   int NP, int t, float B, float T4,
                                                    uint64_t key, uint32_t rng_cell, uint32_t sigma, uint32_t tag,
                                                    int lane, unsigned long long &att, unsigned long long &acc) {
     const int n = Pd.n, nw = Pd.nw;
@@ -136,7 +136,7 @@ __device__ __forceinline__ void sp_sweep_slice_ord(const ProbDev &Pd, uint32_t *
     att += (unsigned long long)n;
     for (int q = 0; q < nw; ++q) {
         if ((q & 3) == 0) rnd = philox((uint32_t)(((q >> 2) << 5) | lane), rng_cell, sigma, tag, key);
-        if (t > 0) wait_at_least(prog + t - 1, q + 1, abortf, err, lane);
+        if (t > 0) pipe_wait(pp, t - 1, q, lane);
         const int pos = (q << 5) | lane;
         const bool valid = pos < n;
         const int i = valid ? ord[pos] : 0;
@@ -166,7 +166,7 @@ __device__ __forceinline__ void sp_sweep_slice_ord(const ProbDev &Pd, uint32_t *
             m = (m & ~pending) | (__ballot_sync(FULL, again) & pending);
             __syncwarp();
         }
-        publish_count(prog + t, q + 1, lane);
+        pipe_publish(pp, t, q, lane);
     }
 }
 
@@ -188,16 +188,13 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
     int *wpart = reinterpret_cast<int *>(ptr); ptr += 32 * 4;
     int *flag = reinterpret_cast<int *>(ptr); ptr += 64;  // [0]: best slice, [3]: lowest slice (final state)
     // qanneal's order: two rows of visiting orders (the current sweep's and
-    // the next one's, copied in the background), the slices' progress
-    // counters, the wait-abort flag
+    // the next one's, copied in the background), the slice pipeline
     OrdT *ob0 = nullptr, *ob1 = nullptr;
-    int *prog = nullptr, *abortf = nullptr;
+    SlicePipe pp{};
     if (p.ref_order) {
         ob0 = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(n32);
         ob1 = reinterpret_cast<OrdT *>(ptr); ptr += ord_row_bytes(n32);
-        prog = reinterpret_cast<int *>(ptr); ptr += align_up((size_t)NP * 4, 16);
-        abortf = reinterpret_cast<int *>(ptr);
-        if (threadIdx.x == 0) *abortf = 0;
+        pp = pipe_open(ptr, NP, p.counters + 4);
     }
 
     for (int idx = threadIdx.x; idx < NP * nw; idx += blockDim.x) S[idx] = p.spins[R.spin_off + idx];
@@ -228,11 +225,11 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
             const uint32_t sigma = (uint32_t)(step * p.spb + sw);
             if (p.ref_order) {
                 const uint32_t tag = p.slice_tag | R.tag_extra;
-                for (int t = threadIdx.x; t < NP; t += blockDim.x) prog[t] = 0;
+                pipe_reset(pp, NP);
                 const OrdT *ord = feed_take(feed);
                 for (int t = warp; t < NP; t += W)
-                    sp_sweep_slice_ord(Pd, S, Wc, h, ord, prog, abortf, p.counters + 4, NP, t, B, T4, R.key,
-                                       (uint32_t)(slot * NP + t), sigma, tag, lane, att_s, acc_s);
+                    sp_sweep_slice_ord(Pd, S, Wc, h, ord, pp, NP, t, B, T4, R.key, (uint32_t)(slot * NP + t), sigma,
+                                       tag, lane, att_s, acc_s);
                 __syncthreads();
             } else {
                 for (int ph = 0; ph < 3; ++ph) {
