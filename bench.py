@@ -768,7 +768,8 @@ def main():
     launches = stats[0].sweep_launches
     sweep_ms_step = sweep_ms / args.steps
     achieved = bytes_step / (sweep_ms_step / 1e3) / 1e9
-    traffic = load_traffic() if reads == WL["reads"] else None
+    # the committed capture is of this workload in qanneal's order (its launches read the order rows)
+    traffic = load_traffic() if reads == WL["reads"] and args.order == "reference" else None
     l2_peak = measure_l2_peak(_lib, local)
 
     # best energy over all ranks (the MINLOC + broadcast of qanneal's MPI reads helper)
