@@ -1271,6 +1271,25 @@ int qa_problem_sparse(qa_ctx *ctx, int n, const double *h, int m, const int64_t 
         spcv.resize(col.size());
         for (size_t e = 0; e < col.size(); ++e) spcv[e] = make_int2(col[e], (int)val[e]);
     }
+    // the same rows as 16-byte records where every row fits one: at most 4
+    // neighbours, values in [-127, 127], columns below 65536
+    bool slab = integer && n < 65536;
+    for (int i = 0; i < n && slab; ++i) {
+        slab = rowptr[i + 1] - rowptr[i] <= 4;
+        for (int e = rowptr[i]; e < rowptr[i + 1] && slab; ++e) slab = std::fabs((double)val[e]) <= 127.0;
+    }
+    std::vector<uint4> spslab;
+    if (slab) {
+        spslab.assign(n, make_uint4(0u, 0u, 0u, 0u));
+        for (int i = 0; i < n; ++i) {
+            uint32_t c4[4] = {0u, 0u, 0u, 0u}, v4 = 0u;
+            for (int e = rowptr[i], k = 0; e < rowptr[i + 1]; ++e, ++k) {
+                c4[k] = (uint32_t)col[e];
+                v4 |= ((uint32_t)(int)val[e] & 0xFFu) << (8 * k);
+            }
+            spslab[i] = make_uint4(c4[0] | (c4[1] << 16), c4[2] | (c4[3] << 16), v4, 0u);
+        }
+    }
     std::vector<int> e_i(m), e_j(m);
     for (int e = 0; e < m; ++e) { e_i[e] = (int)ei[e]; e_j[e] = (int)ej[e]; }
     qa_problem *P = new qa_problem();
@@ -1288,6 +1307,7 @@ int qa_problem_sparse(qa_ctx *ctx, int n, const double *h, int m, const int64_t 
     if (rc == QA_OK) rc = upload(P, e_j.data(), e_j.size(), &P->dev.ej);
     if (rc == QA_OK) rc = upload(P, w, (size_t)m, &P->dev.ew);
     if (rc == QA_OK && integer) rc = upload(P, spcv.data(), spcv.size(), &P->dev.spcv);
+    if (rc == QA_OK && slab) rc = upload(P, spslab.data(), spslab.size(), &P->dev.spslab);
     if (rc != QA_OK) {
         qa_problem_free(P);
         return rc;

@@ -160,6 +160,11 @@ struct ProbDev {
     const int4 *trec;
     // sparse with integer couplings: CSR (column, value) pairs; else null
     const int2 *spcv;
+    // sparse with integer couplings in [-127, 127], at most 4 neighbours a
+    // spin and n < 65536: spin i's row in one 16-byte record {c0 | c1 << 16,
+    // c2 | c3 << 16, int8 values v0 .. v3, 0} (unused entries: column 0,
+    // value 0), the same neighbours and values as its CSR row; else null
+    const uint4 *spslab;
 };
 
 __device__ __forceinline__ int spin_of(const uint32_t *S, int i) { return ((S[i >> 5] >> (i & 31)) & 1u) ? 1 : -1; }

@@ -30,25 +30,49 @@ __host__ __device__ inline size_t sparse_smem_bytes(int P, int n, bool ref_order
     return b + 64;
 }
 
-// Local field of spin i in slice St (its spin bits), from the CSR row.
-__device__ __forceinline__ int sp_field(const int2 *cv, const int *rowptr, const uint32_t *St, int i) {
-    const int e0 = __ldg(rowptr + i), e1 = __ldg(rowptr + i + 1);
+// Neighbour k (0..3) of a slab record: column and value.
+__device__ __forceinline__ int slab_col(const uint4 &r, int k) {
+    return (int)(((k < 2 ? r.x : r.y) >> (16 * (k & 1))) & 0xFFFFu);
+}
+__device__ __forceinline__ int slab_val(const uint4 &r, int k) { return (int)(signed char)(r.z >> (8 * k)); }
+
+// Local field of spin i in slice St (its spin bits): from the spin's slab
+// record where the model has one (one 16-byte load), else its CSR row.  The
+// sum of the same integers either way.
+__device__ __forceinline__ int sp_field(const ProbDev &Pd, const uint32_t *St, int i) {
     int g = 0;
+    if (Pd.spslab) {
+        const uint4 r = __ldg(Pd.spslab + i);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int c = slab_col(r, k), v = slab_val(r, k);
+            g += ((St[c >> 5] >> (c & 31)) & 1u) ? v : -v;
+        }
+        return g;
+    }
+    const int e0 = __ldg(Pd.rowptr + i), e1 = __ldg(Pd.rowptr + i + 1);
     for (int e = e0; e < e1; ++e) {
-        const int2 c = __ldg(cv + e);
+        const int2 c = __ldg(Pd.spcv + e);
         g += ((St[c.x >> 5] >> (c.x & 31)) & 1u) ? c.y : -c.y;
     }
     return g;
 }
 
 // Slice sum over the worldlines: sum_t s_t,i g_t,i.
-__device__ __forceinline__ int sp_world_sum(const int2 *cv, const int *rowptr, const unsigned long long *Wc,
+__device__ __forceinline__ int sp_world_sum(const ProbDev &Pd, const unsigned long long *Wc,
                                             unsigned long long pmask, int NP, int i) {
-    const int e0 = __ldg(rowptr + i), e1 = __ldg(rowptr + i + 1);
     const unsigned long long wi = Wc[i];
     int g = 0;
+    if (Pd.spslab) {
+        const uint4 r = __ldg(Pd.spslab + i);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            g += slab_val(r, k) * (NP - 2 * __popcll((wi ^ Wc[slab_col(r, k)]) & pmask));
+        return g;
+    }
+    const int e0 = __ldg(Pd.rowptr + i), e1 = __ldg(Pd.rowptr + i + 1);
     for (int e = e0; e < e1; ++e) {
-        const int2 c = __ldg(cv + e);
+        const int2 c = __ldg(Pd.spcv + e);
         g += c.y * (NP - 2 * __popcll((wi ^ Wc[c.x]) & pmask));
     }
     return g;
@@ -59,7 +83,7 @@ __device__ __forceinline__ int sp_world_sum(const int2 *cv, const int *rowptr, c
 __device__ __forceinline__ bool sp_world_ok(const ProbDev &Pd, const unsigned long long *Wc, const float *h,
                                             unsigned long long pmask, int NP, int i, float B, float u) {
     const int sh = 2 * __popcll(Wc[i] & pmask) - NP;
-    const int gs = sp_world_sum(Pd.spcv, Pd.rowptr, Wc, pmask, NP, i);
+    const int gs = sp_world_sum(Pd, Wc, pmask, NP, i);
     const float x = __double2float_rn(__dadd_rn(__dmul_rn((double)h[i], (double)sh), (double)gs));
     return metropolis_nb24(__fmul_rn(x, B), u);
 }
@@ -89,7 +113,7 @@ __device__ __forceinline__ void sp_sweep_slice(const ProbDev &Pd, uint32_t *S, u
         // evaluated again (later blocks read their fields from the current
         // bits anyway), so every decision is the spin-at-a-time sweep's
         auto decide = [&]() {
-            const int g = valid ? sp_field(Pd.spcv, Pd.rowptr, St, i) : 0;
+            const int g = valid ? sp_field(Pd, St, i) : 0;
             const float loc = __fadd_rn(hi, __int2float_rn(g));
             return valid & metropolis_nb24(__fsub_rn(__fmul_rn(signed_by_bit(loc, sbit), B), tro), u);
         };
@@ -147,7 +171,7 @@ __device__ __forceinline__ void sp_sweep_slice_ord(const ProbDev &Pd, uint32_t *
         const float u = u24(pick(rnd, q & 3));
         const float hi = h[i];
         auto decide = [&]() {
-            const int g = valid ? sp_field(Pd.spcv, Pd.rowptr, St, i) : 0;
+            const int g = valid ? sp_field(Pd, St, i) : 0;
             const float loc = __fadd_rn(hi, __int2float_rn(g));
             return valid & metropolis_nb24(__fsub_rn(__fmul_rn(signed_by_bit(loc, sbit), B), tro), u);
         };
@@ -388,7 +412,7 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
             for (int i = lane; i < n; i += 32) {
                 const bool up = (St[i >> 5] >> (i & 31)) & 1u;
                 ph = __dadd_rn(ph, up ? (double)h[i] : -(double)h[i]);
-                const int g = sp_field(Pd.spcv, Pd.rowptr, St, i);
+                const int g = sp_field(Pd, St, i);
                 pg += up ? g : -g;
             }
             ph = warp_sum_d(ph);

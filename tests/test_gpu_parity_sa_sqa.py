@@ -47,6 +47,14 @@ def make(kind, n, seed):
     if kind == "sparse":
         h, e = regular3(n, seed)
         return qa.SparseIsing(h, e, n, -2.0)
+    if kind == "sparse_deg6":
+        # rows of up to six neighbours, couplings in {-2, -1, 1, 2}: integer
+        # couplings whose rows do not fit the 16-byte neighbour records, so the
+        # on-demand-field kernel reads its CSR rows
+        h, e1 = regular3(n, seed)
+        _, e2 = regular3(n, seed + 1)
+        rng = np.random.default_rng(seed + 5)
+        return qa.SparseIsing(h, [(a, b, w * float(rng.choice([1.0, 2.0]))) for a, b, w in e1 + e2], n, 0.0)
     if kind == "sparse_real":
         h, e = regular3(n, seed)
         rng = np.random.default_rng(seed + 3)
@@ -126,6 +134,7 @@ SQA_CASES = [
     ("sparse", 64, 7, 2, 2, 1, 1.0),
     ("sparse", 2048, 16, 1, 1, 2, 0.5),  # integer couplings: on-demand fields
     ("sparse", 150, 64, 1, 1, 1, 1.0),
+    ("sparse_deg6", 96, 8, 1, 1, 1, 1.0),  # integer couplings in CSR rows
     ("sparse_real", 96, 6, 1, 1, 1, 1.0),  # real couplings: the field cache
     ("hubo", 48, 4, 2, 1, 1, 1.0),
     # real couplings: field updates in the same float order as the oracle's

@@ -40,6 +40,7 @@ SQA_CASES = [
     ("dense_h", 96, 7, 1, 2, 1, 0, 1.0),
     ("sparse", 100, 4, 1, 2, 1, 0, 1.0),
     ("sparse", 64, 9, 2, 1, 2, 0, 0.3),
+    ("sparse_deg6", 80, 6, 1, 1, 1, 0, 1.0),
     ("sparse_real", 80, 4, 1, 1, 1, 0, 1.0),
     ("hubo", 40, 4, 1, 1, 1, 0, 1.0),
     ("dense", 48, 6, 1, 1, 1, 1, 1.0),
