@@ -925,6 +925,105 @@ static RingParams ring_offset(RingParams r, int g0) {
     return r;
 }
 
+// Instance sets of uneven size.  A whole-grid launch sizes every CTA's shared
+// memory for the largest model, which can cost the smaller models resident
+// rings.  Instead each model's rings run in launches of their own, with the
+// plan of that model alone, side by side on the context's side streams
+// (forked from and joined into the context stream, like the rotated launches);
+// the kernels, keys and per-ring records are those of the whole-grid launch,
+// so the results are the same bit for bit.
+struct ModelRun {
+    RingPlan pl;
+    int g0 = 0, nr = 0;  // the model's rings: g0 .. g0 + nr - 1
+};
+
+// The per-model plans of a set, or an empty list where they would not pay:
+// one model, or no model whose own ring needs 80% of the set's shared memory
+// or less.  A model whose own plan picks another kernel keeps the set's.
+static int plan_models(qa_ctx *ctx, const qa_problem *const *probs, int np, int kind, int P, const RingPlan &set_pl,
+                       int nr, bool clusters, bool ref_order, std::vector<ModelRun> *out) {
+    out->clear();
+    if (np < 2 || nr % np) return QA_OK;
+    std::vector<ModelRun> mr(np);
+    bool pays = false;
+    for (int m = 0; m < np; ++m) {
+        QA_TRY(plan_rings(ctx, probs + m, 1, kind, P, probs[m]->n, &mr[m].pl, clusters, ref_order));
+        if (mr[m].pl.pm1 != set_pl.pm1 || mr[m].pl.sparse != set_pl.sparse) mr[m].pl = set_pl;
+        mr[m].g0 = m * (nr / np);
+        mr[m].nr = nr / np;
+        pays = pays || 5 * mr[m].pl.smem <= 4 * set_pl.smem;
+    }
+    if (pays) *out = std::move(mr);
+    return QA_OK;
+}
+
+static int ensure_side_streams(qa_ctx *ctx, int count) {
+    while ((int)ctx->side.size() < count) {
+        cudaStream_t x;
+        cudaEvent_t e;
+        QA_CK(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        ctx->side.push_back(x);
+        QA_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->side_ev.push_back(e);
+    }
+    return QA_OK;
+}
+
+// Steps [s_begin, s_end) of every model of a set, each model on its own
+// side stream (at most 128; models beyond share them), in launches of at most
+// 256 steps.  qanneal's order: model m's visiting orders at its own row
+// stride, the rows of all models for one launch's steps in the W_ORDER
+// workspace (at most 1 GB: fewer steps per launch when they would not fit).
+static int run_models(qa_ctx *ctx, int kind, const std::vector<ModelRun> &mr, const RingParams &rp, int s_begin,
+                      int s_end, int *launches) {
+    const int nm = (int)mr.size(), streams = std::min(nm, 128);
+    int chunk = std::max(1, std::min(256, s_end - s_begin));
+    const bool ordered = mr[0].pl.ref_order;
+    OrdT *rows = nullptr;
+    if (ordered) {
+        size_t per_step = 0;
+        for (const auto &m : mr) per_step += (size_t)m.nr * ord_rows_per_step(m.pl, rp) * ord_row_bytes(m.pl.n_max);
+        if (per_step) chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)chunk, (4 * kOrderBudget) / per_step));
+        void *v;
+        QA_TRY(ws_get(ctx, W_ORDER, std::max<size_t>(per_step * (size_t)chunk, 16), &v));
+        rows = static_cast<OrdT *>(v);
+    }
+    QA_TRY(ensure_side_streams(ctx, streams));
+    QA_CK(cudaEventRecord(ctx->side_ev[0], ctx->stream));
+    for (int k = 0; k < streams; ++k) QA_CK(cudaStreamWaitEvent(ctx->side[k], ctx->side_ev[0], 0));
+    int n = 0, rc = QA_OK;
+    for (int c0 = s_begin; c0 < s_end && rc == QA_OK; c0 += chunk) {
+        const int c1 = std::min(s_end, c0 + chunk);
+        size_t off = 0;  // entries
+        for (int m = 0; m < nm && rc == QA_OK; ++m) {
+            RingParams r2 = ring_offset(rp, mr[m].g0);
+            if (r2.bsamp) r2.bsamp += (size_t)(c0 - s_begin) * (rp.spb + rp.cls);  // indexed from step0
+            r2.step0 = c0;
+            r2.step1 = c1;
+            r2.init_fields = rp.init_fields && c0 == s_begin;
+            r2.init_scan = rp.init_scan && c0 == s_begin;
+            if (ordered) {
+                r2.ord_per_step = ord_rows_per_step(mr[m].pl, rp);
+                r2.ord_stride = ord_row_entries(mr[m].pl.n_max);
+                r2.ord_ring = (long long)(c1 - c0) * std::max(r2.ord_per_step, 1) * r2.ord_stride;
+                r2.ordg = rows + off;
+                off += (size_t)mr[m].nr * (size_t)r2.ord_ring;
+            }
+            rc = launch_rings(ctx, kind, mr[m].pl, r2, mr[m].nr, ctx->side[m % streams]);
+            if (rc == QA_OK) ++n;
+        }
+    }
+    // join, also after a failed launch
+    for (int k = 0; k < streams; ++k) {
+        cudaError_t e1 = cudaEventRecord(ctx->side_ev[k], ctx->side[k]);
+        cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(ctx->stream, ctx->side_ev[k], 0) : e1;
+        if (e2 != cudaSuccess && rc == QA_OK)
+            rc = fail(QA_ERR_CUDA, std::string("per-model launches, join: ") + cudaGetErrorString(e2));
+    }
+    *launches = n;
+    return rc;
+}
+
 // Steps [s_begin, s_end) of every ring as independent chains of short
 // launches: groups of G rings, each group on its own stream, one launch per
 // seg steps.  When the rings outnumber the SMs but do not fill whole waves,
@@ -1853,9 +1952,17 @@ static int sqa_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_proble
     // rotated launches where whole-grid ones would leave slots idle (a traced
     // run's records are indexed by the position in a whole-grid launch, so
     // those stay whole)
-    if (!traces && steps >= 200 && rotation_pays(ctx, kind, pl, nr)) {
+    std::vector<ModelRun> mr;  // an instance set of uneven size: per-model launches
+    const bool rotate = !traces && steps >= 200 && rotation_pays(ctx, kind, pl, nr);
+    if (!traces && !rotate)
+        QA_TRY(plan_models(ctx, problems, n_problems, kind, P, pl, nr, prm->cluster_sweeps > 0,
+                           ctx->update_order == QA_ORDER_REFERENCE, &mr));
+    if (rotate) {
         rp.init_fields = 1;
         QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, 0, steps, sqa_rot_seg(ctx, steps), &n_seg));
+    } else if (!mr.empty()) {
+        rp.init_fields = 1;
+        QA_TRY(run_models(ctx, kind, mr, rp, 0, steps, &n_seg));
     } else {
         for (int s0 = 0; s0 < steps; s0 += seg) {
             rp.step0 = s0;
@@ -2597,6 +2704,10 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
     QA_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
     int n_seg = 0, n_launch = 0;
     const bool rotate = rotation_pays(ctx, kind, pl, nr);
+    std::vector<ModelRun> mr;  // an instance set of uneven size: per-model launches
+    if (!rotate)
+        QA_TRY(plan_models(ctx, problems, n_problems, kind, P, pl, nr, prm->cluster_sweeps > 0,
+                           !classical && ctx->update_order == QA_ORDER_REFERENCE, &mr));
     for (int s0 = 0; s0 < steps;) {
         const int s1 = std::min({steps, (s0 / prm->swap_interval + 1) * prm->swap_interval, s0 + 256});
         rp.step0 = s0;
@@ -2609,6 +2720,10 @@ static int sqapt_impl(qa_ctx *ctx, const qa_problem *const *problems, int n_prob
             int nl = 0;
             QA_TRY(run_rings_rotated(ctx, kind, pl, rp, nr, s0, s1, rot_seg(ctx, std::max(1, (s1 - s0) / 8), s1 - s0),
                                          &nl));
+            n_launch += nl;
+        } else if (!mr.empty()) {
+            int nl = 0;
+            QA_TRY(run_models(ctx, kind, mr, rp, s0, s1, &nl));
             n_launch += nl;
         } else {
             QA_TRY(launch_rings(ctx, kind, pl, rp, nr));
