@@ -323,6 +323,46 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
                         m = (m & ~dq) | (__ballot_sync(FULL, ok) & dq);
                     }
                     uint32_t pending = FULL;
+                    if (Pd.spslab && m) {
+                        // a decision of m stands unless an earlier lane of the
+                        // block that flips is a neighbour: every lane before the
+                        // first lane with an accepted earlier neighbour is final,
+                        // so those moves are applied together
+                        const uint4 rec = __ldg(Pd.spslab + i);
+                        uint32_t nbl = 0;  // earlier lanes holding a neighbour of this lane's spin
+                        for (int l = 0; l < 31; ++l) {
+                            const int il = __shfl_sync(FULL, i, l);
+                            bool nb = false;
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) nb |= slab_val(rec, k) != 0 && slab_col(rec, k) == il;
+                            if (l < lane && nb) nbl |= 1u << l;
+                        }
+                        const uint32_t conf = __ballot_sync(FULL, valid && (nbl & m) != 0u);
+                        const uint32_t pre = conf ? (1u << (__ffs(conf) - 1)) - 1u : FULL;
+                        const uint32_t F = m & pre;
+                        if (F) {
+                            if ((F >> lane) & 1u) {
+                                for (int t = 0; t < NP; ++t) atomicXor(S + t * nw + (i >> 5), 1u << (i & 31));
+                                Wc[i] ^= pmask;
+#pragma unroll
+                                for (int k = 0; k < 4; ++k)
+                                    if (slab_val(rec, k) != 0) {
+                                        const int v = slab_col(rec, k);
+                                        atomicOr(wdirty + (v >> 5), 1u << (v & 31));
+                                    }
+                            }
+                            acc_w += (unsigned long long)__popc(F);
+                            pending = ~pre;  // the first conflicted lane and after (none when pre == FULL)
+                            __syncwarp();
+                            const bool mark = ((pending >> lane) & 1u) && valid && ((wdirty[i >> 5] >> (i & 31)) & 1u);
+                            const uint32_t here = __ballot_sync(FULL, mark);
+                            if (here) {
+                                const bool ok = mark && sp_world_ok(Pd, Wc, h, pmask, NP, i, B, u);
+                                m = (m & ~here) | (__ballot_sync(FULL, ok) & here);
+                            }
+                            __syncwarp();
+                        }
+                    }
                     while (m & pending) {
                         const int j = __ffs(m & pending) - 1;
                         const int jj = __shfl_sync(FULL, i, j);
@@ -376,6 +416,45 @@ __global__ void __launch_bounds__(1024, 1) ring_sparse_kernel(RingParams p) {
                         m = (m & ~dq) | (__ballot_sync(FULL, ok) & dq);
                     }
                     uint32_t pending = FULL;
+                    if (Pd.spslab && m) {
+                        // as in qanneal's order: the moves before the first lane
+                        // with an accepted earlier neighbour in the block are final
+                        const uint4 rec = __ldg(Pd.spslab + (valid ? i : 0));
+                        uint32_t nbl = 0, nbi = 0;  // in-block neighbours: earlier lanes, all lanes
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int c = slab_col(rec, k);
+                            if (slab_val(rec, k) != 0 && (c >> 5) == q) {
+                                nbi |= 1u << (c & 31);
+                                if ((c & 31) < lane) nbl |= 1u << (c & 31);
+                            }
+                        }
+                        const uint32_t conf = __ballot_sync(FULL, valid && (nbl & m) != 0u);
+                        const uint32_t pre = conf ? (1u << (__ffs(conf) - 1)) - 1u : FULL;
+                        const uint32_t F = m & pre;
+                        if (F) {
+                            const bool fl = (F >> lane) & 1u;
+                            for (int t = lane; t < NP; t += 32) S[t * nw + q] ^= F;
+                            if (fl) {
+                                Wc[i] ^= pmask;
+#pragma unroll
+                                for (int k = 0; k < 4; ++k) {
+                                    const int v = slab_col(rec, k);
+                                    if (slab_val(rec, k) != 0 && (v >> 5) > q) atomicOr(wdirty + (v >> 5), 1u << (v & 31));
+                                }
+                            }
+                            acc_w += (unsigned long long)__popc(F);
+                            pending = ~pre;
+                            const uint32_t here = __reduce_or_sync(FULL, fl ? nbi : 0u) & pending;
+                            __syncwarp();
+                            if (here) {
+                                const bool ok =
+                                    valid && ((here >> lane) & 1u) && sp_world_ok(Pd, Wc, h, pmask, NP, i, B, u);
+                                m = (m & ~here) | (__ballot_sync(FULL, ok) & here);
+                            }
+                            __syncwarp();
+                        }
+                    }
                     while (m & pending) {
                         const int j = __ffs(m & pending) - 1;
                         const int jj = (q << 5) | j;

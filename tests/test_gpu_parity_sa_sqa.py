@@ -135,6 +135,7 @@ SQA_CASES = [
     ("sparse", 2048, 16, 1, 1, 2, 0.5),  # integer couplings: on-demand fields
     ("sparse", 150, 64, 1, 1, 1, 1.0),
     ("sparse_deg6", 96, 8, 1, 1, 1, 1.0),  # integer couplings in CSR rows
+    ("sparse", 96, 8, 1, 0, 3, 0.1),  # many accepted worldline moves, neighbours in one block
     ("sparse_real", 96, 6, 1, 1, 1, 1.0),  # real couplings: the field cache
     ("hubo", 48, 4, 2, 1, 1, 1.0),
     # real couplings: field updates in the same float order as the oracle's

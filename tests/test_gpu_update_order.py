@@ -41,6 +41,7 @@ SQA_CASES = [
     ("sparse", 100, 4, 1, 2, 1, 0, 1.0),
     ("sparse", 64, 9, 2, 1, 2, 0, 0.3),
     ("sparse_deg6", 80, 6, 1, 1, 1, 0, 1.0),
+    ("sparse", 96, 8, 1, 1, 3, 0, 0.15),  # many accepted worldline moves
     ("sparse_real", 80, 4, 1, 1, 1, 0, 1.0),
     ("hubo", 40, 4, 1, 1, 1, 0, 1.0),
     ("dense", 48, 6, 1, 1, 1, 1, 1.0),
