@@ -187,7 +187,8 @@ def cpu_reference_sample(target_s=12.0, threads=None):
     sites = reads * steps * (WL["spb"] + WL["wls"]) * P * WL["n"]
     return {"value": sites / dt, "unit": "site-attempts/s", "cores": threads, "kind": "reference",
             "sample": f"{reads} reads x first {steps} of {WL['steps']} schedule steps "
-                      f"({sites:.3e} site-attempts, {dt:.1f} s, one SQAAnnealer per thread)"}
+                      f"({sites:.3e} site-attempts, {dt:.1f} s, one SQAAnnealer per thread)",
+            "sample_reads": reads, "sample_steps": steps, "sample_site_attempts": sites}
 
 
 def run_reference_arm(args):
@@ -211,7 +212,12 @@ def run_reference_arm(args):
         "impl": "reference", "metric": "spin-flip attempts/s (site-attempts)", "value": v, "unit": "site-attempts/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, "sample": base["sample"]},
+        # a bounded sample of the workload: the rate per site-attempt of
+        # sample_reads of the configured reads over the first sample_steps
+        # steps, which stands for the whole run's rate
+        "config": {"workload": WORKLOAD_NAME, "sample": base["sample"], "configured_reads": WL["reads"],
+                   "configured_steps": WL["steps"], "sample_reads": base["sample_reads"],
+                   "sample_steps": base["sample_steps"], "rate": "per site-attempt over the sample"},
         "cpu_baseline": {"value": v, "unit": "site-attempts/s", "cores": base["cores"], "kind": "reference",
                          "sample": base["sample"]},
         "e2e": {"value": v, "unit": "site-attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
