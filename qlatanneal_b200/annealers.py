@@ -716,6 +716,7 @@ class SQAChiAnnealer(_Seeded):
         o = _lib.qa_chi_out(*[a[f].ctypes.data for f, _ in _lib.qa_chi_out._fields_])
         st = _lib.qa_stats()
         probs = (C.c_void_p * 1)(prob)
+        autotune.apply(eng, self.hamiltonian.kind + "-chi", n, self.trotter_slices, int(reads) * self.replicas)
         _lib.check(eng.L.qa_chi_run(eng.h, probs, 1, C.byref(prm), C.byref(o), C.byref(st)))
         self.last_stats = RunStats.from_c(st)
         out = []

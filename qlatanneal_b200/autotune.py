@@ -7,13 +7,15 @@ steps per rotated launch and the rings per rotated group.  Every choice leaves
 the results unchanged bit for bit (the engine's random streams are keyed by
 ring, slice, sweep and spin, not by launch); it moves only time.
 
-``tune_sqa`` / ``tune_sqapt`` time candidate shapes on a run of the caller's
-own workload (the first ``timing_steps`` steps of its schedule), check that
+``tune_sqa`` / ``tune_sqapt`` / ``tune_chi`` time candidate shapes on a run of
+the caller's own workload (the first ``timing_steps`` steps of its schedule;
+SQA-Chi in buckets of its own, kind "<model kind>-chi"), check that
 every candidate's results agree with the automatic shape's, and cache the
 fastest per bucket -- (model kind, n rounded up to a power of two, P, rings
 rounded up to a power of two) -- in a JSON file.  ``use_cache(path)`` (or the
-environment variable QA_TUNE_CACHE) makes later runs of the SQA, SQA-PT and
-instance-set paths apply the cached shape of their bucket.
+environment variable QA_TUNE_CACHE) makes later runs of the SQA, SQA-PT,
+SQA-Chi and instance-set paths apply the cached shape of their bucket; the
+runs a tuning times keep their candidate shape.
 
 The search is coordinate-wise: warps per ring, then the ring-state form (dense
 models), then rotation (off, or on with steps 25 / 50 / 100 and groups of 2 /
@@ -36,6 +38,9 @@ AUTO = {"warps_per_ring": 0, "field_form": -1, "rotate": -1, "rot_steps": 0, "ro
 _lock = threading.Lock()
 _cache: Optional[Dict[str, dict]] = None
 _cache_path: Optional[str] = None
+# while a tuning runs, the runs it times keep the candidate shape instead of
+# taking their bucket's cached one
+_suspend = threading.local()
 
 
 def _pow2(x: int) -> int:
@@ -93,7 +98,7 @@ def set_tuning(eng, tuning: Optional[dict]) -> None:
 
 def apply(eng, kind: str, n: int, P: int, rings: int) -> None:
     """Before a run: the cached shape of its bucket, else automatic."""
-    if _active() is None:
+    if getattr(_suspend, "on", False) or _active() is None:
         return
     set_tuning(eng, lookup(kind, n, P, rings))
 
@@ -104,7 +109,7 @@ def _candidates_stage(stage: str, base: dict, kind: str, P: int, rings: int, sms
         for w in sorted({max(1, (P + 1) // 2), max(1, (P + 3) // 4), min(32, P)}):
             out.append(dict(base, warps_per_ring=w))
     elif stage == "form":
-        if kind == "dense":
+        if kind.split("-")[0] == "dense":
             out = [dict(base, field_form=f) for f in (-1, 0, 1, 2)]
     elif stage == "rotation":
         out = [dict(base, rotate=0)]
@@ -125,10 +130,14 @@ def _tune(key: str, run, kind: str, P: int, rings: int, cache_path: Optional[str
     def timed(tuning):
         set_tuning(eng, tuning)
         ms, sig = [], None
-        for _ in range(repeats + 1):  # the first run warms the shape
-            res, st = run()
-            ms.append(st.total_ms)
-            sig = _signature(res)
+        _suspend.on = True
+        try:
+            for _ in range(repeats + 1):  # the first run warms the shape
+                res, st = run()
+                ms.append(st.total_ms)
+                sig = _signature(res)
+        finally:
+            _suspend.on = False
         return float(sorted(ms[1:])[len(ms[1:]) // 2]), sig
 
     base = dict(AUTO)
@@ -205,3 +214,25 @@ def tune_sqapt(annealer, sweeps_per_step: int, worldline_sweeps: int, steps: int
     rings = reads * len(annealer.betas)
     key = bucket(m.kind, m.size(), annealer.trotter_slices, rings)
     return _tune(key, run, m.kind, annealer.trotter_slices, rings, cache_path, device=annealer.device)
+
+
+def tune_chi(annealer, reads: int, timing_steps: Optional[int] = None, cache_path: Optional[str] = None,
+             seed: int = 1, **run_chi_kwargs) -> dict:
+    """Tune the launch shape of ``annealer.run_chi_reads(reads=reads,
+    **run_chi_kwargs)`` (an SQAChiAnnealer; pass ``scan_chi`` to time the
+    production anneal without the pilot scan).  ``timing_steps`` shortens
+    ``num_steps`` for the timing.  SQA-Chi has buckets of its own (kind
+    "<model kind>-chi"): its production anneal keeps the checkerboard order."""
+    kw = dict(run_chi_kwargs)
+    if timing_steps is not None:
+        kw["num_steps"] = min(int(kw.get("num_steps", 100)), int(timing_steps))
+
+    def run():
+        res = annealer.run_chi_reads(reads=reads, seed=seed, **kw)
+        return res, annealer.last_stats
+
+    m = annealer.hamiltonian
+    kind = m.kind + "-chi"
+    rings = reads * annealer.replicas
+    key = bucket(kind, m.size(), annealer.trotter_slices, rings)
+    return _tune(key, run, kind, annealer.trotter_slices, rings, cache_path, device=annealer.device)

@@ -37,3 +37,38 @@ def test_candidate_stages():
     rot = autotune._candidates_stage("rotation", base, "dense", 32, 256, 148)
     assert rot[0]["rotate"] == 0 and len(rot) == 10
     assert len(autotune._candidates_stage("rotation", base, "dense", 32, 100, 148)) == 1
+
+
+def test_chi_buckets_and_forms():
+    """SQA-Chi has buckets of its own; its dense models get the ring-state forms."""
+    assert autotune.bucket("dense-chi", 1024, 64, 512) == "dense-chi|n1024|P64|rings512"
+    base = dict(autotune.AUTO)
+    assert len(autotune._candidates_stage("form", base, "dense-chi", 64, 512, 148)) == 4
+    assert autotune._candidates_stage("form", base, "sparse-chi", 64, 512, 148) == []
+
+
+def test_apply_is_suspended_while_tuning(tmp_path):
+    """A run that a tuning times keeps the candidate shape even when a cache
+    with an entry for its bucket is active."""
+    path = os.path.join(tmp_path, "t.json")
+    key = autotune.bucket("dense", 64, 8, 16)
+    with open(path, "w") as f:
+        json.dump({key: {"tuning": {"warps_per_ring": 2}, "ms": 1.0}}, f)
+    seen = []
+
+    class FakeEngine:
+        pass
+
+    orig = autotune.set_tuning
+    autotune.set_tuning = lambda eng, t: seen.append(t)
+    autotune.use_cache(path)
+    try:
+        autotune.apply(FakeEngine(), "dense", 64, 8, 16)
+        assert seen == [{"warps_per_ring": 2}]
+        autotune._suspend.on = True
+        autotune.apply(FakeEngine(), "dense", 64, 8, 16)
+        assert seen == [{"warps_per_ring": 2}]
+    finally:
+        autotune._suspend.on = False
+        autotune.set_tuning = orig
+        autotune.use_cache(None)

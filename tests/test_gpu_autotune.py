@@ -70,3 +70,43 @@ def test_tune_and_apply_cache(tmp_path):
         autotune.set_tuning(_lib.Engine.get(None), None)
     for a, b in zip(base, tuned):
         assert a.best_energy == b.best_energy and a.energy_trace == b.energy_trace
+
+
+def test_chi_shapes_bit_exact_and_tune(tmp_path):
+    """SQA-Chi under every launch shape (pilot and production; more rings than
+    SMs and >= 200 production sweeps, so rotated launches can run) returns the
+    automatic shape's reads bit for bit; tune_chi caches an entry in the
+    SQA-Chi bucket and later runs apply it with the same results."""
+    model = make("dense", 40, 43)
+    P, K, steps, spb, points, sweeps, burn = 4, 2, 30, 8, 5, 6, 2
+    beta, g0, g1, reads, seed = 0.4 * P, 3.0, 0.05, 80, 2468
+    ann = qa.SQAChiAnnealer(model, P, K)
+    eng = _lib.Engine.get(None)
+    args = (beta, g0, g1, steps, spb, points, sweeps, burn)
+    want = ann.run_chi_reads(*args, reads=reads, seed=seed)
+    try:
+        for shape in SHAPES:
+            autotune.set_tuning(eng, shape)
+            got = ann.run_chi_reads(*args, reads=reads, seed=seed)
+            for a, b in zip(want, got):
+                assert a.best_energy == b.best_energy, shape
+                np.testing.assert_array_equal(a.best_state.as_array(), b.best_state.as_array(), err_msg=str(shape))
+                np.testing.assert_array_equal(np.asarray(a.energy_trace), np.asarray(b.energy_trace),
+                                              err_msg=str(shape))
+    finally:
+        autotune.set_tuning(eng, None)
+    path = os.path.join(tmp_path, "tune.json")
+    entry = autotune.tune_chi(ann, reads, cache_path=path, seed=seed, beta=beta, gamma_start=g0, gamma_end=g1,
+                              num_steps=steps, sweeps_per_step=spb, scan_points=points, scan_sweeps=sweeps,
+                              scan_burn=burn)
+    assert entry["ms"] <= entry["auto_ms"] and len(entry["candidates"]) > 4
+    assert autotune.bucket("dense-chi", 40, P, reads * K) in json.load(open(path))
+    autotune.use_cache(path)
+    try:
+        got = ann.run_chi_reads(*args, reads=reads, seed=seed)
+    finally:
+        autotune.use_cache(None)
+        autotune.set_tuning(eng, None)
+    for a, b in zip(want, got):
+        assert a.best_energy == b.best_energy
+        np.testing.assert_array_equal(np.asarray(a.energy_trace), np.asarray(b.energy_trace))
