@@ -125,39 +125,67 @@ def test_tracking_energy_exact_for_integer_models(oracle):
             assert oracle.energy_track(mod, s) == oracle.energy64(mod, s)
 
 
-def _ci95(x):
-    x = np.asarray(x, float)
-    return x.mean(), 1.96 * x.std(ddof=1) / math.sqrt(len(x))
+def _diff_z(a, b):
+    """|mean(a) - mean(b)| in standard errors of the difference."""
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    se = math.sqrt(a.var(ddof=1) / len(a) + b.var(ddof=1) / len(b))
+    d = abs(a.mean() - b.mean())
+    if se == 0.0:
+        return 0.0 if d <= 1e-12 else math.inf
+    return d / se
+
+
+def _agree(sample, reads):
+    """sample(reads, stage) -> [(oracle values, reference values), ...] of one
+    configuration.  Every statistic's means must lie within the combined 95%
+    interval of the difference; a configuration that misses is drawn once more
+    with fresh seeds (stage 1) and four times the reads, and must then agree
+    within the combined 99% interval: a chance miss rarely repeats, a real
+    bias persists with the added power.  Seeds are fixed, so the outcome is
+    too."""
+    z1 = [_diff_z(a, b) for a, b in sample(reads, 0)]
+    if max(z1) <= 1.96:
+        return
+    z2 = [_diff_z(a, b) for a, b in sample(4 * reads, 1)]
+    assert max(z2) <= 2.576, (z1, z2)
+
+
+# seeds of the second stage start this far from the first's
+STAGE = 1_000_003
 
 
 def test_sa_restatement_matches_reference_statistics(oracle, ref):
     """The replay-model SA and qanneal's Annealer sample the same distribution
-    of best energies (means inside each other's 95% CIs, 400 reads each)."""
+    of best energies (means within the combined 95% interval, 400 reads each)."""
     h, J = sk_dense(48, 5)
     m, rm = oracle.dense(h, J), ref.dense(h, J)
     betas = geometric_betas(0.1, 2.0, 12)
-    eo = [oracle.sa_run(m, betas, 2, 1000, k)[1] for k in range(400)]
-    er = [rm.sa_run(betas, 2, 5000 + k)[1] for k in range(400)]
-    (mo, co), (mr, cr) = _ci95(eo), _ci95(er)
-    assert abs(mo - mr) <= 1.5 * (co + cr), (mo, co, mr, cr)
+
+    def sample(R, st):
+        eo = [oracle.sa_run(m, betas, 2, 1000 + st * STAGE, k)[1] for k in range(R)]
+        er = [rm.sa_run(betas, 2, 5000 + st * STAGE + k)[1] for k in range(R)]
+        return [(eo, er)]
+    _agree(sample, 400)
 
 
 def test_sqapt_restatement_matches_reference_statistics(oracle, ref):
     """Replay-model SQA-PT vs qanneal's SQAParallelTemperingAnnealer: final
-    average projected energy and mean swap acceptance inside 95% CIs."""
+    average projected energy and mean swap acceptance agree (combined 95%
+    interval)."""
     h, J = sk_dense(24, 7)
     m, rm = oracle.dense(h, J), ref.dense(h, J)
     betas = np.geomspace(0.3, 3.0, 4)
     gammas = np.linspace(2.0, 0.1, 4)
     P, steps = 6, 8
-    eo, er, so, sr = [], [], [], []
-    for k in range(250):
-        o = oracle.sqapt_run(m, betas, gammas, P, 1, 1, steps, 2, 100, k)
-        r = rm.sqapt_run(betas, gammas, P, 1, 1, steps, 2, 7000 + k)
-        eo.append(o[4][-1]); er.append(r[3][-1]); so.append(o[5].sum()); sr.append(r[4].sum())
-    for a, b in ((eo, er), (so, sr)):
-        (ma, ca), (mb, cb) = _ci95(a), _ci95(b)
-        assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
+
+    def sample(R, st):
+        eo, er, so, sr = [], [], [], []
+        for k in range(R):
+            o = oracle.sqapt_run(m, betas, gammas, P, 1, 1, steps, 2, 100 + st * STAGE, k)
+            r = rm.sqapt_run(betas, gammas, P, 1, 1, steps, 2, 7000 + st * STAGE + k)
+            eo.append(o[4][-1]); er.append(r[3][-1]); so.append(o[5].sum()); sr.append(r[4].sum())
+        return [(eo, er), (so, sr)]
+    _agree(sample, 250)
 
 
 def test_sqa_restatement_matches_reference_statistics(oracle, ref):
@@ -166,10 +194,12 @@ def test_sqa_restatement_matches_reference_statistics(oracle, ref):
     steps, P, K = 10, 8, 1
     betas = np.full(steps, 1.5)
     gammas = np.linspace(2.0, 0.2, steps)
-    eo = [oracle.sqa_run(m, betas, gammas, P, K, 1, 1, 1000, k)[2][-1] for k in range(300)]
-    er = [rm.sqa_run(betas, gammas, P, K, 1, 1, 9000 + k)[2][-1] for k in range(300)]
-    (mo, co), (mr, cr) = _ci95(eo), _ci95(er)
-    assert abs(mo - mr) <= 1.5 * (co + cr), (mo, co, mr, cr)
+
+    def sample(R, st):
+        eo = [oracle.sqa_run(m, betas, gammas, P, K, 1, 1, 1000 + st * STAGE, k)[2][-1] for k in range(R)]
+        er = [rm.sqa_run(betas, gammas, P, K, 1, 1, 9000 + st * STAGE + k)[2][-1] for k in range(R)]
+        return [(eo, er)]
+    _agree(sample, 300)
 
 
 def test_cluster_sqa_restatement_matches_reference_statistics(oracle, ref):
@@ -185,10 +215,13 @@ def test_cluster_sqa_restatement_matches_reference_statistics(oracle, ref):
     steps, P = 100, 4
     for beta, gamma in ((0.5, 1.0), (2.0, 2.0)):
         b, g = np.full(steps, beta), np.full(steps, gamma)
-        eo = [oracle.sqa_run(m, b, g, P, 1, 0, 0, 100, k, cls=1)[2][-50:].mean() for k in range(300)]
-        er = [rm.sqa_run(b, g, P, 1, 0, 0, 7000 + k, cls=1)[2][-50:].mean() for k in range(300)]
-        (mo, co), (mr, cr) = _ci95(eo), _ci95(er)
-        assert abs(mo - mr) <= 1.5 * (co + cr), (beta, gamma, mo, co, mr, cr)
+
+        def sample(R, st):
+            eo = [oracle.sqa_run(m, b, g, P, 1, 0, 0, 100 + st * STAGE, k, cls=1)[2][-50:].mean() for k in range(R)]
+            er = [rm.sqa_run(b, g, P, 1, 0, 0, 7000 + st * STAGE + k, cls=1)[2][-50:].mean() for k in range(R)]
+            return [(eo, er)]
+        _agree(sample, 300)
+        mo = np.mean(sample(50, 0)[0][0])
         start = [oracle.sqa_run(m, b[:1], g[:1], P, 1, 0, 0, 100, k, cls=1)[2][0] for k in range(50)]
         assert mo < np.mean(start) - 1.0  # the moves do anneal
 
@@ -199,31 +232,34 @@ def test_cluster_sqapt_restatement_matches_reference_statistics(oracle, ref):
     betas = np.geomspace(0.5, 3.0, 3)
     gammas = np.linspace(1.5, 0.2, 3)
     P, steps = 6, 80
-    eo, er = [], []
-    for k in range(300):
-        eo.append(oracle.sqapt_run(m, betas, gammas, P, 0, 0, steps, 2, 100, k, cls=2)[4][-20:].mean())
-        er.append(rm.sqapt_run(betas, gammas, P, 0, 0, steps, 2, 7000 + k, cls=2)[3][-20:].mean())
-    (ma, ca), (mb, cb) = _ci95(eo), _ci95(er)
-    assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
+
+    def sample(R, st):
+        eo = [oracle.sqapt_run(m, betas, gammas, P, 0, 0, steps, 2, 100 + st * STAGE, k, cls=2)[4][-20:].mean()
+              for k in range(R)]
+        er = [rm.sqapt_run(betas, gammas, P, 0, 0, steps, 2, 7000 + st * STAGE + k, cls=2)[3][-20:].mean()
+              for k in range(R)]
+        return [(eo, er)]
+    _agree(sample, 300)
 
 
 def test_classical_pt_restatement_matches_reference_statistics(oracle, ref):
     """Classical parallel tempering (parallel_tempering.cpp:36-122): at
     equilibrium the replay form and qanneal's ParallelTemperingAnnealer have
-    the same average energy and swap acceptance (95% CIs, 300 reads)."""
+    the same average energy and swap acceptance (combined 95% interval, 300 reads)."""
     h, J = sk_dense(20, 13)
     m, rm = oracle.dense(h, J), ref.dense(h, J)
     betas = np.geomspace(0.2, 2.0, 4)
     steps = 60
-    eo, er, so, sr = [], [], [], []
-    for k in range(300):
-        o = oracle.pt_run(m, betas, 1, steps, 2, 100, k)
-        r = rm.pt_run(betas, 1, steps, 2, 7000 + k)
-        eo.append(o[4][-20:].mean()); er.append(r[3][-20:].mean())
-        so.append(o[5][1::2].mean()); sr.append(r[4][1::2].mean())
-    for a, b in ((eo, er), (so, sr)):
-        (ma, ca), (mb, cb) = _ci95(a), _ci95(b)
-        assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
+
+    def sample(R, st):
+        eo, er, so, sr = [], [], [], []
+        for k in range(R):
+            o = oracle.pt_run(m, betas, 1, steps, 2, 100 + st * STAGE, k)
+            r = rm.pt_run(betas, 1, steps, 2, 7000 + st * STAGE + k)
+            eo.append(o[4][-20:].mean()); er.append(r[3][-20:].mean())
+            so.append(o[5][1::2].mean()); sr.append(r[4][1::2].mean())
+        return [(eo, er), (so, sr)]
+    _agree(sample, 300)
 
 
 def test_replica_restatement_matches_reference_statistics(oracle, ref):
@@ -235,15 +271,16 @@ def test_replica_restatement_matches_reference_statistics(oracle, ref):
     m, rm = oracle.dense(h, J), ref.dense(h, J)
     betas = geometric_betas(0.1, 2.0, 10)
     R = 8
-    eo, mo, er, mr = [], [], [], []
-    for k in range(60):
-        runs = [oracle.replica_run(m, betas, 2, 500 + 100 * k, r) for r in range(R)]
-        eo.append(np.mean([x[2][-1] for x in runs])); mo.append(np.mean([x[3][-1] for x in runs]))
-        _, avg, mag = rm.replica_run(betas, 2, R, 9000 + k)
-        er.append(avg[-1]); mr.append(mag[-1])
-    for a, b in ((eo, er), (mo, mr)):
-        (ma, ca), (mb, cb) = _ci95(a), _ci95(b)
-        assert abs(ma - mb) <= 1.5 * (ca + cb), (ma, ca, mb, cb)
+
+    def sample(N, st):
+        eo, mo, er, mr = [], [], [], []
+        for k in range(N):
+            runs = [oracle.replica_run(m, betas, 2, 500 + st * STAGE + 100 * k, r) for r in range(R)]
+            eo.append(np.mean([x[2][-1] for x in runs])); mo.append(np.mean([x[3][-1] for x in runs]))
+            _, avg, mag = rm.replica_run(betas, 2, R, 9000 + st * STAGE + k)
+            er.append(avg[-1]); mr.append(mag[-1])
+        return [(eo, er), (mo, mr)]
+    _agree(sample, 60)
 
 
 @pytest.mark.parametrize("eps", [0.0, 0.02])
@@ -251,17 +288,19 @@ def test_run_optimal_restatement_matches_reference_statistics(oracle, ref, eps):
     """SQAAnnealer::run_optimal (sqa_annealer.cpp:499-952): beta ramp,
     calibration pilot (eps_tilde <= 0) or online J_perp updates (eps_tilde > 0),
     chi_B from bond-sum samples.  Final energy, the J_perp reached mid-run and
-    the calibrated budget agree with qanneal within 95% CIs (200 reads)."""
+    the calibrated budget agree with qanneal (combined 95% interval, 200 reads)."""
     h, J = sk_dense(24, 17)
     m, rm = oracle.dense(h, J), ref.dense(h, J)
     a = (8, 2, 2.0, 0.05, 2.0, eps, 15 / 14, 30, 2, 1, 1, 8, 4, 0.3, 0.1)
-    A = [oracle.sqa_opt_run(m, *a, seed=100, read=k) for k in range(200)]
-    B = [rm.sqa_opt_run(*a, seed=5000 + k) for k in range(200)]
-    for f in (lambda d: d["trace"][-1], lambda d: d["j_perp"][20], lambda d: d["scalars"][0],
-              lambda d: d["best_energy"]):
-        (ma, ca), (mb, cb) = _ci95([f(d) for d in A]), _ci95([f(d) for d in B])
-        assert abs(ma - mb) <= 1.5 * (ca + cb) + 1e-12, (ma, ca, mb, cb)
-    d = A[0]
+    fs = (lambda d: d["trace"][-1], lambda d: d["j_perp"][20], lambda d: d["scalars"][0],
+          lambda d: d["best_energy"])
+
+    def sample(R, st):
+        A = [oracle.sqa_opt_run(m, *a, seed=100 + st * STAGE, read=k) for k in range(R)]
+        B = [rm.sqa_opt_run(*a, seed=5000 + st * STAGE + k) for k in range(R)]
+        return [([f(d) for d in A], [f(d) for d in B]) for f in fs]
+    _agree(sample, 200)
+    d = oracle.sqa_opt_run(m, *a, seed=100, read=0)
     assert d["scalars"][1] == 0.05 and d["scalars"][2] == 2.0
     assert np.all(np.diff(d["j_perp"][9:]) >= 0) and d["j_perp"][-1] <= 2.0 + 1e-12
 
@@ -272,28 +311,32 @@ def test_sqapt_run_optimal_restatement_matches_reference_statistics(oracle, ref,
     one J_perp shared by every rung, calibration from the starting states
     (eps_tilde <= 0) or online updates (eps_tilde > 0), classical swaps.  The
     final rung energies, J_perp mid-run, the calibrated budget, the best energy
-    and the swap rate agree with qanneal within 95% CIs (150 reads); J_end = 0
+    and the swap rate agree with qanneal (combined 95% interval, 150 reads); J_end = 0
     resolves to the coldest rung's coupling."""
     h, J = sk_dense(20, 23)
     m, rm = oracle.dense(h, J), ref.dense(h, J)
     betas, gammas = np.geomspace(0.5, 3.0, 4), np.geomspace(2.0, 0.3, 4)
     a = (betas, gammas, 6, 2, 1, 1, 24, 2, eps, 15 / 14, je, 6, 3)
-    A = [oracle.sqapt_opt_run(m, *a, seed=300, read=k) for k in range(150)]
+    d = oracle.sqapt_opt_run(m, *a, seed=300, read=0)
+    b = a
     if je <= 0.0:
         # the sentinel resolves to the coldest rung's coupling; the reference is
         # handed that value (its warning for the sentinel, written through
         # std::cerr, does not survive being loaded through ctypes here)
         je = 0.5 * np.log(1.0 / np.tanh(betas[-1] * gammas[-1] / 6))
-        assert A[0]["scalars"][2] == pytest.approx(je, rel=1e-14)
-        a = a[:10] + (je,) + a[11:]
-    B = [rm.sqapt_opt_run(*a, seed=7000 + k) for k in range(150)]
-    for f in (lambda d: d["avg"][-1], lambda d: d["final_E"][-1], lambda d: d["j_perp"][12],
-              lambda d: d["scalars"][0], lambda d: d["best_energy"], lambda d: np.mean(d["swap"][1::2])):
-        (ma, ca), (mb, cb) = _ci95([f(d) for d in A]), _ci95([f(d) for d in B])
-        assert abs(ma - mb) <= 1.5 * (ca + cb) + 1e-12, (ma, ca, mb, cb)
+        assert d["scalars"][2] == pytest.approx(je, rel=1e-14)
+        b = a[:10] + (je,) + a[11:]
+    fs = (lambda x: x["avg"][-1], lambda x: x["final_E"][-1], lambda x: x["j_perp"][12],
+          lambda x: x["scalars"][0], lambda x: x["best_energy"], lambda x: np.mean(x["swap"][1::2]))
+
+    def sample(R, st):
+        A = [oracle.sqapt_opt_run(m, *a, seed=300 + st * STAGE, read=k) for k in range(R)]
+        B = [rm.sqapt_opt_run(*b, seed=7000 + st * STAGE + k) for k in range(R)]
+        return [([f(x) for x in A], [f(x) for x in B]) for f in fs]
+    _agree(sample, 150)
     # the resolved J range is deterministic
+    B0 = rm.sqapt_opt_run(*b, seed=7000)
     for k in (1, 2):
-        assert A[0]["scalars"][k] == pytest.approx(B[0]["scalars"][k], rel=1e-15)
-    d = A[0]
+        assert d["scalars"][k] == pytest.approx(B0["scalars"][k], rel=1e-15)
     assert np.all(np.diff(d["j_perp"]) >= 0) and d["j_perp"][-1] <= d["scalars"][2] + 1e-12
     assert np.all(d["swap"][0::2] == 0.0)
